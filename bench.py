@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Benchmark of the swarm collision hot path: exact kNN queries/s (and swarm steps/s) at N = 10^7,
+K = 64 on synthetic data with the c3 shapes (3D disk, log-uniform radius, Gaussian vertical
+profile, log-uniform grain radii).
+
+One step = geometry build (site init, Morton radix sort, bucket tree) + exact top-K of every owner.
+`value` is device-timed with inputs resident; `e2e` goes through the C ABI with host buffers and
+host<->device copies inside the timed region.  `--impl reference` times the CPU restatement of the
+reference algorithm (KD tree + heap) on the host cores.  Under torchrun every rank runs an
+independent replica (the path does not shard across GPUs).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "exact kNN queries/s & swarm steps/s at N=1e7,K=64: learned-radius vs plain tree"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c3_learned_3d")
+    ap.add_argument("--n", type=int, default=None, help="override the particle count (tests only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-step", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_init(n_gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def reduce_max(x, world):
+    import torch
+
+    if world <= 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x, world):
+    import torch
+
+    if world <= 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def load_traffic(kernel: str, n: int, k: int):
+    """dram bytes per launch of `kernel` from the committed ncu summary, scaled to n owners."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text()).get(kernel)
+    if not d or d.get("k") != k:
+        return None
+    return d["dram_bytes_per_launch"] * n / d["n"]
+
+
+def cpu_baseline(cfg, particles, sample, threads):
+    """The oracle (KD tree + the reference heap) on the host cores: build over all sites, then a
+    bounded sample of owners queried with every thread."""
+    import numpy as np
+
+    from oracle import oracle
+
+    n = particles.shape[0]
+    site4, q, active, _ = oracle.site_init(cfg, particles)
+    t0 = time.perf_counter()
+    tree = oracle.KdTree(site4, active)
+    t_build = time.perf_counter() - t0
+    sample = min(sample, n)
+    first = (n - sample) // 2
+    codes = np.empty((n, cfg.n_k), np.int32) if n * cfg.n_k * 4 < 8e9 else None
+    d2 = None
+    t0 = time.perf_counter()
+    tree.query(q, cfg.n_k, codes, d2, threads=threads, first=first, count=sample)
+    t_query = time.perf_counter() - t0
+    tree.close()
+    return {"queries_per_s": sample / t_query, "build_s": t_build, "query_s": t_query, "sample": sample}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference algorithm, rank 0 only."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+
+    from gamedev_b200 import workloads
+    from oracle import oracle
+
+    cfg = workloads.config(args.workload)
+    n = args.n or workloads.CONFIGS[args.workload]["n"]
+    p = workloads.particles(args.workload, n=n)
+    threads = os.cpu_count()
+    site4, q, active, _ = oracle.site_init(cfg, p)
+    t0 = time.perf_counter()
+    tree = oracle.KdTree(site4, active)
+    t_build = time.perf_counter() - t0
+    sample = min(args.cpu_sample, n)
+    codes = np.empty((n, cfg.n_k), np.int32)
+    times = []
+    for s in range(args.warmup + args.steps):
+        first = (s * 7919 * sample) % max(1, n - sample)
+        t0 = time.perf_counter()
+        tree.query(q, cfg.n_k, codes, None, threads=threads, first=first, count=sample)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    tree.close()
+    step = statistics.mean(times)
+    value = sample / step
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "k": cfg.n_k},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} owners of the {n}-site workload per step, KD tree over all "
+                                   f"sites built once ({t_build:.1f} s, not in the step)"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import gamedev_b200 as gd
+    from gamedev_b200 import workloads
+
+    world, rank, local = dist_init(args.gpus)
+    cfg = workloads.config(args.workload)
+    n = args.n or workloads.CONFIGS[args.workload]["n"]
+    K = cfg.n_k
+    p_host = workloads.particles(args.workload, n=n, seed=workloads.CONFIGS[args.workload]["seed"] + rank)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p_host, device=dev)
+    codes = torch.empty((n, K), dtype=torch.int32, device=dev)
+    measure = torch.empty(n, dtype=torch.float64, device=dev)
+    kth = torch.empty(n, dtype=torch.float32, device=dev)
+
+    def step():
+        sw.col_site_init(dp)
+        sw.col_cache_get(dp, codes, measure, kth)
+
+    for _ in range(args.warmup):
+        step()
+    site4, q, active = sw.get_sites()
+    n_active = int(active.sum().item())
+
+    clocks = Clocks(torch.cuda.current_device())
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = sw.launch_count()
+    barrier(world)
+    clocks.start()
+    start.record(stream)
+    for s in range(args.steps):
+        ev0[s].record(stream)
+        sw.col_site_init(dp)
+        ev1[s].record(stream)
+        sw.col_cache_get(dp, codes, measure, kth)
+        ev2[s].record(stream)
+    stop.record(stream)
+    barrier(world)
+    clk = clocks.stop()
+    launches = sw.launch_count() - launches0
+    total_ms = start.elapsed_time(stop)
+    total_ms = reduce_max(total_ms, world)
+    knn_ms = statistics.mean(ev1[s].elapsed_time(ev2[s]) for s in range(args.steps))
+    build_ms = statistics.mean(ev0[s].elapsed_time(ev1[s]) for s in range(args.steps))
+    ms_per_step = total_ms / args.steps
+    queries = reduce_sum(float(n_active * args.steps), world)
+    value = queries / (total_ms / 1e3)
+
+    peak, peak_kind = peaks()
+    bytes_per_query = 24 + 4 * K
+    achieved = n_active * bytes_per_query / (knn_ms / 1e3) / 1e9
+    traffic = load_traffic("k_knn_query", n_active, K)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n": n, "k": K, "active": n_active, "geometry": "3d" if cfg.n_z > 1 else "2d",
+                   "index": "Morton bucket tree, 32-site buckets", "order": "ascending (d2, code)",
+                   "l2": "inputs and outputs larger than L2 (sites 16 B x N, codes 4K B x N)",
+                   "parallelism": f"replicas x{world}"},
+        "phases_ms": {"geometry_build": build_ms, "knn_query": knn_ms},
+        "roofline": {"bound": "hbm", "kernel": "k_knn_query (+k_inactive_rows)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "bytes_per_unit": bytes_per_query, "units_per_launch": n_active, "traffic": traffic},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+
+    # ---- end to end through the C ABI with host buffers ------------------------------------
+    if not args.no_e2e:
+        host_in = torch.from_numpy(np.ascontiguousarray(p_host)).pin_memory()
+        host_codes = torch.empty((n, K), dtype=torch.int32).pin_memory()
+        host_measure = torch.empty(n, dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            dp.copy_(host_in, non_blocking=True)
+            sw.col_site_init(dp)
+            sw.col_cache_get(dp, codes, measure, kth)
+            host_codes.copy_(codes, non_blocking=True)
+            host_measure.copy_(measure, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        barrier(world)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(stream)
+        barrier(world)
+        e_ms = reduce_max(a.elapsed_time(b), world)
+        result["e2e"] = {"value": queries / (e_ms / 1e3), "unit": "queries/s",
+                         "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * K * 4 + n * 8,
+                         "ms_per_step": e_ms / args.steps}
+        del host_in, host_codes, host_measure
+
+    # ---- one plain swarm step: geometry + top-K + two collision half-operators -------------
+    if not args.no_step:
+        try:
+            rng = gd.rngstate_init(n, seed=1 + rank, device=dev)
+            half = 0.5 * workloads.orbital_time()
+            dp.copy_(torch.from_numpy(np.ascontiguousarray(p_host)).to(dev))
+
+            def swarm_step():
+                sw.invalidate_col_geometry()
+                sw.evolve_collisions(dp, rng, half, workloads.DUST_MASS)
+                sw.evolve_collisions(dp, rng, half, workloads.DUST_MASS)
+
+            swarm_step()
+            barrier(world)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st_steps = max(1, min(args.steps, 3))
+            a.record(stream)
+            for _ in range(st_steps):
+                swarm_step()
+            b.record(stream)
+            barrier(world)
+            s_ms = reduce_max(a.elapsed_time(b), world) / st_steps
+            stats = sw.last_operator_stats()
+            result["swarm_step"] = {"steps_per_s": world * 1e3 / s_ms, "ms_per_step": s_ms,
+                                    "definition": "geometry + exact top-K + 2 collision half-operators of "
+                                                  "0.5/Omega(1 au) each, plain tree",
+                                    "last_operator": stats}
+        except Exception as e:  # reported, never hidden
+            result["swarm_step"] = {"error": str(e)}
+
+    # ---- CPU baseline: the oracle on the host cores, rank 0 at N = 1 -----------------------
+    if not args.no_cpu and rank == 0 and world == 1:
+        cb = cpu_baseline(cfg, p_host, args.cpu_sample, os.cpu_count())
+        result["cpu_baseline"] = {"value": cb["queries_per_s"], "unit": "queries/s", "cores": os.cpu_count(),
+                                  "kind": "port",
+                                  "sample": f"{cb['sample']} owners of the {n}-site workload, KD tree over all "
+                                            f"active sites built in {cb['build_s']:.1f} s (not counted)"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    sw.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import gamedev_b200
+
+    gamedev_b200.load()  # the prebuilt in-tree libgd_b200.so; raises if it is missing
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

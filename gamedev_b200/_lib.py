@@ -1,0 +1,125 @@
+"""ctypes binding of libgd_b200.so (the C ABI in include/gd_b200.h).
+
+The shared library is loaded from this package directory.  There is no fallback: if the library
+is missing or cannot be loaded, every entry point raises, so no CPU path can stand in for the
+CUDA kernels.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libgd_b200.so"
+
+GD_OK = 0
+STATUS_NAMES = {
+    0: "GD_OK",
+    1: "GD_ERR_INVALID_ARGUMENT",
+    2: "GD_ERR_CUDA",
+    3: "GD_ERR_NONFINITE",
+    4: "GD_ERR_CHAIN",
+    5: "GD_ERR_CAPACITY",
+    6: "GD_ERR_CONTINUATION_LIMIT",
+    7: "GD_ERR_TIME_RESOLUTION",
+    8: "GD_ERR_CONTROLLER",
+    9: "GD_ERR_NOT_READY",
+    10: "GD_ERR_OUT_OF_MEMORY",
+}
+GD_SEARCH_KDTREE, GD_SEARCH_MORTON = 0, 1
+GD_KERNEL_CONSTANT, GD_KERNEL_LINEAR, GD_KERNEL_PRODUCT, GD_KERNEL_CUSTOM = 0, 1, 2, 3
+
+
+class GdConfig(C.Structure):
+    """gd_config: the const_defs.cuh constants of one model."""
+
+    _fields_ = [
+        ("G", C.c_double), ("M_S", C.c_double), ("R_0", C.c_double), ("S_0", C.c_double),
+        ("n_x", C.c_int), ("n_y", C.c_int), ("n_z", C.c_int),
+        ("x_min", C.c_double), ("x_max", C.c_double), ("y_min", C.c_double), ("y_max", C.c_double),
+        ("z_min", C.c_double), ("z_max", C.c_double),
+        ("sigma_0", C.c_double), ("aspr_0", C.c_double), ("idx_p", C.c_double), ("idx_q", C.c_double),
+        ("const_nu", C.c_int), ("nu", C.c_double), ("alpha", C.c_double),
+        ("code_unit", C.c_int), ("reynolds_0", C.c_double), ("m_mol", C.c_double), ("x_sec", C.c_double),
+        ("half_disk", C.c_int), ("const_st", C.c_int),
+        ("stokes_0", C.c_double), ("rho_0", C.c_double),
+        ("coag_kernel", C.c_int), ("n_k", C.c_int), ("h_search", C.c_double), ("v_frag", C.c_double),
+        ("col_event_cap", C.c_int),
+        ("col_bin_x", C.c_int), ("col_bin_y", C.c_int), ("col_bin_z", C.c_int), ("col_bin_s", C.c_int),
+        ("col_bin_min", C.c_int),
+        ("col_bath_max", C.c_double), ("col_bath_eps", C.c_double), ("col_bath_alpha", C.c_double),
+        ("init_smin", C.c_double), ("init_smax", C.c_double),
+        ("search", C.c_int), ("morton_leaf_target", C.c_int), ("morton_max_level", C.c_int),
+    ]
+
+    def to_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class GdOperatorStats(C.Structure):
+    _fields_ = [("waves", C.c_int), ("chain_launches", C.c_int), ("owner_updates", C.c_longlong),
+                ("events", C.c_longlong), ("min_duration", C.c_double), ("max_duration", C.c_double)]
+
+
+PARTICLE_BYTES = 64
+
+# every symbol include/gd_b200.h declares, with (restype, argtypes)
+_P = C.c_void_p
+SIGNATURES = {
+    "gd_rng_state_bytes": (C.c_size_t, []),
+    "gd_config_default": (None, [C.POINTER(GdConfig)]),
+    "gd_create": (C.c_int, [C.POINTER(GdConfig), C.c_int, C.POINTER(_P)]),
+    "gd_destroy": (None, [_P]),
+    "gd_set_stream": (C.c_int, [_P, _P]),
+    "gd_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "gd_error_detail": (C.c_longlong, [_P]),
+    "gd_rng_init": (C.c_int, [_P, C.c_int, C.c_ulonglong, _P]),
+    "gd_geometry_build": (C.c_int, [_P, _P]),
+    "gd_knn": (C.c_int, [_P, _P, _P, _P, _P]),
+    "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
+    "gd_get_cache": (C.c_int, [_P, _P, _P]),
+    "gd_set_cache": (C.c_int, [_P, _P, _P]),
+    "gd_space_bin": (C.c_int, [_P, _P, _P]),
+    "gd_invalidate_geometry": (C.c_int, [_P]),
+    "gd_reset_controller": (C.c_int, [_P]),
+    "gd_collision_operator": (C.c_int, [_P, _P, _P, C.c_double, C.c_double]),
+    "gd_evolve_collisions": (C.c_int, [_P, _P, _P, C.c_double, C.c_double]),
+    "gd_last_operator_stats": (C.c_int, [_P, C.POINTER(GdOperatorStats)]),
+    "gd_launch_count": (C.c_longlong, [_P]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libgd_b200.so; raise if it is absent (build it with gamedev_b200.build.build())."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build the CUDA extension first "
+                               "(python -c 'import gamedev_b200.build as b; b.build()')")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class GdError(RuntimeError):
+    def __init__(self, status: int, message: str, detail: int):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message} (detail {detail})")
+        self.status = status
+        self.message = message
+        self.detail = detail
+
+
+def default_config(**overrides) -> GdConfig:
+    cfg = GdConfig()
+    load().gd_config_default(C.byref(cfg))
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg

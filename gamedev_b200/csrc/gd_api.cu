@@ -1,0 +1,313 @@
+// C ABI of libgd_b200: handle lifecycle and the entry points declared in include/gd_b200.h.
+#include <curand_kernel.h>
+
+#include <climits>
+#include <cstring>
+#include <new>
+
+#include "gd_collide.cuh"
+#include "gd_internal.cuh"
+
+namespace gd {
+
+Status cuda_status(cudaError_t e, const char *what) {
+    Status s;
+    s.code = (e == cudaErrorMemoryAllocation) ? GD_ERR_OUT_OF_MEMORY : GD_ERR_CUDA;
+    s.detail = static_cast<long long>(e);
+    s.msg = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();  // clear a sticky launch error so the handle stays usable
+    return s;
+}
+
+Model make_model(const gd_config &c) {
+    Model m;
+    m.G = c.G; m.M_S = c.M_S; m.R_0 = c.R_0; m.S_0 = c.S_0;
+    m.n_x = c.n_x; m.n_y = c.n_y; m.n_z = c.n_z;
+    m.x_min = c.x_min; m.x_max = c.x_max; m.y_min = c.y_min; m.y_max = c.y_max;
+    m.z_min = c.z_min; m.z_max = c.z_max;
+    m.sigma_0 = c.sigma_0; m.aspr_0 = c.aspr_0; m.idx_p = c.idx_p; m.idx_q = c.idx_q;
+    m.const_nu = c.const_nu; m.nu = c.nu; m.alpha = c.alpha;
+    m.code_unit = c.code_unit; m.reynolds_0 = c.reynolds_0; m.m_mol = c.m_mol; m.x_sec = c.x_sec;
+    m.half_disk = c.half_disk; m.const_st = c.const_st;
+    m.stokes_0 = c.stokes_0; m.rho_0 = c.rho_0;
+    m.coag_kernel = c.coag_kernel; m.n_k = c.n_k; m.h_search = c.h_search; m.v_frag = c.v_frag;
+    m.col_event_cap = c.col_event_cap;
+    m.col_bin_x = c.col_bin_x; m.col_bin_y = c.col_bin_y; m.col_bin_z = c.col_bin_z;
+    m.col_bin_s = c.col_bin_s; m.col_bin_min = c.col_bin_min;
+    m.col_bath_max = c.col_bath_max; m.col_bath_eps = c.col_bath_eps; m.col_bath_alpha = c.col_bath_alpha;
+    m.init_smin = c.init_smin; m.init_smax = c.init_smax;
+    m.dim = (c.n_z > 1) ? 3 : 2;
+    m.local_groups = ((c.n_x > 1) ? c.col_bin_x : 1) * c.col_bin_y * ((c.n_z > 1) ? c.col_bin_z : 1);
+    m.raw_bins = m.local_groups * c.col_bin_s;
+    return m;
+}
+
+// rngstate_init (src/swarm/rngstate_init.cu:11-18)
+__global__ void k_rng_init(curandState *st, int n, unsigned long long seed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) curand_init(seed, static_cast<unsigned long long>(i), 0ull, &st[i]);
+}
+
+}  // namespace gd
+
+struct gd_handle {
+    gd_config cfg;
+    gd::Model m;
+    int n = 0;
+    cudaStream_t stream = nullptr;
+    gd::Geometry geo;
+    gd::DevBuf<int32_t> codes;
+    gd::DevBuf<double> measure;
+    gd::DevBuf<float> kth;
+    gd::DevBuf<int32_t> spatial;
+    gd::Collider col;
+    bool geom_valid = false;   // col_geom_valid (swarm_runtime.cu:332)
+    bool cache_valid = false;
+    std::string err;
+    long long detail = 0;
+};
+
+static gd_status fail(gd_handle *h, const gd::Status &s) {
+    if (h) {
+        h->err = s.msg;
+        h->detail = s.detail;
+    }
+    return s.code;
+}
+
+static gd_status fail(gd_handle *h, gd_status code, const std::string &msg, long long detail = 0) {
+    gd::Status s;
+    s.code = code;
+    s.msg = msg;
+    s.detail = detail;
+    return fail(h, s);
+}
+
+static gd_status done(gd_handle *h, const gd::Status &s) {
+    if (!s) return fail(h, s);
+    h->err.clear();
+    h->detail = 0;
+    return GD_OK;
+}
+
+extern "C" {
+
+size_t gd_rng_state_bytes(void) { return sizeof(curandState); }
+
+void gd_config_default(gd_config *c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->G = 1.0; c->M_S = 1.0; c->R_0 = 1.0; c->S_0 = 1.0;
+    c->n_x = 100; c->n_y = 100; c->n_z = 1;
+    c->x_min = -M_PI; c->x_max = M_PI; c->y_min = 0.5; c->y_max = 1.5;
+    c->z_min = 0.5 * M_PI; c->z_max = 0.5 * M_PI;
+    c->sigma_0 = 1.0e-2; c->aspr_0 = 0.05; c->idx_p = -1.0; c->idx_q = -0.4;
+    c->const_nu = 0; c->nu = 1.0e-5; c->alpha = 1.0e-4;
+    c->code_unit = 0; c->reynolds_0 = 1.0e8; c->m_mol = 2.3 * 1.66054e-24; c->x_sec = 2.0e-15;
+    c->half_disk = 0; c->const_st = 0;
+    c->stokes_0 = 1.0e-3; c->rho_0 = 1.0;
+    c->coag_kernel = GD_KERNEL_CONSTANT; c->n_k = 200; c->h_search = 1.0; c->v_frag = 1.0;
+    c->col_event_cap = 32;
+    c->col_bin_x = 8; c->col_bin_y = 4; c->col_bin_z = 2; c->col_bin_s = 8; c->col_bin_min = 64;
+    c->col_bath_max = 0.05; c->col_bath_eps = 0.02; c->col_bath_alpha = 1.0e-3;
+    c->init_smin = 1.0; c->init_smax = 1.0;
+    c->search = GD_SEARCH_KDTREE;
+    c->morton_leaf_target = 128; c->morton_max_level = 20;
+}
+
+static std::string validate(const gd_config &c, int n) {
+    if (n <= 0) return "particle count must be positive";
+    if (static_cast<long long>(n) * 3 > INT_MAX) return "particle count too large for packed neighbour codes";
+    if (c.n_k < 1 || c.n_k > gd::kMaxK) return "n_k must be in 1..256";
+    if (c.n_x < 1 || c.n_y < 1 || c.n_z < 1) return "grid counts must be positive";
+    if (!(c.y_max > c.y_min) || !(c.y_min >= 0)) return "invalid radial domain";
+    if (c.coag_kernel < 0 || c.coag_kernel > 3) return "coag_kernel must be 0..3";
+    if (c.col_bin_x < 1 || c.col_bin_y < 1 || c.col_bin_z < 1 || c.col_bin_s < 1) return "controller bins must be positive";
+    if (c.search != GD_SEARCH_KDTREE && c.search != GD_SEARCH_MORTON) return "unknown search";
+    // a wedge (azimuth shorter than 2 pi) needs periodic images, which this build does not create
+    const bool wedge = c.n_x > 1 && static_cast<float>(c.x_max) - static_cast<float>(c.x_min) <
+                                        6.28318530717958647692f - 1.0e-06f;
+    if (wedge) return "azimuthal wedges (periodic images) are not supported";
+    return std::string();
+}
+
+gd_status gd_create(const gd_config *cfg, int n_p, gd_handle **out) {
+    if (!cfg || !out) return GD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    std::string why = validate(*cfg, n_p);
+    if (!why.empty()) return GD_ERR_INVALID_ARGUMENT;
+    gd_handle *h = new (std::nothrow) gd_handle();
+    if (!h) return GD_ERR_OUT_OF_MEMORY;
+    h->cfg = *cfg;
+    h->m = gd::make_model(*cfg);
+    h->n = n_p;
+    gd::Status s = gd::geometry_alloc(h->geo, h->m, n_p);
+    cudaError_t e = cudaSuccess;
+    if (s) e = h->codes.alloc(static_cast<size_t>(n_p) * cfg->n_k);
+    if (s && e == cudaSuccess) e = h->measure.alloc(n_p);
+    if (s && e == cudaSuccess) e = h->kth.alloc(n_p);
+    if (s && e == cudaSuccess) e = h->spatial.alloc(n_p);
+    if (s && e != cudaSuccess) s = gd::cuda_status(e, "allocate neighbour cache");
+    if (s) s = gd::collider_alloc(h->col, h->m, n_p);
+    if (!s) {
+        gd_status code = s.code;
+        delete h;
+        return code;
+    }
+    *out = h;
+    return GD_OK;
+}
+
+void gd_destroy(gd_handle *h) { delete h; }
+
+gd_status gd_set_stream(gd_handle *h, void *stream) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return GD_OK;
+}
+
+size_t gd_last_error(const gd_handle *h, char *buf, size_t len) {
+    if (!h) return 0;
+    if (buf && len) {
+        size_t k = h->err.size() < len - 1 ? h->err.size() : len - 1;
+        std::memcpy(buf, h->err.data(), k);
+        buf[k] = '\0';
+    }
+    return h->err.size();
+}
+
+long long gd_error_detail(const gd_handle *h) { return h ? h->detail : 0; }
+
+gd_status gd_rng_init(void *dev_rng, int n, unsigned long long seed, void *stream) {
+    if (!dev_rng || n < 0) return GD_ERR_INVALID_ARGUMENT;
+    if (n == 0) return GD_OK;
+    gd::k_rng_init<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<curandState *>(dev_rng), n, seed);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle) {
+    if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    h->geom_valid = false;
+    h->cache_valid = false;
+    gd::Status s = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
+    if (s) h->geom_valid = true;
+    return done(h, s);
+}
+
+gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
+                 float *dev_kth_d2) {
+    if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "gd_knn called before gd_geometry_build");
+    const bool own = !dev_codes && !dev_measure;
+    int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
+    double *measure = dev_measure ? dev_measure : h->measure.ptr;
+    float *kth = dev_kth_d2 ? dev_kth_d2 : h->kth.ptr;
+    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream);
+    if (s && own) {
+        h->cache_valid = true;
+        h->col.local_geometry_valid = false;
+    }
+    return done(h, s);
+}
+
+gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned char *dev_active) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "geometry not built");
+    cudaError_t e = cudaSuccess;
+    if (dev_site4)
+        e = cudaMemcpyAsync(dev_site4, h->geo.site.ptr, sizeof(float4) * h->n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess && dev_q)
+        e = cudaMemcpyAsync(dev_q, h->geo.q.ptr, sizeof(float) * h->n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess && dev_active)
+        e = cudaMemcpyAsync(dev_active, h->geo.active.ptr, h->n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e != cudaSuccess) return fail(h, gd::cuda_status(e, "copy sites"));
+    return GD_OK;
+}
+
+gd_status gd_get_cache(gd_handle *h, int32_t *dev_codes, double *dev_measure) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "neighbour cache not built");
+    cudaError_t e = cudaSuccess;
+    if (dev_codes)
+        e = cudaMemcpyAsync(dev_codes, h->codes.ptr, sizeof(int32_t) * h->codes.n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess && dev_measure)
+        e = cudaMemcpyAsync(dev_measure, h->measure.ptr, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e != cudaSuccess) return fail(h, gd::cuda_status(e, "copy neighbour cache"));
+    return GD_OK;
+}
+
+gd_status gd_set_cache(gd_handle *h, const int32_t *dev_codes, const double *dev_measure) {
+    if (!h || !dev_codes || !dev_measure) return fail(h, GD_ERR_INVALID_ARGUMENT, "null cache pointer");
+    cudaError_t e = cudaMemcpyAsync(h->codes.ptr, dev_codes, sizeof(int32_t) * h->codes.n,
+                                    cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->measure.ptr, dev_measure, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e != cudaSuccess) return fail(h, gd::cuda_status(e, "set neighbour cache"));
+    h->cache_valid = true;
+    h->col.local_geometry_valid = false;
+    return GD_OK;
+}
+
+gd_status gd_space_bin(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_spatial) {
+    if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    return done(h, gd::space_bin(h->m, dev_particle, h->n, dev_spatial ? dev_spatial : h->spatial.ptr, h->stream));
+}
+
+gd_status gd_invalidate_geometry(gd_handle *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    h->geom_valid = false;
+    h->cache_valid = false;
+    h->col.local_geometry_valid = false;
+    return GD_OK;
+}
+
+gd_status gd_reset_controller(gd_handle *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    gd::collider_reset_state(h->col);
+    return GD_OK;
+}
+
+gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *dev_rng, double duration,
+                                double total_dust_mass) {
+    if (!h || !dev_particle || !dev_rng) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "collision operator needs a neighbour cache");
+    gd::Status s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
+                                          h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr,
+                                          duration, total_dust_mass, h->stream);
+    return done(h, s);
+}
+
+gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *dev_rng, double duration,
+                               double total_dust_mass) {
+    if (!h || !dev_particle || !dev_rng) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    gd::Status s;
+    if (h->geom_valid && h->cache_valid) {
+        s = gd::state_screen(h->geo, h->m, dev_particle, h->stream);
+    } else {
+        h->geom_valid = false;
+        h->cache_valid = false;
+        s = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
+        if (s) {
+            h->geom_valid = true;
+            s = gd::knn_query(h->geo, h->m, dev_particle, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream);
+        }
+        if (s) s = gd::space_bin(h->m, dev_particle, h->n, h->spatial.ptr, h->stream);
+        if (s) {
+            h->cache_valid = true;
+            h->col.local_geometry_valid = false;
+        }
+    }
+    if (!s) return fail(h, s);
+    return gd_collision_operator(h, dev_particle, dev_rng, duration, total_dust_mass);
+}
+
+long long gd_launch_count(const gd_handle *h) { return h ? h->geo.launches + h->col.launches : 0; }
+
+gd_status gd_last_operator_stats(const gd_handle *h, gd_operator_stats *out) {
+    if (!h || !out) return GD_ERR_INVALID_ARGUMENT;
+    *out = h->col.stats;
+    return GD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1263 @@
+// Frozen-bath collision operator on sm_100a (evolve_local_collisions, _col_chain.cuh:108-539).
+//
+// Kernels (reference kernel in brackets):
+//   k_env_cache      [col_env_cache, col_env_cache.cu:15-20]     thread per owner
+//   k_bath_init      [col_bath_init + col_comp_zero]             thread per owner
+//   k_size_*         [col_size_zero/scan/bnds]                   moving log-size bin bounds
+//   k_bath_rate      [col_bath_rate, col_bath_rate.cu:13-130]    WARP per owner, exact fold order
+//   k_count_bin, k_binmap, k_rate_bins [col_count_bin, _build_col_binmap, col_rate_bins]
+//   k_skip_scan      [col_skip_scan, col_skip_scan.cu:13-59]     thread per owner
+//   k_chain          [col_chain_run, col_chain_run.cu:21-404]    persistent WARPS over a device queue,
+//                                                                each owner run to the end of its bath
+//   k_audit_bin      [col_audit_bin, col_audit_bin.cu:13-60]
+//   k_group_*, k_dep_graph [host owner lists + col_dep_graph]   device counting sort by group
+//
+// Differences in mechanism (results per owner are the same):
+//   * The reference relaunches col_chain_run with a 32-event cap and a device->host read of the
+//     unfinished count after every launch (_col_chain.cuh:379-402).  Its own test shows caps 1 and
+//     32 give identical particle and RNG hashes, so here one persistent launch runs every queued
+//     owner to its bath end, with a bounded event budget that reports GD_ERR_CONTINUATION_LIMIT.
+//   * The queued owner repeats the skip-scan trial draw and restores it (col_chain_run.cu:91-124);
+//     that shortcut can only restore the state, so it is not repeated here.
+//   * One warp holds one owner: the K frozen partners (size_old, numr_old, vertical scale) are
+//     loaded into registers once per owner instead of once per event, the rate folds use the
+//     reference's (count+1)/2 pairing in warp-private shared memory, and every lane replays the
+//     serial partner walk and the XORWOW draws on an identical RNG copy, so no lane waits.
+#include <math_constants.h>
+
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+
+#include "gd_collide.cuh"
+#include "gd_physics.cuh"
+
+namespace gd {
+
+constexpr int kMaxSlots = kMaxK / 32;  // neighbour slots per lane
+constexpr int kMaxGroups = 256;
+constexpr int kChainWarps = 4;
+constexpr long long kEventBudget = 1ll << 22;  // events per owner per bath before giving up
+
+// ------------------------------------------------------------------------------------------------
+// device scratch layout: one block copied to pinned host memory with one cudaMemcpyAsync
+// ------------------------------------------------------------------------------------------------
+struct Small {
+    size_t merged;       // int
+    size_t error_flag;   // int
+    size_t queued;       // int
+    size_t head;         // int
+    size_t events;       // unsigned long long
+    size_t binmap;       // int[raw]
+    size_t ratebin;      // RateBin[raw]
+    size_t audit;        // AuditBin[raw]
+    size_t counts;       // int[raw]
+    size_t dt;           // double[G]
+    size_t mmin, mmax;   // u64[G]
+    size_t lower, upper; // double[G]
+    size_t graph;        // u32[G*words]
+    size_t gcount;       // int[G]
+    size_t gcursor;      // int[G]
+    size_t total;
+};
+
+static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+static Small small_layout(const Model &m) {
+    Small L;
+    const int G = m.local_groups, R = m.raw_bins, W = (G + 31) / 32;
+    size_t o = 0;
+    L.merged = o; o += 4;
+    L.error_flag = o; o += 4;
+    L.queued = o; o += 4;
+    L.head = o; o += 4;
+    L.events = o; o += 8;
+    o = align256(o);
+    L.binmap = o; o = align256(o + 4 * R);
+    L.ratebin = o; o = align256(o + sizeof(RateBin) * R);
+    L.audit = o; o = align256(o + sizeof(AuditBin) * R);
+    L.counts = o; o = align256(o + 4 * R);
+    L.dt = o; o = align256(o + 8 * G);
+    L.mmin = o; o = align256(o + 8 * G);
+    L.mmax = o; o = align256(o + 8 * G);
+    L.lower = o; o = align256(o + 8 * G);
+    L.upper = o; o = align256(o + 8 * G);
+    L.graph = o; o = align256(o + 4 * G * W);
+    L.gcount = o; o = align256(o + 4 * G);
+    L.gcursor = o; o = align256(o + 4 * G);
+    L.total = o;
+    return L;
+}
+
+template <typename T>
+static T *at(DevBuf<unsigned char> &b, size_t off) {
+    return reinterpret_cast<T *>(b.ptr + off);
+}
+template <typename T>
+static T *at(unsigned char *b, size_t off) {
+    return reinterpret_cast<T *>(b + off);
+}
+
+// ------------------------------------------------------------------------------------------------
+// small per-owner kernels
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int owner_at(const int *ids, int slot) { return ids ? ids[slot] : slot; }
+
+__global__ void k_env_cache(Model m, int n, const gd_particle *__restrict__ part, Env *__restrict__ env) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && part[i].position[1] > 0.0) env[i] = make_env(m, part[i].position[1], part[i].position[2]);
+}
+
+// col_bath_init (col_bath_init.cu:11-23) + col_comp_zero (col_comp_zero.cu:11-19)
+__global__ void k_bath_init(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
+                            double *__restrict__ size_old, double *__restrict__ numr_old, double *__restrict__ time,
+                            int *__restrict__ events, unsigned char *__restrict__ complete, double *__restrict__ hazard,
+                            double *__restrict__ jump1, double *__restrict__ jump2, double *__restrict__ jumpmax) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) return;
+    int i = owner_at(ids, slot);
+    size_old[i] = part[i].par_size;
+    numr_old[i] = part[i].par_numr;
+    time[i] = 0.0;
+    events[i] = 0;
+    complete[i] = 0;
+    hazard[i] = jump1[i] = jump2[i] = jumpmax[i] = 0.0;
+}
+
+__global__ void k_size_zero(int G, unsigned long long *mmin, unsigned long long *mmax) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < G) {
+        mmin[g] = static_cast<unsigned long long>(__double_as_longlong(CUDART_INF));
+        mmax[g] = 0ull;
+    }
+}
+
+__global__ void k_size_scan(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
+                            const int32_t *__restrict__ spatial, const unsigned char *__restrict__ active,
+                            unsigned long long *mmin, unsigned long long *mmax) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) return;
+    int i = owner_at(ids, slot);
+    double size = part[i].par_size;
+    if (!active[i] || !(size > 0) || !isfinite(size)) return;
+    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(size));
+    atomicMin(&mmin[spatial[i]], bits);
+    atomicMax(&mmax[spatial[i]], bits);
+}
+
+__global__ void k_size_bnds(int G, const unsigned long long *mmin, const unsigned long long *mmax, double *lower,
+                            double *upper) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < G && mmax[g] != 0) {
+        lower[g] = 0.5 * __longlong_as_double(static_cast<long long>(mmin[g]));
+        upper[g] = 8.0 * __longlong_as_double(static_cast<long long>(mmax[g]));
+    }
+}
+
+// _get_col_sizebin (inc/swarm/_col_sizes.cuh:16-21)
+__device__ __forceinline__ int size_bin(const Model &m, double size, const double *lower, const double *upper, int g) {
+    if (!isfinite(size) || !(size > 0)) return 0;
+    double fraction = log(size / lower[g]) / log(upper[g] / lower[g]);
+    return max(0, min(m.col_bin_s - 1, static_cast<int>(floor(fraction * m.col_bin_s))));
+}
+
+__global__ void k_count_bin(Model m, const int *__restrict__ ids, int count, int *__restrict__ counts,
+                            const gd_particle *__restrict__ part, const int32_t *__restrict__ spatial,
+                            const unsigned char *__restrict__ active, const double *lower, const double *upper) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) return;
+    int i = owner_at(ids, slot);
+    if (!active[i]) return;
+    int g = spatial[i];
+    atomicAdd(counts + g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g), 1);
+}
+
+// _build_col_binmap (inc/swarm/_col_bound.cuh:232-285): merge adjacent sparse size bins inside
+// every spatial group.  Runs on the host (tests) and in a one-thread kernel.
+__host__ __device__ inline int binmap_compute(int groups, int bins, int bin_min, const int *raw_count, int *raw_to_merged) {
+    for (int i = 0; i < groups * bins; ++i) raw_to_merged[i] = -1;
+    int merged = 0;
+    for (int sp = 0; sp < groups; ++sp) {
+        int last = -1;
+        for (int b = 0; b < bins; ++b)
+            if (raw_count[sp * bins + b] > 0) last = b;
+        if (last < 0) {
+            int id = merged++;
+            for (int b = 0; b < bins; ++b) raw_to_merged[sp * bins + b] = id;
+            continue;
+        }
+        int begin = 0, previous = -1;
+        while (begin <= last) {
+            int end = begin, count = 0;
+            while (end <= last && count < bin_min) count += raw_count[sp * bins + end++];
+            bool merge_tail = end > last && count < bin_min && previous >= 0;
+            int id = merge_tail ? previous : merged++;
+            for (int b = begin; b < end; ++b) raw_to_merged[sp * bins + b] = id;
+            previous = id;
+            begin = end;
+        }
+        if (last + 1 < bins) {
+            int id = merged++;
+            for (int b = last + 1; b < bins; ++b) raw_to_merged[sp * bins + b] = id;
+        }
+    }
+    return merged;
+}
+
+__global__ void k_binmap(Model m, const int *counts, int *binmap, int *merged, RateBin *ratebin) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *merged = binmap_compute(m.local_groups, m.col_bin_s, m.col_bin_min, counts, binmap);
+}
+
+__global__ void k_rate_bins(Model m, const int *__restrict__ ids, int count, RateBin *__restrict__ bin,
+                            const gd_particle *__restrict__ part, const double *__restrict__ rate,
+                            const double *__restrict__ change, const double *__restrict__ second,
+                            const int32_t *__restrict__ spatial, const int *__restrict__ binmap,
+                            const unsigned char *__restrict__ active, const double *lower, const double *upper) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) return;
+    int i = owner_at(ids, slot);
+    if (!active[i]) return;
+    int g = spatial[i];
+    int b = binmap[g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g)];
+    double weight = part[i].par_numr * grain_mass(m, part[i].par_size);
+    atomicAdd(&bin[b].owner_count, 1);
+    if (!isfinite(weight) || !(weight > 0.0) || !isfinite(rate[i]) || rate[i] < 0.0 || !isfinite(change[i]) ||
+        change[i] < 0 || !isfinite(second[i]) || second[i] < 0) {
+        atomicAdd(&bin[b].invalid_count, 1);
+        return;
+    }
+    atomicAdd(&bin[b].mass, weight);
+    atomicAdd(&bin[b].weighted_rate, weight * rate[i]);
+    atomicAdd(&bin[b].weighted_change, weight * change[i]);
+    atomicAdd(&bin[b].weighted_second, weight * second[i]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// per-owner context shared by the bath-rate and chain kernels
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ OwnerCtx owner_ctx(const Model &m, const gd_particle *part, const Env *env, int i,
+                                              double measure, double lambda0) {
+    OwnerCtx o;
+    o.y = part[i].position[1];
+    o.z = part[i].position[2];
+    double R = cyl_R(m, o.y, o.z);
+    o.H_i = R * get_hg(m, R);
+    o.measure = measure;
+    o.lambda0 = lambda0;
+    if (env && m.coag_kernel == GD_KERNEL_CUSTOM) o.env = env[i];
+    return o;
+}
+
+// in-place (count+1)/2 fold of a warp-private array (col_bath_rate.cu:105-118)
+template <typename F>
+__device__ __forceinline__ void warp_fold(int K, int lane, F &&combine) {
+    for (int count = K; count > 1; count = (count + 1) / 2) {
+        const int half = (count + 1) / 2;
+        for (int j = lane; j < count / 2; j += 32) combine(j, j + half);
+        __syncwarp();
+    }
+}
+
+struct RateArgs {
+    const int *ids;
+    int count;
+    const gd_particle *part;
+    const int32_t *codes;
+    const double *measure;
+    const unsigned char *active;
+    const double *size_old;
+    const double *numr_old;
+    const Env *env;
+    double lambda0;
+    double *rate, *change, *second;
+    RateMoments *cached;
+};
+
+// col_bath_rate (col_bath_rate.cu:13-130): one warp per owner
+__global__ void __launch_bounds__(128) k_bath_rate(Model m, RateArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int K = m.n_k;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int slot = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (slot >= a.count) return;
+    double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 4 * K;
+    double *rate_w = w, *change_w = w + K, *second_w = w + 2 * K, *max_w = w + 3 * K;
+    int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
+                   static_cast<size_t>(wib) * K;
+    const int i = owner_at(a.ids, slot);
+    const bool act = a.active[i] != 0;
+    const double meas = a.measure[i];
+    const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
+    const double size_i = a.size_old[i];
+    for (int s = lane; s < K; s += 32) {
+        double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
+        const int nb = a.codes[static_cast<size_t>(i) * K + s];
+        if (act && nb >= 0 && meas > 0.0) {
+            const int j = nb / 3;
+            const double size_j = a.size_old[j];
+            double vrel;
+            double pr = pair_rate(m, o, size_i, size_j, a.numr_old[j], a.part, j, vrel);
+            double mean = 0.0, sec = 0.0, maxi = 0.0;
+            pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+            mx = pr > 0.0 ? maxi : 0.0;
+            c = pr * mean;
+            sc = pr * sec;
+            r = pr;
+        }
+        rate_w[s] = r;
+        change_w[s] = c;
+        second_w[s] = sc;
+        max_w[s] = mx;
+        valid_w[s] = isfinite(r) && r >= 0.0;
+    }
+    __syncwarp();
+    warp_fold(K, lane, [&](int j, int h) {
+        rate_w[j] += rate_w[h];
+        change_w[j] += change_w[h];
+        second_w[j] += second_w[h];
+        max_w[j] = fmax(max_w[j], max_w[h]);
+        valid_w[j] = valid_w[j] && valid_w[h];
+    });
+    if (lane == 0) {
+        RateMoments cm;
+        cm.rate = valid_w[0] ? rate_w[0] : -1.0;
+        cm.first = change_w[0];
+        cm.second = second_w[0];
+        cm.maximum = max_w[0];
+        a.cached[i] = cm;
+        a.rate[i] = rate_w[0];
+        a.change[i] = change_w[0];
+        a.second[i] = second_w[0];
+    }
+}
+
+// _get_col_uniform (inc/swarm/_col_rates.cuh:145-149)
+__device__ __forceinline__ double col_uniform(curandState *st) {
+    return fmin(curand_uniform_double(st), nextafter(1.0, 0.0));
+}
+
+struct ChainArgs {
+    const int *ids;
+    int count;
+    curandState *rng;
+    const unsigned char *active;
+    const double *measure;
+    const int32_t *spatial;
+    const double *dt;
+    const RateMoments *cached;
+    double *time, *hazard, *jump1, *jump2, *jumpmax;
+    int *events;
+    unsigned char *complete;
+    int *queue;
+    int *queued;
+};
+
+// col_skip_scan (col_skip_scan.cu:13-59)
+__global__ void k_skip_scan(ChainArgs a) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    bool enqueue = false;
+    int i = 0;
+    if (slot < a.count) {
+        i = owner_at(a.ids, slot);
+        const double end = a.dt[a.spatial[i]];
+        if (!a.active[i] || !(a.measure[i] > 0.0)) {
+            a.time[i] = end;
+            a.complete[i] = 1;
+        } else if (!a.complete[i]) {
+            enqueue = true;
+            if (a.time[i] == 0.0 && a.events[i] == 0) {
+                const RateMoments c = a.cached[i];
+                if (isfinite(c.rate) && c.rate >= 0.0) {
+                    if (c.rate == 0.0) {
+                        a.time[i] = end;
+                        a.complete[i] = 1;
+                        enqueue = false;
+                    } else {
+                        curandState st = a.rng[i];
+                        const double wait = -log(col_uniform(&st)) / c.rate;
+                        const double remaining = end - a.time[i];
+                        if (isfinite(wait) && wait > 0.0 && wait >= remaining) {
+                            a.hazard[i] += c.rate * remaining;
+                            a.jump1[i] += c.first * remaining;
+                            a.jump2[i] += c.second * remaining;
+                            a.jumpmax[i] = fmax(a.jumpmax[i], c.maximum);
+                            a.time[i] = end;
+                            a.complete[i] = 1;
+                            a.rng[i] = st;
+                            enqueue = false;
+                        }
+                        // otherwise the trial draw stays uncommitted: the chain repeats it
+                    }
+                }
+            }
+        }
+    }
+    // warp-aggregated queue append
+    const unsigned int mask = __ballot_sync(0xffffffffu, enqueue);
+    if (mask) {
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == __ffs(mask) - 1) base = atomicAdd(a.queued, __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+        if (enqueue) a.queue[base + __popc(mask & ((1u << lane) - 1u))] = i;
+    }
+}
+
+struct ChainRun {
+    const gd_particle *part_ro;
+    gd_particle *part;
+    const int32_t *codes;
+    const double *size_old, *numr_old;
+    const Env *env;
+    double lambda0;
+    int *error;
+    int *error_flag;
+    int *head;
+    unsigned long long *events_total;
+};
+
+// col_chain_run (col_chain_run.cu:21-404): persistent warps, one owner at a time
+__global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a, ChainRun r) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int K = m.n_k;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 5 * K;
+    double *prate = w, *tot = w + K, *pj1 = w + 2 * K, *pj2 = w + 3 * K, *pjm = w + 4 * K;
+    int *last_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(kChainWarps) * 5 * K) +
+                  static_cast<size_t>(wib) * K;
+    const int nslot = (K + 31) / 32;
+    const int queued = *a.queued;
+
+    while (true) {
+        int qs = 0;
+        if (lane == 0) qs = atomicAdd(r.head, 1);
+        qs = __shfl_sync(0xffffffffu, qs, 0);
+        if (qs >= queued) break;
+        const int i = a.queue[qs];
+        const double bath_end = a.dt[a.spatial[i]];
+        const double meas = a.measure[i];
+
+        double size_i = r.part_ro[i].par_size;
+        double numr_i = r.part_ro[i].par_numr;
+        double time_i = a.time[i];
+        double hazard_i = a.hazard[i], jump1_i = a.jump1[i], jump2_i = a.jump2[i], jumpmax_i = a.jumpmax[i];
+        curandState rng = a.rng[i];  // every lane holds the same state and draws the same numbers
+        int event_count = a.events[i];
+        int err = 0;
+        bool running = a.complete[i] == 0;
+        if (!a.active[i] || !(meas > 0.0)) {
+            time_i = bath_end;
+            running = false;
+        }
+
+        // frozen partners of this owner, kept in registers for every event
+        const OwnerCtx o = owner_ctx(m, r.part_ro, r.env, i, meas, r.lambda0);
+        int nb[kMaxSlots];
+        double sj[kMaxSlots], nj[kMaxSlots];
+#pragma unroll
+        for (int t = 0; t < kMaxSlots; ++t) {
+            nb[t] = -1;
+            sj[t] = 0.0;
+            nj[t] = 0.0;
+            const int s = lane + 32 * t;
+            if (t < nslot && s < K) {
+                nb[t] = r.codes[static_cast<size_t>(i) * K + s];
+                if (nb[t] >= 0) {
+                    sj[t] = r.size_old[nb[t] / 3];
+                    nj[t] = r.numr_old[nb[t] / 3];
+                }
+            }
+        }
+
+        long long accepted = 0;
+        while (running) {
+            if (accepted >= kEventBudget) {
+                err = 7;
+                running = false;
+                break;
+            }
+#pragma unroll
+            for (int t = 0; t < kMaxSlots; ++t) {
+                const int s = lane + 32 * t;
+                if (t < nslot && s < K) {
+                    double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
+                    if (nb[t] >= 0) {
+                        double vrel;
+                        pv = pair_rate(m, o, size_i, sj[t], nj[t], r.part_ro, nb[t] / 3, vrel);
+                        double mean = 0.0, sec = 0.0, maxi = 0.0;
+                        pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
+                        j1 = pv * mean;
+                        j2 = pv * sec;
+                        jm = (pv > 0.0) ? maxi : 0.0;
+                    }
+                    prate[s] = pv;
+                    tot[s] = pv;
+                    pj1[s] = j1;
+                    pj2[s] = j2;
+                    pjm[s] = jm;
+                    last_w[s] = (!isfinite(pv) || pv < 0.0) ? -2 : (pv > 0.0 ? s : -1);
+                }
+            }
+            __syncwarp();
+            warp_fold(K, lane, [&](int j, int h) {
+                tot[j] += tot[h];
+                pj1[j] += pj1[h];
+                pj2[j] += pj2[h];
+                pjm[j] = fmax(pjm[j], pjm[h]);
+                const int left = last_w[j], right = last_w[h];
+                last_w[j] = (left == -2 || right == -2) ? -2 : (left > right ? left : right);
+            });
+            const double total_rate = tot[0], total_j1 = pj1[0], total_j2 = pj2[0], total_jm = pjm[0];
+            const int last_positive = last_w[0];
+            __syncwarp();
+            // the reference's thread-0 section, replayed identically by every lane
+            if (last_positive == -2) {
+                err = 1;
+                running = false;
+            }
+            if (running && (!isfinite(total_rate) || total_rate < 0.0)) {
+                err = 2;
+                running = false;
+            }
+            if (running && total_rate == 0.0) {
+                time_i = bath_end;
+                running = false;
+            }
+            if (!running) break;
+            const double wait = -log(col_uniform(&rng)) / total_rate;
+            const double remaining = bath_end - time_i;
+            if (!isfinite(wait) || !(wait > 0.0)) {
+                err = 3;
+                break;
+            }
+            if (wait >= remaining) {
+                hazard_i += total_rate * remaining;
+                jump1_i += total_j1 * remaining;
+                jump2_i += total_j2 * remaining;
+                jumpmax_i = fmax(jumpmax_i, total_jm);
+                time_i = bath_end;
+                break;
+            }
+            const double event_time = time_i + wait;
+            if (!(event_time > time_i)) {
+                err = 4;
+                break;
+            }
+            hazard_i += total_rate * wait;
+            jump1_i += total_j1 * wait;
+            jump2_i += total_j2 * wait;
+            jumpmax_i = fmax(jumpmax_i, total_jm);
+            // partner: first slot whose cumulative rate exceeds U*total, in slot order
+            const double target = col_uniform(&rng) * total_rate;
+            double cumulative = 0.0;
+            int pick = -1;
+            for (int s = 0; s < K; ++s) {
+                const double pr = prate[s];
+                if (pr <= 0.0) continue;
+                cumulative += pr;
+                if (cumulative > target) {
+                    pick = s;
+                    break;
+                }
+            }
+            if (pick < 0) pick = last_positive;
+            if (pick < 0) {
+                err = 5;
+                break;
+            }
+            const int code_j = r.codes[static_cast<size_t>(i) * K + pick];
+            const double size_j = r.size_old[code_j / 3];
+            double vrel = 0.0;
+            if (m.coag_kernel == GD_KERNEL_CUSTOM) {
+                vrel = use_env_cache(m) ? cached_pair_speed(m, o.env, size_i, size_j)
+                                        : direct_pair_speed(m, o.y, o.z, size_i, size_j);
+            }
+            const double mass_before = numr_i * size_i * size_i * size_i;
+            const bool high_speed = vrel >= m.v_frag;
+            const double sample = high_speed ? col_uniform(&rng) : 0.0;
+            const double size_new = sample_outcome(m, size_i, size_j, high_speed, sample);
+            numr_i = mass_before / (size_new * size_new * size_new);
+            size_i = size_new;
+            time_i = event_time;
+            ++event_count;
+            ++accepted;
+            const double mass_after = numr_i * size_i * size_i * size_i;
+            const double mass_scale = fmax(fabs(mass_before), fabs(mass_after));
+            if (!isfinite(size_i) || !isfinite(numr_i) || !(size_i > 0.0) || !(numr_i > 0.0) ||
+                fabs(mass_after - mass_before) > 2.0e-12 * mass_scale) {
+                err = 6;
+                break;
+            }
+        }
+        if (lane == 0) {
+            r.part[i].par_size = size_i;
+            r.part[i].par_numr = numr_i;
+            a.rng[i] = rng;
+            a.time[i] = time_i;
+            a.events[i] = event_count;
+            a.hazard[i] = hazard_i;
+            a.jump1[i] = jump1_i;
+            a.jump2[i] = jump2_i;
+            a.jumpmax[i] = jumpmax_i;
+            a.complete[i] = 1;
+            if (err) {
+                r.error[i] = err;
+                atomicMax(r.error_flag, err);
+            }
+            if (accepted) atomicAdd(r.events_total, static_cast<unsigned long long>(accepted));
+        }
+        __syncwarp();
+    }
+}
+
+// _col_atomic_max (inc/swarm/_col_rates.cuh:152-164)
+__device__ __forceinline__ void atomic_max_double(double *address, double value) {
+    unsigned long long *p = reinterpret_cast<unsigned long long *>(address);
+    unsigned long long old = *p;
+    while (value > __longlong_as_double(static_cast<long long>(old))) {
+        unsigned long long assumed = old;
+        old = atomicCAS(p, assumed, static_cast<unsigned long long>(__double_as_longlong(value)));
+        if (old == assumed) break;
+    }
+}
+
+struct AuditArgs {
+    const int *ids;
+    int count;
+    AuditBin *bin;
+    const gd_particle *part;
+    const double *size_old, *numr_old, *rate, *hazard, *jump1, *jump2, *jumpmax;
+    const int *events;
+    const int32_t *spatial;
+    const int *binmap;
+    const unsigned char *active;
+    const double *dt;
+    const double *lower, *upper;
+};
+
+// col_audit_bin (col_audit_bin.cu:13-60)
+__global__ void k_audit_bin(Model m, AuditArgs a) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= a.count) return;
+    int i = owner_at(a.ids, slot);
+    if (!a.active[i]) return;
+    int g = a.spatial[i];
+    double duration = a.dt[g];
+    int start = a.binmap[g * m.col_bin_s + size_bin(m, a.size_old[i], a.lower, a.upper, g)];
+    int stop = a.binmap[g * m.col_bin_s + size_bin(m, a.part[i].par_size, a.lower, a.upper, g)];
+    double weight = a.numr_old[i] * grain_mass(m, a.size_old[i]);
+    double probability = -expm1(-a.rate[i] * duration);
+    double expected = a.hazard[i];
+    double events = static_cast<double>(a.events[i]);
+    AuditBin *b = a.bin + start;
+    atomicAdd(&b->owner_count, 1);
+    if (!isfinite(weight) || !(weight > 0.0) || !isfinite(probability) || !isfinite(expected) || expected < 0.0 ||
+        !isfinite(events) || !isfinite(a.jump1[i]) || a.jump1[i] < 0.0 || !isfinite(a.jump2[i]) || a.jump2[i] < 0.0 ||
+        !isfinite(a.jumpmax[i]) || a.jumpmax[i] < 0.0 || !isfinite(a.part[i].par_size) || !(a.part[i].par_size > 0.0)) {
+        atomicAdd(&b->invalid_count, 1);
+        return;
+    }
+    atomicAdd(&b->mass, weight);
+    atomicAdd(&b->predicted_f, weight * probability);
+    atomicAdd(&b->predicted_e, weight * expected);
+    atomicAdd(&b->predicted_var_f, weight * weight * probability * (1.0 - probability));
+    atomicAdd(&b->predicted_var_e, weight * weight * expected);
+    atomicAdd(&b->predicted_g, weight * a.jump1[i]);
+    atomicAdd(&b->predicted_var_g, weight * weight * a.jump2[i]);
+    atomic_max_double(&b->maximum_weight, weight);
+    atomic_max_double(&b->maximum_g_jump, weight * a.jumpmax[i]);
+    if (a.events[i] > 0) atomicAdd(&b->touched, weight);
+    atomicAdd(&b->event_weight, weight * events);
+    atomicAdd(&b->growth, weight * fabs(log(a.part[i].par_size / a.size_old[i])));
+    atomicAdd(&a.bin[stop].end_mass, weight);
+}
+
+// owner lists per spatial group (_col_chain.cuh:162-167) by a device counting sort
+__global__ void k_group_count(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcount) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&gcount[spatial[i]], 1);
+}
+__global__ void k_group_fill(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcursor,
+                             int *__restrict__ sorted) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sorted[atomicAdd(&gcursor[spatial[i]], 1)] = i;
+}
+
+// col_dep_graph (col_dep_graph.cu:43-59): edge c->d when an owner in c has a neighbour in d
+__global__ void k_dep_graph(int n, int K, int words, unsigned int *__restrict__ edges, const int32_t *__restrict__ spatial,
+                            const int32_t *__restrict__ codes, const unsigned char *__restrict__ active) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !active[i]) return;
+    unsigned int bits[kMaxGroups / 32] = {};
+    for (int k = 0; k < K; ++k) {
+        int e = codes[static_cast<size_t>(i) * K + k];
+        if (e < 0) continue;
+        int c = spatial[e / 3];
+        bits[c >> 5] |= 1u << (c & 31);
+    }
+    for (int wd = 0; wd < words; ++wd)
+        if (bits[wd]) atomicOr(edges + spatial[i] * words + wd, bits[wd]);
+}
+
+struct WaveTable {
+    int groups;
+    int start[kMaxGroups];
+    int len[kMaxGroups];
+    int out[kMaxGroups];
+};
+
+// concatenate the owner lists of the due groups into ids
+__global__ void k_wave_ids(WaveTable t, int total, const int *__restrict__ sorted, int *__restrict__ ids) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= total) return;
+    int lo = 0, hi = t.groups - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (t.out[mid] <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    ids[p] = sorted[t.start[lo] + (p - t.out[lo])];
+}
+
+// ------------------------------------------------------------------------------------------------
+// host controller: scheduler and bath bounds
+// ------------------------------------------------------------------------------------------------
+static Status err(gd_status code, const std::string &msg, long long detail = 0) {
+    Status s;
+    s.code = code;
+    s.msg = msg;
+    s.detail = detail;
+    return s;
+}
+
+Status Schedule::init(double h, const std::vector<double> &requested, const std::vector<unsigned int> &edges) {
+    horizon = h;
+    const int n = static_cast<int>(requested.size());
+    level.assign(n, 0);
+    step.assign(n, 0);
+    next.assign(n, 0);
+    links.clear();
+    if (!(h > 0) || !std::isfinite(h)) return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
+    const int words = (n + 31) / 32;
+    for (int c = 0; c < n; ++c) {
+        if (!(requested[c] > 0) || !std::isfinite(requested[c]))
+            return err(GD_ERR_CONTROLLER, "invalid local collision timestep");
+        double dt = h;
+        while (dt > requested[c]) {
+            if (++level[c] > 52) return err(GD_ERR_TIME_RESOLUTION, "local collision timestep exceeds time resolution");
+            dt *= 0.5;
+        }
+    }
+    for (int c = 0; c < n; ++c)
+        for (int d = c + 1; d < n; ++d)
+            if ((edges[c * words + d / 32] & (1u << (d % 32))) || (edges[d * words + c / 32] & (1u << (c % 32))))
+                links.emplace_back(c, d);
+    bool changed;
+    do {
+        changed = false;
+        for (int c = 0; c < n; ++c)
+            for (int d = 0; d < n; ++d) {
+                if (!(edges[c * words + d / 32] & (1u << (d % 32)))) continue;
+                if (level[c] < level[d] - 4) {
+                    level[c] = level[d] - 4;
+                    changed = true;
+                }
+                if (level[d] < level[c] - 4) {
+                    level[d] = level[c] - 4;
+                    changed = true;
+                }
+            }
+    } while (changed);
+    end = std::uint64_t(1) << 52;
+    for (int c = 0; c < n; ++c) step[c] = std::uint64_t(1) << (52 - level[c]);
+    return Status::ok();
+}
+
+std::uint64_t Schedule::time() const {
+    std::uint64_t t = next[0];
+    for (auto v : next) t = v < t ? v : t;
+    return t;
+}
+
+std::vector<int> Schedule::due(std::uint64_t tick) const {
+    std::vector<int> out;
+    for (int c = 0; c < static_cast<int>(next.size()); ++c)
+        if (next[c] == tick) out.push_back(c);
+    return out;
+}
+
+Status Schedule::adapt(std::uint64_t tick, const std::vector<int> &groups, const std::vector<double> &requested,
+                       const std::vector<bool> &passed) {
+    const int n = static_cast<int>(level.size());
+    std::vector<bool> act(n, false);
+    for (int c : groups) act[c] = true;
+    std::vector<int> cap(n, 52), cand = level;
+    for (int c = 0; c < n; ++c)
+        if (!act[c]) cap[c] = level[c];
+    bool changed;
+    do {
+        changed = false;
+        for (const auto &e : links) {
+            int c = e.first, d = e.second;
+            if (act[c] && cap[c] > cap[d] + 4) {
+                cap[c] = cap[d] + 4;
+                changed = true;
+            }
+            if (act[d] && cap[d] > cap[c] + 4) {
+                cap[d] = cap[c] + 4;
+                changed = true;
+            }
+        }
+    } while (changed);
+    for (int c : groups) {
+        if (!(requested[c] > 0) || !std::isfinite(requested[c]))
+            return err(GD_ERR_CONTROLLER, "invalid adaptive collision timestep");
+        int want = 0;
+        double h = horizon;
+        while (h > requested[c]) {
+            if (++want > 52) return err(GD_ERR_TIME_RESOLUTION, "adaptive collision time resolution exceeded");
+            h *= 0.5;
+        }
+        cand[c] = passed[c] ? want : std::max(want, level[c]);
+        while (tick % (std::uint64_t(1) << (52 - cand[c]))) ++cand[c];
+        cand[c] = std::min(cand[c], cap[c]);
+    }
+    do {
+        changed = false;
+        for (const auto &e : links) {
+            int c = e.first, d = e.second;
+            if (act[c] && cand[c] < cand[d] - 4) {
+                cand[c] = cand[d] - 4;
+                changed = true;
+            }
+            if (act[d] && cand[d] < cand[c] - 4) {
+                cand[d] = cand[c] - 4;
+                changed = true;
+            }
+        }
+    } while (changed);
+    for (int c : groups) {
+        level[c] = cand[c];
+        step[c] = std::uint64_t(1) << (52 - level[c]);
+    }
+    return Status::ok();
+}
+
+// change_limit (inc/swarm/_col_bound.cuh:209-220)
+Status change_limit(double A, double B, double epsilon, double horizon, ChangeBound &out) {
+    if (!std::isfinite(A) || A < 0 || !std::isfinite(B) || B < 0 || !std::isfinite(epsilon) || !(epsilon > 0) ||
+        !std::isfinite(horizon) || !(horizon > 0))
+        return err(GD_ERR_CONTROLLER, "invalid change-based refresh inputs");
+    out = {horizon, 0};
+    if (A > 0 && epsilon / A < out.duration) out = {epsilon / A, 1};
+    if (B > 0 && epsilon * epsilon / B < out.duration) out = {epsilon * epsilon / B, 2};
+    if (!(out.duration > 0)) return err(GD_ERR_CONTROLLER, "change-based timestep underflow");
+    return Status::ok();
+}
+
+int build_binmap(const Model &m, const std::vector<int> &raw_count, std::vector<int> &raw_to_merged) {
+    raw_to_merged.assign(raw_count.size(), -1);
+    return binmap_compute(m.local_groups, m.col_bin_s, m.col_bin_min, raw_count.data(), raw_to_merged.data());
+}
+
+// _choose_col_bath (inc/swarm/_col_bound.cuh:288-310)
+Status choose_bath(const Model &m, const RateBin *bins, int count, double remaining, double limit_scale, double &out,
+                   int *binding) {
+    double duration = std::min(remaining, m.col_bath_max);
+    double tolerance = m.col_bath_eps * limit_scale;
+    int reason = 0;
+    for (int b = 0; b < count; ++b) {
+        const RateBin &v = bins[b];
+        if (v.invalid_count) return err(GD_ERR_CONTROLLER, "invalid change-based rate moments");
+        if (!(v.mass > 0)) continue;
+        ChangeBound bound;
+        GD_TRY(change_limit(v.weighted_change / v.mass, v.weighted_second / v.mass, tolerance, duration, bound));
+        if (bound.duration < duration) {
+            duration = bound.duration;
+            reason = bound.reason;
+        }
+    }
+    if (binding) *binding = reason;
+    out = duration;
+    return Status::ok();
+}
+
+// _finish_col_bath (inc/swarm/_col_bound.cuh:313-403)
+Status finish_bath(const Model &m, const AuditBin *bins, int count, BathState &state, BathResult &result) {
+    result = BathResult();
+    int active_count = 0;
+    double total_mass = 0.0;
+    for (int b = 0; b < count; ++b) {
+        if (bins[b].invalid_count != 0)
+            return err(GD_ERR_CONTROLLER, "collision bath controller returned an invalid audit state");
+        if (bins[b].mass > 0.0) active_count++;
+        total_mass += bins[b].mass;
+    }
+    if (!(total_mass > 0.0)) return err(GD_ERR_CONTROLLER, "collision bath controller found no active represented mass");
+    double confidence_log = std::log(2.0 * static_cast<double>(active_count) / m.col_bath_alpha);
+    double mass_difference = 0.0;
+    for (int b = 0; b < count; ++b) {
+        const AuditBin &v = bins[b];
+        mass_difference += std::abs(v.end_mass - v.mass);
+        if (!(v.mass > 0.0)) continue;
+        double mass_sq = v.mass * v.mass;
+        double predicted_f = v.predicted_f / v.mass;
+        double predicted_e = v.predicted_e / v.mass;
+        double predicted_g = v.predicted_g / v.mass;
+        double touched = v.touched / v.mass;
+        double events = v.event_weight / v.mass;
+        double growth = v.growth / v.mass;
+        double weight_max = v.maximum_weight / v.mass;
+        double jump_max = v.maximum_g_jump / v.mass;
+        double upper_f = std::min(1.0, predicted_f + std::sqrt(2.0 * v.predicted_var_f / mass_sq * confidence_log) +
+                                           weight_max * confidence_log / 3.0);
+        double upper_e = predicted_e + std::sqrt(2.0 * v.predicted_var_e / mass_sq * confidence_log) +
+                         weight_max * confidence_log / 3.0;
+        double upper_g = predicted_g + std::sqrt(2.0 * v.predicted_var_g / mass_sq * confidence_log) +
+                         jump_max * confidence_log / 3.0;
+        result.max_f = std::max(result.max_f, predicted_f);
+        result.max_e = std::max(result.max_e, predicted_e);
+        result.max_touched = std::max(result.max_touched, touched);
+        result.max_events = std::max(result.max_events, events);
+        result.max_g = std::max(result.max_g, growth);
+        result.max_g_upper = std::max(result.max_g_upper, upper_g);
+        result.activity_overshoot = result.activity_overshoot || std::min(touched, 1.0) > upper_f || events > upper_e;
+        result.distribution_overshoot = result.distribution_overshoot || growth > std::max(m.col_bath_eps, upper_g);
+    }
+    result.d_bath = mass_difference / (2.0 * total_mass);
+    result.distribution_overshoot = result.distribution_overshoot || result.d_bath > m.col_bath_eps;
+    bool issue = result.activity_overshoot || result.distribution_overshoot;
+    bool at_floor = state.limit_scale <= 0.25 * (1.0 + 8.0 * std::numeric_limits<double>::epsilon());
+    if (issue) {
+        state.activity_streak++;
+        state.quiet_streak = 0;
+        state.floor_streak = at_floor ? state.floor_streak + 1 : 0;
+    } else {
+        state.activity_streak = 0;
+        state.quiet_streak++;
+        state.floor_streak = 0;
+    }
+    if (result.distribution_overshoot || state.activity_streak >= 2) {
+        state.limit_scale = std::max(0.25, 0.5 * state.limit_scale);
+        state.activity_streak = 0;
+    } else if (state.quiet_streak >= 3) {
+        state.limit_scale = std::min(1.0, 1.25 * state.limit_scale);
+        state.quiet_streak = 0;
+    }
+    result.persistent_overshoot = state.floor_streak >= 2;
+    return Status::ok();
+}
+
+// ------------------------------------------------------------------------------------------------
+// allocation and the operator
+// ------------------------------------------------------------------------------------------------
+Collider::~Collider() {
+    if (host_small) cudaFreeHost(host_small);
+}
+
+Status collider_alloc(Collider &c, const Model &m, int n) {
+    if (m.local_groups > kMaxGroups) return err(GD_ERR_INVALID_ARGUMENT, "more than 256 controller groups");
+    c.n = n;
+    for (DevBuf<double> *b : {&c.size_old, &c.numr_old, &c.time, &c.hazard, &c.jump1, &c.jump2, &c.jumpmax, &c.rate,
+                              &c.change_rate, &c.second_rate})
+        GD_TRY_CUDA(b->alloc(n));
+    GD_TRY_CUDA(c.events.alloc(n));
+    GD_TRY_CUDA(c.error.alloc(n));
+    GD_TRY_CUDA(c.complete.alloc(n));
+    GD_TRY_CUDA(c.env.alloc(static_cast<size_t>(n) * 8));
+    GD_TRY_CUDA(c.cached.alloc(static_cast<size_t>(n) * 4));
+    GD_TRY_CUDA(c.ids.alloc(n));
+    GD_TRY_CUDA(c.queue.alloc(n));
+    GD_TRY_CUDA(c.group_sorted.alloc(n));
+    GD_TRY_CUDA(c.spatial.alloc(n));
+    Small L = small_layout(m);
+    GD_TRY_CUDA(c.small.alloc(L.total));
+    GD_TRY_CUDA(cudaMemset(c.small.ptr, 0, L.total));
+    GD_TRY_CUDA(cudaMemset(c.error.ptr, 0, sizeof(int) * n));
+    GD_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&c.host_small), L.total));
+    c.state.assign(m.local_groups, BathState());
+    return Status::ok();
+}
+
+void collider_reset_state(Collider &c) {
+    for (auto &s : c.state) s = BathState();
+}
+
+static int chain_grid(const Model &m, size_t smem) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chain, kChainWarps * 32, smem);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
+                          const double *measure, const unsigned char *active, int32_t *spatial_out, double duration,
+                          double total_dust_mass, cudaStream_t s) {
+    const int K = m.n_k;
+    const int G = m.local_groups, S = m.col_bin_s, R = m.raw_bins, W = (G + 31) / 32;
+    const Small L = small_layout(m);
+    int32_t *spatial = c.spatial.ptr;
+    const int TPB = 256;
+    c.stats = gd_operator_stats{};
+    c.stats.min_duration = std::numeric_limits<double>::infinity();
+    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
+        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+
+    GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.events, 0, 8, s));
+    const bool env_on = use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM;
+    if (env_on) k_env_cache<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, reinterpret_cast<Env *>(c.env.ptr));
+
+    // owner lists and the group dependency graph, once per geometry epoch
+    if (!c.local_geometry_valid) {
+        GD_TRY(space_bin(m, part, n, spatial, s));
+        if (spatial_out && spatial_out != spatial)
+            GD_TRY_CUDA(cudaMemcpyAsync(spatial_out, spatial, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.gcount, 0, 4 * G, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.graph, 0, 4 * G * W, s));
+        ++c.launches;
+        k_group_count<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, spatial, at<int>(c.small, L.gcount));
+        ++c.launches;
+        k_dep_graph<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, K, W, at<unsigned int>(c.small, L.graph), spatial, codes, active);
+        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.graph, c.small.ptr + L.graph, L.gcursor - L.graph,
+                                    cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaStreamSynchronize(s));
+        const int *gcount = at<int>(c.host_small, L.gcount);
+        c.group_start.assign(G + 1, 0);
+        for (int g = 0; g < G; ++g) c.group_start[g + 1] = c.group_start[g] + gcount[g];
+        const unsigned int *gr = at<unsigned int>(c.host_small, L.graph);
+        c.edges.assign(gr, gr + G * W);
+        GD_TRY_CUDA(cudaMemcpyAsync(c.small.ptr + L.gcursor, c.group_start.data(), 4 * G, cudaMemcpyHostToDevice, s));
+        ++c.launches;
+        k_group_fill<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, spatial, at<int>(c.small, L.gcursor), c.group_sorted.ptr);
+        GD_TRY_CUDA(cudaGetLastError());
+        c.local_geometry_valid = true;
+    }
+
+    const double lambda0 = n / static_cast<double>(K) / total_dust_mass;
+    const Env *env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
+    const size_t rate_smem = static_cast<size_t>(4) * (4 * 8 + 4) * K;
+    if (rate_smem > 48 * 1024)
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rate_smem)));
+    const size_t chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
+    if (chain_smem > 48 * 1024)
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(chain_smem)));
+
+    int *ids = c.ids.ptr;
+    double *lower = at<double>(c.small, L.lower), *upper = at<double>(c.small, L.upper);
+    double *dt = at<double>(c.small, L.dt);
+    int *binmap = at<int>(c.small, L.binmap);
+    RateBin *ratebin = at<RateBin>(c.small, L.ratebin);
+    AuditBin *audit = at<AuditBin>(c.small, L.audit);
+
+    auto initialize = [&](const int *idp, int count) {
+        ++c.launches;
+        k_bath_init<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, c.size_old.ptr, c.numr_old.ptr, c.time.ptr,
+                                                            c.events.ptr, c.complete.ptr, c.hazard.ptr, c.jump1.ptr,
+                                                            c.jump2.ptr, c.jumpmax.ptr);
+    };
+    // rates, size bins and merged rate bins, then one copy of binmap + rate bins to the host
+    auto rates_and_bins = [&](const int *idp, int count, int &merged) -> Status {
+        ++c.launches;
+        k_size_zero<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
+                                                         at<unsigned long long>(c.small, L.mmax));
+        ++c.launches;
+        k_size_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, spatial, active,
+                                                             at<unsigned long long>(c.small, L.mmin),
+                                                             at<unsigned long long>(c.small, L.mmax));
+        ++c.launches;
+        k_size_bnds<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
+                                                         at<unsigned long long>(c.small, L.mmax), lower, upper);
+        RateArgs ra;
+        ra.ids = idp;
+        ra.count = count;
+        ra.part = part;
+        ra.codes = codes;
+        ra.measure = measure;
+        ra.active = active;
+        ra.size_old = c.size_old.ptr;
+        ra.numr_old = c.numr_old.ptr;
+        ra.env = env;
+        ra.lambda0 = lambda0;
+        ra.rate = c.rate.ptr;
+        ra.change = c.change_rate.ptr;
+        ra.second = c.second_rate.ptr;
+        ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
+        ++c.launches;
+        k_bath_rate<<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, s));
+        ++c.launches;
+        k_count_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, at<int>(c.small, L.counts), part, spatial,
+                                                             active, lower, upper);
+        GD_TRY_CUDA(cudaMemsetAsync(ratebin, 0, sizeof(RateBin) * R, s));
+        ++c.launches;
+        k_binmap<<<1, 1, 0, s>>>(m, at<int>(c.small, L.counts), binmap, at<int>(c.small, L.merged), ratebin);
+        ++c.launches;
+        k_rate_bins<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, ratebin, part, c.rate.ptr, c.change_rate.ptr,
+                                                             c.second_rate.ptr, spatial, binmap, active, lower, upper);
+        GD_TRY_CUDA(cudaGetLastError());
+        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.merged, c.small.ptr + L.merged, 4, cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.binmap, c.small.ptr + L.binmap, L.audit - L.binmap,
+                                    cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaStreamSynchronize(s));
+        merged = *at<int>(c.host_small, L.merged);
+        return Status::ok();
+    };
+    const int *h_binmap = at<int>(c.host_small, L.binmap);
+    const RateBin *h_ratebin = at<RateBin>(c.host_small, L.ratebin);
+    auto bin_end = [&](int g, int merged) { return g + 1 < G ? h_binmap[(g + 1) * S] : merged; };
+    auto requested_step = [&](int g, int merged, double &out) -> Status {
+        int first = h_binmap[g * S];
+        int last = bin_end(g, merged);
+        return choose_bath(m, h_ratebin + first, last - first, duration, c.state[g].limit_scale, out, nullptr);
+    };
+
+    // tick zero: every group starts from the same published reservoir
+    initialize(nullptr, n);
+    int merged = 0;
+    GD_TRY(rates_and_bins(nullptr, n, merged));
+    std::vector<double> requested(G);
+    for (int g = 0; g < G; ++g) GD_TRY(requested_step(g, merged, requested[g]));
+    Schedule sched;
+    GD_TRY(sched.init(duration, requested, c.edges));
+    std::vector<double> steps(G);
+    for (int g = 0; g < G; ++g) steps[g] = sched.seconds(sched.step[g]);
+    std::vector<bool> passed(G, true);
+    std::vector<double> current = requested;
+    const int grid_chain = chain_grid(m, chain_smem);
+
+    while (sched.time() < sched.end) {
+        const std::uint64_t tick = sched.time();
+        std::vector<int> groups = sched.due(tick);
+        WaveTable wt;
+        wt.groups = 0;
+        int count = 0;
+        for (int g : groups) {
+            const int len = c.group_start[g + 1] - c.group_start[g];
+            if (len == 0) continue;
+            wt.start[wt.groups] = c.group_start[g];
+            wt.len[wt.groups] = len;
+            wt.out[wt.groups] = count;
+            wt.groups++;
+            count += len;
+        }
+        if (count == 0) {
+            sched.advance(groups);
+            continue;
+        }
+        ++c.launches;
+        k_wave_ids<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(wt, count, c.group_sorted.ptr, ids);
+        if (tick != 0) {
+            initialize(ids, count);
+            GD_TRY(rates_and_bins(ids, count, merged));
+            for (int g : groups) GD_TRY(requested_step(g, merged, current[g]));
+            GD_TRY(sched.adapt(tick, groups, current, passed));
+            for (int g : groups) steps[g] = sched.seconds(sched.step[g]);
+        }
+        GD_TRY_CUDA(cudaMemcpyAsync(dt, steps.data(), sizeof(double) * G, cudaMemcpyHostToDevice, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, s));  // error_flag, queued, head
+        ChainArgs ca;
+        ca.ids = ids;
+        ca.count = count;
+        ca.rng = rng;
+        ca.active = active;
+        ca.measure = measure;
+        ca.spatial = spatial;
+        ca.dt = dt;
+        ca.cached = reinterpret_cast<const RateMoments *>(c.cached.ptr);
+        ca.time = c.time.ptr;
+        ca.hazard = c.hazard.ptr;
+        ca.jump1 = c.jump1.ptr;
+        ca.jump2 = c.jump2.ptr;
+        ca.jumpmax = c.jumpmax.ptr;
+        ca.events = c.events.ptr;
+        ca.complete = c.complete.ptr;
+        ca.queue = c.queue.ptr;
+        ca.queued = at<int>(c.small, L.queued);
+        ++c.launches;
+        k_skip_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(ca);
+        ChainRun cr;
+        cr.part_ro = part;
+        cr.part = part;
+        cr.codes = codes;
+        cr.size_old = c.size_old.ptr;
+        cr.numr_old = c.numr_old.ptr;
+        cr.env = env;
+        cr.lambda0 = lambda0;
+        cr.error = c.error.ptr;
+        cr.error_flag = at<int>(c.small, L.error_flag);
+        cr.head = at<int>(c.small, L.head);
+        cr.events_total = at<unsigned long long>(c.small, L.events);
+        const int blocks = std::min(grid_chain, (count + kChainWarps - 1) / kChainWarps);
+        ++c.launches;
+        k_chain<<<blocks, kChainWarps * 32, chain_smem, s>>>(m, ca, cr);
+        // audit of the completed baths
+        GD_TRY_CUDA(cudaMemsetAsync(audit, 0, sizeof(AuditBin) * R, s));
+        AuditArgs aa;
+        aa.ids = ids;
+        aa.count = count;
+        aa.bin = audit;
+        aa.part = part;
+        aa.size_old = c.size_old.ptr;
+        aa.numr_old = c.numr_old.ptr;
+        aa.rate = c.rate.ptr;
+        aa.hazard = c.hazard.ptr;
+        aa.jump1 = c.jump1.ptr;
+        aa.jump2 = c.jump2.ptr;
+        aa.jumpmax = c.jumpmax.ptr;
+        aa.events = c.events.ptr;
+        aa.spatial = spatial;
+        aa.binmap = binmap;
+        aa.active = active;
+        aa.dt = dt;
+        aa.lower = lower;
+        aa.upper = upper;
+        ++c.launches;
+        k_audit_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, aa);
+        GD_TRY_CUDA(cudaGetLastError());
+        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small, c.small.ptr, L.binmap, cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.audit, c.small.ptr + L.audit, sizeof(AuditBin) * merged,
+                                    cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaStreamSynchronize(s));
+        const int error_flag = *at<int>(c.host_small, L.error_flag);
+        c.stats.waves++;
+        c.stats.chain_launches++;
+        c.stats.owner_updates += count;
+        c.stats.events = static_cast<long long>(*at<unsigned long long>(c.host_small, L.events));
+        if (error_flag == 7)
+            return err(GD_ERR_CONTINUATION_LIMIT, "local collision continuation limit exceeded", error_flag);
+        if (error_flag) return err(GD_ERR_CHAIN, "local collision chain error " + std::to_string(error_flag), error_flag);
+        const AuditBin *h_audit = at<AuditBin>(c.host_small, L.audit);
+        for (int g : groups) {
+            if (c.group_start[g + 1] == c.group_start[g]) continue;
+            int first = h_binmap[g * S];
+            int last = bin_end(g, merged);
+            double mass = 0.0;
+            for (int b = first; b < last; ++b) {
+                if (h_audit[b].invalid_count) return err(GD_ERR_CONTROLLER, "invalid local audit state");
+                mass += h_audit[b].mass;
+            }
+            if (!(mass > 0)) continue;
+            BathResult res;
+            GD_TRY(finish_bath(m, h_audit + first, last - first, c.state[g], res));
+            passed[g] = !(res.activity_overshoot || res.distribution_overshoot || res.persistent_overshoot);
+        }
+        for (int g : groups) {
+            c.stats.min_duration = std::min(c.stats.min_duration, steps[g]);
+            c.stats.max_duration = std::max(c.stats.max_duration, steps[g]);
+        }
+        sched.advance(groups);
+    }
+    return Status::ok();
+}
+
+}  // namespace gd

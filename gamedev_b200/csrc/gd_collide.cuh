@@ -1,0 +1,98 @@
+// Frozen-bath collision operator state (the reference's local_workspace, _col_chain.cuh:36-96,
+// plus the dev_col_* caches of swarm_runtime.cu:120-184) and its host controller.
+#pragma once
+
+#include <curand_kernel.h>
+
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "gd_internal.cuh"
+
+namespace gd {
+
+// col_rate_bin (inc/swarm/_col_types.cuh:376-384)
+struct RateBin {
+    double mass, weighted_rate, weighted_change, weighted_second;
+    int owner_count, invalid_count;
+};
+
+// col_audit_accum (inc/swarm/_col_types.cuh:386-403)
+struct AuditBin {
+    double mass, predicted_f, predicted_e, predicted_var_f, predicted_var_e, predicted_g, predicted_var_g,
+        maximum_weight, maximum_g_jump, touched, event_weight, growth, end_mass;
+    int owner_count, invalid_count;
+};
+
+// col_bath_state / col_bath_result (inc/swarm/_col_types.cuh:405-425)
+struct BathState {
+    double limit_scale = 1.0;
+    int activity_streak = 0, quiet_streak = 0, floor_streak = 0;
+};
+struct BathResult {
+    double max_f = 0, max_e = 0, max_touched = 0, max_events = 0, max_g = 0, max_g_upper = 0, d_bath = 0;
+    bool activity_overshoot = false, distribution_overshoot = false, persistent_overshoot = false;
+};
+
+// Power-of-two group scheduler on a 2^52-tick lattice (local_schedule, _col_sched.cuh:17-183).
+struct Schedule {
+    double horizon = 0;
+    std::vector<std::pair<int, int>> links;
+    std::vector<int> level;
+    std::vector<std::uint64_t> step, next;
+    std::uint64_t end = 0;
+    Status init(double h, const std::vector<double> &requested, const std::vector<unsigned int> &edges);
+    std::uint64_t time() const;
+    double seconds(std::uint64_t tick) const { return horizon * (double(tick) / double(end)); }
+    std::vector<int> due(std::uint64_t tick) const;
+    Status adapt(std::uint64_t tick, const std::vector<int> &groups, const std::vector<double> &requested,
+                 const std::vector<bool> &passed);
+    void advance(const std::vector<int> &groups) {
+        for (int c : groups) next[c] += step[c];
+    }
+};
+
+// Host controller pieces (inc/swarm/_col_bound.cuh:209-403), usable without a GPU.
+struct ChangeBound {
+    double duration;
+    int reason;
+};
+Status change_limit(double A, double B, double epsilon, double horizon, ChangeBound &out);
+int build_binmap(const Model &m, const std::vector<int> &raw_count, std::vector<int> &raw_to_merged);
+Status choose_bath(const Model &m, const RateBin *bins, int count, double remaining, double limit_scale,
+                   double &out, int *binding);
+Status finish_bath(const Model &m, const AuditBin *bins, int count, BathState &state, BathResult &out);
+
+struct Collider {
+    int n = 0;
+    // per-owner SoA state
+    DevBuf<double> size_old, numr_old, time, hazard, jump1, jump2, jumpmax, rate, change_rate, second_rate;
+    DevBuf<int> events, error;
+    DevBuf<unsigned char> complete;
+    DevBuf<double> env;               // 8 doubles per owner (query_environment)
+    DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
+    DevBuf<int> ids, queue, group_sorted, spatial;
+    // per-group / per-bin device scratch, one contiguous block so one copy returns it
+    DevBuf<unsigned char> small;      // see small_layout() in gd_collide.cu
+    // pinned host mirror of `small`
+    unsigned char *host_small = nullptr;
+    // host controller state
+    std::vector<int> group_start;     // [groups + 1] offsets into group_sorted
+    std::vector<unsigned int> edges;  // dependency rows, LOCAL_WORDS per group
+    std::vector<BathState> state;
+    bool local_geometry_valid = false;
+    gd_operator_stats stats{};
+    long long launches = 0;           // kernels launched by the operator (reported by the ABI)
+    ~Collider();
+};
+
+Status collider_alloc(Collider &c, const Model &m, int n);
+void collider_reset_state(Collider &c);
+
+// evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539)
+Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
+                          const int32_t *codes, const double *measure, const unsigned char *active,
+                          int32_t *spatial, double duration, double total_dust_mass, cudaStream_t s);
+
+}  // namespace gd

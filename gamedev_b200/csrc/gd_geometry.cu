@@ -1,0 +1,572 @@
+// Geometry stage of the swarm collision path on sm_100a:
+//   col_site_init (src/swarm/col_site_init.cu:17-119)  -> k_site_init
+//   index build (kdtree::buildTree, builder.h:109-152 / morton_index::build,
+//                morton_index.cuh:168-229)              -> Morton keys + LSD radix sort + bucket tree
+//   col_cache_get (inc/swarm/_col_cache.cuh:15-159)      -> k_knn_query (exact top-K + measure)
+//   colstate_flag (src/swarm/colstate_flag.cu:13-29)     -> k_state_screen
+//   col_space_bin (src/swarm/col_space_bin.cu:11-35)     -> k_space_bin
+//
+// Design.  Sites are kept as 16-byte float4 records (x, y, z, code bits) so every site read is
+// one 128-bit load.  Active sites are ordered along a 63-bit Morton curve by a hand-written
+// 8-bit-digit LSD radix sort, cut into buckets of 32 consecutive sites, and covered by an
+// implicit complete binary tree of axis-aligned boxes.  A query warp owns one bucket: each lane
+// is one owner, the warp walks the tree once for all 32 owners, and every candidate bucket is
+// staged once in shared memory and read by all 32 lanes, so one 512-byte tile load serves 1024
+// distance tests.  Each lane keeps its exact top-K as a max-heap of packed (d^2 bits, code) keys
+// in shared memory, the same key the reference heap uses (kdtree/index_heap.cuh:59-69), so the
+// kept set is the reference's set; a final in-place heap sort yields ascending (d^2, code), the
+// order of the reference Morton search (morton_types.cuh:68-72).
+#include <cfloat>
+#include <climits>
+#include <cmath>
+
+#include "gd_internal.cuh"
+#include "gd_geom_device.cuh"
+
+namespace gd {
+
+// ------------------------------------------------------------------------------------------------
+// col_site_init (col_site_init.cu:17-55 / 78-118) fused with the Morton key generation
+// (morton_keygen, morton_index.cuh:41-60).  One thread per particle.
+// ------------------------------------------------------------------------------------------------
+__global__ void k_site_init(Model m, int n, const gd_particle *__restrict__ part,
+                            float4 *__restrict__ site, float *__restrict__ qrad,
+                            unsigned char *__restrict__ active, unsigned long long *__restrict__ key,
+                            unsigned int *__restrict__ val, int n_sort, int *__restrict__ counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_sort) return;
+    if (i >= n) {  // sort padding: sorts after every active site
+        key[i] = ~0ull;
+        val[i] = static_cast<unsigned int>(i);
+        return;
+    }
+    const double2 *rec = reinterpret_cast<const double2 *>(part + i);
+    double2 a = rec[0], b = rec[1], c = rec[2], d = rec[3];  // 4 x 128-bit loads of the 64 B record
+    double x = a.x, y = a.y, z = b.x;
+    bool finite = isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y) && isfinite(c.x) &&
+                  isfinite(c.y) && isfinite(d.x) && isfinite(d.y);
+    unsigned long long k = ~0ull;
+    float4 s = make_float4(0.f, 0.f, 0.f, __int_as_float(3 * i));
+    float qi = 0.f;
+    bool act = false;
+    if (!finite) {
+        atomicMin(&counters[1], i);
+    } else {
+        act = site_active(m, y, z);
+        double R = cyl_R(m, y, z);
+        double Z = cyl_Z(m, y, z);
+        float3 p = (m.n_x == 1 && m.n_z == 1)
+                       ? make_float3(static_cast<float>(R), 0.0f, 0.0f)
+                       : make_float3(static_cast<float>(R * cos(x)), static_cast<float>(R * sin(x)),
+                                     static_cast<float>(Z));
+        s.x = p.x;
+        s.y = p.y;
+        s.z = p.z;
+        if (act) {
+            qi = static_cast<float>(m.h_search * get_hg(m, R) * R);
+            k = morton_key(m, p);
+        }
+    }
+    site[i] = s;
+    qrad[i] = qi;
+    active[i] = act ? 1 : 0;
+    key[i] = k;
+    val[i] = static_cast<unsigned int>(i);
+    // count active sites with one atomic per warp
+    unsigned int ballot = __ballot_sync(__activemask(), act);
+    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot) atomicAdd(&counters[0], __popc(ballot));
+}
+
+// colstate_flag (colstate_flag.cu:13-29): non-finite screen when the geometry is reused.
+__global__ void k_state_screen(int n, const gd_particle *__restrict__ part, int *__restrict__ counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 *rec = reinterpret_cast<const double2 *>(part + i);
+    double2 a = rec[0], b = rec[1], c = rec[2], d = rec[3];
+    bool finite = isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y) && isfinite(c.x) &&
+                  isfinite(c.y) && isfinite(d.x) && isfinite(d.y);
+    if (!finite) atomicMin(&counters[1], i);
+}
+
+// ------------------------------------------------------------------------------------------------
+// LSD radix sort of (u64 key, u32 value), 8-bit digits, stable.  Three kernels per digit:
+// per-tile digit histogram, one exclusive scan over [digit][tile], stable scatter.
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const unsigned long long *__restrict__ key,
+                                                              int shift, int tiles,
+                                                              unsigned int *__restrict__ hist) {
+    __shared__ unsigned int h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const unsigned long long *tk = key + static_cast<size_t>(blockIdx.x) * kRadixTile;
+#pragma unroll
+    for (int it = 0; it < kRadixItems; ++it) {
+        unsigned int dg = static_cast<unsigned int>(tk[it * kRadixThreads + threadIdx.x] >> shift) & 255u;
+        atomicAdd(&h[dg], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of cnt[0..len) in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_exclusive(unsigned int *__restrict__ cnt, int len) {
+    __shared__ unsigned int part[1024];
+    int chunk = (len + 1023) / 1024;
+    int b = threadIdx.x * chunk;
+    int e = min(len, b + chunk);
+    unsigned int sum = 0;
+    for (int i = b; i < e; ++i) sum += cnt[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        unsigned int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned int run = part[threadIdx.x] - sum;
+    for (int i = b; i < e; ++i) {
+        unsigned int v = cnt[i];
+        cnt[i] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(kRadixThreads)
+    k_radix_scatter(const unsigned long long *__restrict__ kin, const unsigned int *__restrict__ vin,
+                    unsigned long long *__restrict__ kout, unsigned int *__restrict__ vout, int shift,
+                    int tiles, const unsigned int *__restrict__ offs) {
+    constexpr int kWarps = kRadixThreads / 32;
+    __shared__ unsigned int wcnt[kWarps][256];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = threadIdx.x; j < kWarps * 256; j += kRadixThreads) (&wcnt[0][0])[j] = 0;
+    __syncthreads();
+    // warp w ranks tile elements [w*512, w*512+512) in 16 rounds of 32: element order inside the
+    // tile is (warp, round, lane), so the ranks are stable.
+    size_t base = static_cast<size_t>(blockIdx.x) * kRadixTile + warp * (kRadixItems * 32);
+    unsigned long long k[kRadixItems];
+    unsigned int rank[kRadixItems];
+    unsigned int lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kRadixItems; ++r) {
+        k[r] = kin[base + r * 32 + lane];
+        unsigned int dg = static_cast<unsigned int>(k[r] >> shift) & 255u;
+        unsigned int peers = __match_any_sync(0xffffffffu, dg);
+        unsigned int before = wcnt[warp][dg];
+        __syncwarp();
+        rank[r] = before + __popc(peers & lt);
+        if ((peers & lt) == 0) wcnt[warp][dg] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive prefix over warps for every digit, plus the tile's global digit offset
+    {
+        int dg = threadIdx.x;  // kRadixThreads == 256
+        unsigned int run = offs[dg * tiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            unsigned int c = wcnt[w][dg];
+            wcnt[w][dg] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRadixItems; ++r) {
+        unsigned int dg = static_cast<unsigned int>(k[r] >> shift) & 255u;
+        unsigned int dst = wcnt[warp][dg] + rank[r];
+        kout[dst] = k[r];
+        vout[dst] = vin[base + r * 32 + lane];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Bucket tree: gather Morton-ordered sites, leaf boxes, then internal boxes level by level.
+// ------------------------------------------------------------------------------------------------
+__global__ void k_gather_sorted(int n_slots, const int *__restrict__ counters, const unsigned int *__restrict__ val,
+                                const float4 *__restrict__ site, float4 *__restrict__ sorted) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_slots) return;
+    int n_act = counters[0];
+    int n_pad = (n_act + kLeaf - 1) / kLeaf * kLeaf;
+    if (i >= n_pad) return;
+    float4 s;
+    if (i < n_act) {
+        s = site[val[i]];
+    } else {
+        s = make_float4(CUDART_INF_F_, CUDART_INF_F_, CUDART_INF_F_, __int_as_float(-1));
+    }
+    sorted[i] = s;
+}
+
+// one warp per leaf slot
+__global__ void k_leaf_bounds(int leaf_slots, const int *__restrict__ counters, const float4 *__restrict__ sorted,
+                              float4 *__restrict__ lo, float4 *__restrict__ hi) {
+    int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (leaf >= leaf_slots) return;
+    int n_act = counters[0];
+    int i = leaf * kLeaf + lane;
+    float3 a = make_float3(CUDART_INF_F_, CUDART_INF_F_, CUDART_INF_F_);
+    float3 b = make_float3(-CUDART_INF_F_, -CUDART_INF_F_, -CUDART_INF_F_);
+    if (i < n_act) {
+        float4 s = sorted[i];
+        a = make_float3(s.x, s.y, s.z);
+        b = a;
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        a.x = fminf(a.x, __shfl_xor_sync(0xffffffffu, a.x, off));
+        a.y = fminf(a.y, __shfl_xor_sync(0xffffffffu, a.y, off));
+        a.z = fminf(a.z, __shfl_xor_sync(0xffffffffu, a.z, off));
+        b.x = fmaxf(b.x, __shfl_xor_sync(0xffffffffu, b.x, off));
+        b.y = fmaxf(b.y, __shfl_xor_sync(0xffffffffu, b.y, off));
+        b.z = fmaxf(b.z, __shfl_xor_sync(0xffffffffu, b.z, off));
+    }
+    if (lane == 0) {
+        int node = leaf_slots - 1 + leaf;
+        lo[node] = make_float4(a.x, a.y, a.z, 0.f);
+        hi[node] = make_float4(b.x, b.y, b.z, 0.f);
+    }
+}
+
+// internal nodes [first, first+count) from their two children
+__global__ void k_tree_level(int first, int count, float4 *__restrict__ lo, float4 *__restrict__ hi) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    int node = first + t;
+    float4 l0 = lo[2 * node + 1], l1 = lo[2 * node + 2];
+    float4 h0 = hi[2 * node + 1], h1 = hi[2 * node + 2];
+    lo[node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+    hi[node] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Exact top-K query.  One warp per bucket of 32 Morton-ordered active owners.
+// ------------------------------------------------------------------------------------------------
+struct QueryArgs {
+    const float4 *sorted;
+    const float4 *lo;
+    const float4 *hi;
+    const float *qrad;      // by particle index
+    const int *counters;
+    const gd_particle *part;
+    int leaf_slots;
+    int k;
+    int32_t *codes;         // may be null
+    double *measure;        // may be null
+    float *kth;             // may be null
+};
+
+__device__ __forceinline__ void heap_sift(unsigned long long *h, int lane, unsigned long long key, int slot, int n) {
+    while (true) {
+        int child = 2 * slot + 1;
+        if (child >= n) break;
+        unsigned long long cv = h[child * 32 + lane];
+        if (child + 1 < n) {
+            unsigned long long rv = h[(child + 1) * 32 + lane];
+            if (rv > cv) {
+                cv = rv;
+                ++child;
+            }
+        }
+        if (cv < key) break;
+        h[slot * 32 + lane] = cv;
+        slot = child;
+    }
+    h[slot * 32 + lane] = key;
+}
+
+__global__ void k_knn_query(Model m, QueryArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int K = a.k;
+    const size_t per_warp = static_cast<size_t>(K) * 32 * 8 + 32 * 16 + 64 * 4;
+    unsigned char *wbase = smem + wib * per_warp;
+    unsigned long long *heap = reinterpret_cast<unsigned long long *>(wbase);
+    float4 *tile = reinterpret_cast<float4 *>(wbase + static_cast<size_t>(K) * 32 * 8);
+    int *stack = reinterpret_cast<int *>(wbase + static_cast<size_t>(K) * 32 * 8 + 32 * 16);
+
+    const int n_act = a.counters[0];
+    const int n_leaves = (n_act + kLeaf - 1) / kLeaf;
+    const int leaf = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (leaf >= n_leaves) return;
+
+    const int i = leaf * kLeaf + lane;
+    const bool valid = i < n_act;
+    const float4 me = a.sorted[i];
+    const float3 qp = make_float3(me.x, me.y, me.z);
+    const int code = __float_as_int(me.w);
+    const int idx = valid ? code / 3 : 0;
+    const float qr = valid ? a.qrad[idx] : 0.f;
+    // heap sentinel (q^2, 0xffffffff): every eligible candidate (d^2 <= q^2) sorts before it
+    // (kdtree/index_heap.cuh:58-61)
+    const float q2 = qr * qr;
+    const unsigned long long sentinel = (static_cast<unsigned long long>(__float_as_uint(q2)) << 32) | 0xffffffffull;
+    for (int s = 0; s < K; ++s) heap[s * 32 + lane] = sentinel;
+    float cut = valid ? q2 : -1.0f;
+
+    // warp centre (own bucket box) orders child visits
+    const int own_node = a.leaf_slots - 1 + leaf;
+    const float4 own_lo = a.lo[own_node], own_hi = a.hi[own_node];
+    const float3 ctr = make_float3(0.5f * (own_lo.x + own_hi.x), 0.5f * (own_lo.y + own_hi.y), 0.5f * (own_lo.z + own_hi.z));
+
+    auto scan_leaf = [&](int lf) {
+        const int base = lf * kLeaf;
+        tile[lane] = a.sorted[base + lane];
+        __syncwarp();
+        const int cnt = min(kLeaf, n_act - base);
+        for (int c = 0; c < cnt; ++c) {
+            const float4 p = tile[c];
+            const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
+            if (d2 <= cut) {
+                const unsigned long long cand =
+                    (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned int>(__float_as_int(p.w));
+                if (cand < heap[lane]) {
+                    heap_sift(heap, lane, cand, 0, K);
+                    cut = __uint_as_float(static_cast<unsigned int>(heap[lane] >> 32));
+                }
+            }
+        }
+        __syncwarp();
+    };
+
+    // own bucket first: it holds the nearest sites, so the heaps tighten before the walk
+    scan_leaf(leaf);
+
+    int sp = 0;
+    stack[0] = 0;
+    sp = 1;
+    while (sp > 0) {
+        const int node = stack[--sp];
+        const float4 nl = a.lo[node], nh = a.hi[node];
+        const float bd = box_dist2(qp, nl, nh);
+        if (!__any_sync(0xffffffffu, bd <= cut)) continue;
+        if (node >= a.leaf_slots - 1) {
+            const int lf = node - (a.leaf_slots - 1);
+            if (lf != leaf) scan_leaf(lf);
+            continue;
+        }
+        const int c0 = 2 * node + 1, c1 = 2 * node + 2;
+        const float4 l0 = a.lo[c0], h0 = a.hi[c0], l1 = a.lo[c1], h1 = a.hi[c1];
+        const bool need0 = __any_sync(0xffffffffu, box_dist2(qp, l0, h0) <= cut);
+        const bool need1 = __any_sync(0xffffffffu, box_dist2(qp, l1, h1) <= cut);
+        const float e0 = box_dist2(ctr, l0, h0), e1 = box_dist2(ctr, l1, h1);
+        const int nearc = (e0 <= e1) ? c0 : c1, farc = (e0 <= e1) ? c1 : c0;
+        const bool need_near = (e0 <= e1) ? need0 : need1, need_far = (e0 <= e1) ? need1 : need0;
+        // stack depth is bounded by the tree depth (<= 31 levels) + 1: well inside 64 entries
+        if (need_far) stack[sp++] = farc;
+        if (need_near) stack[sp++] = nearc;
+        __syncwarp();
+    }
+
+    // in-place heap sort: ascending (d^2 bits, code)
+    for (int end = K - 1; end > 0; --end) {
+        const unsigned long long top = heap[lane];
+        const unsigned long long last = heap[end * 32 + lane];
+        heap[end * 32 + lane] = top;
+        heap_sift(heap, lane, last, 0, end);
+    }
+    if (!valid) return;
+
+    float maxd2 = 0.f;
+    int32_t *row = a.codes ? a.codes + static_cast<size_t>(idx) * K : nullptr;
+    if ((K & 3) == 0 && row) {
+        for (int s = 0; s < K; s += 4) {
+            int4 v;
+            int *vp = &v.x;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const unsigned long long kk = heap[(s + t) * 32 + lane];
+                const unsigned int cc = static_cast<unsigned int>(kk);
+                if (cc != 0xffffffffu) maxd2 = __uint_as_float(static_cast<unsigned int>(kk >> 32));
+                vp[t] = (cc == 0xffffffffu) ? -1 : static_cast<int>(cc);
+            }
+            reinterpret_cast<int4 *>(row)[s >> 2] = v;
+        }
+    } else {
+        for (int s = 0; s < K; ++s) {
+            const unsigned long long kk = heap[s * 32 + lane];
+            const unsigned int cc = static_cast<unsigned int>(kk);
+            if (cc != 0xffffffffu) maxd2 = __uint_as_float(static_cast<unsigned int>(kk >> 32));
+            if (row) row[s] = (cc == 0xffffffffu) ? -1 : static_cast<int>(cc);
+        }
+    }
+    if (a.kth) a.kth[idx] = maxd2;
+    if (a.measure) {
+        const double y = a.part[idx].position[1];
+        const double z = a.part[idx].position[2];
+        a.measure[idx] = ball_measure(m, y, z, sqrt(static_cast<double>(maxd2)));
+    }
+}
+
+// inactive owners: a row of -1 and zero measure (_col_cache.cuh:26-34)
+__global__ void k_inactive_rows(int n, int K, const unsigned char *__restrict__ active, int32_t *__restrict__ codes,
+                                double *__restrict__ measure, float *__restrict__ kth) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || active[i]) return;
+    if (codes)
+        for (int s = 0; s < K; ++s) codes[static_cast<size_t>(i) * K + s] = -1;
+    if (measure) measure[i] = 0.0;
+    if (kth) kth[i] = 0.f;
+}
+
+// col_space_bin (col_space_bin.cu:11-35)
+__global__ void k_space_bin(Model m, int n, const gd_particle *__restrict__ part, int32_t *__restrict__ spatial) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x = part[i].position[0], y = part[i].position[1], z = part[i].position[2];
+    int bx = 0, bz = 0;
+    int by = static_cast<int>(floor((y - m.y_min) / (m.y_max - m.y_min) * m.col_bin_y));
+    if (m.n_x > 1) bx = static_cast<int>(floor((x - m.x_min) / (m.x_max - m.x_min) * m.col_bin_x));
+    if (m.n_z > 1) bz = static_cast<int>(floor((z - m.z_min) / (m.z_max - m.z_min) * m.col_bin_z));
+    bx = bx < 0 ? 0 : (bx >= m.col_bin_x ? m.col_bin_x - 1 : bx);
+    by = by < 0 ? 0 : (by >= m.col_bin_y ? m.col_bin_y - 1 : by);
+    bz = bz < 0 ? 0 : (bz >= m.col_bin_z ? m.col_bin_z - 1 : bz);
+    int cx = (m.n_x > 1) ? m.col_bin_x : 1;
+    spatial[i] = bx + cx * (by + m.col_bin_y * bz);
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+static int next_pow2(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+Status geometry_alloc(Geometry &g, const Model &m, int n) {
+    g.n = n;
+    g.n_sort = (n + kRadixTile - 1) / kRadixTile * kRadixTile;
+    int leaves = (n + kLeaf - 1) / kLeaf;
+    g.leaf_slots = next_pow2(leaves < 1 ? 1 : leaves);
+    g.key_bits = 21 * m.dim;
+    int tiles = g.n_sort / kRadixTile;
+    GD_TRY_CUDA(g.site.alloc(n));
+    GD_TRY_CUDA(g.q.alloc(n));
+    GD_TRY_CUDA(g.active.alloc(n));
+    GD_TRY_CUDA(g.key_a.alloc(g.n_sort));
+    GD_TRY_CUDA(g.key_b.alloc(g.n_sort));
+    GD_TRY_CUDA(g.val_a.alloc(g.n_sort));
+    GD_TRY_CUDA(g.val_b.alloc(g.n_sort));
+    GD_TRY_CUDA(g.hist.alloc(static_cast<size_t>(256) * tiles));
+    GD_TRY_CUDA(g.sorted.alloc(static_cast<size_t>(g.leaf_slots) * kLeaf));
+    GD_TRY_CUDA(g.node_lo.alloc(2 * static_cast<size_t>(g.leaf_slots)));
+    GD_TRY_CUDA(g.node_hi.alloc(2 * static_cast<size_t>(g.leaf_slots)));
+    GD_TRY_CUDA(g.counters.alloc(4));
+    return Status::ok();
+}
+
+static Status read_counters(Geometry &g, cudaStream_t s, int out[2]) {
+    GD_TRY_CUDA(cudaMemcpyAsync(out, g.counters.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    return Status::ok();
+}
+
+Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
+    const int n = g.n;
+    int init[4] = {0, INT_MAX, 0, 0};
+    GD_TRY_CUDA(cudaMemcpyAsync(g.counters.ptr, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    g.launches += 1;
+    k_site_init<<<(g.n_sort + 255) / 256, 256, 0, s>>>(m, n, dev_particle, g.site.ptr, g.q.ptr, g.active.ptr,
+                                                        g.key_a.ptr, g.val_a.ptr, g.n_sort, g.counters.ptr);
+    GD_TRY_CUDA(cudaGetLastError());
+    // the reference stops on the first non-finite particle before building (swarm_runtime.cu:382-393)
+    int cnt[2];
+    GD_TRY(read_counters(g, s, cnt));
+    if (cnt[1] != INT_MAX) {
+        Status st;
+        st.code = GD_ERR_NONFINITE;
+        st.detail = cnt[1];
+        st.msg = "non-finite particle state before collision search at particle " + std::to_string(cnt[1]);
+        return st;
+    }
+    // radix sort over the bits that carry key information (inactive keys are all ones)
+    const int tiles = g.n_sort / kRadixTile;
+    const int passes = (g.key_bits + 7) / 8;
+    unsigned long long *kin = g.key_a.ptr, *kout = g.key_b.ptr;
+    unsigned int *vin = g.val_a.ptr, *vout = g.val_b.ptr;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        g.launches += 3;
+        k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, shift, tiles, g.hist.ptr);
+        k_scan_exclusive<<<1, 1024, 0, s>>>(g.hist.ptr, 256 * tiles);
+        k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, kout, vout, shift, tiles, g.hist.ptr);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    GD_TRY_CUDA(cudaGetLastError());
+    g.sorted_val = vin;
+    const int slots = g.leaf_slots * kLeaf;
+    g.launches += 2;
+    k_gather_sorted<<<(slots + 255) / 256, 256, 0, s>>>(slots, g.counters.ptr, vin, g.site.ptr, g.sorted.ptr);
+    k_leaf_bounds<<<(g.leaf_slots * 32 + 255) / 256, 256, 0, s>>>(g.leaf_slots, g.counters.ptr, g.sorted.ptr,
+                                                                  g.node_lo.ptr, g.node_hi.ptr);
+    for (int count = g.leaf_slots / 2; count >= 1; count /= 2) {
+        const int first = count - 1;
+        g.launches += 1;
+        k_tree_level<<<(count + 255) / 256, 256, 0, s>>>(first, count, g.node_lo.ptr, g.node_hi.ptr);
+    }
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
+size_t knn_smem_per_warp(int K) { return static_cast<size_t>(K) * 32 * 8 + 32 * 16 + 64 * 4; }
+
+Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
+                 float *kth_d2, cudaStream_t s) {
+    const int K = m.n_k;
+    const size_t per_warp = knn_smem_per_warp(K);
+    int warps = static_cast<int>((96 * 1024) / per_warp);
+    warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
+    const size_t smem = per_warp * warps;
+    GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    QueryArgs qa;
+    qa.sorted = g.sorted.ptr;
+    qa.lo = g.node_lo.ptr;
+    qa.hi = g.node_hi.ptr;
+    qa.qrad = g.q.ptr;
+    qa.counters = g.counters.ptr;
+    qa.part = dev_particle;
+    qa.leaf_slots = g.leaf_slots;
+    qa.k = K;
+    qa.codes = codes;
+    qa.measure = measure;
+    qa.kth = kth_d2;
+    const int max_leaves = (g.n + kLeaf - 1) / kLeaf;
+    const int blocks = (max_leaves + warps - 1) / warps;
+    g.launches += 2;
+    k_knn_query<<<blocks, warps * 32, smem, s>>>(m, qa);
+    k_inactive_rows<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, K, g.active.ptr, codes, measure, kth_d2);
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
+Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
+    (void)m;
+    int init[2] = {0, INT_MAX};
+    GD_TRY_CUDA(cudaMemcpyAsync(g.counters.ptr, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    g.launches += 1;
+    k_state_screen<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, dev_particle, g.counters.ptr);
+    GD_TRY_CUDA(cudaGetLastError());
+    int cnt[2];
+    GD_TRY(read_counters(g, s, cnt));
+    if (cnt[1] != INT_MAX) {
+        Status st;
+        st.code = GD_ERR_NONFINITE;
+        st.detail = cnt[1];
+        st.msg = "non-finite particle state before collision search at particle " + std::to_string(cnt[1]);
+        return st;
+    }
+    return Status::ok();
+}
+
+Status space_bin(const Model &m, const gd_particle *dev_particle, int n, int32_t *spatial, cudaStream_t s) {
+    k_space_bin<<<(n + 255) / 256, 256, 0, s>>>(m, n, dev_particle, spatial);
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
+}  // namespace gd

@@ -1,0 +1,134 @@
+// Internal declarations shared by the translation units of libgd_b200.
+//
+// Layout in HBM (one handle, n_p particles, K = n_k):
+//   caller-owned  : gd_particle[n_p] (64 B AoS, the reference `struct swarm`), curandState[n_p]
+//   geometry      : site[n_p] float4 (x, y, z, code bits), q[n_p] float search radius,
+//                   active[n_p] u8, key/val ping-pong [n_sort] u64/u32 (radix sort),
+//                   sorted[n_pad] float4 (Morton order, w = code), node lo/hi [2*leaf_slots] float4
+//   neighbour cache: codes[n_p*K] int32 owner-major, measure[n_p] f64, kth_d2[n_p] f32
+//   controller    : SoA owner state f64 (size_old, numr_old, time, hazard, jump1/2/max, rates),
+//                   query_environment[n_p] (8 x f64), group/bin scratch
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/gd_b200.h"
+
+namespace gd {
+
+// Leaf width of the bucket tree: one Morton-ordered bucket of 32 sites is one warp's query tile
+// and one candidate tile.
+constexpr int kLeaf = 32;
+constexpr int kMaxK = 256;
+constexpr int kRadixThreads = 256;
+constexpr int kRadixItems = 16;
+constexpr int kRadixTile = kRadixThreads * kRadixItems;  // 4096 keys per sort tile
+
+// Device copy of the model constants, passed by value to kernels.
+struct Model {
+    double G, M_S, R_0, S_0;
+    int n_x, n_y, n_z;
+    double x_min, x_max, y_min, y_max, z_min, z_max;
+    double sigma_0, aspr_0, idx_p, idx_q;
+    int const_nu;
+    double nu, alpha;
+    int code_unit;
+    double reynolds_0, m_mol, x_sec;
+    int half_disk, const_st;
+    double stokes_0, rho_0;
+    int coag_kernel, n_k;
+    double h_search, v_frag;
+    int col_event_cap, col_bin_x, col_bin_y, col_bin_z, col_bin_s, col_bin_min;
+    double col_bath_max, col_bath_eps, col_bath_alpha;
+    double init_smin, init_smax;
+    // derived
+    int dim;          // 2 when the polar direction is collapsed, else 3
+    int local_groups; // spatial controller groups (_col_types.cuh:463)
+    int raw_bins;     // local_groups * col_bin_s (_col_bound.cuh:223-229)
+};
+
+Model make_model(const gd_config &c);
+
+// Status carried out of a call: code, message, numeric detail.
+struct Status {
+    gd_status code = GD_OK;
+    std::string msg;
+    long long detail = 0;
+    static Status ok() { return {}; }
+    explicit operator bool() const { return code == GD_OK; }
+};
+
+Status cuda_status(cudaError_t e, const char *what);
+
+#define GD_TRY_CUDA(expr)                                              \
+    do {                                                               \
+        cudaError_t gd_e_ = (expr);                                    \
+        if (gd_e_ != cudaSuccess) return ::gd::cuda_status(gd_e_, #expr); \
+    } while (0)
+
+#define GD_TRY(expr)                   \
+    do {                               \
+        ::gd::Status gd_s_ = (expr);   \
+        if (!gd_s_) return gd_s_;      \
+    } while (0)
+
+// Owned device allocation.
+template <typename T>
+struct DevBuf {
+    T *ptr = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(reinterpret_cast<void **>(&ptr), sizeof(T) * count);
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+};
+
+// Geometry (index) state of one swarm.
+struct Geometry {
+    int n = 0;              // particles
+    int n_sort = 0;         // n rounded up to the sort tile
+    int leaf_slots = 0;     // power of two >= ceil(n / kLeaf)
+    int key_bits = 0;       // Morton bits sorted (3*21 or 2*21)
+    DevBuf<float4> site;    // by particle index
+    DevBuf<float> q;        // search radius by particle index
+    DevBuf<unsigned char> active;
+    DevBuf<unsigned long long> key_a, key_b;
+    DevBuf<unsigned int> val_a, val_b;
+    DevBuf<unsigned int> hist;    // [256][tiles]
+    DevBuf<float4> sorted;        // [leaf_slots*kLeaf] Morton-ordered sites, w = code bits
+    DevBuf<float4> node_lo, node_hi;  // implicit tree, 2*leaf_slots-1 nodes
+    DevBuf<int> counters;         // [0] active count, [1] first bad index (INT_MAX if none)
+    unsigned int *sorted_val = nullptr;  // points into val_a or val_b after the sort
+    long long launches = 0;              // kernels launched by this geometry (reported by the ABI)
+};
+
+Status geometry_alloc(Geometry &g, const Model &m, int n);
+// col_site_init + Morton keys + radix sort + bucket tree.  Returns GD_ERR_NONFINITE with the
+// smallest bad index when a particle is non-finite.
+Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
+// Exact top-K over the bucket tree.  Writes codes/measure/kth (any may be null).
+Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
+                 double *measure, float *kth_d2, cudaStream_t s);
+// colstate_flag: non-finite screen only.
+Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
+// col_space_bin
+Status space_bin(const Model &m, const gd_particle *dev_particle, int n, int32_t *spatial,
+                 cudaStream_t s);
+
+}  // namespace gd

@@ -1,0 +1,164 @@
+"""Host-side mirror of the reference's swarm collision interface over the C ABI.
+
+The names follow the reference's operator surface (src/swarm/swarm_runtime.cu:331-471,
+inc/swarm/_col_chain.cuh:108): ``col_site_init`` + index build, ``col_cache_get``,
+``evolve_local_collisions``, ``evolve_collisions``, ``invalidate_col_geometry`` and
+``rngstate_init``.  Device memory comes from torch (plumbing only); every computation runs in
+libgd_b200.so.  Errors raise :class:`GdError` carrying the reference's error meaning.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import GdConfig, GdError, GdOperatorStats
+
+# gd_particle / reference `struct swarm` with MULTISIZE: 8 doubles
+PARTICLE_FIELDS = ["x", "y", "z", "lx", "vy", "lz", "par_size", "par_numr"]
+PARTICLE_DTYPE = np.dtype([(f, "<f8") for f in PARTICLE_FIELDS])
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def _stream():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class SwarmCollision:
+    """One swarm of n_p representative particles bound to a libgd_b200 handle."""
+
+    def __init__(self, cfg: GdConfig, n_p: int):
+        self.lib = _lib.load()
+        self.cfg = cfg
+        self.n_p = int(n_p)
+        self.n_k = int(cfg.n_k)
+        h = C.c_void_p()
+        st = self.lib.gd_create(C.byref(cfg), self.n_p, C.byref(h))
+        if st != _lib.GD_OK:
+            raise GdError(st, "gd_create failed", 0)
+        self.h = h
+        self.lib.gd_set_stream(self.h, _stream())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != _lib.GD_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.gd_last_error(self.h, buf, 512)
+            raise GdError(st, buf.value.decode(), int(self.lib.gd_error_detail(self.h)))
+
+    # ---- geometry stage -------------------------------------------------------------------
+    def col_site_init(self, particles):
+        """col_site_init + index build (swarm_runtime.cu:376-409)."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_geometry_build(self.h, C.c_void_p(_ptr(particles))))
+
+    def col_cache_get(self, particles, codes=None, measure=None, kth_d2=None):
+        """col_cache_get (_col_cache.cuh:15-159): fills codes [n_p, n_k] int32, measure [n_p] f64."""
+        self._check(self.lib.gd_knn(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(codes)),
+                                    C.c_void_p(_ptr(measure)), C.c_void_p(_ptr(kth_d2))))
+
+    def knn(self, particles):
+        """Geometry + exact top-K into fresh torch tensors: (codes, measure, kth_d2)."""
+        torch = _torch()
+        dev = particles.device
+        codes = torch.empty((self.n_p, self.n_k), dtype=torch.int32, device=dev)
+        measure = torch.empty(self.n_p, dtype=torch.float64, device=dev)
+        kth = torch.empty(self.n_p, dtype=torch.float32, device=dev)
+        self.col_site_init(particles)
+        self.col_cache_get(particles, codes, measure, kth)
+        return codes, measure, kth
+
+    def build_cache(self, particles):
+        """Geometry + top-K into the handle's own cache (used by the collision operator)."""
+        self.col_site_init(particles)
+        self.col_cache_get(particles)
+
+    def get_sites(self):
+        """Site-init outputs of the last geometry build: (site4 float32 [n,4], q [n], active [n])."""
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        site4 = torch.empty((self.n_p, 4), dtype=torch.float32, device=dev)
+        q = torch.empty(self.n_p, dtype=torch.float32, device=dev)
+        active = torch.empty(self.n_p, dtype=torch.uint8, device=dev)
+        self._check(self.lib.gd_get_sites(self.h, C.c_void_p(site4.data_ptr()), C.c_void_p(q.data_ptr()),
+                                          C.c_void_p(active.data_ptr())))
+        return site4, q, active
+
+    def get_cache(self, codes, measure):
+        self._check(self.lib.gd_get_cache(self.h, C.c_void_p(_ptr(codes)), C.c_void_p(_ptr(measure))))
+
+    def set_cache(self, codes, measure):
+        self._check(self.lib.gd_set_cache(self.h, C.c_void_p(_ptr(codes)), C.c_void_p(_ptr(measure))))
+
+    def col_space_bin(self, particles, spatial):
+        self._check(self.lib.gd_space_bin(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(spatial))))
+
+    def invalidate_col_geometry(self):
+        self._check(self.lib.gd_invalidate_geometry(self.h))
+
+    def reset_controller(self):
+        self._check(self.lib.gd_reset_controller(self.h))
+
+    # ---- collision operator ---------------------------------------------------------------
+    def evolve_local_collisions(self, particles, rng, duration: float, total_dust_mass: float):
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_collision_operator(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
+                                                   float(duration), float(total_dust_mass)))
+
+    def evolve_collisions(self, particles, rng, duration: float, total_dust_mass: float):
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_evolve_collisions(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
+                                                  float(duration), float(total_dust_mass)))
+
+    def launch_count(self) -> int:
+        return int(self.lib.gd_launch_count(self.h))
+
+    def last_operator_stats(self) -> dict:
+        s = GdOperatorStats()
+        self._check(self.lib.gd_last_operator_stats(self.h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+
+def rng_state_bytes() -> int:
+    return int(_lib.load().gd_rng_state_bytes())
+
+
+def rngstate_init(n: int, seed: int = 1, device="cuda:0"):
+    """rngstate_init (src/swarm/rngstate_init.cu:11-18): curand_init(seed, i, 0) per particle."""
+    torch = _torch()
+    st = torch.empty(n * rng_state_bytes(), dtype=torch.uint8, device=device)
+    r = _lib.load().gd_rng_init(C.c_void_p(st.data_ptr()), int(n), C.c_ulonglong(seed), _stream())
+    if r != _lib.GD_OK:
+        raise GdError(r, "gd_rng_init failed", 0)
+    return st
+
+
+def particles_to_device(arr: np.ndarray, device="cuda:0"):
+    """Structured or (n, 8) float64 host array -> contiguous (n, 8) float64 device tensor."""
+    torch = _torch()
+    a = np.ascontiguousarray(arr).view(np.float64).reshape(-1, 8)
+    return torch.from_numpy(a.copy()).to(device)

@@ -1,0 +1,138 @@
+"""Model constants and seeded synthetic swarms for the benchmark configurations.
+
+The reference fixes every constant at compile time in a model's const_defs.cuh and draws its
+initial swarm with host samplers (inc/swarm/swarm_host.cuh:51-737).  This module gives each
+benchmark configuration its gd_config (the same constants a model directory would hold) and a
+deterministic particle array in the reference record layout (position = azimuth, spherical radius,
+polar angle; velocity = l_phi, v_r, l_theta; grain diameter; grain count).
+
+Units are cgs: G in cm^3 g^-1 s^-2, the star in grams, R_0 = 1 au, grain sizes are DIAMETERS in
+cm (the reference's par_size, const_defs.cuh:200), times in s.  The gas disk is
+Sigma = Sigma_0 (R/au)^-1 carrying 100x the dust mass on [1, 100] au, h = 0.05 (R/au)^0.25, so
+IDX_P = -1, IDX_Q = -0.5, ASPR_0 = 0.05; STOKES_0 is the Epstein midplane Stokes number of a 1 cm
+grain at 1 au.
+
+Config names:
+  c0_plain_small   3D, N = 65,536, K = 32, KD search, monodisperse radius 1e-4 cm, coagulation only
+  c1_multisize_2d  radial-azimuthal, N = 2^20, K = 64, Morton search, gap at 9-11 au, ring at 30 au,
+                   radii log-uniform on [1e-4, 10] cm, fragmentation above 1 m/s
+  c3_learned_3d    3D, N = 10^7, K = 64, c0 positions, radii log-uniform on [1e-4, 10] cm
+  c4_production_3d as c3 (its collision operator; transport, diffusion and radiation are not in
+                   this build)
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ._lib import GD_KERNEL_CUSTOM, GD_SEARCH_KDTREE, GD_SEARCH_MORTON, default_config
+
+AU = 1.495978707e13
+MSUN = 1.98847e33
+G_CGS = 6.6743e-8
+R_IN_AU, R_OUT_AU = 1.0, 100.0
+DUST_MASS = 1.0e-4 * MSUN
+GAS_TO_DUST = 100.0
+
+
+def orbital_time() -> float:
+    """1 / Omega_K at R_0 = 1 au, the time unit the reference's code-unit constants assume."""
+    return math.sqrt(AU ** 3 / (G_CGS * MSUN))
+
+
+def _base_config(n_k: int, three_d: bool, search: int, v_frag: float, smin: float, smax: float):
+    cfg = default_config()
+    cfg.G, cfg.M_S, cfg.R_0, cfg.S_0 = G_CGS, MSUN, AU, 1.0
+    cfg.n_x, cfg.n_y = 64, 64
+    cfg.n_z = 32 if three_d else 1
+    cfg.x_min, cfg.x_max = -math.pi, math.pi
+    cfg.y_min, cfg.y_max = R_IN_AU * AU, R_OUT_AU * AU * (1.0 + 1e-12)
+    if three_d:
+        cfg.z_min, cfg.z_max = 0.5 * math.pi - 1.0, 0.5 * math.pi + 1.0
+    else:
+        cfg.z_min = cfg.z_max = 0.5 * math.pi
+    gas_mass = GAS_TO_DUST * DUST_MASS
+    sigma_0 = gas_mass / (2.0 * math.pi * AU * (R_OUT_AU - R_IN_AU) * AU)
+    cfg.sigma_0, cfg.aspr_0, cfg.idx_p, cfg.idx_q = sigma_0, 0.05, -1.0, -0.5
+    cfg.const_nu, cfg.alpha = 0, 1.0e-3
+    cfg.code_unit = 0
+    cfg.rho_0 = 1.0
+    cfg.stokes_0 = math.pi * cfg.rho_0 * cfg.S_0 / (4.0 * sigma_0)
+    cfg.coag_kernel = GD_KERNEL_CUSTOM
+    cfg.n_k = n_k
+    cfg.h_search = 1.0
+    cfg.v_frag = v_frag
+    cfg.col_bath_max = 0.05 * orbital_time()
+    cfg.init_smin, cfg.init_smax = smin, smax
+    cfg.search = search
+    return cfg
+
+
+CONFIGS = {
+    "c0_plain_small": dict(n=65536, k=32, three_d=True, search=GD_SEARCH_KDTREE, v_frag=1.0e30,
+                           sizes=("mono", 2.0e-4), radial="loguniform", seed=1),
+    "c1_multisize_2d": dict(n=1 << 20, k=64, three_d=False, search=GD_SEARCH_MORTON, v_frag=100.0,
+                            sizes=("loguniform", 2.0e-4, 20.0), radial="gap_ring", seed=2),
+    "c3_learned_3d": dict(n=10_000_000, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                          sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=3),
+    "c4_production_3d": dict(n=10_000_000, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                             sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=4),
+}
+
+
+def config(name: str, n: int | None = None, k: int | None = None):
+    spec = CONFIGS[name]
+    sizes = spec["sizes"]
+    smin = sizes[1]
+    smax = sizes[1] if sizes[0] == "mono" else sizes[2]
+    cfg = _base_config(k or spec["k"], spec["three_d"], spec["search"], spec["v_frag"], smin, smax)
+    return cfg
+
+
+def _radius_samples(rng, n: int, kind: str) -> np.ndarray:
+    if kind == "loguniform":
+        return np.exp(rng.uniform(math.log(R_IN_AU), math.log(R_OUT_AU), n))
+    # Sigma ~ r^-1 with a x0.1 gap on [9, 11] au and a x5 Gaussian ring at 30 au (width 1 au);
+    # equal-mass representatives follow dN/dr ~ r Sigma(r), drawn by inverse CDF on a fine grid
+    grid = np.linspace(R_IN_AU, R_OUT_AU, 200_001)
+    dens = np.ones_like(grid)
+    dens[(grid >= 9.0) & (grid <= 11.0)] *= 0.1
+    dens *= 1.0 + 4.0 * np.exp(-0.5 * (grid - 30.0) ** 2)
+    cdf = np.concatenate([[0.0], np.cumsum(0.5 * (dens[1:] + dens[:-1]) * np.diff(grid))])
+    cdf /= cdf[-1]
+    return np.interp(rng.uniform(0.0, 1.0, n), cdf, grid)
+
+
+def particles(name: str, n: int | None = None, seed: int | None = None) -> np.ndarray:
+    """Seeded swarm of config `name` as a float64 array [n, 8] in the reference record layout."""
+    spec = CONFIGS[name]
+    n = int(n or spec["n"])
+    rng = np.random.Generator(np.random.PCG64(spec["seed"] if seed is None else seed))
+    phi = rng.uniform(0.0, 2.0 * math.pi, n)
+    r_au = _radius_samples(rng, n, spec["radial"])
+    if spec["three_d"]:
+        h = 0.05 * r_au ** 0.25
+        theta = 0.5 * math.pi + rng.standard_normal(n) * h
+    else:
+        theta = np.full(n, 0.5 * math.pi)
+    sizes = spec["sizes"]
+    if sizes[0] == "mono":
+        diam = np.full(n, sizes[1])
+    else:
+        diam = np.exp(rng.uniform(math.log(sizes[1]), math.log(sizes[2]), n))
+    grain = math.pi * 1.0 * diam ** 3 / 6.0
+    numr = (DUST_MASS / n) / grain
+    y = r_au * AU
+    R = y * np.sin(theta)
+    out = np.empty((n, 8), np.float64)
+    out[:, 0] = phi - math.pi  # azimuth in [-pi, pi)
+    out[:, 1] = y
+    out[:, 2] = theta
+    out[:, 3] = np.sqrt(G_CGS * MSUN * R)  # Keplerian l_phi
+    out[:, 4] = 0.0
+    out[:, 5] = 0.0
+    out[:, 6] = diam
+    out[:, 7] = numr
+    return out

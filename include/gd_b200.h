@@ -1,0 +1,196 @@
+/*
+ * gd_b200.h -- C ABI of the B200-native swarm collision path.
+ *
+ * The reference (GameDev) has no runtime plugin ABI: its collision step is compiled into the
+ * `gamedev` executable from a model directory (`make MODEL=<m>`, Makefile:56-77, 131-151) and is
+ * entered through the `evolve_collisions(duration)` lambda (src/swarm/swarm_runtime.cu:357-471),
+ * which runs the geometry stage (col_site_init -> index build -> col_cache_get -> col_space_bin)
+ * and then `evolve_local_collisions(...)` (inc/swarm/_col_chain.cuh:108-539).  Every entry point
+ * below replaces one of those pieces; the comment on each names the reference code it stands in
+ * for.  A model-local bridge (mod/gd_bridge/) forwards the reference's calls here.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Pointers named dev_* are CUDA device pointers owned by the
+ *     caller (particles, RNG states, output caches), exactly as in the reference, where
+ *     swarm_runtime.cu:76-184 allocates them.  The library owns its index, workspace and scratch.
+ *   - Every call is asynchronous on the handle's stream unless it reports a device-side status
+ *     (non-finite input, chain error), in which case it synchronises that stream once.
+ *   - No call throws or exits.  A non-zero gd_status is returned and gd_last_error() gives the
+ *     message; gd_error_detail() gives the particle index or chain error code where one applies.
+ *   - One handle is not re-entrant; distinct handles are independent.
+ */
+#ifndef GD_B200_H
+#define GD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference stops the process instead (gpu.cuh:103-120 GPU_CHECK -> exit,
+ * col_chain_run.cu:256-375 chain errors -> std::runtime_error in _col_chain.cuh:403-405). */
+typedef enum gd_status {
+    GD_OK = 0,
+    GD_ERR_INVALID_ARGUMENT = 1,   /* bad size, null pointer, unsupported configuration      */
+    GD_ERR_CUDA = 2,               /* a CUDA runtime call failed; detail = cudaError_t        */
+    GD_ERR_NONFINITE = 3,          /* non-finite particle state; detail = particle index       */
+    GD_ERR_CHAIN = 4,              /* event-chain error; detail = reference code 1..6          */
+    GD_ERR_CAPACITY = 5,           /* a bounded structure (stack, queue, scratch) overflowed   */
+    GD_ERR_CONTINUATION_LIMIT = 6, /* chain did not finish within its bounded event budget     */
+    GD_ERR_TIME_RESOLUTION = 7,    /* scheduler needed more than 2^52 subdivisions             */
+    GD_ERR_CONTROLLER = 8,         /* invalid rate or audit state seen by the bath controller   */
+    GD_ERR_NOT_READY = 9,          /* geometry or model used before it was built               */
+    GD_ERR_OUT_OF_MEMORY = 10
+} gd_status;
+
+/* Search structure requested by the model (Makefile COLLISION_SEARCH=kdtree|morton).  Both
+ * produce the same exact top-K list in canonical order (ascending float d^2, then code). */
+enum { GD_SEARCH_KDTREE = 0, GD_SEARCH_MORTON = 1 };
+
+/* Coagulation kernels (inc/swarm/_collision.cuh:22-28). */
+enum { GD_KERNEL_CONSTANT = 0, GD_KERNEL_LINEAR = 1, GD_KERNEL_PRODUCT = 2, GD_KERNEL_CUSTOM = 3 };
+
+/*
+ * Model constants that the reference fixes at compile time in const_defs.cuh
+ * (inc/swarm/const_defs.cuh:30-159) and flags.mk (-DCODE_UNIT, -DCONST_NU, -DHALF_DISK ...).
+ * gd_config_default() fills the reference defaults; a bridge copies the model's constexprs.
+ */
+typedef struct gd_config {
+    /* code units (const_defs.cuh:30-33) */
+    double G, M_S, R_0, S_0;
+    /* mesh domain (const_defs.cuh:41-51) */
+    int    n_x, n_y, n_z;
+    double x_min, x_max, y_min, y_max, z_min, z_max;
+    /* gas (const_defs.cuh:68-88) */
+    double sigma_0, aspr_0, idx_p, idx_q;
+    int    const_nu;          /* 1: CONST_NU, 0: CONST_ALPHA                                  */
+    double nu, alpha;
+    int    code_unit;         /* 1: CODE_UNIT (Reynolds from REYNOLDS_0, no Brownian term)     */
+    double reynolds_0, m_mol, x_sec;
+    int    half_disk;         /* HALF_DISK: polar upper bound inclusive (_transport.cuh:39-48) */
+    int    const_st;          /* CONST_ST: Stokes number without gas scaling (param_phys.cuh:202) */
+    /* dust (const_defs.cuh:95-97) */
+    double stokes_0, rho_0;
+    /* collision (const_defs.cuh:118-140) */
+    int    coag_kernel;       /* GD_KERNEL_*                                                   */
+    int    n_k;               /* neighbour slots per owner, 1..256                              */
+    double h_search;          /* search radius in local gas scale heights                      */
+    double v_frag;            /* fragmentation threshold speed                                  */
+    int    col_event_cap;
+    int    col_bin_x, col_bin_y, col_bin_z, col_bin_s, col_bin_min;
+    double col_bath_max, col_bath_eps, col_bath_alpha;
+    /* multisize initialisation bounds, used by fragmentation (const_defs.cuh:165-168) */
+    double init_smin, init_smax;
+    /* search selection (Makefile COLLISION_SEARCH, const_defs.cuh:142-145) */
+    int    search;            /* GD_SEARCH_*                                                    */
+    int    morton_leaf_target, morton_max_level;
+} gd_config;
+
+/* One representative particle, byte-identical to the reference `struct swarm` built with
+ * -DMULTISIZE (const_defs.cuh:194-203): position (azimuth, spherical radius, polar angle),
+ * velocity (l_phi, v_r, l_theta), grain diameter, represented grain count.  64 bytes. */
+typedef struct gd_particle {
+    double position[3];
+    double velocity[3];
+    double par_size;
+    double par_numr;
+} gd_particle;
+
+/* Size in bytes of one per-particle RNG state (cuRAND XORWOW curandState, 48 bytes), the record
+ * the reference keeps in dev_rngstate and writes to rngstate_<n>.dat (swarm_host.cuh:867-899). */
+size_t gd_rng_state_bytes(void);
+
+typedef struct gd_handle gd_handle;
+
+/* Fill *cfg with the reference's default const_defs.cuh values. */
+void gd_config_default(gd_config *cfg);
+
+/* Create a handle for n_p particles (const_defs.cuh:39 N_P) on the current CUDA device.
+ * Allocates the index, neighbour cache, controller workspace (the reference's local_workspace,
+ * _col_chain.cuh:36-96) and the caches the reference allocates in swarm_runtime.cu:120-184. */
+gd_status gd_create(const gd_config *cfg, int n_p, gd_handle **out);
+void      gd_destroy(gd_handle *h);
+
+/* Run all later work of this handle on `stream` (a cudaStream_t; NULL = legacy default stream,
+ * the stream every reference launch uses, _col_chain.cuh:147-149). */
+gd_status gd_set_stream(gd_handle *h, void *stream);
+
+/* Message and numeric detail of the last failed call on this handle. */
+size_t    gd_last_error(const gd_handle *h, char *buf, size_t len);
+long long gd_error_detail(const gd_handle *h);
+
+/* rngstate_init (src/swarm/rngstate_init.cu:11-18): curand_init(seed, subsequence = i, 0) for
+ * i < n, written to dev_rng (n * gd_rng_state_bytes() bytes). */
+gd_status gd_rng_init(void *dev_rng, int n, unsigned long long seed, void *stream);
+
+/* Geometry stage: col_site_init (src/swarm/col_site_init.cu:17-119) + index build
+ * (kdtree::buildTree, builder.h:109-152, or morton_index::build, morton_index.cuh:168-229).
+ * Non-finite particle -> GD_ERR_NONFINITE with the smallest bad index as detail (the reference
+ * reports the index its atomicCAS kept and exits, swarm_runtime.cu:382-393). */
+gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle);
+
+/* col_cache_get (inc/swarm/_col_cache.cuh:15-159): exact top-K neighbour codes (code = 3*index +
+ * image, _col_image.cuh:11-35) of every active owner, owner-major [n_p][n_k], in ascending
+ * (float d^2, code) order with -1 padding; inactive owners get a row of -1 and measure 0.
+ * dev_codes / dev_measure / dev_kth_d2 may be NULL, in which case the handle's own cache is
+ * written (and used by the collision operator).  dev_kth_d2 receives the largest kept d^2
+ * (0 for an empty row).  Requires gd_geometry_build. */
+gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle,
+                 int32_t *dev_codes, double *dev_measure, float *dev_kth_d2);
+
+/* Copy the site-init outputs of the last gd_geometry_build to caller device buffers (any may be
+ * NULL): sites [n_p] x (x, y, z, code bits) as float4, search radius q [n_p] (0 when inactive),
+ * active flags [n_p] (the reference's dev_kdtree_node cartesian / dev_search_dist /
+ * dev_col_active, col_site_init.cu:44-55, 106-117). */
+gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned char *dev_active);
+
+/* Copy the handle's neighbour cache (codes, measures) to caller device buffers. */
+gd_status gd_get_cache(gd_handle *h, int32_t *dev_codes, double *dev_measure);
+
+/* Replace the handle's neighbour cache with caller-provided codes and measures (device
+ * pointers, [n_p][n_k] and [n_p]), e.g. a cache restored from a file, and mark geometry valid. */
+gd_status gd_set_cache(gd_handle *h, const int32_t *dev_codes, const double *dev_measure);
+
+/* col_space_bin (src/swarm/col_space_bin.cu:11-35): controller group of every particle. */
+gd_status gd_space_bin(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_spatial);
+
+/* Geometry epoch control (swarm_runtime.cu:350-354): positions changed, rebuild on next use. */
+gd_status gd_invalidate_geometry(gd_handle *h);
+
+/* Reset the per-group bath controller memory (local.state), as the reference does at every
+ * output boundary (swarm_runtime.cu:490-496). */
+gd_status gd_reset_controller(gd_handle *h);
+
+/* evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539): advance every owner through one
+ * fixed-position frozen-bath collision operator of length `duration`, mutating par_size and
+ * par_numr of dev_particle and the RNG states in dev_rng.  Uses the neighbour cache built by
+ * gd_knn (or set by gd_set_cache).  total_dust_mass enters lambda_0 = N_P/(N_K*M_dust)
+ * (_col_chain.cuh:187). */
+gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *dev_rng,
+                                double duration, double total_dust_mass);
+
+/* evolve_collisions (swarm_runtime.cu:357-471): non-finite screen (colstate_flag) when the
+ * geometry is valid, else geometry build + gd_knn + space bins; then the collision operator. */
+gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *dev_rng,
+                               double duration, double total_dust_mass);
+
+/* Controller statistics of the last operator: waves, chain launches, owners updated. */
+typedef struct gd_operator_stats {
+    int    waves;
+    int    chain_launches;
+    long long owner_updates;
+    long long events;
+    double min_duration, max_duration;
+} gd_operator_stats;
+gd_status gd_last_operator_stats(const gd_handle *h, gd_operator_stats *out);
+
+/* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
+long long gd_launch_count(const gd_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GD_B200_H */

@@ -1,0 +1,55 @@
+/*
+ * gd_oracle.h -- CPU restatement of the reference swarm collision path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for libgd_b200: only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline / reference arm may load it.  The product
+ * never calls it and has no CPU fallback.
+ *
+ * Each function cites the reference file:line it restates (paths inside the GameDev tree).
+ * Floating-point policy: single-precision distances use the fmaf chain pinned in the CUDA
+ * kernels (compiled with -ffp-contract=off so no other contraction happens); FP64 physics uses
+ * libm, so it agrees with the GPU to a few ulps, not bit for bit.
+ */
+#ifndef GD_ORACLE_H
+#define GD_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/gd_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* col_site_init (src/swarm/col_site_init.cu:17-55): sites [n][4] = (x, y, z, code bits),
+ * search radius q[n] (0 when inactive), active[n].  Returns the smallest non-finite index or -1. */
+int gdo_site_init(const gd_config *cfg, const gd_particle *p, int n, float *site4, float *q, unsigned char *active);
+
+/* Exact top-K of every active owner among active sites with d^2 <= q_i^2, keyed by
+ * (float d^2 bits << 32 | code) as in kdtree/index_heap.cuh:58-69, written ascending.
+ * codes[n][K] (-1 padding, inactive rows all -1), d2[n][K] (may be NULL).
+ * gdo_knn_brute: O(n^2) loop, the brute force of val/swarm/mod/test_knn/knn_benchmark.cu:508-548.
+ * gdo_knn_kdtree: KD tree with widest-dimension median splits (the split rule of
+ * kdtree/builder_thrust.h:263-318) and the reference heap; `threads` OpenMP threads. */
+void gdo_knn_brute(int n, const float *site4, const float *q, const unsigned char *active, int K, int32_t *codes,
+                   float *d2, int threads);
+void gdo_knn_kdtree(int n, const float *site4, const float *q, const unsigned char *active, int K, int32_t *codes,
+                    float *d2, int threads, int first, int count);
+
+/* The pinned single-precision squared distance. */
+float gdo_dist2(const float *a, const float *b);
+
+/* _get_ball_measure (inc/swarm/_collision.cuh:66-115) of every owner from its largest kept d^2
+ * (kth_d2[i], 0 for an empty row); 0 for inactive owners. */
+void gdo_ball_measure(const gd_config *cfg, const gd_particle *p, int n, const unsigned char *active,
+                      const float *kth_d2, double *measure);
+
+/* col_space_bin (src/swarm/col_space_bin.cu:11-35) */
+void gdo_space_bin(const gd_config *cfg, const gd_particle *p, int n, int32_t *spatial);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,163 @@
+"""ctypes binding of the CPU oracle (oracle/_build/libgd_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU arms,
+never by the gamedev_b200 package.  The oracle restates the reference algorithm on the host; see
+gd_oracle.h for the reference file:line each function follows.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libgd_oracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    r = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        lib = C.CDLL(str(LIB))
+        P = C.c_void_p
+        lib.gdo_site_init.restype = C.c_int
+        lib.gdo_site_init.argtypes = [P, P, C.c_int, P, P, P]
+        lib.gdo_knn_brute.restype = None
+        lib.gdo_knn_brute.argtypes = [C.c_int, P, P, P, C.c_int, P, P, C.c_int]
+        lib.gdo_knn_kdtree.restype = None
+        lib.gdo_knn_kdtree.argtypes = [C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_int]
+        lib.gdo_kdtree_build.restype = P
+        lib.gdo_kdtree_build.argtypes = [C.c_int, P, P]
+        lib.gdo_kdtree_query.restype = None
+        lib.gdo_kdtree_query.argtypes = [P, C.c_int, P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_int]
+        lib.gdo_kdtree_free.restype = None
+        lib.gdo_kdtree_free.argtypes = [P]
+        lib.gdo_ball_measure.restype = None
+        lib.gdo_ball_measure.argtypes = [P, P, C.c_int, P, P, P]
+        lib.gdo_space_bin.restype = None
+        lib.gdo_space_bin.argtypes = [P, P, C.c_int, P]
+        _extend(lib)
+        _lib = lib
+    return _lib
+
+
+def _extend(lib):
+    """Bind the collision-operator restatement when present."""
+    P = C.c_void_p
+    if hasattr(lib, "gdo_env"):
+        lib.gdo_env.restype = None
+        lib.gdo_env.argtypes = [P, C.c_double, C.c_double, P]
+    for name in ("gdo_pair_speed_cached", "gdo_pair_speed_direct"):
+        if hasattr(lib, name):
+            getattr(lib, name).restype = C.c_double
+    if hasattr(lib, "gdo_pair_speed_cached"):
+        lib.gdo_pair_speed_cached.argtypes = [P, P, C.c_double, C.c_double]
+        lib.gdo_pair_speed_direct.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_double]
+    if hasattr(lib, "gdo_outcome_moments"):
+        lib.gdo_outcome_moments.restype = C.c_double
+        lib.gdo_outcome_moments.argtypes = [P, C.c_double, C.c_double, C.c_int, P]
+        lib.gdo_sample_outcome.restype = C.c_double
+        lib.gdo_sample_outcome.argtypes = [P, C.c_double, C.c_double, C.c_int, C.c_double]
+    if hasattr(lib, "gdo_bath_rate"):
+        lib.gdo_bath_rate.restype = None
+        lib.gdo_bath_rate.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_double, P, P, P, P, C.c_int]
+    if hasattr(lib, "gdo_chain_owner"):
+        lib.gdo_chain_owner.restype = C.c_int
+        lib.gdo_chain_owner.argtypes = [P, C.c_int, P, P, P, P, P, C.c_double, C.c_double, P, P, C.c_int, P, P]
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _cfg_ptr(cfg):
+    return C.byref(cfg)
+
+
+def site_init(cfg, particles: np.ndarray):
+    """col_site_init restated: returns (site4 float32 [n,4], q float32 [n], active uint8 [n], bad)."""
+    p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
+    n = p.shape[0]
+    site4 = np.zeros((n, 4), np.float32)
+    q = np.zeros(n, np.float32)
+    active = np.zeros(n, np.uint8)
+    bad = load().gdo_site_init(_cfg_ptr(cfg), _p(p), n, _p(site4), _p(q), _p(active))
+    return site4, q, active, bad
+
+
+def knn_brute(site4, q, active, k: int, threads: int | None = None):
+    n = site4.shape[0]
+    codes = np.empty((n, k), np.int32)
+    d2 = np.empty((n, k), np.float32)
+    load().gdo_knn_brute(n, _p(site4), _p(q), _p(active), k, _p(codes), _p(d2), threads or os.cpu_count())
+    return codes, d2
+
+
+def knn_kdtree(site4, q, active, k: int, threads: int | None = None, first: int = 0, count: int = -1):
+    n = site4.shape[0]
+    codes = np.full((n, k), -1, np.int32)
+    d2 = np.zeros((n, k), np.float32)
+    load().gdo_knn_kdtree(n, _p(site4), _p(q), _p(active), k, _p(codes), _p(d2), threads or os.cpu_count(),
+                          first, count)
+    return codes, d2
+
+
+class KdTree:
+    """The oracle KD tree kept alive between queries (for timing the CPU baseline)."""
+
+    def __init__(self, site4, active):
+        self.site4 = np.ascontiguousarray(site4, np.float32)
+        self.active = np.ascontiguousarray(active, np.uint8)
+        self.n = self.site4.shape[0]
+        self.h = load().gdo_kdtree_build(self.n, _p(self.site4), _p(self.active))
+
+    def query(self, q, k, codes, d2=None, threads=None, first=0, count=-1):
+        load().gdo_kdtree_query(self.h, self.n, _p(q), _p(self.active), k, _p(codes), _p(d2),
+                                threads or os.cpu_count(), first, count)
+
+    def close(self):
+        if self.h:
+            load().gdo_kdtree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kth_from_rows(codes, d2):
+    """Largest kept d^2 per row (0 for an empty row)."""
+    valid = codes >= 0
+    out = np.where(valid, d2, 0.0).max(axis=1) if codes.shape[1] else np.zeros(codes.shape[0])
+    return out.astype(np.float32)
+
+
+def ball_measure(cfg, particles, active, kth):
+    p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
+    n = p.shape[0]
+    out = np.empty(n, np.float64)
+    load().gdo_ball_measure(_cfg_ptr(cfg), _p(p), n, _p(active), _p(np.ascontiguousarray(kth, np.float32)), _p(out))
+    return out
+
+
+def space_bin(cfg, particles):
+    p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
+    out = np.empty(p.shape[0], np.int32)
+    load().gdo_space_bin(_cfg_ptr(cfg), _p(p), p.shape[0], _p(out))
+    return out

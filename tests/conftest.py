@@ -1,0 +1,41 @@
+import os
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libgd_b200.so")
+
+
+@pytest.fixture(scope="session")
+def oracle_lib():
+    from oracle import oracle
+
+    oracle.build()
+    return oracle
+
+
+@pytest.fixture(scope="session")
+def gd():
+    import gamedev_b200.build as b
+
+    b.build()
+    import gamedev_b200
+
+    gamedev_b200.load()
+    return gamedev_b200
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a CUDA device")
+    return torch.device("cuda:0")

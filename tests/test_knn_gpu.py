@@ -1,0 +1,120 @@
+"""GPU parity of the geometry stage (col_site_init + index + col_cache_get) against the CPU oracle.
+
+Bar: neighbour codes and the kept d^2 bit-identical to the oracle's exact top-K in ascending
+(d^2, code) order; sites bit-identical except where the host libm and the device math library
+round a double cos/sin/pow to different floats (counted, must be a vanishing fraction; the oracle
+is then run on the device's own sites so the neighbour comparison stays exact); the FP64 ball
+measure within 1e-12 relative (libm vs device acos/sqrt)."""
+
+import math
+
+import numpy as np
+import pytest
+
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+MEASURE_RTOL = 1e-12
+
+
+def _run_gpu(gd, cfg, p):
+    import torch
+
+    sw = gd.SwarmCollision(cfg, len(p))
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    site4, q, active = sw.get_sites()
+    torch.cuda.synchronize()
+    out = dict(codes=codes.cpu().numpy(), measure=measure.cpu().numpy(), kth=kth.cpu().numpy(),
+               site4=site4.cpu().numpy(), q=q.cpu().numpy(), active=active.cpu().numpy())
+    sw.close()
+    return out
+
+
+def _compare(oracle_lib, cfg, p, g, name):
+    site4, q, active, bad = oracle_lib.site_init(cfg, p)
+    assert bad == -1
+    assert np.array_equal(active, g["active"]), name
+    site_mismatch = int((site4.view(np.uint32) != g["site4"].view(np.uint32)).any(axis=1).sum())
+    q_mismatch = int((q.view(np.uint32) != g["q"].view(np.uint32)).sum())
+    assert site_mismatch <= max(2, len(p) // 10000), (name, site_mismatch)
+    assert q_mismatch <= max(2, len(p) // 10000), (name, q_mismatch)
+    # exact top-K on the device's own sites and radii
+    ck, dk = oracle_lib.knn_kdtree(g["site4"], g["q"], g["active"], cfg.n_k)
+    assert np.array_equal(g["codes"], ck), name
+    kth = oracle_lib.kth_from_rows(ck, dk)
+    assert np.array_equal(g["kth"].view(np.uint32), kth.view(np.uint32)), name
+    m = oracle_lib.ball_measure(cfg, p, g["active"], kth)
+    np.testing.assert_allclose(g["measure"], m, rtol=MEASURE_RTOL, atol=0, err_msg=name)
+    return site_mismatch, q_mismatch
+
+
+@pytest.mark.parametrize("idx", range(11))
+def test_gpu_topk_matches_oracle(gd, cuda, oracle_lib, idx):
+    name, cfg, p = cases.small_cases(gd)[idx]
+    g = _run_gpu(gd, cfg, p)
+    _compare(oracle_lib, cfg, p, g, name)
+
+
+def test_gpu_c0_full_size_matches_oracle(gd, cuda, oracle_lib):
+    """C0 plain-small at its BASELINE size: N = 65,536, K = 32, every row bit-exact."""
+    from gamedev_b200 import workloads
+
+    cfg = workloads.config("c0_plain_small")
+    p = workloads.particles("c0_plain_small")
+    g = _run_gpu(gd, cfg, p)
+    _compare(oracle_lib, cfg, p, g, "c0")
+
+
+def test_gpu_handle_cache_and_repeat_determinism(gd, cuda):
+    import torch
+
+    cfg = cases.code_unit_config(gd, n_k=32)
+    p = cases.random_swarm(cfg, 5000, 31, inactive_frac=0.05)
+    sw = gd.SwarmCollision(cfg, len(p))
+    dp = gd.particles_to_device(p)
+    c1, m1, _ = sw.knn(dp)
+    sw.build_cache(dp)
+    c2 = torch.empty_like(c1)
+    m2 = torch.empty_like(m1)
+    sw.get_cache(c2, m2)
+    assert torch.equal(c1, c2) and torch.equal(m1, m2)
+    c3, m3, _ = sw.knn(dp)
+    assert torch.equal(c1, c3) and torch.equal(m1, m3)
+
+
+def test_gpu_nonfinite_particle_is_reported(gd, cuda):
+    cfg = cases.code_unit_config(gd, n_k=8)
+    p = cases.random_swarm(cfg, 2000, 5)
+    p[1234, 3] = np.inf
+    p[1500, 6] = np.nan
+    sw = gd.SwarmCollision(cfg, len(p))
+    with pytest.raises(gd.GdError) as e:
+        sw.col_site_init(gd.particles_to_device(p))
+    assert e.value.status == 3 and e.value.detail == 1234
+    # the handle stays usable after the error
+    p[1234, 3] = 1.0
+    p[1500, 6] = 0.5
+    sw.col_site_init(gd.particles_to_device(p))
+
+
+def test_gpu_large_sample_parity(gd, cuda, oracle_lib):
+    """N = 2^20 C3-distributed swarm, K = 64: 4096 sampled owners checked bit-exactly against the
+    oracle's KD search over all sites (a size-independent property of the full-size run)."""
+    from gamedev_b200 import workloads
+
+    n = 1 << 20
+    cfg = workloads.config("c3_learned_3d")
+    p = workloads.particles("c3_learned_3d", n=n)
+    g = _run_gpu(gd, cfg, p)
+    rng = np.random.default_rng(7)
+    sample = np.sort(rng.choice(n, 4096, replace=False))
+    tree = oracle_lib.KdTree(g["site4"], g["active"])
+    codes = np.full((n, cfg.n_k), -1, np.int32)
+    d2 = np.zeros((n, cfg.n_k), np.float32)
+    for i in sample:
+        tree.query(g["q"], cfg.n_k, codes, d2, first=int(i), count=1)
+    assert np.array_equal(g["codes"][sample], codes[sample])
+    kth = oracle_lib.kth_from_rows(codes[sample], d2[sample])
+    assert np.array_equal(g["kth"][sample].view(np.uint32), kth.view(np.uint32))
