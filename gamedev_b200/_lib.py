@@ -86,6 +86,20 @@ SIGNATURES = {
     "gd_evolve_collisions": (C.c_int, [_P, _P, _P, C.c_double, C.c_double]),
     "gd_last_operator_stats": (C.c_int, [_P, C.POINTER(GdOperatorStats)]),
     "gd_launch_count": (C.c_longlong, [_P]),
+    "gd_rng_uniforms": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
+    "gd_get_owner_state": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    # include/gd_b200_controller.h (host only)
+    "gd_ctl_binmap": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P]),
+    "gd_ctl_choose_bath": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int, C.c_double, C.c_double, _P, _P]),
+    "gd_ctl_finish_bath": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int, _P, _P]),
+    "gd_ctl_schedule_create": (_P, [C.c_double, _P, C.c_int, _P, _P]),
+    "gd_ctl_schedule_destroy": (None, [_P]),
+    "gd_ctl_schedule_time": (C.c_ulonglong, [_P]),
+    "gd_ctl_schedule_end": (C.c_ulonglong, [_P]),
+    "gd_ctl_schedule_due": (C.c_int, [_P, C.c_ulonglong, _P]),
+    "gd_ctl_schedule_adapt": (C.c_int, [_P, C.c_ulonglong, _P, C.c_int, _P, _P]),
+    "gd_ctl_schedule_advance": (None, [_P, _P, C.c_int]),
+    "gd_ctl_schedule_levels": (None, [_P, _P]),
 }
 
 _lib = None

@@ -48,6 +48,15 @@ __global__ void k_rng_init(curandState *st, int n, unsigned long long seed) {
     if (i < n) curand_init(seed, static_cast<unsigned long long>(i), 0ull, &st[i]);
 }
 
+// _get_col_uniform (_col_rates.cuh:145-149) replayed on a copy of each state
+__global__ void k_rng_uniforms(const curandState *st, int n, int count, double *out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    curandState s = st[i];
+    for (int k = 0; k < count; ++k)
+        out[static_cast<size_t>(i) * count + k] = fmin(curand_uniform_double(&s), nextafter(1.0, 0.0));
+}
+
 }  // namespace gd
 
 struct gd_handle {
@@ -303,6 +312,31 @@ gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *de
 }
 
 long long gd_launch_count(const gd_handle *h) { return h ? h->geo.launches + h->col.launches : 0; }
+
+gd_status gd_rng_uniforms(const void *dev_rng, int n, int count, double *dev_out, void *stream) {
+    if (!dev_rng || !dev_out || n < 0 || count < 0) return GD_ERR_INVALID_ARGUMENT;
+    if (n == 0 || count == 0) return GD_OK;
+    gd::k_rng_uniforms<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const curandState *>(dev_rng), n, count, dev_out);
+    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+gd_status gd_get_owner_state(gd_handle *h, double *dev_cached4, double *dev_time, int32_t *dev_events,
+                             double *dev_size_old, double *dev_numr_old) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    const size_t n = static_cast<size_t>(h->n);
+    cudaError_t e = cudaSuccess;
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+        if (dst && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, h->stream);
+    };
+    cp(dev_cached4, h->col.cached.ptr, sizeof(double) * 4 * n);
+    cp(dev_time, h->col.time.ptr, sizeof(double) * n);
+    cp(dev_events, h->col.events.ptr, sizeof(int) * n);
+    cp(dev_size_old, h->col.size_old.ptr, sizeof(double) * n);
+    cp(dev_numr_old, h->col.numr_old.ptr, sizeof(double) * n);
+    if (e != cudaSuccess) return fail(h, gd::cuda_status(e, "copy owner state"));
+    return GD_OK;
+}
 
 gd_status gd_last_operator_stats(const gd_handle *h, gd_operator_stats *out) {
     if (!h || !out) return GD_ERR_INVALID_ARGUMENT;

@@ -1012,6 +1012,8 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
     c.stats.min_duration = std::numeric_limits<double>::infinity();
     if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
         return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+    // the reference's horizon check (_col_sched.cuh:30-33), made before any work is queued
+    if (!(duration > 0) || !std::isfinite(duration)) return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
 
     GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.events, 0, 8, s));
     const bool env_on = use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM;

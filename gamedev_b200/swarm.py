@@ -134,6 +134,19 @@ class SwarmCollision:
         self._check(self.lib.gd_evolve_collisions(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
                                                   float(duration), float(total_dust_mass)))
 
+    def owner_state(self):
+        """(cached [n,4], time [n], events [n], size_old [n], numr_old [n]) of the last operator."""
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        cached = torch.empty((self.n_p, 4), dtype=torch.float64, device=dev)
+        time = torch.empty(self.n_p, dtype=torch.float64, device=dev)
+        events = torch.empty(self.n_p, dtype=torch.int32, device=dev)
+        size_old = torch.empty(self.n_p, dtype=torch.float64, device=dev)
+        numr_old = torch.empty(self.n_p, dtype=torch.float64, device=dev)
+        self._check(self.lib.gd_get_owner_state(self.h, *(C.c_void_p(t.data_ptr()) for t in
+                                                          (cached, time, events, size_old, numr_old))))
+        return cached, time, events, size_old, numr_old
+
     def launch_count(self) -> int:
         return int(self.lib.gd_launch_count(self.h))
 
@@ -155,6 +168,17 @@ def rngstate_init(n: int, seed: int = 1, device="cuda:0"):
     if r != _lib.GD_OK:
         raise GdError(r, "gd_rng_init failed", 0)
     return st
+
+
+def rng_uniforms(rng, n: int, count: int):
+    """The next `count` chain deviates of every particle's stream, drawn from copies (rng unchanged)."""
+    torch = _torch()
+    out = torch.empty((n, count), dtype=torch.float64, device=rng.device)
+    r = _lib.load().gd_rng_uniforms(C.c_void_p(rng.data_ptr()), int(n), int(count), C.c_void_p(out.data_ptr()),
+                                    _stream())
+    if r != _lib.GD_OK:
+        raise GdError(r, "gd_rng_uniforms failed", 0)
+    return out
 
 
 def particles_to_device(arr: np.ndarray, device="cuda:0"):

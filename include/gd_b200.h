@@ -186,6 +186,18 @@ typedef struct gd_operator_stats {
 } gd_operator_stats;
 gd_status gd_last_operator_stats(const gd_handle *h, gd_operator_stats *out);
 
+/* Draw `count` deviates per particle exactly as the collision chain does
+ * (_get_col_uniform, _col_rates.cuh:145-149: min(curand_uniform_double, nextafter(1, 0))) from a
+ * COPY of each RNG state; dev_rng is left unchanged.  dev_out is [n][count] f64. */
+gd_status gd_rng_uniforms(const void *dev_rng, int n, int count, double *dev_out, void *stream);
+
+/* Per-owner state of the last collision operator, copied to caller device buffers (any may be
+ * NULL): bath-start rate moments [n_p][4] = (rate or -1 when invalid, first, second, maximum)
+ * (cached_rate_moments, _col_types.cuh:366), owner clock, accepted events, and the reservoir
+ * published at the start of the owner's last bath (size_old, numr_old). */
+gd_status gd_get_owner_state(gd_handle *h, double *dev_cached4, double *dev_time, int32_t *dev_events,
+                             double *dev_size_old, double *dev_numr_old);
+
 /* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
 long long gd_launch_count(const gd_handle *h);
 

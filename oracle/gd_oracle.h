@@ -48,6 +48,22 @@ void gdo_ball_measure(const gd_config *cfg, const gd_particle *p, int n, const u
 /* col_space_bin (src/swarm/col_space_bin.cu:11-35) */
 void gdo_space_bin(const gd_config *cfg, const gd_particle *p, int n, int32_t *spatial);
 
+/* ---- collision operator (gd_oracle_collide.c) ---- */
+void   gdo_env(const gd_config *c, double y, double z, double *env8);
+double gdo_pair_speed_cached(const gd_config *c, const double *env8, double size_i, double size_j);
+double gdo_pair_speed_direct(const gd_config *c, double y, double z, double size_i, double size_j);
+double gdo_pair_rate(const gd_config *c, double yi, double zi, double yj, double zj, double size_i, double size_j,
+                     double numr_j, double lambda0, double measure, double *vrel);
+double gdo_outcome_moments(const gd_config *c, double si, double sj, int high, double *mean_second_max);
+double gdo_sample_outcome(const gd_config *c, double si, double sj, int high, double u);
+void   gdo_bath_rate(const gd_config *c, int n, const gd_particle *p, const int32_t *codes, const double *measure,
+                     const unsigned char *active, const double *size_old, const double *numr_old, double lambda0,
+                     double *cached4, double *rate, double *change, double *second, int threads);
+int    gdo_chain_owner(const gd_config *c, int i, const gd_particle *p, const int32_t *codes,
+                       const double *measure, const unsigned char *active, const double *size_old,
+                       const double *numr_old, double lambda0, double bath_end, const double *cached4,
+                       const double *u, int nu, double *state8, int *used);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,12 +72,15 @@ def _extend(lib):
         lib.gdo_outcome_moments.argtypes = [P, C.c_double, C.c_double, C.c_int, P]
         lib.gdo_sample_outcome.restype = C.c_double
         lib.gdo_sample_outcome.argtypes = [P, C.c_double, C.c_double, C.c_int, C.c_double]
+    if hasattr(lib, "gdo_pair_rate"):
+        lib.gdo_pair_rate.restype = C.c_double
+        lib.gdo_pair_rate.argtypes = [P] + [C.c_double] * 9 + [P]
     if hasattr(lib, "gdo_bath_rate"):
         lib.gdo_bath_rate.restype = None
         lib.gdo_bath_rate.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_double, P, P, P, P, C.c_int]
     if hasattr(lib, "gdo_chain_owner"):
         lib.gdo_chain_owner.restype = C.c_int
-        lib.gdo_chain_owner.argtypes = [P, C.c_int, P, P, P, P, P, C.c_double, C.c_double, P, P, C.c_int, P, P]
+        lib.gdo_chain_owner.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_double, C.c_double, P, P, C.c_int, P, P]
 
 
 def _p(a: np.ndarray | None):
@@ -161,3 +164,67 @@ def space_bin(cfg, particles):
     out = np.empty(p.shape[0], np.int32)
     load().gdo_space_bin(_cfg_ptr(cfg), _p(p), p.shape[0], _p(out))
     return out
+
+
+# ---- collision operator restatement ------------------------------------------------------------
+def env(cfg, y, z):
+    out = np.zeros(8, np.float64)
+    load().gdo_env(_cfg_ptr(cfg), float(y), float(z), _p(out))
+    return out
+
+
+def pair_speed(cfg, y, z, size_i, size_j):
+    """Pair speed as the operator evaluates it: cached environment in physical units, direct
+    formula in code units."""
+    lib = load()
+    if not cfg.code_unit and not cfg.const_st:
+        e = env(cfg, y, z)
+        return lib.gdo_pair_speed_cached(_cfg_ptr(cfg), _p(e), float(size_i), float(size_j))
+    return lib.gdo_pair_speed_direct(_cfg_ptr(cfg), float(y), float(z), float(size_i), float(size_j))
+
+
+def pair_rate(cfg, yi, zi, yj, zj, size_i, size_j, numr_j, lambda0, measure):
+    """(rate / measure, pair speed) of one owner-partner pair."""
+    v = C.c_double(0.0)
+    r = load().gdo_pair_rate(_cfg_ptr(cfg), float(yi), float(zi), float(yj), float(zj), float(size_i),
+                             float(size_j), float(numr_j), float(lambda0), float(measure), C.byref(v))
+    return r, v.value
+
+
+def outcome_moments(cfg, si, sj, high):
+    out = np.zeros(3, np.float64)
+    f = load().gdo_outcome_moments(_cfg_ptr(cfg), float(si), float(sj), int(bool(high)), _p(out))
+    return f, out[0], out[1], out[2]
+
+
+def sample_outcome(cfg, si, sj, high, u):
+    return load().gdo_sample_outcome(_cfg_ptr(cfg), float(si), float(sj), int(bool(high)), float(u))
+
+
+def bath_rate(cfg, particles, codes, measure, active, size_old, numr_old, lambda0, threads=None):
+    p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
+    n = p.shape[0]
+    cached = np.zeros((n, 4), np.float64)
+    rate = np.zeros(n)
+    change = np.zeros(n)
+    second = np.zeros(n)
+    load().gdo_bath_rate(_cfg_ptr(cfg), n, _p(p), _p(np.ascontiguousarray(codes, np.int32)),
+                         _p(np.ascontiguousarray(measure, np.float64)), _p(np.ascontiguousarray(active, np.uint8)),
+                         _p(np.ascontiguousarray(size_old, np.float64)), _p(np.ascontiguousarray(numr_old, np.float64)),
+                         float(lambda0), _p(cached), _p(rate), _p(change), _p(second), threads or os.cpu_count())
+    return cached, rate, change, second
+
+
+def chain_owner(cfg, i, particles, codes, measure, active, size_old, numr_old, lambda0, bath_end, cached4, uniforms):
+    """One owner through one bath; returns (error, state[8], uniforms used)."""
+    p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
+    state = np.zeros(8, np.float64)
+    state[0] = p[i, 6]
+    state[1] = p[i, 7]
+    used = C.c_int(0)
+    u = np.ascontiguousarray(uniforms, np.float64)
+    err = load().gdo_chain_owner(_cfg_ptr(cfg), int(i), _p(p), _p(codes), _p(measure), _p(active), _p(size_old),
+                                 _p(numr_old), float(lambda0), float(bath_end),
+                                 _p(np.ascontiguousarray(cached4, np.float64)), _p(u), len(u), _p(state),
+                                 C.byref(used))
+    return err, state, used.value

@@ -1,0 +1,178 @@
+"""GPU parity of the frozen-bath collision operator against the CPU oracle.
+
+Bars (written in the checks):
+  * bath-start rate moments (col_bath_rate) within 1e-12 relative: FP64 with device vs host
+    transcendental functions and FMA contraction, identical (count+1)/2 fold order;
+  * one-wave operator: every owner's event count identical, grain size and count within 1e-12
+    relative, and the device RNG advanced by exactly the number of deviates the oracle's replay of
+    the same cuRAND stream consumed (checked bit for bit on the next deviate);
+  * represented mass N_i m_i conserved per owner to 2e-12 and in total to 1e-12 relative;
+  * repeat runs bit-identical (the reference's run_chain.py hash check);
+  * invalid input reported as a status, never a trap.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+RATE_RTOL = 1e-12
+STATE_RTOL = 1e-12
+
+
+def _setup(gd, cfg, p, seed=1):
+    import torch
+
+    sw = gd.SwarmCollision(cfg, len(p))
+    dp = gd.particles_to_device(p)
+    sw.build_cache(dp)
+    codes = torch.empty((len(p), cfg.n_k), dtype=torch.int32, device=dp.device)
+    measure = torch.empty(len(p), dtype=torch.float64, device=dp.device)
+    sw.get_cache(codes, measure)
+    rng = gd.rngstate_init(len(p), seed=seed)
+    site4, q, active = sw.get_sites()
+    torch.cuda.synchronize()
+    return sw, dp, rng, codes.cpu().numpy(), measure.cpu().numpy(), active.cpu().numpy()
+
+
+def _one_wave(cfg):
+    cfg.col_bath_max = 1.0e300
+    cfg.col_bath_eps = 1.0e150
+    return cfg
+
+
+def _chain_cases(gd):
+    from gamedev_b200 import workloads
+
+    out = []
+    cfg = cases.code_unit_config(gd, n_k=16, coag_kernel=0)
+    out.append(("constant_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 41), 1.0e-0))
+    cfg = cases.code_unit_config(gd, n_k=32, coag_kernel=1, three_d=False)
+    out.append(("linear_kernel_2d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 42), 1.0))
+    cfg = cases.code_unit_config(gd, n_k=24, coag_kernel=2)
+    out.append(("product_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 2500, 43), 1.0))
+    cfg = cases.code_unit_config(gd, n_k=32, coag_kernel=3)
+    cfg.code_unit = 1
+    cfg.v_frag = 3.0e-4
+    cfg.init_smin = 1.0e-3
+    out.append(("physical_kernel_code_units_frag", _one_wave(cfg), cases.random_swarm(cfg, 3000, 44), 1.0))
+    cfg = workloads.config("c0_plain_small")
+    out.append(("c0_physical_units", _one_wave(cfg), workloads.particles("c0_plain_small", n=4000), 1.0))
+    cfg = workloads.config("c1_multisize_2d")
+    out.append(("c1_frag_2d", _one_wave(cfg), workloads.particles("c1_multisize_2d", n=4000), 1.0))
+    return out
+
+
+def _calibrated_duration(oracle_lib, cfg, p, codes, measure, active, events_per_owner):
+    lam = len(p) / cfg.n_k / _total_mass(p)
+    cached, rate, _, _ = oracle_lib.bath_rate(cfg, p, codes, measure, active, p[:, 6], p[:, 7], lam)
+    r = rate[active.astype(bool) & (rate > 0)]
+    return events_per_owner / float(np.median(r)), lam, cached
+
+
+def _total_mass(p):
+    return float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+
+
+@pytest.mark.parametrize("idx", range(6))
+def test_operator_one_wave_matches_oracle_chain(gd, cuda, oracle_lib, idx):
+    import torch
+
+    name, cfg, p, evpo = _chain_cases(gd)[idx]
+    sw, dp, rng, codes, measure, active = _setup(gd, cfg, p)
+    duration, lam, cached_o = _calibrated_duration(oracle_lib, cfg, p, codes, measure, active, evpo)
+    # total dust mass enters lambda_0 exactly as the caller passes it
+    mass = _total_mass(p)
+    U = gd.rng_uniforms(rng, len(p), 96).cpu().numpy()
+    sw.evolve_local_collisions(dp, rng, duration, mass)
+    stats = sw.last_operator_stats()
+    assert stats["waves"] == 1, stats
+    cached, time_g, events_g, size_old, numr_old = (t.cpu().numpy() for t in sw.owner_state())
+    out = dp.cpu().numpy()
+    nxt = gd.rng_uniforms(rng, len(p), 1).cpu().numpy()[:, 0]
+    torch.cuda.synchronize()
+
+    # bath-start moments
+    act = active.astype(bool)
+    np.testing.assert_allclose(cached[act], cached_o[act], rtol=RATE_RTOL, atol=0, err_msg=name)
+
+    n_events = 0
+    for i in np.nonzero(act)[0]:
+        err, st, used = oracle_lib.chain_owner(cfg, int(i), p, codes, measure, active, p[:, 6].copy(),
+                                               p[:, 7].copy(), lam, duration, cached_o[i], U[i])
+        assert err == 0, (name, i, err)
+        assert int(st[7]) == events_g[i], (name, i, st[7], events_g[i])
+        n_events += int(st[7])
+        assert math.isclose(st[0], out[i, 6], rel_tol=STATE_RTOL), (name, i, st[0], out[i, 6])
+        assert math.isclose(st[1], out[i, 7], rel_tol=STATE_RTOL), (name, i)
+        assert st[2] == time_g[i]
+        # the device stream advanced by exactly `used` deviates
+        assert nxt[i] == U[i, used], (name, i, used)
+    assert n_events > 0, name
+    assert stats["events"] == n_events
+    # mass: per owner and in total
+    m0 = p[:, 7] * p[:, 6] ** 3
+    m1 = out[:, 7] * out[:, 6] ** 3
+    assert (np.abs(m1 - m0) <= 2e-12 * np.maximum(m0, m1)).all()
+    assert abs(m1.sum() - m0.sum()) <= 1e-12 * m0.sum()
+    sw.close()
+
+
+def test_operator_repeat_is_bit_identical_and_multiwave(gd, cuda):
+    """Full controller (moving bins, merged bins, many waves): two runs from the same state give
+    byte-identical particles and RNG states, and represented mass is conserved."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    cfg = workloads.config("c1_multisize_2d")
+    p = workloads.particles("c1_multisize_2d", n=20000)
+    results = []
+    for _ in range(2):
+        sw, dp, rng, *_ = _setup(gd, cfg, p, seed=5)
+        for _ in range(3):
+            sw.evolve_local_collisions(dp, rng, 2.0 * workloads.orbital_time(), workloads.DUST_MASS * 20000 / cfg.n_k)
+        torch.cuda.synchronize()
+        results.append((dp.cpu().numpy().copy(), rng.cpu().numpy().copy(), sw.last_operator_stats()))
+        sw.close()
+    (a, ra, sa), (b, rb, sb) = results
+    assert np.array_equal(a, b) and np.array_equal(ra, rb)
+    assert sa["waves"] >= 1
+    m0 = (p[:, 7] * p[:, 6] ** 3).sum()
+    assert abs((a[:, 7] * a[:, 6] ** 3).sum() - m0) <= 1e-12 * m0
+
+
+def test_operator_rejects_nonfinite_state(gd, cuda):
+    """A non-finite grain count is reported as a status (screen or controller), never a trap."""
+    import torch
+
+    cfg = cases.code_unit_config(gd, n_k=16, coag_kernel=0)
+    p = cases.random_swarm(cfg, 2000, 61)
+    sw, dp, rng, *_ = _setup(gd, cfg, p)
+    bad = dp.clone()
+    bad[123, 7] = float("nan")
+    with pytest.raises(gd.GdError) as e:
+        sw.evolve_collisions(bad, rng, 1.0, _total_mass(p))
+    assert e.value.status == 3 and e.value.detail == 123  # GD_ERR_NONFINITE, the reference's exit path
+    with pytest.raises(gd.GdError) as e:
+        sw.evolve_local_collisions(bad, rng, 1.0, _total_mass(p))
+    assert e.value.status in (4, 8)  # chain error or invalid controller state
+    # the handle recovers on valid input
+    sw.evolve_local_collisions(dp, rng, 1.0e-3, _total_mass(p))
+    torch.cuda.synchronize()
+
+
+def test_operator_rejects_invalid_arguments(gd, cuda):
+    cfg = cases.code_unit_config(gd, n_k=8)
+    p = cases.random_swarm(cfg, 500, 62)
+    sw, dp, rng, *_ = _setup(gd, cfg, p)
+    with pytest.raises(gd.GdError) as e:
+        sw.evolve_local_collisions(dp, rng, float("nan"), 1.0)
+    assert e.value.status == 1
+    with pytest.raises(gd.GdError) as e:
+        sw.evolve_local_collisions(dp, rng, 1.0, -1.0)
+    assert e.value.status == 1
