@@ -50,20 +50,20 @@ def _chain_cases(gd):
 
     out = []
     cfg = cases.code_unit_config(gd, n_k=16, coag_kernel=0)
-    out.append(("constant_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 41), 1.0e-0))
+    out.append(("constant_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 41), 3.0))
     cfg = cases.code_unit_config(gd, n_k=32, coag_kernel=1, three_d=False)
-    out.append(("linear_kernel_2d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 42), 1.0))
+    out.append(("linear_kernel_2d", _one_wave(cfg), cases.random_swarm(cfg, 3000, 42), 3.0))
     cfg = cases.code_unit_config(gd, n_k=24, coag_kernel=2)
-    out.append(("product_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 2500, 43), 1.0))
+    out.append(("product_kernel_3d", _one_wave(cfg), cases.random_swarm(cfg, 2500, 43), 3.0))
     cfg = cases.code_unit_config(gd, n_k=32, coag_kernel=3)
     cfg.code_unit = 1
     cfg.v_frag = 3.0e-4
     cfg.init_smin = 1.0e-3
-    out.append(("physical_kernel_code_units_frag", _one_wave(cfg), cases.random_swarm(cfg, 3000, 44), 1.0))
+    out.append(("physical_kernel_code_units_frag", _one_wave(cfg), cases.random_swarm(cfg, 3000, 44), 3.0))
     cfg = workloads.config("c0_plain_small")
-    out.append(("c0_physical_units", _one_wave(cfg), workloads.particles("c0_plain_small", n=4000), 1.0))
+    out.append(("c0_physical_units", _one_wave(cfg), workloads.particles("c0_plain_small", n=4000), 3.0))
     cfg = workloads.config("c1_multisize_2d")
-    out.append(("c1_frag_2d", _one_wave(cfg), workloads.particles("c1_multisize_2d", n=4000), 1.0))
+    out.append(("c1_frag_2d", _one_wave(cfg), workloads.particles("c1_multisize_2d", n=4000), 3.0))
     return out
 
 
@@ -71,7 +71,8 @@ def _calibrated_duration(oracle_lib, cfg, p, codes, measure, active, events_per_
     lam = len(p) / cfg.n_k / _total_mass(p)
     cached, rate, _, _ = oracle_lib.bath_rate(cfg, p, codes, measure, active, p[:, 6], p[:, 7], lam)
     r = rate[active.astype(bool) & (rate > 0)]
-    return events_per_owner / float(np.median(r)), lam, cached
+    # the fastest owner expects `events_per_owner` events; slower owners proportionally fewer
+    return events_per_owner / float(r.max()), lam, cached
 
 
 def _total_mass(p):
@@ -131,11 +132,17 @@ def test_operator_repeat_is_bit_identical_and_multiwave(gd, cuda):
 
     cfg = workloads.config("c1_multisize_2d")
     p = workloads.particles("c1_multisize_2d", n=20000)
+    mass = _total_mass(p)
     results = []
     for _ in range(2):
         sw, dp, rng, *_ = _setup(gd, cfg, p, seed=5)
+        sw.evolve_local_collisions(dp, rng, 1.0e-9 * workloads.orbital_time(), mass)
+        rate_max = float(sw.owner_state()[0][:, 0].max().item())
+        dp.copy_(gd.particles_to_device(p))
+        rng = gd.rngstate_init(len(p), seed=5)
         for _ in range(3):
-            sw.evolve_local_collisions(dp, rng, 2.0 * workloads.orbital_time(), workloads.DUST_MASS * 20000 / cfg.n_k)
+            # ~20 expected events for the fastest owner: the change bounds split it into many waves
+            sw.evolve_local_collisions(dp, rng, 20.0 / rate_max, mass)
         torch.cuda.synchronize()
         results.append((dp.cpu().numpy().copy(), rng.cpu().numpy().copy(), sw.last_operator_stats()))
         sw.close()
