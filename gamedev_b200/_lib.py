@@ -77,6 +77,7 @@ SIGNATURES = {
     "gd_geometry_build": (C.c_int, [_P, _P]),
     "gd_knn": (C.c_int, [_P, _P, _P, _P, _P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
+    "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "gd_get_cache": (C.c_int, [_P, _P, _P]),
     "gd_set_cache": (C.c_int, [_P, _P, _P]),
     "gd_space_bin": (C.c_int, [_P, _P, _P]),

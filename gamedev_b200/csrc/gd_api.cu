@@ -220,6 +220,22 @@ gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_cod
     return done(h, s);
 }
 
+gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int32_t *dev_codes,
+                         double *dev_measure, float *dev_kth_d2, unsigned long long *dev_stats) {
+    if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "gd_knn_bounded called before gd_geometry_build");
+    const bool own = !dev_codes && !dev_measure;
+    int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
+    double *measure = dev_measure ? dev_measure : h->measure.ptr;
+    float *kth = dev_kth_d2 ? dev_kth_d2 : h->kth.ptr;
+    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream, dev_radius, dev_stats);
+    if (s && own) {
+        h->cache_valid = true;
+        h->col.local_geometry_valid = false;
+    }
+    return done(h, s);
+}
+
 gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned char *dev_active) {
     if (!h) return GD_ERR_INVALID_ARGUMENT;
     if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "geometry not built");

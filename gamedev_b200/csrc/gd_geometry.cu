@@ -256,6 +256,8 @@ struct QueryArgs {
     int32_t *codes;         // may be null
     double *measure;        // may be null
     float *kth;             // may be null
+    const float *radius;    // proposed search radius by particle index, or null for the plain query
+    unsigned long long *stats;  // optional counters: leaves scanned, nodes tested, offers, fallbacks
 };
 
 __device__ __forceinline__ void heap_sift(unsigned long long *h, int lane, unsigned long long key, int slot, int n) {
@@ -276,6 +278,13 @@ __device__ __forceinline__ void heap_sift(unsigned long long *h, int lane, unsig
     }
     h[slot * 32 + lane] = key;
 }
+
+// Floyd heap construction over the first n entries of one lane's column
+__device__ __forceinline__ void heap_build(unsigned long long *h, int lane, int n) {
+    for (int s = n / 2 - 1; s >= 0; --s) heap_sift(h, lane, h[s * 32 + lane], s, n);
+}
+
+__device__ __forceinline__ float key_d2(unsigned long long k) { return __uint_as_float(static_cast<unsigned int>(k >> 32)); }
 
 __global__ void k_knn_query(Model m, QueryArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -300,97 +309,147 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
     const int code = __float_as_int(me.w);
     const int idx = valid ? code / 3 : 0;
     const float qr = valid ? a.qrad[idx] : 0.f;
-    // heap sentinel (q^2, 0xffffffff): every eligible candidate (d^2 <= q^2) sorts before it
-    // (kdtree/index_heap.cuh:58-61)
+    // Reference acceptance: key < (q^2 bits, 0xffffffff), i.e. d^2 <= q^2 with the float q^2 the
+    // reference heap is seeded with (kdtree/index_heap.cuh:58-61, morton_index.cuh:276).
     const float q2 = qr * qr;
-    const unsigned long long sentinel = (static_cast<unsigned long long>(__float_as_uint(q2)) << 32) | 0xffffffffull;
-    for (int s = 0; s < K; ++s) heap[s * 32 + lane] = sentinel;
-    float cut = valid ? q2 : -1.0f;
+    // Radius-bounded pass: accept d^2 <= lim2 = min(q, r)^2.  Finding K sites there proves they are
+    // the K nearest overall; otherwise the lane repeats the walk with lim2 = q^2.
+    float lim2 = q2;
+    if (a.radius && valid) {
+        const float r = a.radius[idx];
+        if (r < qr) lim2 = r * r;
+    }
+    int cnt = 0;                              // real entries held by this lane (fill phase below K)
+    float cut = valid ? lim2 : -1.0f;         // d^2 bound of an acceptable candidate
+    long long st_leaves = 0, st_nodes = 0, st_offers = 0;
 
     // warp centre (own bucket box) orders child visits
     const int own_node = a.leaf_slots - 1 + leaf;
     const float4 own_lo = a.lo[own_node], own_hi = a.hi[own_node];
     const float3 ctr = make_float3(0.5f * (own_lo.x + own_hi.x), 0.5f * (own_lo.y + own_hi.y), 0.5f * (own_lo.z + own_hi.z));
 
+    auto offer = [&](unsigned long long key) {
+        if (cnt < K) {
+            heap[cnt * 32 + lane] = key;  // fill phase: no ordering work until K entries exist
+            if (++cnt == K) {
+                heap_build(heap, lane, K);
+                cut = key_d2(heap[lane]);
+            }
+        } else if (key < heap[lane]) {
+            heap_sift(heap, lane, key, 0, K);
+            cut = key_d2(heap[lane]);
+        }
+    };
+
     auto scan_leaf = [&](int lf) {
         const int base = lf * kLeaf;
         tile[lane] = a.sorted[base + lane];
         __syncwarp();
-        const int cnt = min(kLeaf, n_act - base);
-        for (int c = 0; c < cnt; ++c) {
+        const int ncand = min(kLeaf, n_act - base);
+        // all 32 distances first (independent work), then this lane's accepted candidates only
+        unsigned int mask = 0;
+#pragma unroll
+        for (int c = 0; c < kLeaf; ++c) {
+            const float4 p = tile[c];
+            const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
+            mask |= ((c < ncand) && (d2 <= cut)) ? (1u << c) : 0u;
+        }
+        st_leaves += 1;
+        while (mask) {
+            const int c = __ffs(mask) - 1;
+            mask &= mask - 1;
             const float4 p = tile[c];
             const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
             if (d2 <= cut) {
-                const unsigned long long cand =
-                    (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned int>(__float_as_int(p.w));
-                if (cand < heap[lane]) {
-                    heap_sift(heap, lane, cand, 0, K);
-                    cut = __uint_as_float(static_cast<unsigned int>(heap[lane] >> 32));
-                }
+                ++st_offers;
+                offer((static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                      static_cast<unsigned int>(__float_as_int(p.w)));
             }
         }
         __syncwarp();
     };
 
-    // own bucket first: it holds the nearest sites, so the heaps tighten before the walk
-    scan_leaf(leaf);
-
-    int sp = 0;
-    stack[0] = 0;
-    sp = 1;
-    while (sp > 0) {
-        const int node = stack[--sp];
-        const float4 nl = a.lo[node], nh = a.hi[node];
-        const float bd = box_dist2(qp, nl, nh);
-        if (!__any_sync(0xffffffffu, bd <= cut)) continue;
-        if (node >= a.leaf_slots - 1) {
-            const int lf = node - (a.leaf_slots - 1);
-            if (lf != leaf) scan_leaf(lf);
-            continue;
+    auto walk = [&]() {
+        // own bucket first: it holds the nearest sites, so the bounds tighten before the walk
+        scan_leaf(leaf);
+        int sp = 1;
+        stack[0] = 0;
+        while (sp > 0) {
+            const int node = stack[--sp];
+            const float4 nl = a.lo[node], nh = a.hi[node];
+            st_nodes += 1;
+            if (!__any_sync(0xffffffffu, box_dist2(qp, nl, nh) <= cut)) continue;
+            if (node >= a.leaf_slots - 1) {
+                const int lf = node - (a.leaf_slots - 1);
+                if (lf != leaf) scan_leaf(lf);
+                continue;
+            }
+            const int c0 = 2 * node + 1, c1 = 2 * node + 2;
+            const float4 l0 = a.lo[c0], h0 = a.hi[c0], l1 = a.lo[c1], h1 = a.hi[c1];
+            const bool need0 = __any_sync(0xffffffffu, box_dist2(qp, l0, h0) <= cut);
+            const bool need1 = __any_sync(0xffffffffu, box_dist2(qp, l1, h1) <= cut);
+            const float e0 = box_dist2(ctr, l0, h0), e1 = box_dist2(ctr, l1, h1);
+            const int nearc = (e0 <= e1) ? c0 : c1, farc = (e0 <= e1) ? c1 : c0;
+            const bool need_near = (e0 <= e1) ? need0 : need1, need_far = (e0 <= e1) ? need1 : need0;
+            // the stack holds at most one pending sibling per tree level (<= 31) plus one
+            if (need_far) stack[sp++] = farc;
+            if (need_near) stack[sp++] = nearc;
+            __syncwarp();
         }
-        const int c0 = 2 * node + 1, c1 = 2 * node + 2;
-        const float4 l0 = a.lo[c0], h0 = a.hi[c0], l1 = a.lo[c1], h1 = a.hi[c1];
-        const bool need0 = __any_sync(0xffffffffu, box_dist2(qp, l0, h0) <= cut);
-        const bool need1 = __any_sync(0xffffffffu, box_dist2(qp, l1, h1) <= cut);
-        const float e0 = box_dist2(ctr, l0, h0), e1 = box_dist2(ctr, l1, h1);
-        const int nearc = (e0 <= e1) ? c0 : c1, farc = (e0 <= e1) ? c1 : c0;
-        const bool need_near = (e0 <= e1) ? need0 : need1, need_far = (e0 <= e1) ? need1 : need0;
-        // stack depth is bounded by the tree depth (<= 31 levels) + 1: well inside 64 entries
-        if (need_far) stack[sp++] = farc;
-        if (need_near) stack[sp++] = nearc;
-        __syncwarp();
+    };
+
+    walk();
+    bool fell_back = false;
+    if (a.radius) {
+        // lanes that found fewer than K sites inside a radius shorter than q repeat the walk with q
+        const bool need_fb = valid && lim2 < q2 && cnt < K;
+        if (__any_sync(0xffffffffu, need_fb)) {
+            if (need_fb) {
+                lim2 = q2;
+                cnt = 0;
+                cut = q2;
+                fell_back = true;
+            } else {
+                cut = -1.0f;  // this lane's heap is final: keep it out of the second walk
+            }
+            walk();
+        }
     }
 
-    // in-place heap sort: ascending (d^2 bits, code)
-    for (int end = K - 1; end > 0; --end) {
+    // ascending (d^2 bits, code): heap sort of the cnt real entries
+    if (cnt < K) heap_build(heap, lane, cnt);
+    for (int end = cnt - 1; end > 0; --end) {
         const unsigned long long top = heap[lane];
         const unsigned long long last = heap[end * 32 + lane];
         heap[end * 32 + lane] = top;
         heap_sift(heap, lane, last, 0, end);
     }
+    if (a.stats && lane == 0) {
+        atomicAdd(&a.stats[0], static_cast<unsigned long long>(st_leaves));
+        atomicAdd(&a.stats[1], static_cast<unsigned long long>(st_nodes));
+    }
+    if (a.stats) {
+        unsigned long long offers = static_cast<unsigned long long>(st_offers);
+        if (valid) atomicAdd(&a.stats[2], offers);
+        if (fell_back) atomicAdd(&a.stats[3], 1ull);
+    }
     if (!valid) return;
 
-    float maxd2 = 0.f;
+    const float maxd2 = cnt > 0 ? key_d2(heap[(cnt - 1) * 32 + lane]) : 0.f;
     int32_t *row = a.codes ? a.codes + static_cast<size_t>(idx) * K : nullptr;
-    if ((K & 3) == 0 && row) {
-        for (int s = 0; s < K; s += 4) {
-            int4 v;
-            int *vp = &v.x;
+    if (row) {
+        if ((K & 3) == 0) {
+            for (int s = 0; s < K; s += 4) {
+                int4 v;
+                int *vp = &v.x;
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const unsigned long long kk = heap[(s + t) * 32 + lane];
-                const unsigned int cc = static_cast<unsigned int>(kk);
-                if (cc != 0xffffffffu) maxd2 = __uint_as_float(static_cast<unsigned int>(kk >> 32));
-                vp[t] = (cc == 0xffffffffu) ? -1 : static_cast<int>(cc);
+                for (int t = 0; t < 4; ++t)
+                    vp[t] = (s + t < cnt) ? static_cast<int>(static_cast<unsigned int>(heap[(s + t) * 32 + lane])) : -1;
+                reinterpret_cast<int4 *>(row)[s >> 2] = v;
             }
-            reinterpret_cast<int4 *>(row)[s >> 2] = v;
-        }
-    } else {
-        for (int s = 0; s < K; ++s) {
-            const unsigned long long kk = heap[s * 32 + lane];
-            const unsigned int cc = static_cast<unsigned int>(kk);
-            if (cc != 0xffffffffu) maxd2 = __uint_as_float(static_cast<unsigned int>(kk >> 32));
-            if (row) row[s] = (cc == 0xffffffffu) ? -1 : static_cast<int>(cc);
+        } else {
+            for (int s = 0; s < K; ++s)
+                row[s] = (s < cnt) ? static_cast<int>(static_cast<unsigned int>(heap[s * 32 + lane])) : -1;
         }
     }
     if (a.kth) a.kth[idx] = maxd2;
@@ -516,7 +575,7 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
 size_t knn_smem_per_warp(int K) { return static_cast<size_t>(K) * 32 * 8 + 32 * 16 + 64 * 4; }
 
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
-                 float *kth_d2, cudaStream_t s) {
+                 float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats) {
     const int K = m.n_k;
     const size_t per_warp = knn_smem_per_warp(K);
     int warps = static_cast<int>((96 * 1024) / per_warp);
@@ -535,6 +594,8 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     qa.codes = codes;
     qa.measure = measure;
     qa.kth = kth_d2;
+    qa.radius = radius;
+    qa.stats = stats;
     const int max_leaves = (g.n + kLeaf - 1) / kLeaf;
     const int blocks = (max_leaves + warps - 1) / warps;
     g.launches += 2;

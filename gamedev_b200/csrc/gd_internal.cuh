@@ -123,8 +123,12 @@ Status geometry_alloc(Geometry &g, const Model &m, int n);
 // smallest bad index when a particle is non-finite.
 Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
 // Exact top-K over the bucket tree.  Writes codes/measure/kth (any may be null).
+// With `radius` (per particle, may be null) the walk is first bounded by min(q, radius) and falls
+// back to q for owners that find fewer than K sites inside; `stats` (may be null) accumulates
+// [leaves scanned, nodes tested, candidate offers, fallbacks].
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
-                 double *measure, float *kth_d2, cudaStream_t s);
+                 double *measure, float *kth_d2, cudaStream_t s, const float *radius = nullptr,
+                 unsigned long long *stats = nullptr);
 // colstate_flag: non-finite screen only.
 Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
 // col_space_bin

@@ -81,6 +81,13 @@ class SwarmCollision:
         self._check(self.lib.gd_knn(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(codes)),
                                     C.c_void_p(_ptr(measure)), C.c_void_p(_ptr(kth_d2))))
 
+    def col_cache_get_bounded(self, particles, radius=None, codes=None, measure=None, kth_d2=None, stats=None):
+        """Radius-bounded exact top-K (gd_knn_bounded); radius [n_p] float32 by particle index or
+        None; stats a uint64 [4] device tensor (leaves, nodes, offers, fallbacks) or None."""
+        self._check(self.lib.gd_knn_bounded(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(radius)),
+                                            C.c_void_p(_ptr(codes)), C.c_void_p(_ptr(measure)),
+                                            C.c_void_p(_ptr(kth_d2)), C.c_void_p(_ptr(stats))))
+
     def knn(self, particles):
         """Geometry + exact top-K into fresh torch tensors: (codes, measure, kth_d2)."""
         torch = _torch()

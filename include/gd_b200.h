@@ -140,6 +140,16 @@ gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle);
 gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle,
                  int32_t *dev_codes, double *dev_measure, float *dev_kth_d2);
 
+/* Radius-bounded exact top-K: the same output as gd_knn, computed by first walking each owner's
+ * neighbourhood only out to min(q_i, dev_radius[i]) (a proposed radius, e.g. from the learned
+ * radius model); an owner that finds fewer than K sites inside repeats the walk with q_i, so the
+ * result is exact by construction.  dev_radius may be NULL (plain query).  dev_stats, when not
+ * NULL, receives 4 accumulated counters: leaves scanned, tree nodes tested, candidate offers to a
+ * top-K heap, owners that fell back to the full radius (add to existing values; zero it first). */
+gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius,
+                         int32_t *dev_codes, double *dev_measure, float *dev_kth_d2,
+                         unsigned long long *dev_stats);
+
 /* Copy the site-init outputs of the last gd_geometry_build to caller device buffers (any may be
  * NULL): sites [n_p] x (x, y, z, code bits) as float4, search radius q [n_p] (0 when inactive),
  * active flags [n_p] (the reference's dev_kdtree_node cartesian / dev_search_dist /

@@ -155,7 +155,9 @@ def ball_measure(cfg, particles, active, kth):
     p = np.ascontiguousarray(particles).view(np.float64).reshape(-1, 8)
     n = p.shape[0]
     out = np.empty(n, np.float64)
-    load().gdo_ball_measure(_cfg_ptr(cfg), _p(p), n, _p(active), _p(np.ascontiguousarray(kth, np.float32)), _p(out))
+    act = np.ascontiguousarray(active, np.uint8)
+    kth = np.ascontiguousarray(kth, np.float32)
+    load().gdo_ball_measure(_cfg_ptr(cfg), _p(p), n, _p(act), _p(kth), _p(out))
     return out
 
 
@@ -208,9 +210,13 @@ def bath_rate(cfg, particles, codes, measure, active, size_old, numr_old, lambda
     rate = np.zeros(n)
     change = np.zeros(n)
     second = np.zeros(n)
-    load().gdo_bath_rate(_cfg_ptr(cfg), n, _p(p), _p(np.ascontiguousarray(codes, np.int32)),
-                         _p(np.ascontiguousarray(measure, np.float64)), _p(np.ascontiguousarray(active, np.uint8)),
-                         _p(np.ascontiguousarray(size_old, np.float64)), _p(np.ascontiguousarray(numr_old, np.float64)),
+    # keep every converted array alive across the call
+    codes = np.ascontiguousarray(codes, np.int32)
+    measure = np.ascontiguousarray(measure, np.float64)
+    active = np.ascontiguousarray(active, np.uint8)
+    size_old = np.ascontiguousarray(size_old, np.float64)
+    numr_old = np.ascontiguousarray(numr_old, np.float64)
+    load().gdo_bath_rate(_cfg_ptr(cfg), n, _p(p), _p(codes), _p(measure), _p(active), _p(size_old), _p(numr_old),
                          float(lambda0), _p(cached), _p(rate), _p(change), _p(second), threads or os.cpu_count())
     return cached, rate, change, second
 
@@ -223,8 +229,13 @@ def chain_owner(cfg, i, particles, codes, measure, active, size_old, numr_old, l
     state[1] = p[i, 7]
     used = C.c_int(0)
     u = np.ascontiguousarray(uniforms, np.float64)
+    codes = np.ascontiguousarray(codes, np.int32)
+    measure = np.ascontiguousarray(measure, np.float64)
+    active = np.ascontiguousarray(active, np.uint8)
+    size_old = np.ascontiguousarray(size_old, np.float64)
+    numr_old = np.ascontiguousarray(numr_old, np.float64)
+    cached4 = np.ascontiguousarray(cached4, np.float64)
     err = load().gdo_chain_owner(_cfg_ptr(cfg), int(i), _p(p), _p(codes), _p(measure), _p(active), _p(size_old),
-                                 _p(numr_old), float(lambda0), float(bath_end),
-                                 _p(np.ascontiguousarray(cached4, np.float64)), _p(u), len(u), _p(state),
-                                 C.byref(used))
+                                 _p(numr_old), float(lambda0), float(bath_end), _p(cached4), _p(u), len(u),
+                                 _p(state), C.byref(used))
     return err, state, used.value

@@ -118,3 +118,43 @@ def test_gpu_large_sample_parity(gd, cuda, oracle_lib):
     assert np.array_equal(g["codes"][sample], codes[sample])
     kth = oracle_lib.kth_from_rows(codes[sample], d2[sample])
     assert np.array_equal(g["kth"][sample].view(np.uint32), kth.view(np.uint32))
+
+
+def test_gpu_radius_bounded_query_is_exact(gd, cuda):
+    """gd_knn_bounded is exact by construction: with proposed radii below the true K-th distance
+    (owners must fall back) and above it (owners finish inside the radius) the output equals the
+    plain query bit for bit, and exactly the owners with a short radius fall back."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = 1 << 18
+    cfg = workloads.config("c3_learned_3d")
+    p = workloads.particles("c3_learned_3d", n=n)
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    site4, q, active = sw.get_sites()
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    short = torch.rand(n, device="cuda", generator=gen) < 0.3
+    factor = torch.where(short, 0.5 + 0.48 * torch.rand(n, device="cuda", generator=gen),
+                         1.02 + torch.rand(n, device="cuda", generator=gen))
+    radius = (kth.double().sqrt() * factor.double()).float()
+    codes_b = torch.empty_like(codes)
+    measure_b = torch.empty_like(measure)
+    kth_b = torch.empty_like(kth)
+    stats = torch.zeros(4, dtype=torch.int64, device="cuda")
+    sw.col_cache_get_bounded(dp, radius, codes_b, measure_b, kth_b, stats)
+    torch.cuda.synchronize()
+    assert torch.equal(codes, codes_b)
+    assert torch.equal(measure, measure_b) and torch.equal(kth, kth_b)
+    # a short radius falls back unless q itself is shorter than the proposal (then no fallback is needed)
+    expect = int((short & (radius < q) & (active > 0)).sum().item())
+    assert int(stats[3].item()) == expect
+    # the plain query through the bounded entry point, with counters
+    stats0 = torch.zeros(4, dtype=torch.int64, device="cuda")
+    codes_p = torch.empty_like(codes)
+    sw.col_cache_get_bounded(dp, None, codes_p, None, None, stats0)
+    torch.cuda.synchronize()
+    assert torch.equal(codes, codes_p) and int(stats0[3].item()) == 0
+    assert int(stats0[0].item()) > 0
