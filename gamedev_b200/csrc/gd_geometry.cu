@@ -199,9 +199,10 @@ __global__ void k_gather_sorted(int n_slots, const int *__restrict__ counters, c
     sorted[i] = s;
 }
 
-// one warp per leaf slot
+// one warp per leaf slot: four 8-site sub-boxes (8-lane reductions) and their union
 __global__ void k_leaf_bounds(int leaf_slots, const int *__restrict__ counters, const float4 *__restrict__ sorted,
-                              float4 *__restrict__ lo, float4 *__restrict__ hi) {
+                              float4 *__restrict__ lo, float4 *__restrict__ hi, float4 *__restrict__ sub_lo,
+                              float4 *__restrict__ sub_hi) {
     int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (leaf >= leaf_slots) return;
@@ -215,7 +216,14 @@ __global__ void k_leaf_bounds(int leaf_slots, const int *__restrict__ counters, 
         b = a;
     }
 #pragma unroll
-    for (int off = 16; off; off >>= 1) {
+    for (int off = 1; off < 32; off <<= 1) {
+        if (off == kSub) {
+            // lanes 0, 8, 16, 24 now hold their sub-box
+            if ((lane & (kSub - 1)) == 0) {
+                sub_lo[leaf * kSubs + lane / kSub] = make_float4(a.x, a.y, a.z, 0.f);
+                sub_hi[leaf * kSubs + lane / kSub] = make_float4(b.x, b.y, b.z, 0.f);
+            }
+        }
         a.x = fminf(a.x, __shfl_xor_sync(0xffffffffu, a.x, off));
         a.y = fminf(a.y, __shfl_xor_sync(0xffffffffu, a.y, off));
         a.z = fminf(a.z, __shfl_xor_sync(0xffffffffu, a.z, off));
@@ -248,6 +256,8 @@ struct QueryArgs {
     const float4 *sorted;
     const float4 *lo;
     const float4 *hi;
+    const float4 *sub_lo;   // 8-site sub-boxes of every leaf
+    const float4 *sub_hi;
     const float *qrad;      // by particle index
     const int *counters;
     const gd_particle *part;
@@ -343,18 +353,32 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
 
     auto scan_leaf = [&](int lf) {
         const int base = lf * kLeaf;
+        // which 8-site groups of this leaf can hold a candidate for some lane
+        unsigned int groups = 0;
+#pragma unroll
+        for (int gq = 0; gq < kSubs; ++gq) {
+            const float4 sl = a.sub_lo[lf * kSubs + gq], sh = a.sub_hi[lf * kSubs + gq];
+            if (__any_sync(0xffffffffu, box_dist2(qp, sl, sh) <= cut)) groups |= 1u << gq;
+        }
+        if (!groups) return;
         tile[lane] = a.sorted[base + lane];
         __syncwarp();
         const int ncand = min(kLeaf, n_act - base);
-        // all 32 distances first (independent work), then this lane's accepted candidates only
+        // the distances of every needed group first (independent work), then this lane's accepted
+        // candidates only
         unsigned int mask = 0;
 #pragma unroll
-        for (int c = 0; c < kLeaf; ++c) {
-            const float4 p = tile[c];
-            const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
-            mask |= ((c < ncand) && (d2 <= cut)) ? (1u << c) : 0u;
+        for (int gq = 0; gq < kSubs; ++gq) {
+            if (!(groups & (1u << gq))) continue;
+#pragma unroll
+            for (int c8 = 0; c8 < kSub; ++c8) {
+                const int c = gq * kSub + c8;
+                const float4 p = tile[c];
+                const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
+                mask |= ((c < ncand) && (d2 <= cut)) ? (1u << c) : 0u;
+            }
+            st_leaves += 1;
         }
-        st_leaves += 1;
         while (mask) {
             const int c = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -370,8 +394,11 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
     };
 
     auto walk = [&]() {
-        // own bucket first: it holds the nearest sites, so the bounds tighten before the walk
+        // own bucket and its two Morton neighbours first: they hold near sites, so the heaps fill
+        // and the bounds tighten before the tree walk
         scan_leaf(leaf);
+        if (leaf > 0) scan_leaf(leaf - 1);
+        if (leaf + 1 < n_leaves) scan_leaf(leaf + 1);
         int sp = 1;
         stack[0] = 0;
         while (sp > 0) {
@@ -381,7 +408,7 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
             if (!__any_sync(0xffffffffu, box_dist2(qp, nl, nh) <= cut)) continue;
             if (node >= a.leaf_slots - 1) {
                 const int lf = node - (a.leaf_slots - 1);
-                if (lf != leaf) scan_leaf(lf);
+                if (lf < leaf - 1 || lf > leaf + 1) scan_leaf(lf);
                 continue;
             }
             const int c0 = 2 * node + 1, c1 = 2 * node + 2;
@@ -514,6 +541,8 @@ Status geometry_alloc(Geometry &g, const Model &m, int n) {
     GD_TRY_CUDA(g.sorted.alloc(static_cast<size_t>(g.leaf_slots) * kLeaf));
     GD_TRY_CUDA(g.node_lo.alloc(2 * static_cast<size_t>(g.leaf_slots)));
     GD_TRY_CUDA(g.node_hi.alloc(2 * static_cast<size_t>(g.leaf_slots)));
+    GD_TRY_CUDA(g.sub_lo.alloc(static_cast<size_t>(g.leaf_slots) * kSubs));
+    GD_TRY_CUDA(g.sub_hi.alloc(static_cast<size_t>(g.leaf_slots) * kSubs));
     GD_TRY_CUDA(g.counters.alloc(4));
     return Status::ok();
 }
@@ -562,7 +591,8 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     g.launches += 2;
     k_gather_sorted<<<(slots + 255) / 256, 256, 0, s>>>(slots, g.counters.ptr, vin, g.site.ptr, g.sorted.ptr);
     k_leaf_bounds<<<(g.leaf_slots * 32 + 255) / 256, 256, 0, s>>>(g.leaf_slots, g.counters.ptr, g.sorted.ptr,
-                                                                  g.node_lo.ptr, g.node_hi.ptr);
+                                                                  g.node_lo.ptr, g.node_hi.ptr, g.sub_lo.ptr,
+                                                                  g.sub_hi.ptr);
     for (int count = g.leaf_slots / 2; count >= 1; count /= 2) {
         const int first = count - 1;
         g.launches += 1;
@@ -586,6 +616,8 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     qa.sorted = g.sorted.ptr;
     qa.lo = g.node_lo.ptr;
     qa.hi = g.node_hi.ptr;
+    qa.sub_lo = g.sub_lo.ptr;
+    qa.sub_hi = g.sub_hi.ptr;
     qa.qrad = g.q.ptr;
     qa.counters = g.counters.ptr;
     qa.part = dev_particle;

@@ -24,6 +24,8 @@ namespace gd {
 // Leaf width of the bucket tree: one Morton-ordered bucket of 32 sites is one warp's query tile
 // and one candidate tile.
 constexpr int kLeaf = 32;
+constexpr int kSub = 8;              // sites per leaf sub-box
+constexpr int kSubs = kLeaf / kSub;  // sub-boxes per leaf
 constexpr int kMaxK = 256;
 constexpr int kRadixThreads = 256;
 constexpr int kRadixItems = 16;
@@ -113,6 +115,7 @@ struct Geometry {
     DevBuf<unsigned int> hist;    // [256][tiles]
     DevBuf<float4> sorted;        // [leaf_slots*kLeaf] Morton-ordered sites, w = code bits
     DevBuf<float4> node_lo, node_hi;  // implicit tree, 2*leaf_slots-1 nodes
+    DevBuf<float4> sub_lo, sub_hi;    // four 8-site sub-boxes per leaf, [leaf_slots*4]
     DevBuf<int> counters;         // [0] active count, [1] first bad index (INT_MAX if none)
     unsigned int *sorted_val = nullptr;  // points into val_a or val_b after the sort
     long long launches = 0;              // kernels launched by this geometry (reported by the ABI)
@@ -125,7 +128,7 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
 // Exact top-K over the bucket tree.  Writes codes/measure/kth (any may be null).
 // With `radius` (per particle, may be null) the walk is first bounded by min(q, radius) and falls
 // back to q for owners that find fewer than K sites inside; `stats` (may be null) accumulates
-// [leaves scanned, nodes tested, candidate offers, fallbacks].
+// [8-site leaf groups scanned, nodes tested, candidate offers, fallbacks].
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
                  double *measure, float *kth_d2, cudaStream_t s, const float *radius = nullptr,
                  unsigned long long *stats = nullptr);

@@ -144,7 +144,7 @@ gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle,
  * neighbourhood only out to min(q_i, dev_radius[i]) (a proposed radius, e.g. from the learned
  * radius model); an owner that finds fewer than K sites inside repeats the walk with q_i, so the
  * result is exact by construction.  dev_radius may be NULL (plain query).  dev_stats, when not
- * NULL, receives 4 accumulated counters: leaves scanned, tree nodes tested, candidate offers to a
+ * NULL, receives 4 accumulated counters: 8-site leaf groups scanned, tree nodes tested, candidate offers to a
  * top-K heap, owners that fell back to the full radius (add to existing values; zero it first). */
 gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius,
                          int32_t *dev_codes, double *dev_measure, float *dev_kth_d2,
