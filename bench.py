@@ -233,6 +233,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed(stream, fn):
+    import torch
+
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    return a, b
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -245,50 +255,95 @@ def run_ours(args):
     n = args.n or workloads.CONFIGS[args.workload]["n"]
     K = cfg.n_k
     p_host = workloads.particles(args.workload, n=n, seed=workloads.CONFIGS[args.workload]["seed"] + rank)
+    mass = float((p_host[:, 7] * math.pi * p_host[:, 6] ** 3 / 6.0).sum())
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream()
 
     sw = gd.SwarmCollision(cfg, n)
     dp = gd.particles_to_device(p_host, device=dev)
     codes = torch.empty((n, K), dtype=torch.int32, device=dev)
+    codes_ref = torch.empty((n, K), dtype=torch.int32, device=dev)
     measure = torch.empty(n, dtype=torch.float64, device=dev)
     kth = torch.empty(n, dtype=torch.float32, device=dev)
+    stats = torch.zeros(4, dtype=torch.int64, device=dev)
 
-    def step():
+    # ---- plain tree: geometry + exact top-K, inputs resident -------------------------------
+    for _ in range(args.warmup):
         sw.col_site_init(dp)
         sw.col_cache_get(dp, codes, measure, kth)
-
-    for _ in range(args.warmup):
-        step()
     site4, q, active = sw.get_sites()
     n_active = int(active.sum().item())
+    plain_ev = []
+    barrier(world)
+    for s_ in range(args.steps):
+        e0 = _timed(stream, lambda: sw.col_site_init(dp))
+        e1 = _timed(stream, lambda: sw.col_cache_get(dp, codes, measure, kth))
+        plain_ev.append((e0, e1))
+    barrier(world)
+    plain_build = statistics.mean(e[0][0].elapsed_time(e[0][1]) for e in plain_ev)
+    plain_knn = statistics.mean(e[1][0].elapsed_time(e[1][1]) for e in plain_ev)
+    plain_ms = reduce_max(plain_build + plain_knn, world)
+    sw.col_cache_get_bounded(dp, None, codes, None, None, stats)
+    torch.cuda.synchronize()
+    plain_offers = float(stats[2].item()) / max(1, n_active)
 
+    # ---- learned radius: 20 plain steps with Keplerian drift train the network online -----
+    model = gd.RadiusModel(cfg.R_0, seed=1 + rank)
+    drift_dt = 0.02 * workloads.orbital_time()
+    prev = kth.clone()
+    train_loss = None
+    feats = torch.zeros((n, 8), dtype=torch.float32, device=dev)
+    for _ in range(20):
+        sw.drift_keplerian(dp, drift_dt)
+        sw.col_site_init(dp)
+        sw.col_cache_get(dp, codes, measure, kth)
+        sw.radius_features(dp, prev, mass, out=feats)
+        train_loss = model.train(feats, kth, iterations=100, batch=16384, lr=2e-3)
+        prev.copy_(kth)
+    margin = model.calibrate(feats, kth, 0.999)
+    radius = torch.empty(n, dtype=torch.float32, device=dev)
+
+    def learned_step():
+        sw.col_site_init(dp)
+        sw.radius_features(dp, prev, mass, out=feats)
+        model.predict(feats, out=radius)
+        sw.col_cache_get_bounded(dp, radius, codes, measure, kth, stats)
+
+    learned_ev, exact_steps = [], 0
+    fallbacks = offers = 0
+    for s_ in range(args.warmup + args.steps):
+        sw.drift_keplerian(dp, drift_dt)  # positions move between steps (outside the timed region)
+        stats.zero_()
+        ev = _timed(stream, learned_step)
+        if s_ >= args.warmup:
+            learned_ev.append(ev)
+            # verification against the plain query on the same geometry (untimed)
+            sw.col_cache_get(dp, codes_ref, None, None)
+            exact_steps += int(torch.equal(codes, codes_ref))
+            fallbacks += int(stats[3].item())
+            offers += int(stats[2].item())
+        prev.copy_(kth)
+    barrier(world)
+    learned_ms = reduce_max(statistics.mean(e[0].elapsed_time(e[1]) for e in learned_ev), world)
+    queries = reduce_sum(float(n_active), world)
+    value = queries / (learned_ms / 1e3)
+    plain_value = queries / (plain_ms / 1e3)
+
+    # dominant kernel of the learned step (the bounded top-K), timed alone for the roofline
+    knn_alone = []
+    for _ in range(args.steps):
+        knn_alone.append(_timed(stream, lambda: sw.col_cache_get_bounded(dp, radius, codes, measure, kth, None)))
+    # clocks and launch count over one more timed window of learned steps
     clocks = Clocks(torch.cuda.current_device())
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev2 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = sw.launch_count()
     barrier(world)
     clocks.start()
-    start.record(stream)
-    for s in range(args.steps):
-        ev0[s].record(stream)
-        sw.col_site_init(dp)
-        ev1[s].record(stream)
-        sw.col_cache_get(dp, codes, measure, kth)
-        ev2[s].record(stream)
-    stop.record(stream)
+    for _ in range(args.steps):
+        learned_step()
     barrier(world)
     clk = clocks.stop()
-    launches = sw.launch_count() - launches0
-    total_ms = start.elapsed_time(stop)
-    total_ms = reduce_max(total_ms, world)
-    knn_ms = statistics.mean(ev1[s].elapsed_time(ev2[s]) for s in range(args.steps))
-    build_ms = statistics.mean(ev0[s].elapsed_time(ev1[s]) for s in range(args.steps))
-    ms_per_step = total_ms / args.steps
-    queries = reduce_sum(float(n_active * args.steps), world)
-    value = queries / (total_ms / 1e3)
+    launches = (sw.launch_count() - launches0) // max(1, args.steps)
+    knn_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in knn_alone)
 
     peak, peak_kind = peaks()
     bytes_per_query = 24 + 4 * K
@@ -297,44 +352,51 @@ def run_ours(args):
 
     result = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": learned_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "n": n, "k": K, "active": n_active, "geometry": "3d" if cfg.n_z > 1 else "2d",
-                   "index": "Morton bucket tree, 32-site buckets", "order": "ascending (d2, code)",
+        "config": {"workload": args.workload, "n": n, "k": K, "active": n_active,
+                   "geometry": "3d" if cfg.n_z > 1 else "2d", "index": "Morton bucket tree, 32-site buckets",
+                   "order": "ascending (d2, code)", "step": "geometry build + features + MLP + radius-bounded top-K",
                    "l2": "inputs and outputs larger than L2 (sites 16 B x N, codes 4K B x N)",
                    "parallelism": f"replicas x{world}"},
-        "phases_ms": {"geometry_build": build_ms, "knn_query": knn_ms},
-        "roofline": {"bound": "hbm", "kernel": "k_knn_query (+k_inactive_rows)", "achieved": achieved,
+        "plain": {"queries_per_s": plain_value, "ms_per_step": plain_ms, "geometry_build_ms": plain_build,
+                  "knn_query_ms": plain_knn, "offers_per_owner": plain_offers},
+        "learned": {"queries_per_s": value, "vs_plain": value / plain_value, "ms_per_step": learned_ms,
+                    "knn_query_ms": knn_ms, "hit_rate": 1.0 - fallbacks / max(1, n_active * args.steps),
+                    "fallback_fraction": fallbacks / max(1, n_active * args.steps),
+                    "offers_per_owner": offers / max(1, n_active * args.steps),
+                    "bit_exact_steps": f"{exact_steps}/{args.steps}", "margin_log": margin,
+                    "train_loss": train_loss, "training": "20 plain steps, 100 Adam iterations each, batch 16384",
+                    "drift_between_steps": "Keplerian, 0.02/Omega(1 au)"},
+        "roofline": {"bound": "hbm", "kernel": "k_knn_query (radius-bounded)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "bytes_per_unit": bytes_per_query, "units_per_launch": n_active, "traffic": traffic},
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if exact_steps != args.steps:
+        result["error"] = "learned-radius neighbour lists differ from the plain query"
 
-    # ---- end to end through the C ABI with host buffers ------------------------------------
+    # ---- end to end through the C ABI with host buffers (learned path) ---------------------
     if not args.no_e2e:
-        host_in = torch.from_numpy(np.ascontiguousarray(p_host)).pin_memory()
+        p_now = dp.cpu()
+        host_in = p_now.pin_memory()
         host_codes = torch.empty((n, K), dtype=torch.int32).pin_memory()
         host_measure = torch.empty(n, dtype=torch.float64).pin_memory()
 
         def e2e_step():
             dp.copy_(host_in, non_blocking=True)
-            sw.col_site_init(dp)
-            sw.col_cache_get(dp, codes, measure, kth)
+            learned_step()
             host_codes.copy_(codes, non_blocking=True)
             host_measure.copy_(measure, non_blocking=True)
 
         for _ in range(max(1, args.warmup)):
             e2e_step()
         barrier(world)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(args.steps):
-            e2e_step()
-        b.record(stream)
+        a, b = _timed(stream, lambda: [e2e_step() for _ in range(args.steps)])
         barrier(world)
         e_ms = reduce_max(a.elapsed_time(b), world)
-        result["e2e"] = {"value": queries / (e_ms / 1e3), "unit": "queries/s",
+        result["e2e"] = {"value": queries * args.steps / (e_ms / 1e3), "unit": "queries/s",
                          "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * K * 4 + n * 8,
                          "ms_per_step": e_ms / args.steps}
         del host_in, host_codes, host_measure
@@ -344,7 +406,6 @@ def run_ours(args):
         try:
             rng = gd.rngstate_init(n, seed=1 + rank, device=dev)
             dp.copy_(torch.from_numpy(np.ascontiguousarray(p_host)).to(dev))
-            mass = float((p_host[:, 7] * math.pi * p_host[:, 6] ** 3 / 6.0).sum())
             # The half-operator length is set from the bath-start rates so that the fastest owner
             # expects two events per half step (the c3 grain sizes span five decades, so a fixed
             # orbital fraction would ask the fastest owners for millions of events).
@@ -361,21 +422,16 @@ def run_ours(args):
 
             swarm_step()
             barrier(world)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             st_steps = max(1, min(args.steps, 3))
-            a.record(stream)
-            for _ in range(st_steps):
-                swarm_step()
-            b.record(stream)
+            a, b = _timed(stream, lambda: [swarm_step() for _ in range(st_steps)])
             barrier(world)
             s_ms = reduce_max(a.elapsed_time(b), world) / st_steps
-            stats = sw.last_operator_stats()
             result["swarm_step"] = {"steps_per_s": world * 1e3 / s_ms, "ms_per_step": s_ms,
                                     "definition": "geometry + exact top-K + 2 collision half-operators, "
                                                   "plain tree; half-operator = min(0.5/Omega(1 au), "
                                                   "2/max bath-start rate)",
                                     "half_operator_s": half, "max_bath_rate_per_s": rate_max,
-                                    "last_operator": stats}
+                                    "last_operator": sw.last_operator_stats()}
         except Exception as e:  # reported, never hidden
             result["swarm_step"] = {"error": str(e)}
 
@@ -388,6 +444,7 @@ def run_ours(args):
                                             f"active sites built in {cb['build_s']:.1f} s (not counted)"}
     if rank == 0:
         print(json.dumps(result), flush=True)
+    model.close()
     sw.close()
     if world > 1:
         import torch.distributed as dist

@@ -78,6 +78,17 @@ SIGNATURES = {
     "gd_knn": (C.c_int, [_P, _P, _P, _P, _P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "gd_drift_keplerian": (C.c_int, [_P, _P, C.c_double]),
+    "gd_radius_model_create": (C.c_int, [C.c_ulonglong, C.c_double, C.POINTER(_P)]),
+    "gd_radius_model_destroy": (None, [_P]),
+    "gd_radius_features": (C.c_int, [_P, _P, _P, C.c_double, _P]),
+    "gd_radius_model_train": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                        C.POINTER(C.c_float), _P]),
+    "gd_radius_model_gradient": (C.c_int, [_P, _P, _P, C.c_int, _P, C.POINTER(C.c_float), _P]),
+    "gd_radius_model_calibrate": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.POINTER(C.c_float), _P]),
+    "gd_radius_model_predict": (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    "gd_radius_model_get": (C.c_int, [_P, _P, _P]),
+    "gd_radius_model_set": (C.c_int, [_P, _P, _P]),
     "gd_get_cache": (C.c_int, [_P, _P, _P]),
     "gd_set_cache": (C.c_int, [_P, _P, _P]),
     "gd_space_bin": (C.c_int, [_P, _P, _P]),

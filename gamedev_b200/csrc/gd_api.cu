@@ -2,6 +2,7 @@
 #include <curand_kernel.h>
 
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -234,6 +235,25 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
         h->col.local_geometry_valid = false;
     }
     return done(h, s);
+}
+
+gd_status gd_drift_keplerian(gd_handle *h, gd_particle *dev_particle, double dt) {
+    if (!h || !dev_particle || !std::isfinite(dt)) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer or bad dt");
+    h->geo.launches += 1;
+    gd::Status s = gd::drift_keplerian(h->m, h->n, dev_particle, dt, h->stream);
+    h->geom_valid = false;
+    h->cache_valid = false;
+    h->col.local_geometry_valid = false;
+    return done(h, s);
+}
+
+gd_status gd_radius_features(gd_handle *h, const gd_particle *dev_particle, const float *dev_prev_kth_d2,
+                             double total_mass, float *dev_features) {
+    if (!h || !dev_particle || !dev_features || !(total_mass > 0))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer or non-positive mass");
+    if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "gd_radius_features called before gd_geometry_build");
+    return done(h, gd::radius_features(h->geo, h->m, dev_particle, dev_prev_kth_d2, total_mass, dev_features,
+                                       h->stream));
 }
 
 gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned char *dev_active) {

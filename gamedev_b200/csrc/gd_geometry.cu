@@ -397,8 +397,10 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
         // own bucket and its two Morton neighbours first: they hold near sites, so the heaps fill
         // and the bounds tighten before the tree walk
         scan_leaf(leaf);
-        if (leaf > 0) scan_leaf(leaf - 1);
-        if (leaf + 1 < n_leaves) scan_leaf(leaf + 1);
+        for (int d = 1; d <= kPrescan; ++d) {
+            if (leaf - d >= 0) scan_leaf(leaf - d);
+            if (leaf + d < n_leaves) scan_leaf(leaf + d);
+        }
         int sp = 1;
         stack[0] = 0;
         while (sp > 0) {
@@ -408,7 +410,7 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
             if (!__any_sync(0xffffffffu, box_dist2(qp, nl, nh) <= cut)) continue;
             if (node >= a.leaf_slots - 1) {
                 const int lf = node - (a.leaf_slots - 1);
-                if (lf < leaf - 1 || lf > leaf + 1) scan_leaf(lf);
+                if (lf < leaf - kPrescan || lf > leaf + kPrescan) scan_leaf(lf);
                 continue;
             }
             const int c0 = 2 * node + 1, c1 = 2 * node + 2;
@@ -496,6 +498,26 @@ __global__ void k_inactive_rows(int n, int K, const unsigned char *__restrict__ 
         for (int s = 0; s < K; ++s) codes[static_cast<size_t>(i) * K + s] = -1;
     if (measure) measure[i] = 0.0;
     if (kth) kth[i] = 0.f;
+}
+
+// Keplerian azimuthal advance phi += Omega_K(R) dt, wrapped into [x_min, x_max)
+__global__ void k_drift_keplerian(Model m, int n, gd_particle *__restrict__ part, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double y = part[i].position[1], z = part[i].position[2];
+    if (!site_active(m, y, z)) return;
+    const double R = cyl_R(m, y, z);
+    const double width = m.x_max - m.x_min;
+    double x = part[i].position[0] + sqrt(m.G * m.M_S / R / R / R) * dt;
+    x = m.x_min + fmod(x - m.x_min, width);
+    if (x < m.x_min) x += width;
+    part[i].position[0] = x;
+}
+
+Status drift_keplerian(const Model &m, int n, gd_particle *part, double dt, cudaStream_t s) {
+    k_drift_keplerian<<<(n + 255) / 256, 256, 0, s>>>(m, n, part, dt);
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
 }
 
 // col_space_bin (col_space_bin.cu:11-35)
@@ -587,6 +609,7 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     }
     GD_TRY_CUDA(cudaGetLastError());
     g.sorted_val = vin;
+    g.sorted_key = kin;
     const int slots = g.leaf_slots * kLeaf;
     g.launches += 2;
     k_gather_sorted<<<(slots + 255) / 256, 256, 0, s>>>(slots, g.counters.ptr, vin, g.site.ptr, g.sorted.ptr);
@@ -608,8 +631,19 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
                  float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats) {
     const int K = m.n_k;
     const size_t per_warp = knn_smem_per_warp(K);
-    int warps = static_cast<int>((96 * 1024) / per_warp);
-    warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
+    // the per-lane heaps bound residency: pick the block width that keeps the most warps per SM
+    // (227 KB of shared memory per SM, at most 8 warps per block)
+    const size_t sm_bytes = 227 * 1024;
+    int best = 1, best_res = 0;
+    for (int w = 1; w <= 8; ++w) {
+        if (per_warp * w > sm_bytes) break;
+        const int res = static_cast<int>(sm_bytes / (per_warp * w + 1024)) * w;
+        if (res > best_res) {
+            best_res = res;
+            best = w;
+        }
+    }
+    const int warps = best;
     const size_t smem = per_warp * warps;
     GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     QueryArgs qa;

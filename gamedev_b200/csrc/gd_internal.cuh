@@ -26,6 +26,7 @@ namespace gd {
 constexpr int kLeaf = 32;
 constexpr int kSub = 8;              // sites per leaf sub-box
 constexpr int kSubs = kLeaf / kSub;  // sub-boxes per leaf
+constexpr int kPrescan = 2;          // Morton-neighbour buckets scanned on each side before the walk
 constexpr int kMaxK = 256;
 constexpr int kRadixThreads = 256;
 constexpr int kRadixItems = 16;
@@ -118,6 +119,7 @@ struct Geometry {
     DevBuf<float4> sub_lo, sub_hi;    // four 8-site sub-boxes per leaf, [leaf_slots*4]
     DevBuf<int> counters;         // [0] active count, [1] first bad index (INT_MAX if none)
     unsigned int *sorted_val = nullptr;  // points into val_a or val_b after the sort
+    unsigned long long *sorted_key = nullptr;  // points into key_a or key_b after the sort
     long long launches = 0;              // kernels launched by this geometry (reported by the ABI)
 };
 
@@ -132,8 +134,13 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
                  double *measure, float *kth_d2, cudaStream_t s, const float *radius = nullptr,
                  unsigned long long *stats = nullptr);
+// Learned-radius features of every owner (gd_radius.cu).
+Status radius_features(const Geometry &g, const Model &m, const gd_particle *part, const float *prev_kth,
+                       double total_mass, float *feat, cudaStream_t s);
 // colstate_flag: non-finite screen only.
 Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
+// Keplerian azimuthal advance of the active particles
+Status drift_keplerian(const Model &m, int n, gd_particle *part, double dt, cudaStream_t s);
 // col_space_bin
 Status space_bin(const Model &m, const gd_particle *dev_particle, int n, int32_t *spatial,
                  cudaStream_t s);

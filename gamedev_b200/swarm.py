@@ -163,6 +163,99 @@ class SwarmCollision:
         return {name: getattr(s, name) for name, _ in s._fields_}
 
 
+    # ---- learned radius -------------------------------------------------------------------
+    def drift_keplerian(self, particles, dt: float):
+        """Keplerian azimuthal advance (gd_drift_keplerian); invalidates the geometry."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_drift_keplerian(self.h, C.c_void_p(_ptr(particles)), float(dt)))
+
+    def radius_features(self, particles, prev_kth_d2, total_mass: float, out=None):
+        """Learned-radius features [n_p, 8] of the current geometry (gd_radius_features)."""
+        torch = _torch()
+        if out is None:
+            out = torch.zeros((self.n_p, 8), dtype=torch.float32, device=particles.device)
+        self._check(self.lib.gd_radius_features(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(prev_kth_d2)),
+                                                float(total_mass), C.c_void_p(_ptr(out))))
+        return out
+
+
+class RadiusModel:
+    """The learned search-radius network (gd_radius_model_*); every computation is a libgd_b200
+    kernel."""
+
+    N_PARAMS = 4801
+
+    def __init__(self, R_0: float, seed: int = 1):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.gd_radius_model_create(C.c_ulonglong(seed), float(R_0), C.byref(h))
+        if st != _lib.GD_OK:
+            raise GdError(st, "gd_radius_model_create failed", 0)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gd_radius_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != _lib.GD_OK:
+            raise GdError(st, what, 0)
+
+    def train(self, features, kth_d2, iterations: int, batch: int = 16384, lr: float = 1e-3) -> float:
+        loss = C.c_float(0.0)
+        self._check(self.lib.gd_radius_model_train(self.h, C.c_void_p(features.data_ptr()),
+                                                   C.c_void_p(kth_d2.data_ptr()), int(features.shape[0]),
+                                                   int(iterations), int(batch), float(lr), C.byref(loss), _stream()),
+                    "gd_radius_model_train")
+        return float(loss.value)
+
+    def gradient(self, features, kth_d2):
+        torch = _torch()
+        g = torch.empty(self.N_PARAMS, dtype=torch.float32, device=features.device)
+        loss = C.c_float(0.0)
+        self._check(self.lib.gd_radius_model_gradient(self.h, C.c_void_p(features.data_ptr()),
+                                                      C.c_void_p(kth_d2.data_ptr()), int(features.shape[0]),
+                                                      C.c_void_p(g.data_ptr()), C.byref(loss), _stream()),
+                    "gd_radius_model_gradient")
+        return g, float(loss.value)
+
+    def calibrate(self, features, kth_d2, quantile: float = 0.999) -> float:
+        m = C.c_float(0.0)
+        self._check(self.lib.gd_radius_model_calibrate(self.h, C.c_void_p(features.data_ptr()),
+                                                       C.c_void_p(kth_d2.data_ptr()), int(features.shape[0]),
+                                                       float(quantile), C.byref(m), _stream()),
+                    "gd_radius_model_calibrate")
+        return float(m.value)
+
+    def predict(self, features, out=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(features.shape[0], dtype=torch.float32, device=features.device)
+        self._check(self.lib.gd_radius_model_predict(self.h, C.c_void_p(features.data_ptr()), int(features.shape[0]),
+                                                     C.c_void_p(out.data_ptr()), _stream()),
+                    "gd_radius_model_predict")
+        return out
+
+    def get(self):
+        p = np.zeros(self.N_PARAMS, np.float32)
+        norm = np.zeros(17, np.float32)
+        self._check(self.lib.gd_radius_model_get(self.h, p.ctypes.data, norm.ctypes.data), "gd_radius_model_get")
+        return p, norm
+
+    def set(self, params=None, norm=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        nm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        self._check(self.lib.gd_radius_model_set(self.h, None if p is None else p.ctypes.data,
+                                                 None if nm is None else nm.ctypes.data), "gd_radius_model_set")
+
+
 def rng_state_bytes() -> int:
     return int(_lib.load().gd_rng_state_bytes())
 

@@ -150,6 +150,62 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
                          int32_t *dev_codes, double *dev_measure, float *dev_kth_d2,
                          unsigned long long *dev_stats);
 
+/* Keplerian azimuthal advance of every active particle by dt: phi += Omega_K(R) dt wrapped into
+ * [x_min, x_max) (the orbital part of the reference's transport step, _transport.cuh, without drag,
+ * radiation or diffusion).  Invalidates the geometry: positions changed. */
+gd_status gd_drift_keplerian(gd_handle *h, gd_particle *dev_particle, double dt);
+
+/*
+ * Learned search-radius proposal.  No counterpart in the reference: it seeds gd_knn_bounded,
+ * whose fallback keeps the neighbour lists identical to the plain query.
+ *
+ * Features (8 per owner, float32, by particle index): log2(1 + active sites in the owner's Morton
+ * cell) at 3 levels, log(y/R_0), (polar angle - pi/2)/h_g, log(size/S_0), log of the owner's
+ * bucket weight sum over the mean bucket weight, log(sqrt(previous K-th d^2)/R_0) (0 without one).
+ * Target: log(sqrt(K-th d^2)/R_0).  Network: 8 -> 64 -> 64 -> 1 with GELU, BF16 weights, FP32
+ * accumulation, standardised inputs; trained with Adam on MSE by this library's kernels.  The
+ * proposed radius is R_0 exp(prediction + margin), the margin being the calibrated quantile of the
+ * training residuals.
+ */
+typedef struct gd_radius_model gd_radius_model;
+enum { GD_RADIUS_FEATURES = 8, GD_RADIUS_PARAMS = 4801 };
+
+/* A fresh model (seeded initialisation) for a swarm whose length unit is R_0. */
+gd_status gd_radius_model_create(unsigned long long seed, double R_0, gd_radius_model **out);
+void      gd_radius_model_destroy(gd_radius_model *m);
+
+/* Features of every owner of the handle's current geometry (call after gd_geometry_build).
+ * dev_prev_kth_d2 (may be NULL) is the previous step's K-th d^2 by particle index; total_mass
+ * is the swarm's represented mass.  dev_features is [n_p][8]. */
+gd_status gd_radius_features(gd_handle *h, const gd_particle *dev_particle, const float *dev_prev_kth_d2,
+                             double total_mass, float *dev_features);
+
+/* `iterations` Adam steps (learning rate lr) on minibatches of `batch` owners drawn uniformly
+ * from the n rows of (dev_features, dev_kth_d2); rows with kth_d2 <= 0 carry no weight.  The
+ * first call also fixes the input standardisation from these rows.  *loss receives the mean
+ * squared error of the last minibatch (host pointer, may be NULL).  Runs on `stream`. */
+gd_status gd_radius_model_train(gd_radius_model *m, const float *dev_features, const float *dev_kth_d2, int n,
+                                int iterations, int batch, float lr, float *loss, void *stream);
+
+/* Mean-squared-error loss and its gradient with respect to the GD_RADIUS_PARAMS parameters over
+ * all n rows (no update): dev_grad [GD_RADIUS_PARAMS], *loss on the host. */
+gd_status gd_radius_model_gradient(gd_radius_model *m, const float *dev_features, const float *dev_kth_d2, int n,
+                                   float *dev_grad, float *loss, void *stream);
+
+/* Set the radius margin to the `quantile` (e.g. 0.999) of target - prediction over the rows
+ * with kth_d2 > 0; *margin receives it (host pointer, may be NULL). */
+gd_status gd_radius_model_calibrate(gd_radius_model *m, const float *dev_features, const float *dev_kth_d2, int n,
+                                    double quantile, float *margin, void *stream);
+
+/* Proposed radius R_0 exp(prediction + margin) per row into dev_radius [n] (float32). */
+gd_status gd_radius_model_predict(gd_radius_model *m, const float *dev_features, int n, float *dev_radius,
+                                  void *stream);
+
+/* Copy the FP32 master parameters (and standardisation: 8 means, 8 scales, margin) out of or into
+ * the model; host buffers of GD_RADIUS_PARAMS and 17 floats. */
+gd_status gd_radius_model_get(const gd_radius_model *m, float *params, float *norm17);
+gd_status gd_radius_model_set(gd_radius_model *m, const float *params, const float *norm17);
+
 /* Copy the site-init outputs of the last gd_geometry_build to caller device buffers (any may be
  * NULL): sites [n_p] x (x, y, z, code bits) as float4, search radius q [n_p] (0 when inactive),
  * active flags [n_p] (the reference's dev_kdtree_node cartesian / dev_search_dist /

@@ -1,0 +1,140 @@
+"""Learned search-radius proposal on the GPU, checked against the CPU oracle (oracle/mlp.py).
+
+Bars:
+  * gradient of the device backward kernel vs the float64 oracle on the same BF16 weights:
+    |g_dev - g_ref| <= 2e-3 * max|g_ref| per parameter block (FP32 accumulation over 4096 rows);
+  * device forward vs oracle: log-radius within 1e-4 absolute;
+  * features: log(y/R_0), log(size/S_0) within 1e-6 relative of float32 numpy, Morton-cell
+    occupancies equal to a numpy recount on the same quantisation;
+  * a trained and calibrated model seeds gd_knn_bounded with neighbour lists bit-identical to the
+    plain query, while scanning fewer candidates (what the network buys over the plain walk).
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _swarm(gd, n=1 << 16, seed=3):
+    import torch
+
+    from gamedev_b200 import workloads
+
+    cfg = workloads.config("c3_learned_3d")
+    p = workloads.particles("c3_learned_3d", n=n, seed=seed)
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+    torch.cuda.synchronize()
+    return cfg, p, sw, dp, codes, kth, mass
+
+
+def test_radius_gradient_matches_oracle(gd, cuda):
+    import torch
+
+    from oracle import mlp
+
+    cfg, p, sw, dp, codes, kth, mass = _swarm(gd)
+    prev = kth * 1.1
+    feats = sw.radius_features(dp, prev, mass)
+    rows = 4096
+    f = feats[:rows].contiguous()
+    k = kth[:rows].contiguous()
+    model = gd.RadiusModel(cfg.R_0, seed=11)
+    g, loss = model.gradient(f, k)
+    torch.cuda.synchronize()
+    params, norm = model.get()
+    ref_loss, ref_g = mlp.loss_and_grad(params, norm, f.cpu().numpy(), k.cpu().numpy(), cfg.R_0)
+    g = g.cpu().numpy().astype(np.float64)
+    assert loss == pytest.approx(ref_loss, rel=1e-4)
+    blocks = [(mlp.OW1, mlp.OB1), (mlp.OB1, mlp.OW2), (mlp.OW2, mlp.OB2), (mlp.OB2, mlp.OW3),
+              (mlp.OW3, mlp.OB3), (mlp.OB3, mlp.OB3 + 1)]
+    for a, b in blocks:
+        scale = max(np.abs(ref_g[a:b]).max(), 1e-30)
+        assert np.abs(g[a:b] - ref_g[a:b]).max() <= 2e-3 * scale, (a, b)
+
+
+def test_radius_forward_matches_oracle(gd, cuda):
+    import torch
+
+    from oracle import mlp
+
+    cfg, p, sw, dp, codes, kth, mass = _swarm(gd)
+    feats = sw.radius_features(dp, kth, mass)
+    model = gd.RadiusModel(cfg.R_0, seed=5)
+    model.train(feats, kth, iterations=50, batch=4096, lr=3e-3)
+    r = model.predict(feats)
+    torch.cuda.synchronize()
+    params, norm = model.get()
+    ref = mlp.predict_log(params, norm, feats[:2000].cpu().numpy()) + norm[16]
+    got = np.log(r[:2000].cpu().numpy().astype(np.float64) / cfg.R_0)
+    assert np.abs(got - ref).max() < 1e-4
+
+
+def test_radius_features_match_numpy(gd, cuda):
+    import torch
+
+    from gamedev_b200 import workloads
+
+    cfg, p, sw, dp, codes, kth, mass = _swarm(gd, n=1 << 15)
+    feats = sw.radius_features(dp, kth, mass).cpu().numpy()
+    site4, q, active = (t.cpu().numpy() for t in sw.get_sites())
+    act = active.astype(bool)
+    np.testing.assert_allclose(feats[act, 3], np.log(p[act, 1] / cfg.R_0), rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(feats[act, 5], np.log(p[act, 6] / cfg.S_0), rtol=1e-6, atol=1e-6)
+    k = kth.cpu().numpy()
+    np.testing.assert_allclose(feats[act, 7], 0.5 * np.log(k[act].astype(np.float64)) - math.log(cfg.R_0),
+                               rtol=1e-5, atol=1e-5)
+    # Morton occupancy recount with the device quantisation (float32 arithmetic)
+    half = np.float32(1.0001 * cfg.y_max)
+    scale = np.float32(2097152.0) / (np.float32(2.0) * half)
+    xyz = site4[:, :3]
+    q3 = np.clip(((xyz + half) * scale).astype(np.int64), 0, 2097151)
+    for f_idx, level in enumerate((9, 12, 15)):
+        cell = q3[act] >> (21 - level)
+        keys = (cell[:, 0] << 42) | (cell[:, 1] << 21) | cell[:, 2]
+        _, inv, cnt = np.unique(keys, return_inverse=True, return_counts=True)
+        expect = np.log2(1.0 + cnt[inv]).astype(np.float32)
+        np.testing.assert_allclose(feats[act, f_idx], expect, rtol=1e-6)
+
+
+def test_learned_radius_is_exact_and_scans_less(gd, cuda):
+    """Online training over drifted steps, calibration, then a radius-bounded query: identical
+    neighbour lists to the plain query, few fallbacks, fewer candidate offers than the plain walk."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = 1 << 18
+    cfg, p, sw, dp, codes, kth, mass = _swarm(gd, n=n)
+    model = gd.RadiusModel(cfg.R_0, seed=7)
+    dt = 0.02 * workloads.orbital_time()
+    prev = kth.clone()
+    for _ in range(6):
+        sw.drift_keplerian(dp, dt)
+        sw.col_site_init(dp)
+        c, m_, k = torch.empty_like(codes), torch.empty(n, dtype=torch.float64, device="cuda"), torch.empty_like(kth)
+        sw.col_cache_get(dp, c, m_, k)
+        feats = sw.radius_features(dp, prev, mass)
+        model.train(feats, k, iterations=150, batch=16384, lr=2e-3)
+        prev = k
+    margin = model.calibrate(feats, k, 0.999)
+    # a fresh step: plain vs learned
+    sw.drift_keplerian(dp, dt)
+    sw.col_site_init(dp)
+    feats = sw.radius_features(dp, prev, mass)
+    radius = model.predict(feats)
+    st_plain = torch.zeros(4, dtype=torch.int64, device="cuda")
+    st_learn = torch.zeros(4, dtype=torch.int64, device="cuda")
+    c0, c1 = torch.empty_like(codes), torch.empty_like(codes)
+    sw.col_cache_get_bounded(dp, None, c0, None, None, st_plain)
+    sw.col_cache_get_bounded(dp, radius, c1, None, None, st_learn)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    fallbacks = int(st_learn[3].item())
+    assert fallbacks <= 0.01 * n, (fallbacks, margin)
+    assert int(st_learn[2].item()) < 0.8 * int(st_plain[2].item())
