@@ -79,6 +79,7 @@ SIGNATURES = {
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "gd_drift_keplerian": (C.c_int, [_P, _P, C.c_double]),
+    "gd_pair_rates": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, _P]),
     "gd_radius_model_create": (C.c_int, [C.c_ulonglong, C.c_double, C.POINTER(_P)]),
     "gd_radius_model_destroy": (None, [_P]),
     "gd_radius_features": (C.c_int, [_P, _P, _P, C.c_double, _P]),

@@ -237,6 +237,15 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
     return done(h, s);
 }
 
+gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int32_t *dev_owner_ids, int count,
+                        double total_dust_mass, double *dev_out) {
+    if (!h || !dev_particle || !dev_owner_ids || !dev_out || count < 0 || !(total_dust_mass > 0))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer, negative count or non-positive mass");
+    if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "gd_pair_rates needs a neighbour cache");
+    return done(h, gd::pair_rates(h->m, dev_owner_ids, count, dev_particle, h->codes.ptr, h->measure.ptr,
+                                  h->geo.active.ptr, total_dust_mass, h->n, dev_out, h->stream));
+}
+
 gd_status gd_drift_keplerian(gd_handle *h, gd_particle *dev_particle, double dt) {
     if (!h || !dev_particle || !std::isfinite(dt)) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer or bad dt");
     h->geo.launches += 1;

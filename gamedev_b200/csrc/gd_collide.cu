@@ -334,6 +334,59 @@ __global__ void __launch_bounds__(128) k_bath_rate(Model m, RateArgs a) {
     }
 }
 
+// Per-pair terms of the bath-start rate (the values k_bath_rate folds) against the current
+// particle state as reservoir: out[(slot*K + s)*5 + {0..4}] = rate, rate*mean, rate*second,
+// maximum, pair speed.  One thread per (owner, neighbour slot).
+__global__ void k_pair_rates(Model m, const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
+                             const int32_t *__restrict__ codes, const double *__restrict__ measure,
+                             const unsigned char *__restrict__ active, double lambda0, double *__restrict__ out) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int K = m.n_k;
+    if (t >= static_cast<long long>(count) * K) return;
+    const int slot = static_cast<int>(t / K), s = static_cast<int>(t % K);
+    const int i = ids[slot];
+    double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0, vrel = 0.0;
+    const int nb = codes[static_cast<size_t>(i) * K + s];
+    const double meas = measure[i];
+    if (active[i] && nb >= 0 && meas > 0.0) {
+        OwnerCtx o;
+        o.y = part[i].position[1];
+        o.z = part[i].position[2];
+        const double R = cyl_R(m, o.y, o.z);
+        o.H_i = R * get_hg(m, R);
+        o.measure = meas;
+        o.lambda0 = lambda0;
+        if (use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM) o.env = make_env(m, o.y, o.z);
+        const int j = nb / 3;
+        const double size_i = part[i].par_size, size_j = part[j].par_size;
+        double pr = pair_rate(m, o, size_i, size_j, part[j].par_numr, part, j, vrel);
+        double mean = 0.0, sec = 0.0, maxi = 0.0;
+        pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+        mx = pr > 0.0 ? maxi : 0.0;
+        c = pr * mean;
+        sc = pr * sec;
+        r = pr;
+    }
+    double *o5 = out + static_cast<size_t>(t) * 5;
+    o5[0] = r;
+    o5[1] = c;
+    o5[2] = sc;
+    o5[3] = mx;
+    o5[4] = vrel;
+}
+
+Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, int n, double *out,
+                  cudaStream_t s) {
+    if (count <= 0) return Status::ok();
+    const double lambda0 = n / static_cast<double>(m.n_k) / total_dust_mass;
+    const long long threads = static_cast<long long>(count) * m.n_k;
+    k_pair_rates<<<static_cast<unsigned int>((threads + 255) / 256), 256, 0, s>>>(m, ids, count, part, codes, measure,
+                                                                                  active, lambda0, out);
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
 // _get_col_uniform (inc/swarm/_col_rates.cuh:145-149)
 __device__ __forceinline__ double col_uniform(curandState *st) {
     return fmin(curand_uniform_double(st), nextafter(1.0, 0.0));

@@ -90,6 +90,11 @@ struct Collider {
 Status collider_alloc(Collider &c, const Model &m, int n);
 void collider_reset_state(Collider &c);
 
+// per-pair terms of the bath-start rate for the listed owners (diagnostics and parity checks)
+Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, int n, double *out,
+                  cudaStream_t s);
+
 // evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539)
 Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
                           const int32_t *codes, const double *measure, const unsigned char *active,

@@ -333,10 +333,7 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
     float cut = valid ? lim2 : -1.0f;         // d^2 bound of an acceptable candidate
     long long st_leaves = 0, st_nodes = 0, st_offers = 0;
 
-    // warp centre (own bucket box) orders child visits
-    const int own_node = a.leaf_slots - 1 + leaf;
-    const float4 own_lo = a.lo[own_node], own_hi = a.hi[own_node];
-    const float3 ctr = make_float3(0.5f * (own_lo.x + own_hi.x), 0.5f * (own_lo.y + own_hi.y), 0.5f * (own_lo.z + own_hi.z));
+    const int depth_leaves = a.leaf_slots;  // leaves under the root (a power of two)
 
     auto offer = [&](unsigned long long key) {
         if (cnt < K) {
@@ -413,16 +410,16 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
                 if (lf < leaf - kPrescan || lf > leaf + kPrescan) scan_leaf(lf);
                 continue;
             }
+            // Children are tested when popped.  Visit first the child whose leaf range lies closer,
+            // in Morton order, to the warp's own bucket: its sites are the nearer ones.
+            const int depth = 31 - __clz(node + 1);
+            const int span = depth_leaves >> depth;  // leaves under this node
+            const int start = (node + 1 - (1 << depth)) * span;
             const int c0 = 2 * node + 1, c1 = 2 * node + 2;
-            const float4 l0 = a.lo[c0], h0 = a.hi[c0], l1 = a.lo[c1], h1 = a.hi[c1];
-            const bool need0 = __any_sync(0xffffffffu, box_dist2(qp, l0, h0) <= cut);
-            const bool need1 = __any_sync(0xffffffffu, box_dist2(qp, l1, h1) <= cut);
-            const float e0 = box_dist2(ctr, l0, h0), e1 = box_dist2(ctr, l1, h1);
-            const int nearc = (e0 <= e1) ? c0 : c1, farc = (e0 <= e1) ? c1 : c0;
-            const bool need_near = (e0 <= e1) ? need0 : need1, need_far = (e0 <= e1) ? need1 : need0;
+            const bool left_near = leaf < start + (span >> 1);
             // the stack holds at most one pending sibling per tree level (<= 31) plus one
-            if (need_far) stack[sp++] = farc;
-            if (need_near) stack[sp++] = nearc;
+            stack[sp++] = left_near ? c1 : c0;
+            stack[sp++] = left_near ? c0 : c1;
             __syncwarp();
         }
     };

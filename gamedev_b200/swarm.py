@@ -154,6 +154,15 @@ class SwarmCollision:
                                                           (cached, time, events, size_old, numr_old))))
         return cached, time, events, size_old, numr_old
 
+    def pair_rates(self, particles, owner_ids, total_mass: float):
+        """Per-pair bath-start terms [count, n_k, 5] = rate, rate*mean, rate*second, maximum, speed."""
+        torch = _torch()
+        count = int(owner_ids.shape[0])
+        out = torch.empty((count, self.n_k, 5), dtype=torch.float64, device=particles.device)
+        self._check(self.lib.gd_pair_rates(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(owner_ids)), count,
+                                           float(total_mass), C.c_void_p(_ptr(out))))
+        return out
+
     def launch_count(self) -> int:
         return int(self.lib.gd_launch_count(self.h))
 

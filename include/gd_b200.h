@@ -264,6 +264,13 @@ gd_status gd_rng_uniforms(const void *dev_rng, int n, int count, double *dev_out
 gd_status gd_get_owner_state(gd_handle *h, double *dev_cached4, double *dev_time, int32_t *dev_events,
                              double *dev_size_old, double *dev_numr_old);
 
+/* The per-pair terms col_bath_rate folds (src/swarm/col_bath_rate.cu:30-58: _get_col_chain_rate /
+ * measure times the outcome factor of _erosion_outcome_moments) for `count` owners listed in
+ * dev_owner_ids, with the current particle state as reservoir and the handle's neighbour cache:
+ * dev_out[count][n_k][5] = rate, rate*mean, rate*second, maximum, pair speed. */
+gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int32_t *dev_owner_ids, int count,
+                        double total_dust_mass, double *dev_out);
+
 /* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
 long long gd_launch_count(const gd_handle *h);
 

@@ -148,8 +148,10 @@ def test_gpu_radius_bounded_query_is_exact(gd, cuda):
     torch.cuda.synchronize()
     assert torch.equal(codes, codes_b)
     assert torch.equal(measure, measure_b) and torch.equal(kth, kth_b)
-    # a short radius falls back unless q itself is shorter than the proposal (then no fallback is needed)
-    expect = int((short & (radius < q) & (active > 0)).sum().item())
+    # an owner falls back when its radius is shorter than q and fewer than K sites lie inside:
+    # every short proposal, and any proposal for an owner whose row is not full even at q
+    incomplete = (codes < 0).any(dim=1)
+    expect = int(((short | incomplete) & (radius < q) & (active > 0)).sum().item())
     assert int(stats[3].item()) == expect
     # the plain query through the bounded entry point, with counters
     stats0 = torch.zeros(4, dtype=torch.int64, device="cuda")
