@@ -109,6 +109,14 @@ __device__ __forceinline__ double oc07_speed(double stokes_i, double stokes_j, d
     return sqrt(v2);
 }
 
+// si*fi - sj*fj of the radial drift (_collision.cuh:305, _col_rates.cuh:133), with the contraction
+// pinned to one fused multiply-add: fma(si, fi, -(sj*fj)).  Under FMA contraction this difference is
+// not zero for identical grains (it is the rounding residual of sj*fj), which gives a self pair a
+// tiny positive speed; pinning it makes the host oracle reproduce the device value exactly.
+__device__ __forceinline__ double drift_difference(double si, double fi, double sj, double fj) {
+    return __fma_rn(si, fi, -__dmul_rn(sj, fj));
+}
+
 // _cache_query_environment (inc/swarm/_col_rates.cuh:13-24)
 __device__ __forceinline__ Env make_env(const Model &m, double y, double z) {
     double R = cyl_R(m, y, z);
@@ -140,7 +148,7 @@ __device__ __forceinline__ double cached_pair_speed(const Model &m, const Env &e
     sj /= e.strat;
     double fi = 1.0 / (1.0 + si * si);
     double fj = 1.0 / (1.0 + sj * sj);
-    double dvr = 2.0 * e.vn * (si * fi - sj * fj);
+    double dvr = 2.0 * e.vn * drift_difference(si, fi, sj, fj);
     double dvphi = e.vn * (fi - fj);
     double dvz = e.Z * e.omega * (fmin(si, 0.5) - fmin(sj, 0.5));
     double vt = oc07_speed(si, sj, e.re_inv_sqrt, e.vg_sq);
@@ -161,7 +169,7 @@ __device__ __forceinline__ double direct_pair_speed(const Model &m, double y, do
     double vn = -get_eta(m, R, Z, h) * R * omega;
     double fi = 1.0 / (1.0 + si * si);
     double fj = 1.0 / (1.0 + sj * sj);
-    double dvr = 2.0 * vn * (si * fi - sj * fj);
+    double dvr = 2.0 * vn * drift_difference(si, fi, sj, fj);
     double dvphi = vn * (fi - fj);
     double dvz = Z * omega * (fmin(si, 0.5) - fmin(sj, 0.5));
     double sigma_local = sigma_g(m, R) * gas_strat(R, Z, h);

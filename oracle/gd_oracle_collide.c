@@ -109,7 +109,7 @@ double gdo_pair_speed_cached(const gd_config *c, const double *e, double size_i,
     sj /= e[4];
     double fi = 1.0 / (1.0 + si * si);
     double fj = 1.0 / (1.0 + sj * sj);
-    double dvr = 2.0 * e[2] * (si * fi - sj * fj);
+    double dvr = 2.0 * e[2] * fma(si, fi, -(sj * fj));  /* the device's pinned contraction */
     double dvphi = e[2] * (fi - fj);
     double dvz = e[0] * e[1] * (fmin(si, 0.5) - fmin(sj, 0.5));
     double vt = oc07(si, sj, e[6], e[7]);
@@ -136,7 +136,7 @@ double gdo_pair_speed_direct(const gd_config *c, double y, double z, double size
     double vn = -get_eta(c, R, Z, h) * R * omega;
     double fi = 1.0 / (1.0 + si * si);
     double fj = 1.0 / (1.0 + sj * sj);
-    double dvr = 2.0 * vn * (si * fi - sj * fj);
+    double dvr = 2.0 * vn * fma(si, fi, -(sj * fj));  /* the device's pinned contraction */
     double dvphi = vn * (fi - fj);
     double dvz = Z * omega * (fmin(si, 0.5) - fmin(sj, 0.5));
     double sigma_local = sigma_g(c, R) * gas_strat(R, Z, h);

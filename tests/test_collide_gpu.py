@@ -21,6 +21,11 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 
 RATE_RTOL = 1e-12
+# The jump moments of catastrophic fragmentation, 8 - (4L^2 + 8L) exp(-L)/(-expm1(-L)) and its
+# first-moment analogue, cancel almost completely for L just above the 1e-3 series switch
+# (_col_event.cuh:286-298): a last-bit difference between host and device exp/expm1 grows by
+# ~1/L^2 there, so moment terms carry this looser bar.
+MOMENT_RTOL = 1e-8
 STATE_RTOL = 1e-12
 
 
@@ -99,7 +104,8 @@ def test_operator_one_wave_matches_oracle_chain(gd, cuda, oracle_lib, idx):
 
     # bath-start moments
     act = active.astype(bool)
-    np.testing.assert_allclose(cached[act], cached_o[act], rtol=RATE_RTOL, atol=0, err_msg=name)
+    np.testing.assert_allclose(cached[act][:, [0, 3]], cached_o[act][:, [0, 3]], rtol=RATE_RTOL, atol=0, err_msg=name)
+    np.testing.assert_allclose(cached[act][:, 1:3], cached_o[act][:, 1:3], rtol=MOMENT_RTOL, atol=0, err_msg=name)
 
     n_events = 0
     for i in np.nonzero(act)[0]:
@@ -216,7 +222,15 @@ def test_pair_rates_match_oracle(gd, cuda, oracle_lib, idx):
                 r *= f
                 want = np.array([r, r * mean, r * sec, mx if r > 0 else 0.0, v])
             g = got[a, s_]
-            ok = np.all((g == want) | (np.abs(g - want) <= 1e-12 * np.maximum(np.abs(g), np.abs(want))))
+            tol = np.array([RATE_RTOL, MOMENT_RTOL, MOMENT_RTOL, RATE_RTOL, RATE_RTOL])
+            ok = np.all((g == want) | (np.abs(g - want) <= tol * np.maximum(np.abs(g), np.abs(want))))
             if not ok:
-                bad.append((int(i), s_, g.tolist(), want.tolist()))
-    assert not bad, (name, len(bad), bad[:4])
+                bad.append((int(i), s_, int(c), float(measure[i]), g, want))
+    if bad:
+        lines = [f"{name}: {len(bad)} of {len(ids) * cfg.n_k} pairs differ"]
+        for i, s_, c, mv, g, w in bad[:4]:
+            j = c // 3
+            lines.append(f"owner {i} slot {s_} code {c} measure {mv:.17g} si {p[i, 6]:.17g} sj {p[j, 6]:.17g}")
+            lines.append("  gpu    " + " ".join(f"{v:.17g}" for v in g))
+            lines.append("  oracle " + " ".join(f"{v:.17g}" for v in w))
+        pytest.fail("\n".join(lines))

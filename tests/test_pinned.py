@@ -67,6 +67,11 @@ def test_pair_speed_matches_reference_python_formulas(gd, oracle_lib, colphys):
         y, z = math.hypot(R, Z), math.atan2(R, Z)
         got = oracle_lib.pair_speed(cfg, y, z, row["size_i"], row["size_j"])
         want = row["speed"]
+        if want == 0.0:
+            # identical grains: numpy's si*fi - sj*fj is exactly 0, while the pinned fused
+            # multiply-add leaves the rounding residual of sj*fj (2*vn*ulp(si*fi), < 1e-18 here)
+            assert abs(got) < 1e-18, row
+            continue
         err = abs(got - want) / max(abs(want), 1e-300)
         worst = max(worst, err)
         assert err < 2e-11, row
