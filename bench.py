@@ -119,6 +119,13 @@ def dist_init(n_gpus):
     return world, rank, local
 
 
+def _reduce_device():
+    """Where a rank's scalar goes for a collective: host memory under gloo, the GPU under nccl."""
+    import torch.distributed as dist
+
+    return "cpu" if dist.get_backend() == "gloo" else "cuda"
+
+
 def barrier(world):
     import torch
 
@@ -126,7 +133,8 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def reduce_max(x, world):
@@ -136,7 +144,7 @@ def reduce_max(x, world):
         return x
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -148,7 +156,7 @@ def reduce_sum(x, world):
         return x
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
