@@ -104,3 +104,21 @@ def test_measure_of_full_ball_inside_domain(oracle_lib, gd):
     m = oracle_lib.ball_measure(cfg, p, np.ones(1, np.uint8), np.array([0.01 ** 2], np.float32))
     r = math.sqrt(float(np.float32(0.01 ** 2)))
     assert m[0] == pytest.approx(4.0 * math.pi * r ** 3 / 3.0, rel=1e-15)
+
+
+def test_reference_heap_rows_sort_to_canonical_order(oracle_lib, all_cases):
+    """oracle.ref.refknn.canonical turns a heap-ordered reference cache (any row permutation, empty
+    slots carrying d^2 = q^2) into the ascending (d^2, code) rows the B200 search writes."""
+    from oracle.ref import refknn
+
+    name, cfg, p = all_cases[6]  # radius-bounded: rows with fewer than K neighbours
+    site4, q, active, _ = oracle_lib.site_init(cfg, p)
+    codes, d2 = oracle_lib.knn_brute(site4, q, active, cfg.n_k)
+    rng = np.random.default_rng(5)
+    perm = np.argsort(rng.random(codes.shape), axis=1)
+    hc = np.take_along_axis(codes, perm, axis=1)
+    hd = np.take_along_axis(np.where(codes >= 0, d2, (q * q)[:, None]).astype(np.float32), perm, axis=1)
+    c, _, kth = refknn.canonical(hc, hd)
+    assert (codes < 0).any(), name
+    assert np.array_equal(c, codes)
+    assert np.array_equal(kth.view(np.uint32), oracle_lib.kth_from_rows(codes, d2).view(np.uint32))
