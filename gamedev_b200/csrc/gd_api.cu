@@ -390,3 +390,180 @@ gd_status gd_last_operator_stats(const gd_handle *h, gd_operator_stats *out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// gd_knn_static: the neighbour search (site init + Morton radix sort + bucket tree + exact top-K)
+// for swarms of at most kStaticParticles particles, with every scratch array carved from one fixed
+// device array instead of a handle's allocations.  It serves callers that cannot allocate device
+// memory while they run: hosts that hand the whole device to their own memory pool at start-up and
+// allow no allocation outside it, and time loops that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree can imply.  The build and query kernels are the ones
+// gd_geometry_build/gd_knn run; only where their scratch lives differs.
+// ---------------------------------------------------------------------------------------------
+#include <mutex>
+
+namespace gd {
+namespace {
+
+constexpr int kStaticParticles = 1 << 16;  // maximum n_p of gd_knn_static
+constexpr int kStaticSort = (kStaticParticles + kRadixTile - 1) / kRadixTile * kRadixTile;
+constexpr int kStaticLeafSlots = kStaticParticles / kLeaf;  // a power of two: 2048
+static_assert((kStaticLeafSlots & (kStaticLeafSlots - 1)) == 0, "leaf slots must be a power of two");
+
+constexpr size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+// Fixed layout of the scratch at the maximum size; a smaller swarm uses a prefix of each array.
+constexpr size_t kOffSite = 0;
+constexpr size_t kOffQ = kOffSite + round256(sizeof(float4) * kStaticParticles);
+constexpr size_t kOffActive = kOffQ + round256(sizeof(float) * kStaticParticles);
+constexpr size_t kOffKeyA = kOffActive + round256(kStaticParticles);
+constexpr size_t kOffKeyB = kOffKeyA + round256(sizeof(unsigned long long) * kStaticSort);
+constexpr size_t kOffValA = kOffKeyB + round256(sizeof(unsigned long long) * kStaticSort);
+constexpr size_t kOffValB = kOffValA + round256(sizeof(unsigned int) * kStaticSort);
+constexpr size_t kOffHist = kOffValB + round256(sizeof(unsigned int) * kStaticSort);
+constexpr size_t kOffSorted = kOffHist + round256(sizeof(unsigned int) * 256 * (kStaticSort / kRadixTile));
+constexpr size_t kOffNodeLo = kOffSorted + round256(sizeof(float4) * kStaticLeafSlots * kLeaf);
+constexpr size_t kOffNodeHi = kOffNodeLo + round256(sizeof(float4) * 2 * kStaticLeafSlots);
+constexpr size_t kOffSubLo = kOffNodeHi + round256(sizeof(float4) * 2 * kStaticLeafSlots);
+constexpr size_t kOffSubHi = kOffSubLo + round256(sizeof(float4) * kStaticLeafSlots * kSubs);
+constexpr size_t kOffCounters = kOffSubHi + round256(sizeof(float4) * kStaticLeafSlots * kSubs);
+constexpr size_t kStaticBytes = kOffCounters + round256(sizeof(int) * 4);  // 4,407,552 bytes
+static_assert(kStaticBytes == 4407552, "scratch size stated in gd_b200.h");
+
+constexpr int kStaticMaxDevices = 64;
+
+}  // namespace
+
+// The scratch.  Every device that loads this library holds it until the process exits.  In host
+// code this name is only a host-side stand-in: kernels receive the device address resolved below.
+static __device__ __align__(256) unsigned char g_knn_scratch[kStaticBytes];
+
+namespace {
+
+std::mutex g_scratch_mu;
+unsigned char *g_scratch_addr[kStaticMaxDevices] = {};
+
+// Device address of g_knn_scratch on the current device, resolved once per device with that device
+// current (the first call on a device may load this library's device code there).
+Status static_scratch(unsigned char **out) {
+    int dev = -1;
+    GD_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) {
+        Status st;
+        st.code = GD_ERR_CAPACITY;
+        st.detail = dev;
+        st.msg = "gd_knn_static supports device ordinals below 64";
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_knn_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "resolve the gd_knn_static scratch");
+        g_scratch_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return Status::ok();
+}
+
+// Points a Geometry's buffers into the fixed scratch and detaches them again on scope exit, so
+// that the DevBuf destructors never free memory they do not own.
+struct BorrowedGeometry {
+    Geometry g;
+    BorrowedGeometry(const Model &m, int n, unsigned char *base) {
+        g.n = n;
+        g.n_sort = (n + kRadixTile - 1) / kRadixTile * kRadixTile;
+        const int leaves = (n + kLeaf - 1) / kLeaf;
+        int slots = 1;
+        while (slots < leaves) slots <<= 1;
+        g.leaf_slots = slots;
+        g.key_bits = 21 * m.dim;
+        bind(g.site, base + kOffSite, n);
+        bind(g.q, base + kOffQ, n);
+        bind(g.active, base + kOffActive, n);
+        bind(g.key_a, base + kOffKeyA, g.n_sort);
+        bind(g.key_b, base + kOffKeyB, g.n_sort);
+        bind(g.val_a, base + kOffValA, g.n_sort);
+        bind(g.val_b, base + kOffValB, g.n_sort);
+        bind(g.hist, base + kOffHist, static_cast<size_t>(256) * (g.n_sort / kRadixTile));
+        bind(g.sorted, base + kOffSorted, static_cast<size_t>(g.leaf_slots) * kLeaf);
+        bind(g.node_lo, base + kOffNodeLo, 2 * static_cast<size_t>(g.leaf_slots));
+        bind(g.node_hi, base + kOffNodeHi, 2 * static_cast<size_t>(g.leaf_slots));
+        bind(g.sub_lo, base + kOffSubLo, static_cast<size_t>(g.leaf_slots) * kSubs);
+        bind(g.sub_hi, base + kOffSubHi, static_cast<size_t>(g.leaf_slots) * kSubs);
+        bind(g.counters, base + kOffCounters, 4);
+    }
+    ~BorrowedGeometry() {
+        detach(g.site); detach(g.q); detach(g.active);
+        detach(g.key_a); detach(g.key_b); detach(g.val_a); detach(g.val_b); detach(g.hist);
+        detach(g.sorted); detach(g.node_lo); detach(g.node_hi); detach(g.sub_lo); detach(g.sub_hi);
+        detach(g.counters);
+    }
+    BorrowedGeometry(const BorrowedGeometry &) = delete;
+    BorrowedGeometry &operator=(const BorrowedGeometry &) = delete;
+
+  private:
+    template <typename T>
+    static void bind(DevBuf<T> &b, unsigned char *at, size_t count) {
+        b.ptr = reinterpret_cast<T *>(at);
+        b.n = count;
+    }
+    template <typename T>
+    static void detach(DevBuf<T> &b) {
+        b.ptr = nullptr;
+        b.n = 0;
+    }
+};
+
+gd_status static_fail(const Status &s, long long *detail, char *msg, size_t msg_len) {
+    if (detail) *detail = s.detail;
+    if (msg && msg_len) {
+        const size_t k = s.msg.size() < msg_len - 1 ? s.msg.size() : msg_len - 1;
+        std::memcpy(msg, s.msg.data(), k);
+        msg[k] = '\0';
+    }
+    return s.code;
+}
+
+}  // namespace
+}  // namespace gd
+
+extern "C" gd_status gd_knn_static(const gd_config *cfg, const gd_particle *dev_particle, int n_p,
+                                   int32_t *dev_codes, double *dev_measure, float *dev_kth_d2, void *stream,
+                                   long long *detail, char *msg, size_t msg_len) {
+    using gd::Status;
+    if (detail) *detail = 0;
+    if (msg && msg_len) msg[0] = '\0';
+    Status st;
+    if (!cfg || !dev_particle || !dev_codes || !dev_measure || !dev_kth_d2) {
+        st.code = GD_ERR_INVALID_ARGUMENT;
+        st.msg = "gd_knn_static: null configuration, particle or output pointer";
+        return gd::static_fail(st, detail, msg, msg_len);
+    }
+    if (n_p > gd::kStaticParticles) {
+        st.code = GD_ERR_CAPACITY;
+        st.detail = n_p;
+        st.msg = "gd_knn_static: " + std::to_string(n_p) + " particles exceed its fixed scratch of " +
+                 std::to_string(gd::kStaticParticles) + " particles; use gd_create/gd_geometry_build/gd_knn";
+        return gd::static_fail(st, detail, msg, msg_len);
+    }
+    std::string why = validate(*cfg, n_p);
+    if (!why.empty()) {
+        st.code = GD_ERR_INVALID_ARGUMENT;
+        st.msg = "gd_knn_static: " + why;
+        return gd::static_fail(st, detail, msg, msg_len);
+    }
+    unsigned char *base = nullptr;
+    st = gd::static_scratch(&base);
+    if (!st) return gd::static_fail(st, detail, msg, msg_len);
+    const gd::Model m = gd::make_model(*cfg);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    gd::BorrowedGeometry bg(m, n_p, base);
+    // The scratch keeps whatever the previous call left.  geometry_build resets the four counters
+    // (active count, first bad index, two spare) on the stream before any kernel reads them; every
+    // other scratch array is written in full before it is read.
+    st = gd::geometry_build(bg.g, m, dev_particle, s);
+    if (st) st = gd::knn_query(bg.g, m, dev_particle, dev_codes, dev_measure, dev_kth_d2, s);
+    if (!st) return gd::static_fail(st, detail, msg, msg_len);
+    return GD_OK;
+}

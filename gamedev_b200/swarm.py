@@ -295,3 +295,22 @@ def particles_to_device(arr: np.ndarray, device="cuda:0"):
     torch = _torch()
     a = np.ascontiguousarray(arr).view(np.float64).reshape(-1, 8)
     return torch.from_numpy(a.copy()).to(device)
+
+
+STATIC_MAX_PARTICLES = 1 << 16  # gd_knn_static's fixed scratch
+
+
+def knn_static(cfg: GdConfig, particles, codes, measure, kth):
+    """Exact top-K through gd_knn_static, which allocates no device memory: for callers that may
+    not call cudaMalloc while they run (a host that owns the whole device through its own pool, or
+    a time loop that cannot take the synchronisation an allocation can cause).  Its scratch is a
+    fixed 4.4 MB device array, so at most 65536 particles.  The caller provides the outputs; calls
+    whose GPU work overlaps on one device race on the shared scratch."""
+    n = int(particles.shape[0])
+    detail = C.c_longlong(0)
+    msg = C.create_string_buffer(512)
+    r = _lib.load().gd_knn_static(C.byref(cfg), C.c_void_p(particles.data_ptr()), n, C.c_void_p(codes.data_ptr()),
+                                  C.c_void_p(measure.data_ptr()), C.c_void_p(kth.data_ptr()), _stream(),
+                                  C.byref(detail), msg, len(msg))
+    if r != _lib.GD_OK:
+        raise GdError(r, msg.value.decode(errors="replace"), int(detail.value))

@@ -274,6 +274,34 @@ gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int
 /* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
 long long gd_launch_count(const gd_handle *h);
 
+/*
+ * Handle-free exact top-K neighbour search that allocates no device memory.  No counterpart in
+ * the reference (whose col_site_init / col_cache_get run on the swarm's allocated buffers).
+ *
+ * For callers that cannot call cudaMalloc while they run: a host that gives the whole device to its
+ * own memory pool at start-up and permits no allocation outside it, or a time loop that cannot pay
+ * the device-wide synchronisation cudaMalloc/cudaFree can cause.  gd_create allocates per swarm;
+ * this entry point does not.
+ *
+ * Runs the same site init, Morton radix sort, bucket-tree build and top-K query as
+ * gd_geometry_build + gd_knn, and writes the same dev_codes [n_p][n_k], dev_measure [n_p] and
+ * dev_kth_d2 [n_p] (all three required, caller-allocated).  Its scratch is one fixed file-scope
+ * device array of 4,407,552 bytes, which every device that loads the library holds until the
+ * process exits; it bounds n_p to 65536.  A larger n_p returns GD_ERR_CAPACITY with a message,
+ * before any device work.  A non-finite particle returns GD_ERR_NONFINITE with its index in
+ * *detail.  detail and msg (msg_len bytes, NUL-terminated) may be NULL.
+ *
+ * The first call on each device, with that device current, looks up the scratch's device address
+ * (this can load the library's device code on that device); make that first call before any stream
+ * capture begins.  The call synchronises `stream` once (the non-finite screen) and returns with the
+ * query enqueued on it.  All calls on one device share the one scratch: calls whose GPU work
+ * overlaps (from several host threads, or on streams with no ordering between them) race and
+ * corrupt each other's results; order them on one stream or serialise them.
+ */
+gd_status gd_knn_static(const gd_config *cfg, const gd_particle *dev_particle, int n_p, int32_t *dev_codes,
+                        double *dev_measure, float *dev_kth_d2, void *stream, long long *detail, char *msg,
+                        size_t msg_len);
+
 #ifdef __cplusplus
 }
 #endif
