@@ -36,15 +36,17 @@ __host__ __device__ __forceinline__ double get_hg(const Model &m, double R) {
     return m.aspr_0 * pow(R / m.R_0, 0.5 * (m.idx_q + 1.0));
 }
 
-// Single-precision squared distance with the contraction pinned: ((dx*dx) + dy*dy) + dz*dz with
-// each addition fused into its product, the evaluation nvcc gives the reference's
-// dx*dx + dy*dy + dz*dz (morton_types.cuh:76-82, kdtree/math.h:110-111,227-228) under its
-// default -fmad=true.  The host oracle evaluates the same fmaf chain.
+// Single-precision squared distance with the contraction pinned to the evaluation nvcc gives the
+// reference's dx*dx + dy*dy + dz*dz (morton_types.cuh:76-82, kdtree/math.h:110-111,227-228) under
+// its default -fmad=true: the first product of dx*dx + dy*dy is fused (fma(dx, dx, dy*dy)), then
+// dz*dz is fused onto that sum.  The reference's compiled KD search on a B200 returns these bits
+// (checked neighbour by neighbour by the reference-GPU parity test).  The host oracle evaluates
+// the same fmaf chain.
 __device__ __forceinline__ float dist2(const float3 &q, const float3 &p) {
     const float dx = __fsub_rn(q.x, p.x);
     const float dy = __fsub_rn(q.y, p.y);
     const float dz = __fsub_rn(q.z, p.z);
-    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 // Lower bound of dist2 over a box, with the same operation chain: every per-axis gap is at most
@@ -54,7 +56,7 @@ __device__ __forceinline__ float box_dist2(const float3 &q, const float4 &lo, co
     const float dx = fmaxf(fmaxf(__fsub_rn(lo.x, q.x), 0.0f), __fsub_rn(q.x, hi.x));
     const float dy = fmaxf(fmaxf(__fsub_rn(lo.y, q.y), 0.0f), __fsub_rn(q.y, hi.y));
     const float dz = fmaxf(fmaxf(__fsub_rn(lo.z, q.z), 0.0f), __fsub_rn(q.z, hi.z));
-    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 // Spread the low 21 bits of v so that bit b lands on bit 3b.

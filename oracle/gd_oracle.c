@@ -75,7 +75,7 @@ float gdo_dist2(const float *a, const float *b) {
     float dx = a[0] - b[0];
     float dy = a[1] - b[1];
     float dz = a[2] - b[2];
-    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
 }
 
 static float box_dist2(const float *qp, const float *lo, const float *hi) {
@@ -86,7 +86,7 @@ static float box_dist2(const float *qp, const float *lo, const float *hi) {
         float m = a > 0.f ? a : 0.f;
         d[k] = m > b ? m : b;
     }
-    return fmaf(d[2], d[2], fmaf(d[1], d[1], d[0] * d[0]));
+    return fmaf(d[2], d[2], fmaf(d[0], d[0], d[1] * d[1]));
 }
 
 static uint64_t make_key(float d2, uint32_t code) {
