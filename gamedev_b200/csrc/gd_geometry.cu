@@ -89,8 +89,9 @@ __global__ void k_state_screen(int n, const gd_particle *__restrict__ part, int 
 }
 
 // ------------------------------------------------------------------------------------------------
-// LSD radix sort of (u64 key, u32 value), 8-bit digits, stable.  Three kernels per digit:
-// per-tile digit histogram, one exclusive scan over [digit][tile], stable scatter.
+// LSD radix sort of (u64 key, u32 value), 8-bit digits, stable.  Per digit: per-tile digit
+// histogram, exclusive scan over [digit][tile] (chunk-local scans, then the chunk totals), stable
+// scatter.
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const unsigned long long *__restrict__ key,
                                                               int shift, int tiles,
@@ -108,34 +109,63 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const unsigned lon
     hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of cnt[0..len) in place, one block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_scan_exclusive(unsigned int *__restrict__ cnt, int len) {
-    __shared__ unsigned int part[1024];
-    int chunk = (len + 1023) / 1024;
-    int b = threadIdx.x * chunk;
-    int e = min(len, b + chunk);
+// Exclusive scan of the 4096-entry chunk `chunk` of cnt[0..len) in place, 256 threads owning 16
+// consecutive entries each; `carry` is added to every entry.  Returns the chunk total to all threads.
+__device__ __forceinline__ unsigned int scan_chunk(unsigned int *__restrict__ cnt, int len, long long chunk,
+                                                   unsigned int carry) {
+    __shared__ unsigned int warp_tot[kRadixThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const long long first = chunk * kScanChunk + static_cast<long long>(t) * kScanItems;
+    unsigned int v[kScanItems];
     unsigned int sum = 0;
-    for (int i = b; i < e; ++i) sum += cnt[i];
-    part[threadIdx.x] = sum;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = (first + i < len) ? cnt[first + i] : 0u;
+        sum += v[i];
+    }
+    unsigned int x = sum;  // inclusive scan of the per-thread sums across the warp
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        unsigned int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+    unsigned int before = 0, total = 0;
+#pragma unroll
+    for (int j = 0; j < kRadixThreads / 32; ++j) {
+        const unsigned int wt = warp_tot[j];
+        before += (j < w) ? wt : 0u;
+        total += wt;
     }
-    unsigned int run = part[threadIdx.x] - sum;
-    for (int i = b; i < e; ++i) {
-        unsigned int v = cnt[i];
-        cnt[i] = run;
-        run += v;
+    unsigned int run = carry + before + x - sum;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (first + i < len) cnt[first + i] = run;
+        run += v[i];
     }
+    __syncthreads();  // warp_tot is reused by the next chunk
+    return total;
+}
+
+// Chunk-local exclusive scans of cnt[0..len); chunk totals to part[] (null when one chunk covers
+// cnt, which then holds the full exclusive scan).
+__global__ void __launch_bounds__(kRadixThreads) k_scan_chunks(unsigned int *__restrict__ cnt, int len,
+                                                               unsigned int *__restrict__ part) {
+    const unsigned int total = scan_chunk(cnt, len, blockIdx.x, 0u);
+    if (part && threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+// Exclusive scan of the chunk totals part[0..n) in place, one block, 4096 entries at a time.
+__global__ void __launch_bounds__(kRadixThreads) k_scan_parts(unsigned int *__restrict__ part, int n) {
+    unsigned int carry = 0;
+    for (long long c = 0; c * kScanChunk < n; ++c) carry += scan_chunk(part, n, c, carry);
 }
 
 __global__ void __launch_bounds__(kRadixThreads)
     k_radix_scatter(const unsigned long long *__restrict__ kin, const unsigned int *__restrict__ vin,
                     unsigned long long *__restrict__ kout, unsigned int *__restrict__ vout, int shift,
-                    int tiles, const unsigned int *__restrict__ offs) {
+                    int tiles, const unsigned int *__restrict__ offs, const unsigned int *__restrict__ part) {
     constexpr int kWarps = kRadixThreads / 32;
     __shared__ unsigned int wcnt[kWarps][256];
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -159,10 +189,12 @@ __global__ void __launch_bounds__(kRadixThreads)
         __syncwarp();
     }
     __syncthreads();
-    // exclusive prefix over warps for every digit, plus the tile's global digit offset
+    // exclusive prefix over warps for every digit, plus the tile's global digit offset (the
+    // chunk-local scan of [digit][tile] plus its chunk's offset)
     {
         int dg = threadIdx.x;  // kRadixThreads == 256
-        unsigned int run = offs[dg * tiles + blockIdx.x];
+        const int at = dg * tiles + blockIdx.x;
+        unsigned int run = offs[at] + (part ? part[at / kScanChunk] : 0u);
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
             unsigned int c = wcnt[w][dg];
@@ -296,16 +328,34 @@ __device__ __forceinline__ void heap_build(unsigned long long *h, int lane, int 
 
 __device__ __forceinline__ float key_d2(unsigned long long k) { return __uint_as_float(static_cast<unsigned int>(k >> 32)); }
 
+// Per-warp shared memory of k_knn_query: K-entry heaps of 32 lanes, a 32-site tile (also the
+// breadth-first frontier staging, kFrontier ints), and the leaf list / depth-first stack.
+constexpr int kFrontier = 128;   // internal nodes of one breadth-first level
+constexpr int kListInts = 352;   // leaves of the breadth-first walk (also the depth-first stack)
+__host__ __device__ constexpr size_t knn_warp_bytes(int K) {
+    return static_cast<size_t>(K) * 32 * 8 + 32 * 16 + kListInts * 4;
+}
+
+// Loads of one leaf: this lane's site of the 32-site tile and the four 8-site sub-boxes.
+struct LeafLoad {
+    float4 site;
+    float4 sl[kSubs], sh[kSubs];
+};
+
 __global__ void k_knn_query(Model m, QueryArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int K = a.k;
-    const size_t per_warp = static_cast<size_t>(K) * 32 * 8 + 32 * 16 + 64 * 4;
+    const size_t per_warp = knn_warp_bytes(K);
     unsigned char *wbase = smem + wib * per_warp;
     unsigned long long *heap = reinterpret_cast<unsigned long long *>(wbase);
     float4 *tile = reinterpret_cast<float4 *>(wbase + static_cast<size_t>(K) * 32 * 8);
+    // the breadth-first walk stages its next frontier in the tile buffer (no leaf is scanned then)
+    int *staging = reinterpret_cast<int *>(tile);
+    // leaf list of the breadth-first walk; the depth-first walk's stack (never live together)
     int *stack = reinterpret_cast<int *>(wbase + static_cast<size_t>(K) * 32 * 8 + 32 * 16);
+    int *leaf_list = stack;
 
     const int n_act = a.counters[0];
     const int n_leaves = (n_act + kLeaf - 1) / kLeaf;
@@ -348,17 +398,24 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
         }
     };
 
-    auto scan_leaf = [&](int lf) {
+    auto load_leaf = [&](int lf, LeafLoad &L) {
+        L.site = a.sorted[lf * kLeaf + lane];
+#pragma unroll
+        for (int gq = 0; gq < kSubs; ++gq) {
+            L.sl[gq] = a.sub_lo[lf * kSubs + gq];
+            L.sh[gq] = a.sub_hi[lf * kSubs + gq];
+        }
+    };
+
+    auto process_leaf = [&](int lf, const LeafLoad &L) {
         const int base = lf * kLeaf;
         // which 8-site groups of this leaf can hold a candidate for some lane
         unsigned int groups = 0;
 #pragma unroll
-        for (int gq = 0; gq < kSubs; ++gq) {
-            const float4 sl = a.sub_lo[lf * kSubs + gq], sh = a.sub_hi[lf * kSubs + gq];
-            if (__any_sync(0xffffffffu, box_dist2(qp, sl, sh) <= cut)) groups |= 1u << gq;
-        }
+        for (int gq = 0; gq < kSubs; ++gq)
+            if (__any_sync(0xffffffffu, box_dist2(qp, L.sl[gq], L.sh[gq]) <= cut)) groups |= 1u << gq;
         if (!groups) return;
-        tile[lane] = a.sorted[base + lane];
+        tile[lane] = L.site;
         __syncwarp();
         const int ncand = min(kLeaf, n_act - base);
         // the distances of every needed group first (independent work), then this lane's accepted
@@ -390,37 +447,204 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
         __syncwarp();
     };
 
-    auto walk = [&]() {
-        // own bucket and its two Morton neighbours first: they hold near sites, so the heaps fill
-        // and the bounds tighten before the tree walk
-        scan_leaf(leaf);
-        for (int d = 1; d <= kPrescan; ++d) {
-            if (leaf - d >= 0) scan_leaf(leaf - d);
-            if (leaf + d < n_leaves) scan_leaf(leaf + d);
+    auto scan_leaf = [&](int lf) {
+        LeafLoad L;
+        load_leaf(lf, L);
+        process_leaf(lf, L);
+    };
+
+    // Scans leaves id(0..count-1) (warp-uniform ids, -1 = skip), loading the next leaf while the
+    // current one is processed.
+    auto scan_sequence = [&](auto id, int count) {
+        LeafLoad cur, nxt;
+        int i = 0, lf = -1;
+        while (i < count && (lf = id(i)) < 0) ++i;
+        if (lf < 0) return;
+        load_leaf(lf, cur);
+        while (true) {
+            int j = i + 1, nf = -1;
+            while (j < count && (nf = id(j)) < 0) ++j;
+            if (nf >= 0) load_leaf(nf, nxt);
+            process_leaf(lf, cur);
+            if (nf < 0) break;
+            cur = nxt;
+            lf = nf;
+            i = j;
         }
-        int sp = 1;
-        stack[0] = 0;
+    };
+
+    // own bucket and its Morton neighbours: they hold near sites, so the heaps fill and the bounds
+    // tighten before the tree walk
+    auto prescan = [&]() {
+        scan_sequence(
+            [&](int t) {
+                const int lf = (t == 0) ? leaf : ((t & 1) ? leaf - (t + 1) / 2 : leaf + t / 2);
+                return (lf >= 0 && lf < n_leaves) ? lf : -1;
+            },
+            2 * kPrescan + 1);
+    };
+    auto prescanned = [&](int lf) { return lf >= leaf - kPrescan && lf <= leaf + kPrescan; };
+
+    // Depth-first walk.  A node's box is tested when its parent is expanded: both children's
+    // boxes are loaded together and only children that can hold a candidate for some lane are
+    // pushed, so a pop needs no load.  The stack holds at most one pending sibling per tree level
+    // plus the node being expanded.
+    auto walk_dfs = [&]() {
+        int sp = 0;
+        {
+            const float4 rl = a.lo[0], rh = a.hi[0];
+            st_nodes += 1;
+            if (__any_sync(0xffffffffu, box_dist2(qp, rl, rh) <= cut)) stack[sp++] = 0;
+        }
         while (sp > 0) {
             const int node = stack[--sp];
-            const float4 nl = a.lo[node], nh = a.hi[node];
-            st_nodes += 1;
-            if (!__any_sync(0xffffffffu, box_dist2(qp, nl, nh) <= cut)) continue;
             if (node >= a.leaf_slots - 1) {
                 const int lf = node - (a.leaf_slots - 1);
-                if (lf < leaf - kPrescan || lf > leaf + kPrescan) scan_leaf(lf);
+                if (!prescanned(lf)) scan_leaf(lf);
                 continue;
             }
-            // Children are tested when popped.  Visit first the child whose leaf range lies closer,
-            // in Morton order, to the warp's own bucket: its sites are the nearer ones.
+            const int c0 = 2 * node + 1, c1 = 2 * node + 2;
+            const float4 l0 = a.lo[c0], h0 = a.hi[c0], l1 = a.lo[c1], h1 = a.hi[c1];
+            st_nodes += 2;
+            const bool p0 = __any_sync(0xffffffffu, box_dist2(qp, l0, h0) <= cut);
+            const bool p1 = __any_sync(0xffffffffu, box_dist2(qp, l1, h1) <= cut);
+            // Visit first the child whose leaf range lies closer, in Morton order, to the warp's
+            // own bucket: its sites are the nearer ones.
             const int depth = 31 - __clz(node + 1);
             const int span = depth_leaves >> depth;  // leaves under this node
             const int start = (node + 1 - (1 << depth)) * span;
-            const int c0 = 2 * node + 1, c1 = 2 * node + 2;
             const bool left_near = leaf < start + (span >> 1);
-            // the stack holds at most one pending sibling per tree level (<= 31) plus one
-            stack[sp++] = left_near ? c1 : c0;
-            stack[sp++] = left_near ? c0 : c1;
+            const int near = left_near ? c0 : c1, far = left_near ? c1 : c0;
+            const bool pn = left_near ? p0 : p1, pf = left_near ? p1 : p0;
+            if (pf) stack[sp++] = far;
+            if (pn) stack[sp++] = near;
             __syncwarp();
+        }
+    };
+
+    // Breadth-first walk for the lanes in `part`: one level of the tree per memory round trip, up
+    // to 32 nodes tested at once (one per lane).  Internal nodes are pruned against the
+    // axis-aligned box around every participating lane's ball; leaves against each lane's own ball
+    // (d^2 bound `cut`).  The passing leaves are then scanned in one pipelined sequence.  Returns
+    // false (nothing scanned) when a level or the leaf list exceeds its capacity.
+    auto walk_bfs = [&](bool part) -> bool {
+        const int levels = 31 - __clz(a.leaf_slots);  // leaves sit at this depth
+        if (levels == 0) return true;                 // a single leaf: the prescan covered it
+        // conservative union box: radius inflated by 1e-4 and by the rounding of q +- r
+        const float rr = part ? sqrtf(cut) * 1.0001f + (fabsf(qp.x) + fabsf(qp.y) + fabsf(qp.z)) * 1.0e-6f : 0.f;
+        float ulx = part ? qp.x - rr : CUDART_INF_F_, uly = part ? qp.y - rr : CUDART_INF_F_,
+              ulz = part ? qp.z - rr : CUDART_INF_F_;
+        float uhx = part ? qp.x + rr : -CUDART_INF_F_, uhy = part ? qp.y + rr : -CUDART_INF_F_,
+              uhz = part ? qp.z + rr : -CUDART_INF_F_;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            ulx = fminf(ulx, __shfl_xor_sync(0xffffffffu, ulx, off));
+            uly = fminf(uly, __shfl_xor_sync(0xffffffffu, uly, off));
+            ulz = fminf(ulz, __shfl_xor_sync(0xffffffffu, ulz, off));
+            uhx = fmaxf(uhx, __shfl_xor_sync(0xffffffffu, uhx, off));
+            uhy = fmaxf(uhy, __shfl_xor_sync(0xffffffffu, uhy, off));
+            uhz = fmaxf(uhz, __shfl_xor_sync(0xffffffffu, uhz, off));
+        }
+        auto overlaps = [&](const float4 &l, const float4 &h) {
+            return l.x <= uhx && h.x >= ulx && l.y <= uhy && h.y >= uly && l.z <= uhz && h.z >= ulz;
+        };
+        // a lane outside `part` tests against an empty ball
+        const float pcut = part ? cut : -1.0f;
+        const unsigned int lt = (1u << lane) - 1u;
+        const int first_leaf = a.leaf_slots - 1;
+        int fr[kFrontier / 32];
+        fr[0] = 0;  // the root, held by lane 0
+        int nf = 1, nleaf = 0;
+        for (int d = 0; d < levels; ++d) {
+            const bool to_leaves = (d + 1 == levels);
+            int nnext = 0;
+#pragma unroll
+            for (int r = 0; r < kFrontier / 32; ++r) {
+                if (r * 32 >= nf) break;
+                const bool has = r * 32 + lane < nf;
+                const int node = has ? fr[r] : 0;
+                const int c0 = 2 * node + 1, c1 = c0 + 1;
+                float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), h0 = l0, l1 = l0, h1 = l0;
+                if (has) {
+                    l0 = a.lo[c0];
+                    h0 = a.hi[c0];
+                    l1 = a.lo[c1];
+                    h1 = a.hi[c1];
+                }
+                st_nodes += has ? 2 : 0;
+                bool p0 = has && overlaps(l0, h0);
+                bool p1 = has && overlaps(l1, h1);
+                if (to_leaves) {
+                    p0 = p0 && !prescanned(c0 - first_leaf);
+                    p1 = p1 && !prescanned(c1 - first_leaf);
+                    if (__any_sync(0xffffffffu, p0 || p1)) {
+                        // exact: some participating lane's own ball reaches the leaf box
+                        bool e0 = false, e1 = false;
+                        for (int o = 0; o < 32; ++o) {
+                            const float ox = __shfl_sync(0xffffffffu, qp.x, o);
+                            const float oy = __shfl_sync(0xffffffffu, qp.y, o);
+                            const float oz = __shfl_sync(0xffffffffu, qp.z, o);
+                            const float oc = __shfl_sync(0xffffffffu, pcut, o);
+                            const float3 oq = make_float3(ox, oy, oz);
+                            e0 = e0 || (p0 && box_dist2(oq, l0, h0) <= oc);
+                            e1 = e1 || (p1 && box_dist2(oq, l1, h1) <= oc);
+                        }
+                        p0 = e0;
+                        p1 = e1;
+                    }
+                }
+                const unsigned int b0 = __ballot_sync(0xffffffffu, p0), b1 = __ballot_sync(0xffffffffu, p1);
+                const int tot = __popc(b0) + __popc(b1);
+                int k = __popc(b0 & lt) + __popc(b1 & lt);
+                if (to_leaves) {
+                    if (nleaf + tot > kListInts) return false;
+                    k += nleaf;
+                    if (p0) leaf_list[k++] = c0 - first_leaf;
+                    if (p1) leaf_list[k] = c1 - first_leaf;
+                    nleaf += tot;
+                } else {
+                    if (nnext + tot > kFrontier) return false;
+                    k += nnext;
+                    if (p0) staging[k++] = c0;
+                    if (p1) staging[k] = c1;
+                    nnext += tot;
+                }
+            }
+            __syncwarp();
+            if (!to_leaves) {
+#pragma unroll
+                for (int r = 0; r < kFrontier / 32; ++r)
+                    if (r * 32 + lane < nnext) fr[r] = staging[r * 32 + lane];
+                nf = nnext;
+                __syncwarp();
+                if (nf == 0) break;
+            }
+        }
+        // the listed leaves, by this walk's lanes only (the others see them in their own walk)
+        const float keep = cut;
+        if (!part) cut = -1.0f;
+        scan_sequence([&](int t) { return leaf_list[t]; }, nleaf);
+        if (!part) cut = keep;
+        __syncwarp();
+        return true;
+    };
+
+    auto walk = [&]() {
+        prescan();
+        // lanes whose heap is not yet full still search the whole q ball: they walk depth-first
+        // after the others, so that their ball does not widen the breadth-first union box
+        const bool deferred = valid && cut >= 0.0f && cnt < K && !(lim2 < q2);
+        const bool part = valid && cut >= 0.0f && !deferred;
+        const bool bfs_ok = __any_sync(0xffffffffu, part) ? walk_bfs(part) : true;
+        if (!bfs_ok) {
+            walk_dfs();  // nothing was scanned past the prescan: every lane walks depth-first
+            return;
+        }
+        if (__any_sync(0xffffffffu, deferred)) {
+            const float keep = cut;
+            if (!deferred) cut = -1.0f;
+            walk_dfs();
+            if (!deferred) cut = keep;
         }
     };
 
@@ -556,7 +780,10 @@ Status geometry_alloc(Geometry &g, const Model &m, int n) {
     GD_TRY_CUDA(g.key_b.alloc(g.n_sort));
     GD_TRY_CUDA(g.val_a.alloc(g.n_sort));
     GD_TRY_CUDA(g.val_b.alloc(g.n_sort));
-    GD_TRY_CUDA(g.hist.alloc(static_cast<size_t>(256) * tiles));
+    // [digit][tile] counts, then the chunk totals of their scan when it spans several chunks
+    const size_t hist_len = static_cast<size_t>(256) * tiles;
+    const size_t chunks = (hist_len + kScanChunk - 1) / kScanChunk;
+    GD_TRY_CUDA(g.hist.alloc(hist_len + (chunks > 1 ? chunks : 0)));
     GD_TRY_CUDA(g.sorted.alloc(static_cast<size_t>(g.leaf_slots) * kLeaf));
     GD_TRY_CUDA(g.node_lo.alloc(2 * static_cast<size_t>(g.leaf_slots)));
     GD_TRY_CUDA(g.node_hi.alloc(2 * static_cast<size_t>(g.leaf_slots)));
@@ -595,12 +822,16 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     const int passes = (g.key_bits + 7) / 8;
     unsigned long long *kin = g.key_a.ptr, *kout = g.key_b.ptr;
     unsigned int *vin = g.val_a.ptr, *vout = g.val_b.ptr;
+    const int hist_len = 256 * tiles;
+    const int chunks = (hist_len + kScanChunk - 1) / kScanChunk;
+    unsigned int *part = chunks > 1 ? g.hist.ptr + hist_len : nullptr;
     for (int p = 0; p < passes; ++p) {
         const int shift = 8 * p;
-        g.launches += 3;
+        g.launches += part ? 4 : 3;
         k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, shift, tiles, g.hist.ptr);
-        k_scan_exclusive<<<1, 1024, 0, s>>>(g.hist.ptr, 256 * tiles);
-        k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, kout, vout, shift, tiles, g.hist.ptr);
+        k_scan_chunks<<<chunks, kRadixThreads, 0, s>>>(g.hist.ptr, hist_len, part);
+        if (part) k_scan_parts<<<1, kRadixThreads, 0, s>>>(part, chunks);
+        k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, kout, vout, shift, tiles, g.hist.ptr, part);
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
@@ -622,7 +853,7 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     return Status::ok();
 }
 
-size_t knn_smem_per_warp(int K) { return static_cast<size_t>(K) * 32 * 8 + 32 * 16 + 64 * 4; }
+size_t knn_smem_per_warp(int K) { return knn_warp_bytes(K); }
 
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
                  float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats) {

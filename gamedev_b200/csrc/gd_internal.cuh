@@ -31,6 +31,8 @@ constexpr int kMaxK = 256;
 constexpr int kRadixThreads = 256;
 constexpr int kRadixItems = 16;
 constexpr int kRadixTile = kRadixThreads * kRadixItems;  // 4096 keys per sort tile
+constexpr int kScanItems = 16;                            // histogram entries per scan thread
+constexpr int kScanChunk = kRadixThreads * kScanItems;    // 4096 entries per scan block
 
 // Device copy of the model constants, passed by value to kernels.
 struct Model {
