@@ -385,18 +385,7 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
 
     const int depth_leaves = a.leaf_slots;  // leaves under the root (a power of two)
 
-    auto offer = [&](unsigned long long key) {
-        if (cnt < K) {
-            heap[cnt * 32 + lane] = key;  // fill phase: no ordering work until K entries exist
-            if (++cnt == K) {
-                heap_build(heap, lane, K);
-                cut = key_d2(heap[lane]);
-            }
-        } else if (key < heap[lane]) {
-            heap_sift(heap, lane, key, 0, K);
-            cut = key_d2(heap[lane]);
-        }
-    };
+    bool built = false;  // this lane's K entries have been arranged into a max-heap
 
     auto load_leaf = [&](int lf, LeafLoad &L) {
         L.site = a.sorted[lf * kLeaf + lane];
@@ -433,6 +422,30 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
             }
             st_leaves += 1;
         }
+        // Fill phase: a lane with fewer than K entries appends without ordering work.  A lane
+        // that reaches K stops and keeps the rest of its mask; the lanes that filled up in this
+        // leaf then build their heaps together (in step, instead of one lane after another).
+        while (mask && cnt < K) {
+            const int c = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float4 p = tile[c];
+            const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
+            if (d2 <= cut) {
+                ++st_offers;
+                heap[cnt * 32 + lane] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                                        static_cast<unsigned int>(__float_as_int(p.w));
+                ++cnt;
+            }
+        }
+        const bool build_now = cnt == K && !built;
+        if (__any_sync(0xffffffffu, build_now)) {
+            if (build_now) {
+                heap_build(heap, lane, K);
+                cut = key_d2(heap[lane]);
+                built = true;
+            }
+        }
+        // heap phase: a candidate below the heap's largest key replaces it
         while (mask) {
             const int c = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -440,8 +453,12 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
             const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
             if (d2 <= cut) {
                 ++st_offers;
-                offer((static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                      static_cast<unsigned int>(__float_as_int(p.w)));
+                const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                                               static_cast<unsigned int>(__float_as_int(p.w));
+                if (key < heap[lane]) {
+                    heap_sift(heap, lane, key, 0, K);
+                    cut = key_d2(heap[lane]);
+                }
             }
         }
         __syncwarp();
