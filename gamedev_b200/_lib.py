@@ -76,6 +76,8 @@ SIGNATURES = {
     "gd_rng_init": (C.c_int, [_P, C.c_int, C.c_ulonglong, _P]),
     "gd_geometry_build": (C.c_int, [_P, _P]),
     "gd_knn": (C.c_int, [_P, _P, _P, _P, _P]),
+    "gd_set_deferred_checks": (C.c_int, [_P, C.c_int]),
+    "gd_check_geometry": (C.c_int, [_P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "gd_drift_keplerian": (C.c_int, [_P, _P, C.c_double]),

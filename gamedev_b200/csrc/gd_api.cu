@@ -205,6 +205,22 @@ gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle) {
     return done(h, s);
 }
 
+gd_status gd_set_deferred_checks(gd_handle *h, int on) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    h->geo.deferred_check = on != 0;
+    return GD_OK;
+}
+
+gd_status gd_check_geometry(gd_handle *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    if (!h->geo.sorted_key) return fail(h, GD_ERR_NOT_READY, "gd_check_geometry called before gd_geometry_build");
+    // the screen of the most recent build on the stream, eager or replayed from a captured graph
+    gd::Status s = gd::geometry_check(h->geo, h->stream);
+    h->geom_valid = static_cast<bool>(s);
+    if (!s) h->cache_valid = false;
+    return done(h, s);
+}
+
 gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
                  float *dev_kth_d2) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");

@@ -810,6 +810,11 @@ Status geometry_alloc(Geometry &g, const Model &m, int n) {
     return Status::ok();
 }
 
+// counters: [0] active sites, [1] first non-finite index (INT_MAX if none), [2..3] zero
+__global__ void k_counters_reset(int *counters) {
+    if (threadIdx.x < 4) counters[threadIdx.x] = (threadIdx.x == 1) ? INT_MAX : 0;
+}
+
 static Status read_counters(Geometry &g, cudaStream_t s, int out[2]) {
     GD_TRY_CUDA(cudaMemcpyAsync(out, g.counters.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     GD_TRY_CUDA(cudaStreamSynchronize(s));
@@ -818,22 +823,15 @@ static Status read_counters(Geometry &g, cudaStream_t s, int out[2]) {
 
 Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
     const int n = g.n;
-    int init[4] = {0, INT_MAX, 0, 0};
-    GD_TRY_CUDA(cudaMemcpyAsync(g.counters.ptr, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    g.launches += 1;
+    g.launches += 2;
+    k_counters_reset<<<1, 32, 0, s>>>(g.counters.ptr);
     k_site_init<<<(g.n_sort + 255) / 256, 256, 0, s>>>(m, n, dev_particle, g.site.ptr, g.q.ptr, g.active.ptr,
                                                         g.key_a.ptr, g.val_a.ptr, g.n_sort, g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
-    // the reference stops on the first non-finite particle before building (swarm_runtime.cu:382-393)
-    int cnt[2];
-    GD_TRY(read_counters(g, s, cnt));
-    if (cnt[1] != INT_MAX) {
-        Status st;
-        st.code = GD_ERR_NONFINITE;
-        st.detail = cnt[1];
-        st.msg = "non-finite particle state before collision search at particle " + std::to_string(cnt[1]);
-        return st;
-    }
+    // the reference stops on the first non-finite particle before building (swarm_runtime.cu:382-393);
+    // a deferred screen is read by geometry_check instead (non-finite particles are inactive and
+    // carry the all-ones key, so the rest of the build and the query run safely past them)
+    if (!g.deferred_check) GD_TRY(geometry_check(g, s));
     // radix sort over the bits that carry key information (inactive keys are all ones)
     const int tiles = g.n_sort / kRadixTile;
     const int passes = (g.key_bits + 7) / 8;
@@ -870,6 +868,19 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     return Status::ok();
 }
 
+Status geometry_check(Geometry &g, cudaStream_t s) {
+    int cnt[2];
+    GD_TRY(read_counters(g, s, cnt));
+    if (cnt[1] != INT_MAX) {
+        Status st;
+        st.code = GD_ERR_NONFINITE;
+        st.detail = cnt[1];
+        st.msg = "non-finite particle state before collision search at particle " + std::to_string(cnt[1]);
+        return st;
+    }
+    return Status::ok();
+}
+
 size_t knn_smem_per_warp(int K) { return knn_warp_bytes(K); }
 
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
@@ -890,7 +901,16 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     }
     const int warps = best;
     const size_t smem = per_warp * warps;
-    GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    // raise the kernel's shared-memory limit only when a larger one is needed, so that a step
+    // enqueued under stream capture after a first eager call makes no attribute call
+    static int smem_set[64] = {};
+    int dev = 0;
+    GD_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || smem_set[dev] < static_cast<int>(smem)) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+        if (dev >= 0 && dev < 64) smem_set[dev] = static_cast<int>(smem);
+    }
     QueryArgs qa;
     qa.sorted = g.sorted.ptr;
     qa.lo = g.node_lo.ptr;
@@ -918,9 +938,8 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
 
 Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
     (void)m;
-    int init[2] = {0, INT_MAX};
-    GD_TRY_CUDA(cudaMemcpyAsync(g.counters.ptr, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    g.launches += 1;
+    g.launches += 2;
+    k_counters_reset<<<1, 32, 0, s>>>(g.counters.ptr);
     k_state_screen<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, dev_particle, g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
     int cnt[2];

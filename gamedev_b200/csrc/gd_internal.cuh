@@ -123,12 +123,18 @@ struct Geometry {
     unsigned int *sorted_val = nullptr;  // points into val_a or val_b after the sort
     unsigned long long *sorted_key = nullptr;  // points into key_a or key_b after the sort
     long long launches = 0;              // kernels launched by this geometry (reported by the ABI)
+    // Deferred screen: the build enqueues everything without waiting for the non-finite screen,
+    // and geometry_check reads it later (what stream capture into a CUDA graph needs).
+    bool deferred_check = false;
 };
 
 Status geometry_alloc(Geometry &g, const Model &m, int n);
 // col_site_init + Morton keys + radix sort + bucket tree.  Returns GD_ERR_NONFINITE with the
 // smallest bad index when a particle is non-finite.
 Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
+// The non-finite screen of the last build: GD_ERR_NONFINITE with the smallest bad index, if any.
+// Synchronises the stream.
+Status geometry_check(Geometry &g, cudaStream_t s);
 // Exact top-K over the bucket tree.  Writes codes/measure/kth (any may be null).
 // With `radius` (per particle, may be null) the walk is first bounded by min(q, radius) and falls
 // back to q for owners that find fewer than K sites inside; `stats` (may be null) accumulates

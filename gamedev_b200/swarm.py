@@ -76,6 +76,16 @@ class SwarmCollision:
         self.lib.gd_set_stream(self.h, _stream())
         self._check(self.lib.gd_geometry_build(self.h, C.c_void_p(_ptr(particles))))
 
+    def set_deferred_checks(self, on: bool = True):
+        """Defer the non-finite screen of col_site_init to check_geometry(), so a build + query
+        sequence makes no host synchronisation (needed to capture it in a CUDA graph)."""
+        self._check(self.lib.gd_set_deferred_checks(self.h, 1 if on else 0))
+
+    def check_geometry(self):
+        """Read the deferred non-finite screen of the last build; raises GdError on a bad particle."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_check_geometry(self.h))
+
     def col_cache_get(self, particles, codes=None, measure=None, kth_d2=None):
         """col_cache_get (_col_cache.cuh:15-159): fills codes [n_p, n_k] int32, measure [n_p] f64."""
         self._check(self.lib.gd_knn(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(codes)),

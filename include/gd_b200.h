@@ -150,6 +150,19 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
                          int32_t *dev_codes, double *dev_measure, float *dev_kth_d2,
                          unsigned long long *dev_stats);
 
+/* Deferred non-finite screen (on != 0).  gd_geometry_build then enqueues the whole build without
+ * waiting for its non-finite screen (the reference's stop on the first non-finite particle,
+ * swarm_runtime.cu:382-393), so a build + query sequence makes no host synchronisation and can be
+ * captured into a CUDA graph on the handle's stream.  Non-finite particles are treated as inactive
+ * until gd_check_geometry reports them.  Off by default. */
+gd_status gd_set_deferred_checks(gd_handle *h, int on);
+
+/* The deferred screen of the most recent geometry build on the handle's stream (an eager
+ * gd_geometry_build or its replay from a captured graph): GD_ERR_NONFINITE with the smallest bad
+ * index in gd_error_detail (and the geometry invalidated), else GD_OK (and the geometry marked
+ * valid: after a replay it stands for the positions the replay read).  Synchronises the stream. */
+gd_status gd_check_geometry(gd_handle *h);
+
 /* Keplerian azimuthal advance of every active particle by dt: phi += Omega_K(R) dt wrapped into
  * [x_min, x_max) (the orbital part of the reference's transport step, _transport.cuh, without drag,
  * radiation or diffusion).  Invalidates the geometry: positions changed. */
