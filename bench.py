@@ -525,10 +525,100 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """The batched configuration (256 c0-shaped swarms, log-uniform sizes on [2^10, 2^18], K from
+    {16, 32, 64}): per-swarm geometry + one persistent top-K launch, captured as one CUDA graph,
+    against the same swarms searched one handle at a time.  Every swarm is checked bit-exact
+    against its one-swarm result."""
+    import torch
+
+    import gamedev_b200 as gd
+    from gamedev_b200 import workloads
+
+    world, rank, local = dist_init(args.gpus)
+    cfg, sizes, ks, p = workloads.c2_batch(seed=5 + rank)
+    stream = torch.cuda.current_stream()
+    dp = gd.particles_to_device(p)
+    batch = gd.SwarmBatch(cfg, sizes, ks)
+    codes, measure, kth = batch.outputs()
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            batch.knn(dp, codes, measure, kth)
+    stream.wait_stream(side)
+    batch.check()
+    graph = torch.cuda.CUDAGraph()
+    l0 = batch.launch_count()
+    with torch.cuda.graph(graph):
+        batch.knn(dp, codes, measure, kth)
+    kernels = batch.launch_count() - l0
+    for _ in range(args.warmup):
+        graph.replay()
+    barrier(world)
+    a, b = _timed(stream, lambda: [graph.replay() for _ in range(args.steps)])
+    barrier(world)
+    batch.check()
+    b_ms = reduce_max(a.elapsed_time(b) / args.steps, world)
+    # the same swarms one handle at a time (geometry + top-K per swarm, eager)
+    solos = []
+    for s_, n_s in enumerate(sizes):
+        c = workloads.config("c0_plain_small", k=ks[s_])
+        sw = gd.SwarmCollision(c, n_s)
+        sl = dp[int(batch.part_off[s_]):int(batch.part_off[s_ + 1])]
+        out = (torch.empty((n_s, ks[s_]), dtype=torch.int32, device=dp.device),
+               torch.empty(n_s, dtype=torch.float64, device=dp.device),
+               torch.empty(n_s, dtype=torch.float32, device=dp.device))
+        solos.append((sw, sl, out))
+    for sw, sl, out in solos:
+        sw.col_site_init(sl)
+        sw.col_cache_get(sl, *out)
+    barrier(world)
+    a, b = _timed(stream, lambda: [(sw.col_site_init(sl), sw.col_cache_get(sl, *out)) for sw, sl, out in solos])
+    barrier(world)
+    solo_ms = reduce_max(a.elapsed_time(b), world)
+    exact = 0
+    for s_, (sw, sl, out) in enumerate(solos):
+        exact += int(torch.equal(batch.codes_of(codes, s_), out[0])
+                     and torch.equal(batch.rows_of(measure, s_).view(torch.int64), out[1].view(torch.int64))
+                     and torch.equal(batch.rows_of(kth, s_).view(torch.int32), out[2].view(torch.int32)))
+        sw.close()
+    del graph
+    queries = reduce_sum(float(sum(sizes)), world)
+    line = {
+        "metric": "exact kNN queries/s, batched swarms", "value": queries / (b_ms / 1e3), "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "c2_batched", "swarms": len(sizes), "particles": int(sum(sizes)),
+                   "n_range": [min(sizes), max(sizes)], "k_choices": [16, 32, 64],
+                   "step": "per-swarm geometry on 8 streams + one persistent top-K launch, one CUDA graph replay",
+                   "parallelism": f"replicas x{world}"},
+        "kernels_per_step": kernels,
+        "one_handle_at_a_time": {"ms_per_step": solo_ms, "queries_per_s": queries / (solo_ms / 1e3)},
+        "speedup_vs_one_at_a_time": solo_ms / b_ms,
+        "bit_exact_swarms": f"{exact}/{len(sizes)}",
+    }
+    if exact != len(sizes):
+        line["error"] = "batched rows differ from the one-swarm results"
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "c2_batched":
+        import gamedev_b200
+
+        gamedev_b200.load()
+        run_batched(args)
         return
     import gamedev_b200
 

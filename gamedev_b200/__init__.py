@@ -3,11 +3,11 @@ frozen-bath event chain) behind a C ABI (include/gd_b200.h, libgd_b200.so)."""
 
 from ._lib import (GD_KERNEL_CONSTANT, GD_KERNEL_CUSTOM, GD_KERNEL_LINEAR, GD_KERNEL_PRODUCT,
                    GD_SEARCH_KDTREE, GD_SEARCH_MORTON, GdConfig, GdError, default_config, load)
-from .swarm import (PARTICLE_DTYPE, STATIC_MAX_PARTICLES, RadiusModel, SwarmCollision, knn_static,
+from .swarm import (PARTICLE_DTYPE, STATIC_MAX_PARTICLES, RadiusModel, SwarmBatch, SwarmCollision, knn_static,
                     particles_to_device, rng_state_bytes, rng_uniforms, rngstate_init)
 
 __all__ = [
-    "GdConfig", "GdError", "SwarmCollision", "RadiusModel", "default_config", "load", "rngstate_init",
+    "GdConfig", "GdError", "SwarmCollision", "SwarmBatch", "RadiusModel", "default_config", "load", "rngstate_init",
     "rng_state_bytes", "rng_uniforms", "particles_to_device", "PARTICLE_DTYPE", "knn_static",
     "STATIC_MAX_PARTICLES",
     "GD_SEARCH_KDTREE", "GD_SEARCH_MORTON",

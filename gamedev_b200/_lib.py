@@ -77,6 +77,14 @@ SIGNATURES = {
     "gd_geometry_build": (C.c_int, [_P, _P]),
     "gd_knn": (C.c_int, [_P, _P, _P, _P, _P]),
     "gd_set_deferred_checks": (C.c_int, [_P, C.c_int]),
+    "gd_batch_create": (C.c_int, [C.POINTER(GdConfig), C.c_int, _P, _P, C.POINTER(_P)]),
+    "gd_batch_destroy": (None, [_P]),
+    "gd_batch_set_stream": (C.c_int, [_P, _P]),
+    "gd_batch_knn": (C.c_int, [_P, _P, _P, _P, _P]),
+    "gd_batch_check": (C.c_int, [_P]),
+    "gd_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "gd_batch_error_detail": (C.c_longlong, [_P]),
+    "gd_batch_launch_count": (C.c_longlong, [_P]),
     "gd_check_geometry": (C.c_int, [_P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),

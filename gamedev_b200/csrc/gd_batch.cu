@@ -1,0 +1,213 @@
+// Batched neighbour search: many independent swarms of uneven size (and K) per call.  No
+// counterpart in the reference, which runs one swarm per process.
+//
+// Each swarm keeps its own geometry (site init, Morton radix sort, bucket tree: the one-swarm
+// kernels, enqueued on a few internal streams so that small swarms build side by side), and one
+// persistent launch then runs the top-K of every bucket of every swarm (knn_batch_query).  The
+// non-finite screen is deferred to gd_batch_check, so a call makes no host synchronisation and
+// can be captured into a CUDA graph (the internal streams fork from and join back to the batch's
+// stream).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gd_internal.cuh"
+
+struct gd_batch {
+    gd_config cfg;
+    int S = 0;
+    std::vector<int> n, k;
+    std::vector<long long> part_off, codes_off;
+    long long n_total = 0, codes_total = 0;
+    int kcap = 0;
+    std::vector<gd::Model> models;
+    std::vector<std::unique_ptr<gd::Geometry>> geo;
+    gd::DevBuf<gd::BatchSwarm> tab;
+    gd::DevBuf<int> leaf_prefix;
+    gd::DevBuf<long long> part_prefix;
+    gd::DevBuf<int> next;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> workers;
+    std::vector<cudaEvent_t> done;
+    cudaEvent_t start = nullptr;
+    long long launches = 0;
+    std::string err;
+    long long detail = 0;
+
+    ~gd_batch() {
+        for (cudaStream_t w : workers) cudaStreamDestroy(w);
+        for (cudaEvent_t e : done) cudaEventDestroy(e);
+        if (start) cudaEventDestroy(start);
+    }
+};
+
+namespace {
+
+constexpr int kBatchStreams = 8;  // internal streams for the per-swarm geometry builds
+
+gd_status batch_fail(gd_batch *b, const gd::Status &s) {
+    if (b) {
+        b->err = s.msg;
+        b->detail = s.detail;
+    }
+    return s.code;
+}
+
+gd_status batch_fail(gd_batch *b, gd_status code, const std::string &msg, long long detail = 0) {
+    gd::Status s;
+    s.code = code;
+    s.msg = msg;
+    s.detail = detail;
+    return batch_fail(b, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int *n_k, gd_batch **out) {
+    if (!cfg || !n_p || !n_k || !out || S <= 0) return GD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    std::unique_ptr<gd_batch> b(new (std::nothrow) gd_batch());
+    if (!b) return GD_ERR_OUT_OF_MEMORY;
+    b->cfg = *cfg;
+    b->S = S;
+    b->n.assign(n_p, n_p + S);
+    b->k.assign(n_k, n_k + S);
+    std::vector<gd::BatchSwarm> tab(S);
+    std::vector<int> leaf_prefix(S + 1, 0);
+    std::vector<long long> part_prefix(S + 1, 0);
+    for (int s = 0; s < S; ++s) {
+        if (n_p[s] <= 0 || static_cast<long long>(n_p[s]) * 3 > 0x7fffffffLL || n_k[s] < 1 || n_k[s] > gd::kMaxK)
+            return GD_ERR_INVALID_ARGUMENT;
+        gd_config c = *cfg;
+        c.n_k = n_k[s];
+        b->models.push_back(gd::make_model(c));
+        b->part_off.push_back(b->n_total);
+        b->codes_off.push_back(b->codes_total);
+        b->n_total += n_p[s];
+        b->codes_total += static_cast<long long>(n_p[s]) * n_k[s];
+        b->kcap = n_k[s] > b->kcap ? n_k[s] : b->kcap;
+        std::unique_ptr<gd::Geometry> g(new (std::nothrow) gd::Geometry());
+        if (!g) return GD_ERR_OUT_OF_MEMORY;
+        gd::Status st = gd::geometry_alloc(*g, b->models.back(), n_p[s]);
+        if (!st) return st.code;
+        g->deferred_check = true;
+        gd::BatchSwarm &t = tab[s];
+        t.sorted = g->sorted.ptr;
+        t.lo = g->node_lo.ptr;
+        t.hi = g->node_hi.ptr;
+        t.sub_lo = g->sub_lo.ptr;
+        t.sub_hi = g->sub_hi.ptr;
+        t.qrad = g->q.ptr;
+        t.active = g->active.ptr;
+        t.counters = g->counters.ptr;
+        t.leaf_slots = g->leaf_slots;
+        t.k = n_k[s];
+        t.part_off = b->part_off.back();
+        t.codes_off = b->codes_off.back();
+        leaf_prefix[s + 1] = leaf_prefix[s] + (n_p[s] + gd::kLeaf - 1) / gd::kLeaf;
+        part_prefix[s + 1] = b->n_total;
+        b->geo.push_back(std::move(g));
+    }
+    if (b->tab.alloc(S) != cudaSuccess || b->leaf_prefix.alloc(S + 1) != cudaSuccess ||
+        b->part_prefix.alloc(S + 1) != cudaSuccess || b->next.alloc(1) != cudaSuccess)
+        return GD_ERR_OUT_OF_MEMORY;
+    if (cudaMemcpy(b->tab.ptr, tab.data(), sizeof(gd::BatchSwarm) * S, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->leaf_prefix.ptr, leaf_prefix.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(b->part_prefix.ptr, part_prefix.data(), sizeof(long long) * (S + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        return GD_ERR_CUDA;
+    const int W = S < kBatchStreams ? S : kBatchStreams;
+    for (int w = 0; w < W; ++w) {
+        cudaStream_t st;
+        cudaEvent_t ev;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GD_ERR_CUDA;
+        b->workers.push_back(st);
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return GD_ERR_CUDA;
+        b->done.push_back(ev);
+    }
+    if (cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming) != cudaSuccess) return GD_ERR_CUDA;
+    *out = b.release();
+    return GD_OK;
+}
+
+void gd_batch_destroy(gd_batch *b) { delete b; }
+
+gd_status gd_batch_set_stream(gd_batch *b, void *stream) {
+    if (!b) return GD_ERR_INVALID_ARGUMENT;
+    b->stream = static_cast<cudaStream_t>(stream);
+    return GD_OK;
+}
+
+gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
+                       float *dev_kth_d2) {
+    if (!b || !dev_particle || !dev_codes || !dev_measure || !dev_kth_d2)
+        return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "null batch, particle or output pointer");
+    // fork: every internal stream starts after the work already queued on the batch's stream
+    if (cudaEventRecord(b->start, b->stream) != cudaSuccess)
+        return batch_fail(b, gd::cuda_status(cudaGetLastError(), "fork batch streams"));
+    const int W = static_cast<int>(b->workers.size());
+    for (int w = 0; w < W; ++w)
+        if (cudaStreamWaitEvent(b->workers[w], b->start, 0) != cudaSuccess)
+            return batch_fail(b, gd::cuda_status(cudaGetLastError(), "fork batch streams"));
+    for (int s = 0; s < b->S; ++s) {
+        gd::Geometry &g = *b->geo[s];
+        const long long before = g.launches;
+        gd::Status st = gd::geometry_build(g, b->models[s], dev_particle + b->part_off[s], b->workers[s % W]);
+        b->launches += g.launches - before;
+        if (!st) return batch_fail(b, st);
+    }
+    // join
+    for (int w = 0; w < W; ++w) {
+        if (cudaEventRecord(b->done[w], b->workers[w]) != cudaSuccess ||
+            cudaStreamWaitEvent(b->stream, b->done[w], 0) != cudaSuccess)
+            return batch_fail(b, gd::cuda_status(cudaGetLastError(), "join batch streams"));
+    }
+    gd::Status st = gd::knn_batch_query(b->models[0], b->tab.ptr, b->leaf_prefix.ptr, b->part_prefix.ptr, b->S,
+                                        b->n_total, b->kcap, b->next.ptr, dev_particle, dev_codes, dev_measure,
+                                        dev_kth_d2, b->stream, &b->launches);
+    if (!st) return batch_fail(b, st);
+    b->err.clear();
+    b->detail = 0;
+    return GD_OK;
+}
+
+gd_status gd_batch_check(gd_batch *b) {
+    if (!b) return GD_ERR_INVALID_ARGUMENT;
+    for (int s = 0; s < b->S; ++s) {
+        gd::Status st = gd::geometry_check(*b->geo[s], b->stream);
+        if (!st) {
+            if (st.code == GD_ERR_NONFINITE) {
+                st.detail += b->part_off[s];  // index in the concatenated particle array
+                st.msg = "non-finite particle state before collision search at particle " +
+                         std::to_string(st.detail) + " (swarm " + std::to_string(s) + ")";
+            }
+            return batch_fail(b, st);
+        }
+    }
+    b->err.clear();
+    b->detail = 0;
+    return GD_OK;
+}
+
+size_t gd_batch_last_error(const gd_batch *b, char *buf, size_t len) {
+    if (!b) return 0;
+    if (buf && len) {
+        size_t k = b->err.size() < len - 1 ? b->err.size() : len - 1;
+        std::memcpy(buf, b->err.data(), k);
+        buf[k] = '\0';
+    }
+    return b->err.size();
+}
+
+long long gd_batch_error_detail(const gd_batch *b) { return b ? b->detail : 0; }
+
+long long gd_batch_launch_count(const gd_batch *b) { return b ? b->launches : 0; }
+
+}  // extern "C"

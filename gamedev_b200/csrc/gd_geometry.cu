@@ -342,24 +342,22 @@ struct LeafLoad {
     float4 sl[kSubs], sh[kSubs];
 };
 
-__global__ void k_knn_query(Model m, QueryArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// The exact top-K of the 32 owners of bucket (leaf) `leaf` of one swarm, by one warp.  `wbase` is
+// the warp's shared memory laid out for up to kcap neighbours (knn_warp_bytes(kcap)).
+__device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, int leaf, unsigned char *wbase,
+                                           int kcap) {
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
     const int K = a.k;
-    const size_t per_warp = knn_warp_bytes(K);
-    unsigned char *wbase = smem + wib * per_warp;
     unsigned long long *heap = reinterpret_cast<unsigned long long *>(wbase);
-    float4 *tile = reinterpret_cast<float4 *>(wbase + static_cast<size_t>(K) * 32 * 8);
+    float4 *tile = reinterpret_cast<float4 *>(wbase + static_cast<size_t>(kcap) * 32 * 8);
     // the breadth-first walk stages its next frontier in the tile buffer (no leaf is scanned then)
     int *staging = reinterpret_cast<int *>(tile);
     // leaf list of the breadth-first walk; the depth-first walk's stack (never live together)
-    int *stack = reinterpret_cast<int *>(wbase + static_cast<size_t>(K) * 32 * 8 + 32 * 16);
+    int *stack = reinterpret_cast<int *>(wbase + static_cast<size_t>(kcap) * 32 * 8 + 32 * 16);
     int *leaf_list = stack;
 
     const int n_act = a.counters[0];
     const int n_leaves = (n_act + kLeaf - 1) / kLeaf;
-    const int leaf = blockIdx.x * (blockDim.x >> 5) + wib;
     if (leaf >= n_leaves) return;
 
     const int i = leaf * kLeaf + lane;
@@ -725,6 +723,117 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
         const double z = a.part[idx].position[2];
         a.measure[idx] = ball_measure(m, y, z, sqrt(static_cast<double>(maxd2)));
     }
+}
+
+__global__ void k_knn_query(Model m, QueryArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int wib = threadIdx.x >> 5;
+    knn_bucket(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(a.k), a.k);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Many swarms in one persistent launch.  Every warp takes (swarm, bucket) items from a device
+// counter until none is left and runs the same knn_bucket as the one-swarm kernel, so each swarm's
+// rows are bit-identical to its solo query.  Items are numbered swarm by swarm
+// (leaf_prefix[s] .. leaf_prefix[s + 1]).
+// ------------------------------------------------------------------------------------------------
+__global__ void k_knn_batch(Model m, const BatchSwarm *__restrict__ tab, const int *__restrict__ leaf_prefix, int S,
+                            int *__restrict__ next, const gd_particle *__restrict__ part, int32_t *__restrict__ codes,
+                            double *__restrict__ measure, float *__restrict__ kth, int kcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    unsigned char *wbase = smem + wib * knn_warp_bytes(kcap);
+    const int total = leaf_prefix[S];
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(next, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        int lo = 0, hi = S;  // the swarm s with leaf_prefix[s] <= item < leaf_prefix[s + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (leaf_prefix[mid] <= item) lo = mid;
+            else hi = mid;
+        }
+        const BatchSwarm &b = tab[lo];
+        QueryArgs a;
+        a.sorted = b.sorted;
+        a.lo = b.lo;
+        a.hi = b.hi;
+        a.sub_lo = b.sub_lo;
+        a.sub_hi = b.sub_hi;
+        a.qrad = b.qrad;
+        a.counters = b.counters;
+        a.part = part + b.part_off;
+        a.leaf_slots = b.leaf_slots;
+        a.k = b.k;
+        a.codes = codes + b.codes_off;
+        a.measure = measure + b.part_off;
+        a.kth = kth + b.part_off;
+        a.radius = nullptr;
+        a.stats = nullptr;
+        knn_bucket(m, a, item - leaf_prefix[lo], wbase, kcap);
+        __syncwarp();
+    }
+}
+
+// inactive owners of every swarm of a batch: a row of -1 and zero measure
+__global__ void k_batch_inactive_rows(const BatchSwarm *__restrict__ tab, const long long *__restrict__ part_prefix,
+                                      int S, long long total, int32_t *__restrict__ codes, double *__restrict__ measure,
+                                      float *__restrict__ kth) {
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int lo = 0, hi = S;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (part_prefix[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    const BatchSwarm &b = tab[lo];
+    const long long i = g - b.part_off;
+    if (b.active[i]) return;
+    for (int s = 0; s < b.k; ++s) codes[b.codes_off + i * b.k + s] = -1;
+    measure[g] = 0.0;
+    kth[g] = 0.f;
+}
+
+Status knn_batch_query(const Model &m, const BatchSwarm *dev_tab, const int *dev_leaf_prefix,
+                       const long long *dev_part_prefix, int S, long long n_total, int kcap, int *dev_next,
+                       const gd_particle *part, int32_t *codes, double *measure, float *kth, cudaStream_t s,
+                       long long *launches) {
+    const size_t per_warp = knn_warp_bytes(kcap);
+    const size_t sm_bytes = 227 * 1024;
+    int best = 1, best_res = 0;
+    for (int w = 1; w <= 8; ++w) {
+        if (per_warp * w > sm_bytes) break;
+        const int res = static_cast<int>(sm_bytes / (per_warp * w + 1024)) * w;
+        if (res > best_res) {
+            best_res = res;
+            best = w;
+        }
+    }
+    const int warps = best;
+    const size_t smem = per_warp * warps;
+    static int smem_set[64] = {};
+    int dev = 0, sms = 0;
+    GD_TRY_CUDA(cudaGetDevice(&dev));
+    GD_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (dev < 0 || dev >= 64 || smem_set[dev] < static_cast<int>(smem)) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+        if (dev >= 0 && dev < 64) smem_set[dev] = static_cast<int>(smem);
+    }
+    // persistent grid: every resident warp slot of every SM, each pulling items until none is left
+    const int blocks = sms * (best_res / warps);
+    GD_TRY_CUDA(cudaMemsetAsync(dev_next, 0, sizeof(int), s));
+    k_knn_batch<<<blocks, warps * 32, smem, s>>>(m, dev_tab, dev_leaf_prefix, S, dev_next, part, codes, measure, kth,
+                                                 kcap);
+    k_batch_inactive_rows<<<static_cast<unsigned int>((n_total + 255) / 256), 256, 0, s>>>(
+        dev_tab, dev_part_prefix, S, n_total, codes, measure, kth);
+    if (launches) *launches += 2;
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
 }
 
 // inactive owners: a row of -1 and zero measure (_col_cache.cuh:26-34)

@@ -142,6 +142,25 @@ Status geometry_check(Geometry &g, cudaStream_t s);
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
                  double *measure, float *kth_d2, cudaStream_t s, const float *radius = nullptr,
                  unsigned long long *stats = nullptr);
+// One swarm of a batch as the persistent batch query sees it: its geometry and the offsets of its
+// rows in the caller's concatenated particle (part_off) and code (codes_off) buffers.
+struct BatchSwarm {
+    const float4 *sorted, *lo, *hi, *sub_lo, *sub_hi;
+    const float *qrad;
+    const unsigned char *active;
+    const int *counters;
+    int leaf_slots;
+    int k;
+    long long part_off;
+    long long codes_off;
+};
+// Top-K of every swarm of a batch in one persistent launch (plus the inactive rows): dev_tab[S],
+// dev_leaf_prefix[S + 1] (buckets of swarm s are items leaf_prefix[s] ..), dev_part_prefix[S + 1],
+// kcap = the largest K.  dev_next is a device counter the call resets.
+Status knn_batch_query(const Model &m, const BatchSwarm *dev_tab, const int *dev_leaf_prefix,
+                       const long long *dev_part_prefix, int S, long long n_total, int kcap, int *dev_next,
+                       const gd_particle *part, int32_t *codes, double *measure, float *kth, cudaStream_t s,
+                       long long *launches);
 // Learned-radius features of every owner (gd_radius.cu).
 Status radius_features(const Geometry &g, const Model &m, const gd_particle *part, const float *prev_kth,
                        double total_mass, float *feat, cudaStream_t s);

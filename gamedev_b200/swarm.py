@@ -324,3 +324,70 @@ def knn_static(cfg: GdConfig, particles, codes, measure, kth):
                                   C.byref(detail), msg, len(msg))
     if r != _lib.GD_OK:
         raise GdError(r, msg.value.decode(errors="replace"), int(detail.value))
+
+
+class SwarmBatch:
+    """Many independent swarms (uneven n_p and n_k, shared model constants) searched per call:
+    per-swarm geometry builds side by side and one persistent top-K launch (gd_batch_*).  Buffers
+    are concatenated swarm by swarm; `rows(t, s)` slices swarm s out of a concatenated result."""
+
+    def __init__(self, cfg: GdConfig, sizes, ks):
+        self.lib = _lib.load()
+        self.sizes = [int(v) for v in sizes]
+        self.ks = [int(v) for v in ks]
+        self.S = len(self.sizes)
+        n = (C.c_int * self.S)(*self.sizes)
+        k = (C.c_int * self.S)(*self.ks)
+        h = C.c_void_p()
+        st = self.lib.gd_batch_create(C.byref(cfg), self.S, n, k, C.byref(h))
+        if st != _lib.GD_OK:
+            raise GdError(st, "gd_batch_create failed", 0)
+        self.h = h
+        self.part_off = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.codes_off = np.concatenate([[0], np.cumsum(np.array(self.sizes) * np.array(self.ks))]).astype(np.int64)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != _lib.GD_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.gd_batch_last_error(self.h, buf, 512)
+            raise GdError(st, buf.value.decode(), int(self.lib.gd_batch_error_detail(self.h)))
+
+    def outputs(self, device="cuda"):
+        torch = _torch()
+        codes = torch.empty(int(self.codes_off[-1]), dtype=torch.int32, device=device)
+        measure = torch.empty(int(self.part_off[-1]), dtype=torch.float64, device=device)
+        kth = torch.empty(int(self.part_off[-1]), dtype=torch.float32, device=device)
+        return codes, measure, kth
+
+    def knn(self, particles, codes, measure, kth):
+        """Geometry + exact top-K of every swarm (no host synchronisation; see check())."""
+        self.lib.gd_batch_set_stream(self.h, _stream())
+        self._check(self.lib.gd_batch_knn(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(codes)),
+                                          C.c_void_p(_ptr(measure)), C.c_void_p(_ptr(kth))))
+
+    def check(self):
+        """The deferred non-finite screens of the last knn(); raises GdError (detail = index in the
+        concatenated particle array)."""
+        self.lib.gd_batch_set_stream(self.h, _stream())
+        self._check(self.lib.gd_batch_check(self.h))
+
+    def codes_of(self, codes, s: int):
+        a, b = int(self.codes_off[s]), int(self.codes_off[s + 1])
+        return codes[a:b].view(self.sizes[s], self.ks[s])
+
+    def rows_of(self, t, s: int):
+        return t[int(self.part_off[s]):int(self.part_off[s + 1])]
+
+    def launch_count(self) -> int:
+        return int(self.lib.gd_batch_launch_count(self.h))

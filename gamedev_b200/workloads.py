@@ -136,3 +136,16 @@ def particles(name: str, n: int | None = None, seed: int | None = None) -> np.nd
     out[:, 6] = diam
     out[:, 7] = numr
     return out
+
+
+def c2_batch(swarms: int = 256, seed: int = 5, n_min: int = 1 << 10, n_max: int = 1 << 18):
+    """The batched configuration: `swarms` independent 3D swarms with the c0 distributions, sizes
+    log-uniform integers on [n_min, n_max], K drawn from {16, 32, 64}, each swarm with its own
+    seed.  Returns (cfg, sizes, ks, particles) with particles concatenated swarm by swarm."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.floor(np.exp(rng.uniform(math.log(n_min), math.log(n_max + 1), swarms))).astype(np.int64)
+    sizes = np.clip(sizes, n_min, n_max)
+    ks = rng.choice(np.array([16, 32, 64]), swarms)
+    parts = [particles("c0_plain_small", n=int(n), seed=1000 * seed + s) for s, n in enumerate(sizes)]
+    cfg = config("c0_plain_small")
+    return cfg, [int(v) for v in sizes], [int(v) for v in ks], np.concatenate(parts, axis=0)

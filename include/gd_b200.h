@@ -288,6 +288,31 @@ gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int
 long long gd_launch_count(const gd_handle *h);
 
 /*
+ * Batched neighbour search: S independent swarms of uneven size n_p[s] and neighbour count n_k[s]
+ * per call.  No counterpart in the reference, which runs one swarm per process.  All swarms share
+ * the model constants of cfg except n_k.  Every swarm keeps its own geometry (the one-swarm build
+ * kernels, run side by side on internal streams) and one persistent launch computes the top-K of
+ * every bucket of every swarm; each swarm's rows are bit-identical to gd_geometry_build + gd_knn on
+ * that swarm alone.
+ *
+ * Buffers are concatenated swarm by swarm: dev_particle [sum n_p], dev_measure and dev_kth_d2
+ * [sum n_p], dev_codes [sum n_p[s] * n_k[s]] (swarm s's rows start at sum_{t<s} n_p[t] n_k[t]).
+ * The non-finite screen is deferred: gd_batch_knn makes no host synchronisation (so it can be
+ * captured into a CUDA graph on the batch's stream) and gd_batch_check reports a non-finite
+ * particle (GD_ERR_NONFINITE, detail = its index in dev_particle).
+ */
+typedef struct gd_batch gd_batch;
+gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int *n_k, gd_batch **out);
+void      gd_batch_destroy(gd_batch *b);
+gd_status gd_batch_set_stream(gd_batch *b, void *stream);
+gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
+                       float *dev_kth_d2);
+gd_status gd_batch_check(gd_batch *b);
+size_t    gd_batch_last_error(const gd_batch *b, char *buf, size_t len);
+long long gd_batch_error_detail(const gd_batch *b);
+long long gd_batch_launch_count(const gd_batch *b);
+
+/*
  * Handle-free exact top-K neighbour search that allocates no device memory.  No counterpart in
  * the reference (whose col_site_init / col_cache_get run on the swarm's allocated buffers).
  *
