@@ -290,6 +290,9 @@ def run_ours(args):
     stats = torch.zeros(4, dtype=torch.int64, device=dev)
 
     # ---- plain tree: geometry + exact top-K, inputs resident -------------------------------
+    # the autotuner picks the sort order, walk, prescan depth and block width on this input
+    # (every setting gives the same exact lists; it checks that too)
+    plain_tuning, _ = sw.autotune(dp)
     for _ in range(args.warmup):
         sw.col_site_init(dp)
         sw.col_cache_get(dp, codes, measure, kth)
@@ -326,6 +329,11 @@ def run_ours(args):
         prev.copy_(kth)
     margin = model.calibrate(feats, kth, 0.999)
     radius = torch.empty(n, dtype=torch.float32, device=dev)
+    # the radius-bounded query tunes its walk for the proposed radii (same sort order)
+    sw.col_site_init(dp)
+    sw.radius_features(dp, prev, mass, out=feats)
+    model.predict(feats, out=radius)
+    learned_tuning, _ = sw.autotune(dp, radius, tune_sort=False)
 
     def learned_step():
         sw.col_site_init(dp)
@@ -427,9 +435,10 @@ def run_ours(args):
                    "l2": "inputs and outputs larger than L2 (sites 16 B x N, codes 4K B x N)",
                    "parallelism": f"replicas x{world}"},
         "plain": {"queries_per_s": plain_value, "ms_per_step": plain_ms, "geometry_build_ms": plain_build,
-                  "knn_query_ms": plain_knn, "offers_per_owner": plain_offers},
+                  "knn_query_ms": plain_knn, "offers_per_owner": plain_offers, "tuning": plain_tuning},
         "graph": {"queries_per_s": value, "vs_plain": value / plain_value, "ms_per_step": graph_ms,
-                  "bit_exact_steps": f"{graph_exact}/{args.steps}", "kernels_per_step": graph_launches},
+                  "bit_exact_steps": f"{graph_exact}/{args.steps}", "kernels_per_step": graph_launches,
+                  "tuning": learned_tuning},
         "learned": {"queries_per_s": learned_value, "vs_plain": learned_value / plain_value, "ms_per_step": learned_ms,
                     "knn_query_ms": knn_ms, "hit_rate": 1.0 - fallbacks / max(1, n_active * args.steps),
                     "fallback_fraction": fallbacks / max(1, n_active * args.steps),

@@ -56,6 +56,11 @@ class GdConfig(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class GdTuning(C.Structure):
+    _fields_ = [("warps_per_block", C.c_int), ("prescan", C.c_int), ("walk_breadth_first", C.c_int),
+                ("sort_bits", C.c_int)]
+
+
 class GdOperatorStats(C.Structure):
     _fields_ = [("waves", C.c_int), ("chain_launches", C.c_int), ("owner_updates", C.c_longlong),
                 ("events", C.c_longlong), ("min_duration", C.c_double), ("max_duration", C.c_double)]
@@ -85,6 +90,10 @@ SIGNATURES = {
     "gd_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_batch_error_detail": (C.c_longlong, [_P]),
     "gd_batch_launch_count": (C.c_longlong, [_P]),
+    "gd_batch_set_tuning": (C.c_int, [_P, C.POINTER(GdTuning)]),
+    "gd_get_tuning": (C.c_int, [_P, C.POINTER(GdTuning)]),
+    "gd_set_tuning": (C.c_int, [_P, C.POINTER(GdTuning)]),
+    "gd_autotune": (C.c_int, [_P, _P, _P, C.c_int, C.POINTER(GdTuning), C.POINTER(C.c_double)]),
     "gd_check_geometry": (C.c_int, [_P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),

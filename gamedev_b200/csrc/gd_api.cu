@@ -11,6 +11,26 @@
 
 namespace gd {
 
+// Order-independent 64-bit digest of a neighbour cache: every code mixed with its position, and
+// every kept d^2 with its owner (a sum modulo 2^64, so the block order does not matter).
+__global__ void k_codes_digest(const int32_t *codes, size_t n_codes, const float *kth, int n,
+                               unsigned long long *out) {
+    unsigned long long acc = 0;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_codes; i += stride) {
+        unsigned long long v = static_cast<unsigned long long>(static_cast<unsigned int>(codes[i])) + 1ull;
+        v = (v * 0x9E3779B97F4A7C15ull) ^ ((i + 1) * 0xBF58476D1CE4E5B9ull);
+        acc += v ^ (v >> 31);
+    }
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < static_cast<size_t>(n); i += stride) {
+        unsigned long long v = static_cast<unsigned long long>(__float_as_uint(kth[i])) + 0x5851F42D4C957F2Dull;
+        v = (v * 0x94D049BB133111EBull) ^ ((i + 7) * 0x9E3779B97F4A7C15ull);
+        acc += v ^ (v >> 29);
+    }
+    for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
 Status cuda_status(cudaError_t e, const char *what) {
     Status s;
     s.code = (e == cudaErrorMemoryAllocation) ? GD_ERR_OUT_OF_MEMORY : GD_ERR_CUDA;
@@ -71,6 +91,7 @@ struct gd_handle {
     gd::DevBuf<float> kth;
     gd::DevBuf<int32_t> spatial;
     gd::Collider col;
+    gd::Tuning tune;
     bool geom_valid = false;   // col_geom_valid (swarm_runtime.cu:332)
     bool cache_valid = false;
     std::string err;
@@ -200,9 +221,162 @@ gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
     h->geom_valid = false;
     h->cache_valid = false;
+    h->geo.sort_bits = h->tune.sort_bits;
     gd::Status s = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
     if (s) h->geom_valid = true;
     return done(h, s);
+}
+
+static bool tuning_ok(const gd::Model &m, const gd_tuning &t) {
+    const int full = 21 * m.dim;
+    return t.warps_per_block >= 0 && t.warps_per_block <= 32 && t.prescan >= 0 && t.prescan <= 8 &&
+           (t.walk_breadth_first == 0 || t.walk_breadth_first == 1) &&
+           (t.sort_bits == 0 || (t.sort_bits >= 16 * m.dim && t.sort_bits <= full));
+}
+
+static gd::Tuning to_tuning(const gd_tuning &t) {
+    gd::Tuning u;
+    u.warps = t.warps_per_block;
+    u.prescan = t.prescan;
+    u.bfs = t.walk_breadth_first;
+    u.sort_bits = t.sort_bits;
+    return u;
+}
+
+static gd_tuning from_tuning(const gd::Tuning &u) {
+    gd_tuning t;
+    t.warps_per_block = u.warps;
+    t.prescan = u.prescan;
+    t.walk_breadth_first = u.bfs;
+    t.sort_bits = u.sort_bits;
+    return t;
+}
+
+gd_status gd_get_tuning(const gd_handle *h, gd_tuning *out) {
+    if (!h || !out) return GD_ERR_INVALID_ARGUMENT;
+    *out = from_tuning(h->tune);
+    return GD_OK;
+}
+
+gd_status gd_set_tuning(gd_handle *h, const gd_tuning *t) {
+    if (!h || !t) return GD_ERR_INVALID_ARGUMENT;
+    if (!tuning_ok(h->m, *t)) return fail(h, GD_ERR_INVALID_ARGUMENT, "tuning out of range");
+    if (t->warps_per_block > 0 && gd::knn_block_warps(h->m.n_k, to_tuning(*t), nullptr) == 0)
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory");
+    h->tune = to_tuning(*t);
+    return GD_OK;
+}
+
+gd_status gd_autotune(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int tune_sort,
+                      gd_tuning *out_best, double *out_ms) {
+    if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    const bool deferred = h->geo.deferred_check;
+    h->geo.deferred_check = false;  // the tuner screens its input once, eagerly
+    cudaEvent_t a = nullptr, b = nullptr;
+    gd::DevBuf<unsigned long long> digest;
+    gd::Status st;
+    auto cuda = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && st) st = gd::cuda_status(e, what);
+        return static_cast<bool>(st);
+    };
+    cuda(digest.alloc(1), "autotune digest");
+    if (st) cuda(cudaEventCreate(&a), "autotune event");
+    if (st) cuda(cudaEventCreate(&b), "autotune event");
+    // one timed run (best of two): optional geometry build, then the query; returns ms and a digest
+    // of the codes and kept d^2, which every tuning must reproduce bit for bit
+    auto run = [&](const gd::Tuning &t, bool build, float &ms, unsigned long long &dig) {
+        ms = 1e30f;
+        for (int rep = 0; rep < 2 && st; ++rep) {
+            cuda(cudaEventRecord(a, h->stream), "autotune record");
+            if (st && build) {
+                h->geo.sort_bits = t.sort_bits;
+                st = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
+            }
+            if (st)
+                st = gd::knn_query(h->geo, h->m, dev_particle, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream,
+                                   dev_radius, nullptr, t);
+            if (st) cuda(cudaEventRecord(b, h->stream), "autotune record");
+            if (st) cuda(cudaEventSynchronize(b), "autotune run");
+            float e = 0.f;
+            if (st) cuda(cudaEventElapsedTime(&e, a, b), "autotune time");
+            if (st && e < ms) ms = e;
+        }
+        if (!st) return;
+        cuda(cudaMemsetAsync(digest.ptr, 0, sizeof(unsigned long long), h->stream), "autotune digest");
+        gd::k_codes_digest<<<592, 256, 0, h->stream>>>(h->codes.ptr, static_cast<size_t>(h->n) * h->m.n_k, h->kth.ptr,
+                                                       h->n, digest.ptr);
+        cuda(cudaGetLastError(), "autotune digest");
+        if (st) cuda(cudaMemcpy(&dig, digest.ptr, sizeof(dig), cudaMemcpyDeviceToHost), "autotune digest");
+    };
+    gd::Tuning best = h->tune;
+    float best_ms = 0.f, ms = 0.f;
+    unsigned long long ref = 0, dig = 0;
+    run(best, true, best_ms, ref);
+    auto consider = [&](const gd::Tuning &t, bool build) {
+        if (!st) return;
+        run(t, build, ms, dig);
+        if (!st) return;
+        if (dig != ref) {
+            st = gd::Status{GD_ERR_CONTROLLER, "autotune: a tuning changed the neighbour lists", 0};
+            return;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    };
+    if (st && tune_sort) {
+        // sort order: all Morton bits, or the top 16 per axis (fewer radix passes, coarser buckets)
+        for (int sb : {0, 16 * h->m.dim}) {
+            if (sb == best.sort_bits) continue;
+            gd::Tuning t = best;
+            t.sort_bits = sb;
+            consider(t, true);
+        }
+    }
+    if (st) {
+        // the query alone from here on, on the geometry of the chosen sort order
+        const gd::Tuning base = best;
+        run(base, true, best_ms, dig);
+        if (st && dig != ref) st = gd::Status{GD_ERR_CONTROLLER, "autotune: a tuning changed the neighbour lists", 0};
+        if (st) run(base, false, best_ms, dig);
+    }
+    for (int bfs = 1; bfs >= 0 && st; --bfs)
+        for (int pre = 1; pre <= 3 && st; ++pre) {
+            gd::Tuning t = best;
+            t.bfs = bfs;
+            t.prescan = pre;
+            if (t.bfs == best.bfs && t.prescan == best.prescan) continue;
+            consider(t, false);
+        }
+    for (int w : {1, 2, 4, 8}) {
+        if (!st) break;
+        gd::Tuning t = best;
+        t.warps = w;
+        if (gd::knn_block_warps(h->m.n_k, t, nullptr) == 0 || t.warps == best.warps) continue;
+        consider(t, false);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    h->geo.deferred_check = deferred;
+    if (!st) {
+        h->geom_valid = false;
+        h->cache_valid = false;
+        return fail(h, st);
+    }
+    // leave the handle built and cached with the chosen tuning
+    h->tune = best;
+    h->geo.sort_bits = best.sort_bits;
+    gd::Status s2 = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
+    if (s2) s2 = gd::knn_query(h->geo, h->m, dev_particle, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream,
+                               dev_radius, nullptr, best);
+    h->geom_valid = static_cast<bool>(s2);
+    h->cache_valid = static_cast<bool>(s2) && !dev_radius;
+    h->col.local_geometry_valid = false;
+    if (!s2) return fail(h, s2);
+    if (out_best) *out_best = from_tuning(best);
+    if (out_ms) *out_ms = best_ms;
+    return done(h, s2);
 }
 
 gd_status gd_set_deferred_checks(gd_handle *h, int on) {
@@ -229,7 +403,7 @@ gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_cod
     int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
     double *measure = dev_measure ? dev_measure : h->measure.ptr;
     float *kth = dev_kth_d2 ? dev_kth_d2 : h->kth.ptr;
-    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream);
+    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream, nullptr, nullptr, h->tune);
     if (s && own) {
         h->cache_valid = true;
         h->col.local_geometry_valid = false;
@@ -245,7 +419,8 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
     int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
     double *measure = dev_measure ? dev_measure : h->measure.ptr;
     float *kth = dev_kth_d2 ? dev_kth_d2 : h->kth.ptr;
-    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream, dev_radius, dev_stats);
+    gd::Status s = gd::knn_query(h->geo, h->m, dev_particle, codes, measure, kth, h->stream, dev_radius, dev_stats,
+                                 h->tune);
     if (s && own) {
         h->cache_valid = true;
         h->col.local_geometry_valid = false;
@@ -357,10 +532,12 @@ gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *de
     } else {
         h->geom_valid = false;
         h->cache_valid = false;
+        h->geo.sort_bits = h->tune.sort_bits;
         s = gd::geometry_build(h->geo, h->m, dev_particle, h->stream);
         if (s) {
             h->geom_valid = true;
-            s = gd::knn_query(h->geo, h->m, dev_particle, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream);
+            s = gd::knn_query(h->geo, h->m, dev_particle, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream, nullptr,
+                              nullptr, h->tune);
         }
         if (s) s = gd::space_bin(h->m, dev_particle, h->n, h->spatial.ptr, h->stream);
         if (s) {

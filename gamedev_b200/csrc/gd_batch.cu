@@ -35,6 +35,7 @@ struct gd_batch {
     std::vector<cudaEvent_t> done;
     cudaEvent_t start = nullptr;
     long long launches = 0;
+    gd::Tuning tune;
     std::string err;
     long long detail = 0;
 
@@ -158,6 +159,7 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
             return batch_fail(b, gd::cuda_status(cudaGetLastError(), "fork batch streams"));
     for (int s = 0; s < b->S; ++s) {
         gd::Geometry &g = *b->geo[s];
+        g.sort_bits = b->tune.sort_bits;
         const long long before = g.launches;
         gd::Status st = gd::geometry_build(g, b->models[s], dev_particle + b->part_off[s], b->workers[s % W]);
         b->launches += g.launches - before;
@@ -171,7 +173,7 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
     }
     gd::Status st = gd::knn_batch_query(b->models[0], b->tab.ptr, b->leaf_prefix.ptr, b->part_prefix.ptr, b->S,
                                         b->n_total, b->kcap, b->next.ptr, dev_particle, dev_codes, dev_measure,
-                                        dev_kth_d2, b->stream, &b->launches);
+                                        dev_kth_d2, b->stream, &b->launches, b->tune);
     if (!st) return batch_fail(b, st);
     b->err.clear();
     b->detail = 0;
@@ -193,6 +195,24 @@ gd_status gd_batch_check(gd_batch *b) {
     }
     b->err.clear();
     b->detail = 0;
+    return GD_OK;
+}
+
+gd_status gd_batch_set_tuning(gd_batch *b, const gd_tuning *t) {
+    if (!b || !t) return GD_ERR_INVALID_ARGUMENT;
+    const int dim = b->models[0].dim;
+    const bool ok = t->warps_per_block >= 0 && t->warps_per_block <= 32 && t->prescan >= 0 && t->prescan <= 8 &&
+                    (t->walk_breadth_first == 0 || t->walk_breadth_first == 1) &&
+                    (t->sort_bits == 0 || (t->sort_bits >= 16 * dim && t->sort_bits <= 21 * dim));
+    if (!ok) return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "tuning out of range");
+    gd::Tuning u;
+    u.warps = t->warps_per_block;
+    u.prescan = t->prescan;
+    u.bfs = t->walk_breadth_first;
+    u.sort_bits = t->sort_bits;
+    if (u.warps > 0 && gd::knn_block_warps(b->kcap, u, nullptr) == 0)
+        return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory");
+    b->tune = u;
     return GD_OK;
 }
 

@@ -299,6 +299,8 @@ struct QueryArgs {
     double *measure;        // may be null
     float *kth;             // may be null
     const float *radius;    // proposed search radius by particle index, or null for the plain query
+    int prescan;            // Morton-neighbour buckets scanned on each side before the walk
+    int bfs;                // breadth-first (1) or depth-first (0) walk
     unsigned long long *stats;  // optional counters: leaves scanned, nodes tested, offers, fallbacks
 };
 
@@ -496,9 +498,9 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 const int lf = (t == 0) ? leaf : ((t & 1) ? leaf - (t + 1) / 2 : leaf + t / 2);
                 return (lf >= 0 && lf < n_leaves) ? lf : -1;
             },
-            2 * kPrescan + 1);
+            2 * a.prescan + 1);
     };
-    auto prescanned = [&](int lf) { return lf >= leaf - kPrescan && lf <= leaf + kPrescan; };
+    auto prescanned = [&](int lf) { return lf >= leaf - a.prescan && lf <= leaf + a.prescan; };
 
     // Depth-first walk.  A node's box is tested when its parent is expanded: both children's
     // boxes are loaded together and only children that can hold a candidate for some lane are
@@ -646,6 +648,10 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
 
     auto walk = [&]() {
         prescan();
+        if (!a.bfs) {
+            walk_dfs();
+            return;
+        }
         // lanes whose heap is not yet full still search the whole q ball: they walk depth-first
         // after the others, so that their ball does not widen the breadth-first union box
         const bool deferred = valid && cut >= 0.0f && cnt < K && !(lim2 < q2);
@@ -739,7 +745,8 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
 // ------------------------------------------------------------------------------------------------
 __global__ void k_knn_batch(Model m, const BatchSwarm *__restrict__ tab, const int *__restrict__ leaf_prefix, int S,
                             int *__restrict__ next, const gd_particle *__restrict__ part, int32_t *__restrict__ codes,
-                            double *__restrict__ measure, float *__restrict__ kth, int kcap) {
+                            double *__restrict__ measure, float *__restrict__ kth, int kcap, int prescan,
+                            int bfs) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -773,6 +780,8 @@ __global__ void k_knn_batch(Model m, const BatchSwarm *__restrict__ tab, const i
         a.kth = kth + b.part_off;
         a.radius = nullptr;
         a.stats = nullptr;
+        a.prescan = prescan;
+        a.bfs = bfs;
         knn_bucket(m, a, item - leaf_prefix[lo], wbase, kcap);
         __syncwarp();
     }
@@ -801,19 +810,11 @@ __global__ void k_batch_inactive_rows(const BatchSwarm *__restrict__ tab, const 
 Status knn_batch_query(const Model &m, const BatchSwarm *dev_tab, const int *dev_leaf_prefix,
                        const long long *dev_part_prefix, int S, long long n_total, int kcap, int *dev_next,
                        const gd_particle *part, int32_t *codes, double *measure, float *kth, cudaStream_t s,
-                       long long *launches) {
+                       long long *launches, const Tuning &tune) {
     const size_t per_warp = knn_warp_bytes(kcap);
-    const size_t sm_bytes = 227 * 1024;
-    int best = 1, best_res = 0;
-    for (int w = 1; w <= 8; ++w) {
-        if (per_warp * w > sm_bytes) break;
-        const int res = static_cast<int>(sm_bytes / (per_warp * w + 1024)) * w;
-        if (res > best_res) {
-            best_res = res;
-            best = w;
-        }
-    }
-    const int warps = best;
+    int best_res = 0;
+    const int warps = knn_block_warps(kcap, tune, &best_res);
+    if (warps == 0) return Status{GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory", 0};
     const size_t smem = per_warp * warps;
     static int smem_set[64] = {};
     int dev = 0, sms = 0;
@@ -828,7 +829,7 @@ Status knn_batch_query(const Model &m, const BatchSwarm *dev_tab, const int *dev
     const int blocks = sms * (best_res / warps);
     GD_TRY_CUDA(cudaMemsetAsync(dev_next, 0, sizeof(int), s));
     k_knn_batch<<<blocks, warps * 32, smem, s>>>(m, dev_tab, dev_leaf_prefix, S, dev_next, part, codes, measure, kth,
-                                                 kcap);
+                                                 kcap, tune.prescan, tune.bfs);
     k_batch_inactive_rows<<<static_cast<unsigned int>((n_total + 255) / 256), 256, 0, s>>>(
         dev_tab, dev_part_prefix, S, n_total, codes, measure, kth);
     if (launches) *launches += 2;
@@ -943,14 +944,16 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     if (!g.deferred_check) GD_TRY(geometry_check(g, s));
     // radix sort over the bits that carry key information (inactive keys are all ones)
     const int tiles = g.n_sort / kRadixTile;
-    const int passes = (g.key_bits + 7) / 8;
+    const int bits = (g.sort_bits > 0 && g.sort_bits < g.key_bits) ? g.sort_bits : g.key_bits;
+    const int passes = (bits + 7) / 8;
+    const int shift0 = g.key_bits - 8 * passes > 0 ? g.key_bits - 8 * passes : 0;  // the top `bits`
     unsigned long long *kin = g.key_a.ptr, *kout = g.key_b.ptr;
     unsigned int *vin = g.val_a.ptr, *vout = g.val_b.ptr;
     const int hist_len = 256 * tiles;
     const int chunks = (hist_len + kScanChunk - 1) / kScanChunk;
     unsigned int *part = chunks > 1 ? g.hist.ptr + hist_len : nullptr;
     for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
+        const int shift = shift0 + 8 * p;
         g.launches += part ? 4 : 3;
         k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, shift, tiles, g.hist.ptr);
         k_scan_chunks<<<chunks, kRadixThreads, 0, s>>>(g.hist.ptr, hist_len, part);
@@ -992,23 +995,36 @@ Status geometry_check(Geometry &g, cudaStream_t s) {
 
 size_t knn_smem_per_warp(int K) { return knn_warp_bytes(K); }
 
-Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
-                 float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats) {
-    const int K = m.n_k;
+int knn_block_warps(int K, const Tuning &tune, int *resident) {
+    // the per-lane heaps bound residency: by default pick the block width that keeps the most
+    // warps per SM (227 KB of shared memory per SM, at most 8 warps per block)
     const size_t per_warp = knn_smem_per_warp(K);
-    // the per-lane heaps bound residency: pick the block width that keeps the most warps per SM
-    // (227 KB of shared memory per SM, at most 8 warps per block)
     const size_t sm_bytes = 227 * 1024;
+    auto res_of = [&](int w) { return static_cast<int>(sm_bytes / (per_warp * w + 1024)) * w; };
+    if (tune.warps > 0) {
+        if (tune.warps > 32 || per_warp * tune.warps > sm_bytes) return 0;
+        if (resident) *resident = res_of(tune.warps);
+        return tune.warps;
+    }
     int best = 1, best_res = 0;
     for (int w = 1; w <= 8; ++w) {
         if (per_warp * w > sm_bytes) break;
-        const int res = static_cast<int>(sm_bytes / (per_warp * w + 1024)) * w;
+        const int res = res_of(w);
         if (res > best_res) {
             best_res = res;
             best = w;
         }
     }
-    const int warps = best;
+    if (resident) *resident = best_res;
+    return best;
+}
+
+Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
+                 float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats, const Tuning &tune) {
+    const int K = m.n_k;
+    const size_t per_warp = knn_smem_per_warp(K);
+    const int warps = knn_block_warps(K, tune, nullptr);
+    if (warps == 0) return Status{GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory", 0};
     const size_t smem = per_warp * warps;
     // raise the kernel's shared-memory limit only when a larger one is needed, so that a step
     // enqueued under stream capture after a first eager call makes no attribute call
@@ -1036,6 +1052,8 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     qa.kth = kth_d2;
     qa.radius = radius;
     qa.stats = stats;
+    qa.prescan = tune.prescan;
+    qa.bfs = tune.bfs;
     const int max_leaves = (g.n + kLeaf - 1) / kLeaf;
     const int blocks = (max_leaves + warps - 1) / warps;
     g.launches += 2;

@@ -126,6 +126,15 @@ struct Geometry {
     // Deferred screen: the build enqueues everything without waiting for the non-finite screen,
     // and geometry_check reads it later (what stream capture into a CUDA graph needs).
     bool deferred_check = false;
+    int sort_bits = 0;  // top Morton key bits the radix sort orders by (0: all)
+};
+
+// Speed-only settings of the neighbour search (every setting gives the same exact lists).
+struct Tuning {
+    int warps = 0;            // warps per block of the top-K kernel; 0 = the most resident warps
+    int prescan = kPrescan;   // Morton-neighbour buckets scanned on each side before the walk
+    int bfs = 1;              // breadth-first walk (1) or depth-first walk (0)
+    int sort_bits = 0;        // top Morton key bits the radix sort orders by (0: all)
 };
 
 Status geometry_alloc(Geometry &g, const Model &m, int n);
@@ -141,7 +150,10 @@ Status geometry_check(Geometry &g, cudaStream_t s);
 // [8-site leaf groups scanned, nodes tested, candidate offers, fallbacks].
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes,
                  double *measure, float *kth_d2, cudaStream_t s, const float *radius = nullptr,
-                 unsigned long long *stats = nullptr);
+                 unsigned long long *stats = nullptr, const Tuning &tune = Tuning());
+// Warps per block of the top-K kernel for K neighbours under `tune` (0 when infeasible), and the
+// resident warps per SM it gives.
+int knn_block_warps(int K, const Tuning &tune, int *resident);
 // One swarm of a batch as the persistent batch query sees it: its geometry and the offsets of its
 // rows in the caller's concatenated particle (part_off) and code (codes_off) buffers.
 struct BatchSwarm {
@@ -160,7 +172,7 @@ struct BatchSwarm {
 Status knn_batch_query(const Model &m, const BatchSwarm *dev_tab, const int *dev_leaf_prefix,
                        const long long *dev_part_prefix, int S, long long n_total, int kcap, int *dev_next,
                        const gd_particle *part, int32_t *codes, double *measure, float *kth, cudaStream_t s,
-                       long long *launches);
+                       long long *launches, const Tuning &tune = Tuning());
 // Learned-radius features of every owner (gd_radius.cu).
 Status radius_features(const Geometry &g, const Model &m, const gd_particle *part, const float *prev_kth,
                        double total_mass, float *feat, cudaStream_t s);

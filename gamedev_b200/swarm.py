@@ -76,6 +76,24 @@ class SwarmCollision:
         self.lib.gd_set_stream(self.h, _stream())
         self._check(self.lib.gd_geometry_build(self.h, C.c_void_p(_ptr(particles))))
 
+    def tuning(self) -> dict:
+        t = _lib.GdTuning()
+        self._check(self.lib.gd_get_tuning(self.h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in t._fields_}
+
+    def set_tuning(self, **kw):
+        t = _lib.GdTuning(**{**self.tuning(), **kw})
+        self._check(self.lib.gd_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, particles, radius=None, tune_sort: bool = True):
+        """gd_autotune on these particles (and proposed radii): returns (tuning dict, query ms)."""
+        self.lib.gd_set_stream(self.h, _stream())
+        t = _lib.GdTuning()
+        ms = C.c_double(0.0)
+        self._check(self.lib.gd_autotune(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(radius)),
+                                         1 if tune_sort else 0, C.byref(t), C.byref(ms)))
+        return {f: getattr(t, f) for f, _ in t._fields_}, float(ms.value)
+
     def set_deferred_checks(self, on: bool = True):
         """Defer the non-finite screen of col_site_init to check_geometry(), so a build + query
         sequence makes no host synchronisation (needed to capture it in a CUDA graph)."""
@@ -388,6 +406,10 @@ class SwarmBatch:
 
     def rows_of(self, t, s: int):
         return t[int(self.part_off[s]):int(self.part_off[s + 1])]
+
+    def set_tuning(self, warps_per_block=0, prescan=2, walk_breadth_first=1, sort_bits=0):
+        t = _lib.GdTuning(warps_per_block, prescan, walk_breadth_first, sort_bits)
+        self._check(self.lib.gd_batch_set_tuning(self.h, C.byref(t)))
 
     def launch_count(self) -> int:
         return int(self.lib.gd_batch_launch_count(self.h))

@@ -150,6 +150,28 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
                          int32_t *dev_codes, double *dev_measure, float *dev_kth_d2,
                          unsigned long long *dev_stats);
 
+/* Speed-only settings of the neighbour search; every setting gives the same exact lists.  No
+ * counterpart in the reference (whose KD/Morton parameters are compile-time constants).
+ *   warps_per_block     warps per block of the top-K kernel (0: the most resident warps)
+ *   prescan             Morton-neighbour buckets scanned on each side before the tree walk (0..8)
+ *   walk_breadth_first  1: breadth-first walk with a pipelined leaf list; 0: depth-first walk
+ *   sort_bits           top Morton key bits the index sort orders by: 0 (all, 21 per axis) or
+ *                       16..21 per axis (fewer radix passes, coarser buckets) */
+typedef struct gd_tuning {
+    int warps_per_block, prescan, walk_breadth_first, sort_bits;
+} gd_tuning;
+gd_status gd_get_tuning(const gd_handle *h, gd_tuning *out);
+gd_status gd_set_tuning(gd_handle *h, const gd_tuning *t);
+
+/* Autotuner: times the search on the caller's own particles (and proposed radii, or NULL for the
+ * plain query) over the sort order (if tune_sort), the walk and prescan depth, then the block width
+ * (greedy, best of two runs each), checks that every setting reproduces the starting setting's
+ * codes and kept d^2 bit for bit (GD_ERR_CONTROLLER otherwise), keeps the fastest in the handle and
+ * leaves the geometry built with it.  *out_best / *out_ms (may be NULL) receive the setting and its
+ * query time.  Synchronises the stream; not for use under stream capture. */
+gd_status gd_autotune(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int tune_sort,
+                      gd_tuning *out_best, double *out_ms);
+
 /* Deferred non-finite screen (on != 0).  gd_geometry_build then enqueues the whole build without
  * waiting for its non-finite screen (the reference's stop on the first non-finite particle,
  * swarm_runtime.cu:382-393), so a build + query sequence makes no host synchronisation and can be
@@ -308,6 +330,7 @@ gd_status gd_batch_set_stream(gd_batch *b, void *stream);
 gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
                        float *dev_kth_d2);
 gd_status gd_batch_check(gd_batch *b);
+gd_status gd_batch_set_tuning(gd_batch *b, const gd_tuning *t);  /* walk, prescan, block width, sort */
 size_t    gd_batch_last_error(const gd_batch *b, char *buf, size_t len);
 long long gd_batch_error_detail(const gd_batch *b);
 long long gd_batch_launch_count(const gd_batch *b);
