@@ -292,6 +292,10 @@ __global__ void __launch_bounds__(128) k_bath_rate(Model m, RateArgs a) {
     const double meas = a.measure[i];
     const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
     const double size_i = a.size_old[i];
+    // the physical kernel on the cached environment: owner terms once per owner
+    const bool cached = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m) && a.env;
+    PairOwner po{0.0, 0.0, 0.0};
+    if (cached) po = cached_owner_terms(m, o.env, size_i);
     for (int s = lane; s < K; s += 32) {
         double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
         const int nb = a.codes[static_cast<size_t>(i) * K + s];
@@ -299,7 +303,8 @@ __global__ void __launch_bounds__(128) k_bath_rate(Model m, RateArgs a) {
             const int j = nb / 3;
             const double size_j = a.size_old[j];
             double vrel;
-            double pr = pair_rate(m, o, size_i, size_j, a.numr_old[j], a.part, j, vrel);
+            double pr = cached ? pair_rate_cached(m, o, po, size_i, size_j, a.numr_old[j], a.part, j, vrel)
+                               : pair_rate(m, o, size_i, size_j, a.numr_old[j], a.part, j, vrel);
             double mean = 0.0, sec = 0.0, maxi = 0.0;
             pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
             mx = pr > 0.0 ? maxi : 0.0;
@@ -692,40 +697,101 @@ struct AuditArgs {
 };
 
 // col_audit_bin (col_audit_bin.cu:13-60)
-__global__ void k_audit_bin(Model m, AuditArgs a) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= a.count) return;
-    int i = owner_at(a.ids, slot);
-    if (!a.active[i]) return;
-    int g = a.spatial[i];
-    double duration = a.dt[g];
-    int start = a.binmap[g * m.col_bin_s + size_bin(m, a.size_old[i], a.lower, a.upper, g)];
-    int stop = a.binmap[g * m.col_bin_s + size_bin(m, a.part[i].par_size, a.lower, a.upper, g)];
-    double weight = a.numr_old[i] * grain_mass(m, a.size_old[i]);
-    double probability = -expm1(-a.rate[i] * duration);
-    double expected = a.hazard[i];
-    double events = static_cast<double>(a.events[i]);
-    AuditBin *b = a.bin + start;
-    atomicAdd(&b->owner_count, 1);
-    if (!isfinite(weight) || !(weight > 0.0) || !isfinite(probability) || !isfinite(expected) || expected < 0.0 ||
-        !isfinite(events) || !isfinite(a.jump1[i]) || a.jump1[i] < 0.0 || !isfinite(a.jump2[i]) || a.jump2[i] < 0.0 ||
-        !isfinite(a.jumpmax[i]) || a.jumpmax[i] < 0.0 || !isfinite(a.part[i].par_size) || !(a.part[i].par_size > 0.0)) {
-        atomicAdd(&b->invalid_count, 1);
-        return;
+// Audit sums per merged bin.  The lanes of a warp whose owners share a bin combine their terms
+// in shared memory and one of them adds them to the bin (owners of one spatial group sit together,
+// so a warp mostly feeds one or two bins): one atomic per bin and warp instead of one per owner.
+constexpr int kAuditTerms = 13;  // staged doubles per owner besides the two maxima
+constexpr int kAuditTPB = 256;   // threads per block of k_audit_bin
+__global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
+    __shared__ double terms[kAuditTPB / 32][32][kAuditTerms + 2];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = 0;
+    bool on = slot < a.count;
+    if (on) {
+        i = owner_at(a.ids, slot);
+        on = a.active[i] != 0;
     }
-    atomicAdd(&b->mass, weight);
-    atomicAdd(&b->predicted_f, weight * probability);
-    atomicAdd(&b->predicted_e, weight * expected);
-    atomicAdd(&b->predicted_var_f, weight * weight * probability * (1.0 - probability));
-    atomicAdd(&b->predicted_var_e, weight * weight * expected);
-    atomicAdd(&b->predicted_g, weight * a.jump1[i]);
-    atomicAdd(&b->predicted_var_g, weight * weight * a.jump2[i]);
-    atomic_max_double(&b->maximum_weight, weight);
-    atomic_max_double(&b->maximum_g_jump, weight * a.jumpmax[i]);
-    if (a.events[i] > 0) atomicAdd(&b->touched, weight);
-    atomicAdd(&b->event_weight, weight * events);
-    atomicAdd(&b->growth, weight * fabs(log(a.part[i].par_size / a.size_old[i])));
-    atomicAdd(&a.bin[stop].end_mass, weight);
+    int start = -1, stop = -1;
+    bool valid = false;
+    double t[kAuditTerms + 2];
+#pragma unroll
+    for (int f = 0; f < kAuditTerms + 2; ++f) t[f] = 0.0;
+    if (on) {
+        const int g = a.spatial[i];
+        const double duration = a.dt[g];
+        start = a.binmap[g * m.col_bin_s + size_bin(m, a.size_old[i], a.lower, a.upper, g)];
+        stop = a.binmap[g * m.col_bin_s + size_bin(m, a.part[i].par_size, a.lower, a.upper, g)];
+        const double weight = a.numr_old[i] * grain_mass(m, a.size_old[i]);
+        const double probability = -expm1(-a.rate[i] * duration);
+        const double expected = a.hazard[i];
+        const double events = static_cast<double>(a.events[i]);
+        valid = !(!isfinite(weight) || !(weight > 0.0) || !isfinite(probability) || !isfinite(expected) ||
+                  expected < 0.0 || !isfinite(events) || !isfinite(a.jump1[i]) || a.jump1[i] < 0.0 ||
+                  !isfinite(a.jump2[i]) || a.jump2[i] < 0.0 || !isfinite(a.jumpmax[i]) || a.jumpmax[i] < 0.0 ||
+                  !isfinite(a.part[i].par_size) || !(a.part[i].par_size > 0.0));
+        if (valid) {
+            t[0] = weight;
+            t[1] = weight * probability;
+            t[2] = weight * expected;
+            t[3] = weight * weight * probability * (1.0 - probability);
+            t[4] = weight * weight * expected;
+            t[5] = weight * a.jump1[i];
+            t[6] = weight * weight * a.jump2[i];
+            t[7] = a.events[i] > 0 ? weight : 0.0;
+            t[8] = weight * events;
+            t[9] = weight * fabs(log(a.part[i].par_size / a.size_old[i]));
+            t[10] = weight;                  // end mass (bin `stop`)
+            t[11] = 1.0;                     // valid owner
+            t[12] = 0.0;
+            t[13] = weight;                  // maximum weight
+            t[14] = weight * a.jumpmax[i];   // maximum weighted jump
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < kAuditTerms + 2; ++f) terms[wib][lane][f] = t[f];
+    const unsigned int on_mask = __ballot_sync(0xffffffffu, on);
+    const unsigned int valid_mask = __ballot_sync(0xffffffffu, valid);
+    __syncwarp();
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(on_mask, start);
+    if (lane == __ffs(peers) - 1) {
+        AuditBin *b = a.bin + start;
+        double sum[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double mw = 0.0, mg = 0.0;
+        int owners = __popc(peers), invalid = __popc(peers & ~valid_mask);
+        for (unsigned int pm = peers & valid_mask; pm; pm &= pm - 1) {
+            const int l = __ffs(pm) - 1;
+#pragma unroll
+            for (int f = 0; f < 10; ++f) sum[f] += terms[wib][l][f];
+            mw = fmax(mw, terms[wib][l][13]);
+            mg = fmax(mg, terms[wib][l][14]);
+        }
+        atomicAdd(&b->owner_count, owners);
+        if (invalid) atomicAdd(&b->invalid_count, invalid);
+        if (peers & valid_mask) {
+            atomicAdd(&b->mass, sum[0]);
+            atomicAdd(&b->predicted_f, sum[1]);
+            atomicAdd(&b->predicted_e, sum[2]);
+            atomicAdd(&b->predicted_var_f, sum[3]);
+            atomicAdd(&b->predicted_var_e, sum[4]);
+            atomicAdd(&b->predicted_g, sum[5]);
+            atomicAdd(&b->predicted_var_g, sum[6]);
+            atomic_max_double(&b->maximum_weight, mw);
+            atomic_max_double(&b->maximum_g_jump, mg);
+            atomicAdd(&b->touched, sum[7]);
+            atomicAdd(&b->event_weight, sum[8]);
+            atomicAdd(&b->growth, sum[9]);
+        }
+    }
+    // end mass goes to the bin of the owner's new size
+    if (!valid) return;
+    const unsigned int speers = __match_any_sync(valid_mask, stop);
+    if (lane == __ffs(speers) - 1) {
+        double em = 0.0;
+        for (unsigned int pm = speers; pm; pm &= pm - 1) em += terms[wib][__ffs(pm) - 1][10];
+        atomicAdd(&a.bin[stop].end_mass, em);
+    }
 }
 
 // owner lists per spatial group (_col_chain.cuh:162-167) by a device counting sort
@@ -1277,7 +1343,7 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         aa.lower = lower;
         aa.upper = upper;
         ++c.launches;
-        k_audit_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, aa);
+        k_audit_bin<<<(count + kAuditTPB - 1) / kAuditTPB, kAuditTPB, 0, s>>>(m, aa);
         GD_TRY_CUDA(cudaGetLastError());
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small, c.small.ptr, L.binmap, cudaMemcpyDeviceToHost, s));
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.audit, c.small.ptr + L.audit, sizeof(AuditBin) * merged,

@@ -138,24 +138,43 @@ __device__ __forceinline__ Env make_env(const Model &m, double y, double z) {
     return e;
 }
 
-// _cached_pair_velocity (inc/swarm/_col_rates.cuh:127-141): physical units, analytic gas
-__device__ __forceinline__ double cached_pair_speed(const Model &m, const Env &e, double size_i, double size_j) {
+// Owner terms of _cached_pair_velocity (inc/swarm/_col_rates.cuh:127-141): the owner's Stokes
+// number, drag factor and grain mass, the same for all of its pairs.
+struct PairOwner {
+    double si, fi, mi;
+};
+
+__device__ __forceinline__ PairOwner cached_owner_terms(const Model &m, const Env &e, double size_i) {
+    PairOwner o;
     double si = m.stokes_0 * (size_i / m.S_0);
     si /= e.radial;
     si /= e.strat;
+    o.si = si;
+    o.fi = 1.0 / (1.0 + si * si);
+    o.mi = grain_mass(m, size_i);
+    return o;
+}
+
+// _cached_pair_velocity with the owner terms evaluated once (the same operations as below)
+__device__ __forceinline__ double cached_pair_speed_o(const Model &m, const Env &e, const PairOwner &o,
+                                                      double size_j) {
+    const double si = o.si, fi = o.fi, mi = o.mi;
     double sj = m.stokes_0 * (size_j / m.S_0);
     sj /= e.radial;
     sj /= e.strat;
-    double fi = 1.0 / (1.0 + si * si);
     double fj = 1.0 / (1.0 + sj * sj);
     double dvr = 2.0 * e.vn * drift_difference(si, fi, sj, fj);
     double dvphi = e.vn * (fi - fj);
     double dvz = e.Z * e.omega * (fmin(si, 0.5) - fmin(sj, 0.5));
     double vt = oc07_speed(si, sj, e.re_inv_sqrt, e.vg_sq);
-    double mi = grain_mass(m, size_i);
     double mj = grain_mass(m, size_j);
     double vb = fmin(sqrt(8.0 * e.cs * e.cs * m.m_mol * (mi + mj) / (M_PI * mi * mj)), e.cs);
     return sqrt(dvr * dvr + dvphi * dvphi + dvz * dvz + vt * vt + vb * vb);
+}
+
+// _cached_pair_velocity (inc/swarm/_col_rates.cuh:127-141): physical units, analytic gas
+__device__ __forceinline__ double cached_pair_speed(const Model &m, const Env &e, double size_i, double size_j) {
+    return cached_pair_speed_o(m, e, cached_owner_terms(m, e, size_i), size_j);
 }
 
 // _get_vrel_pair (inc/swarm/_collision.cuh:277-325) for analytic gas: code units or CONST_ST
@@ -223,6 +242,20 @@ __device__ __forceinline__ double pair_rate(const Model &m, const OwnerCtx &o, d
             double H_gj = R_j * get_hg(m, R_j);
             r /= sqrt(2.0 * M_PI * (o.H_i * o.H_i + H_gj * H_gj));
         }
+    }
+    return r / o.measure;
+}
+
+// pair_rate for the physical kernel on the cached environment, with the owner terms evaluated once
+__device__ __forceinline__ double pair_rate_cached(const Model &m, const OwnerCtx &o, const PairOwner &po,
+                                                   double size_i, double size_j, double numr_j,
+                                                   const gd_particle *part, int j, double &vrel) {
+    vrel = cached_pair_speed_o(m, o.env, po, size_j);
+    double r = numr_j * vrel * M_PI * (size_i + size_j) * (size_i + size_j) / 4.0;
+    if (m.n_z == 1) {
+        double R_j = cyl_R(m, part[j].position[1], part[j].position[2]);
+        double H_gj = R_j * get_hg(m, R_j);
+        r /= sqrt(2.0 * M_PI * (o.H_i * o.H_i + H_gj * H_gj));
     }
     return r / o.measure;
 }
