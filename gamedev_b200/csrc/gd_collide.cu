@@ -277,7 +277,7 @@ struct RateArgs {
 };
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner
-__global__ void __launch_bounds__(128) k_bath_rate(Model m, RateArgs a) {
+__global__ void __launch_bounds__(128, 4) k_bath_rate(Model m, RateArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
