@@ -135,17 +135,39 @@ __global__ void k_size_zero(int G, unsigned long long *mmin, unsigned long long 
     }
 }
 
+// Warp aggregation of the controller's per-group and per-bin atomics: the lanes holding the same
+// key combine their terms with shuffles inside their group and the lowest one updates memory.
+__device__ __forceinline__ unsigned int lanes_below() { return (1u << (threadIdx.x & 31)) - 1u; }
+
 __global__ void k_size_scan(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
                             const int32_t *__restrict__ spatial, const unsigned char *__restrict__ active,
                             unsigned long long *mmin, unsigned long long *mmax) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= count) return;
-    int i = owner_at(ids, slot);
-    double size = part[i].par_size;
-    if (!active[i] || !(size > 0) || !isfinite(size)) return;
-    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(size));
-    atomicMin(&mmin[spatial[i]], bits);
-    atomicMax(&mmax[spatial[i]], bits);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    bool on = slot < count;
+    int g = 0;
+    unsigned long long bits = 0;
+    if (on) {
+        const int i = owner_at(ids, slot);
+        const double size = part[i].par_size;
+        on = active[i] && size > 0 && isfinite(size);
+        if (on) {
+            g = spatial[i];
+            bits = static_cast<unsigned long long>(__double_as_longlong(size));
+        }
+    }
+    const unsigned int mask = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(mask, g);
+    unsigned long long lo = bits, hi = bits;
+    for (unsigned int pm = peers; pm; pm &= pm - 1) {
+        const unsigned long long v = __shfl_sync(peers, bits, __ffs(pm) - 1);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    if ((peers & lanes_below()) == 0) {
+        atomicMin(&mmin[g], lo);
+        atomicMax(&mmax[g], hi);
+    }
 }
 
 __global__ void k_size_bnds(int G, const unsigned long long *mmin, const unsigned long long *mmax, double *lower,
@@ -167,12 +189,21 @@ __device__ __forceinline__ int size_bin(const Model &m, double size, const doubl
 __global__ void k_count_bin(Model m, const int *__restrict__ ids, int count, int *__restrict__ counts,
                             const gd_particle *__restrict__ part, const int32_t *__restrict__ spatial,
                             const unsigned char *__restrict__ active, const double *lower, const double *upper) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= count) return;
-    int i = owner_at(ids, slot);
-    if (!active[i]) return;
-    int g = spatial[i];
-    atomicAdd(counts + g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g), 1);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    bool on = slot < count;
+    int key = 0;
+    if (on) {
+        const int i = owner_at(ids, slot);
+        on = active[i] != 0;
+        if (on) {
+            const int g = spatial[i];
+            key = g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g);
+        }
+    }
+    const unsigned int mask = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(mask, key);
+    if ((peers & lanes_below()) == 0) atomicAdd(counts + key, __popc(peers));
 }
 
 // _build_col_binmap (inc/swarm/_col_bound.cuh:232-285): merge adjacent sparse size bins inside
@@ -216,23 +247,51 @@ __global__ void k_rate_bins(Model m, const int *__restrict__ ids, int count, Rat
                             const double *__restrict__ change, const double *__restrict__ second,
                             const int32_t *__restrict__ spatial, const int *__restrict__ binmap,
                             const unsigned char *__restrict__ active, const double *lower, const double *upper) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= count) return;
-    int i = owner_at(ids, slot);
-    if (!active[i]) return;
-    int g = spatial[i];
-    int b = binmap[g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g)];
-    double weight = part[i].par_numr * grain_mass(m, part[i].par_size);
-    atomicAdd(&bin[b].owner_count, 1);
-    if (!isfinite(weight) || !(weight > 0.0) || !isfinite(rate[i]) || rate[i] < 0.0 || !isfinite(change[i]) ||
-        change[i] < 0 || !isfinite(second[i]) || second[i] < 0) {
-        atomicAdd(&bin[b].invalid_count, 1);
-        return;
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    bool on = slot < count;
+    int b = 0;
+    bool valid = false;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    if (on) {
+        const int i = owner_at(ids, slot);
+        on = active[i] != 0;
+        if (on) {
+            const int g = spatial[i];
+            b = binmap[g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g)];
+            const double weight = part[i].par_numr * grain_mass(m, part[i].par_size);
+            valid = !(!isfinite(weight) || !(weight > 0.0) || !isfinite(rate[i]) || rate[i] < 0.0 ||
+                      !isfinite(change[i]) || change[i] < 0 || !isfinite(second[i]) || second[i] < 0);
+            if (valid) {
+                t0 = weight;
+                t1 = weight * rate[i];
+                t2 = weight * change[i];
+                t3 = weight * second[i];
+            }
+        }
     }
-    atomicAdd(&bin[b].mass, weight);
-    atomicAdd(&bin[b].weighted_rate, weight * rate[i]);
-    atomicAdd(&bin[b].weighted_change, weight * change[i]);
-    atomicAdd(&bin[b].weighted_second, weight * second[i]);
+    const unsigned int mask = __ballot_sync(0xffffffffu, on);
+    const unsigned int vmask = __ballot_sync(0xffffffffu, valid);
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(mask, b);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (unsigned int pm = peers; pm; pm &= pm - 1) {
+        const int l = __ffs(pm) - 1;
+        s0 += __shfl_sync(peers, t0, l);
+        s1 += __shfl_sync(peers, t1, l);
+        s2 += __shfl_sync(peers, t2, l);
+        s3 += __shfl_sync(peers, t3, l);
+    }
+    if ((peers & lanes_below()) == 0) {
+        atomicAdd(&bin[b].owner_count, __popc(peers));
+        const int invalid = __popc(peers & ~vmask);
+        if (invalid) atomicAdd(&bin[b].invalid_count, invalid);
+        if (peers & vmask) {
+            atomicAdd(&bin[b].mass, s0);
+            atomicAdd(&bin[b].weighted_rate, s1);
+            atomicAdd(&bin[b].weighted_change, s2);
+            atomicAdd(&bin[b].weighted_second, s3);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -796,13 +855,28 @@ __global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
 
 // owner lists per spatial group (_col_chain.cuh:162-167) by a device counting sort
 __global__ void k_group_count(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcount) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) atomicAdd(&gcount[spatial[i]], 1);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = i < n;
+    const int g = on ? spatial[i] : 0;
+    const unsigned int mask = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(mask, g);
+    if ((peers & lanes_below()) == 0) atomicAdd(&gcount[g], __popc(peers));
 }
+// each group's lanes reserve consecutive slots with one atomic and write at their rank
 __global__ void k_group_fill(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcursor,
                              int *__restrict__ sorted) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) sorted[atomicAdd(&gcursor[spatial[i]], 1)] = i;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = i < n;
+    const int g = on ? spatial[i] : 0;
+    const unsigned int mask = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const unsigned int peers = __match_any_sync(mask, g);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if ((threadIdx.x & 31) == leader) base = atomicAdd(&gcursor[g], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    sorted[base + __popc(peers & lanes_below())] = i;
 }
 
 // col_dep_graph (col_dep_graph.cu:43-59): edge c->d when an owner in c has a neighbour in d
