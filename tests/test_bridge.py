@@ -5,6 +5,7 @@ constexprs; it must equal the configuration the library is benchmarked with.  Ne
 tree (for gpu.cuh) and nvcc; runs without a GPU."""
 
 import json
+import re
 import os
 import shutil
 import subprocess
@@ -39,8 +40,11 @@ def test_bridge_maps_model_constants(gd, tmp_path, model):
     src = tmp_path / "bridge_main.cu"
     src.write_text(PROGRAM)
     exe = tmp_path / "bridge_main"
-    search = "-DCOLLISION_MORTON" if model == "c1_multisize_2d" else "-DCOLLISION_KDTREE_OFF"
-    cmd = [nvcc, "-std=c++17", "-DCOLLISION", "-DMULTISIZE", "-DGAMEDEV_CUDA", search,
+    # the model's own flags (flags.mk GPU_FLAGS) and its search, as the reference build sets them
+    mk = (ROOT / "mod" / model / "flags.mk").read_text()
+    flags = re.findall(r"^GPU_FLAGS \+= (-D\S+)", mk, flags=re.M)
+    search = "-DCOLLISION_" + re.search(r"^COLLISION_SEARCH := (\w+)", mk, flags=re.M).group(1).upper()
+    cmd = [nvcc, "-std=c++17", *flags, "-DGAMEDEV_CUDA", search,
            "-I", str(ROOT / "mod" / model), "-I", str(ROOT / "mod" / "gd_bridge"), "-I", str(ROOT / "include"),
            "-I", str(REF / "inc"), "-I", str(REF / "inc" / "swarm"),
            str(src), "-o", str(exe), "-L", str(ROOT / "gamedev_b200"), "-lgd_b200",
