@@ -1,0 +1,45 @@
+"""Runner for oracle/_ref/collide_<model>_<n>/ref_collide: the reference's own CUDA collision step
+(evolve_collisions glue + evolve_local_collisions and its kernels, compiled from the GameDev tree
+by oracle/ref/Makefile against a generated model header with N_P = n).  TEST INFRASTRUCTURE ONLY:
+it pins the B200 collision operator against the reference's CUDA build and times it; absent where
+the reference tree was not mounted at build time."""
+
+from __future__ import annotations
+
+import json
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+REF_DIR = Path(__file__).resolve().parents[1] / "_ref"
+
+
+def binary(model: str, n: int) -> Path:
+    return REF_DIR / f"collide_{model}_{n}" / "ref_collide"
+
+
+def available(model: str, n: int) -> bool:
+    return binary(model, n).exists()
+
+
+def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dust_mass: float,
+        operators: int = 1, timeout: float = 1800):
+    """-> (particles after `operators` evolve_collisions(duration) calls on one geometry, info)"""
+    p = np.ascontiguousarray(particles, dtype=np.float64).reshape(-1, 8)
+    n = len(p)
+    with tempfile.TemporaryDirectory() as d:
+        src, dst = Path(d) / "in.bin", Path(d) / "out.bin"
+        with open(src, "wb") as f:
+            np.array([n], dtype=np.int32).tofile(f)
+            p.tofile(f)
+        r = subprocess.run([str(binary(model, n)), str(src), str(dst), str(int(seed)), repr(float(duration)),
+                            repr(float(total_dust_mass)), str(int(operators))],
+                           capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_collide failed ({r.returncode}): {r.stderr.strip()[-2000:]}")
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        raw = np.fromfile(dst, dtype=np.uint8)
+        out = raw[4:].view(np.float64).reshape(n, 8).copy()
+        return out, info
