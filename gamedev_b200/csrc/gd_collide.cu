@@ -115,12 +115,15 @@ __global__ void k_env_cache(Model m, int n, const gd_particle *__restrict__ part
 __global__ void k_bath_init(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
                             double *__restrict__ size_old, double *__restrict__ numr_old, double *__restrict__ time,
                             int *__restrict__ events, unsigned char *__restrict__ complete, double *__restrict__ hazard,
-                            double *__restrict__ jump1, double *__restrict__ jump2, double *__restrict__ jumpmax) {
+                            double *__restrict__ jump1, double *__restrict__ jump2, double *__restrict__ jumpmax,
+                            int *__restrict__ stamp, int publish) {
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= count) return;
     int i = owner_at(ids, slot);
-    size_old[i] = part[i].par_size;
-    numr_old[i] = part[i].par_numr;
+    const double size = part[i].par_size, numr = part[i].par_numr;
+    if (!(size_old[i] == size && numr_old[i] == numr)) stamp[i] = publish;  // the reservoir value changes
+    size_old[i] = size;
+    numr_old[i] = numr;
     time[i] = 0.0;
     events[i] = 0;
     complete[i] = 0;
@@ -333,6 +336,9 @@ struct RateArgs {
     double lambda0;
     double *rate, *change, *second;
     RateMoments *cached;
+    const int *stamp;  // publish wave of each particle's last reservoir change
+    int *rated;        // publish wave of each owner's stored rates (-1: none)
+    int publish;       // the current publish wave
 };
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner
@@ -347,6 +353,15 @@ __global__ void __launch_bounds__(128, 4) k_bath_rate(Model m, RateArgs a) {
     int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
                    static_cast<size_t>(wib) * K;
     const int i = owner_at(a.ids, slot);
+    // stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
+    // since they were evaluated (same geometry and lambda0)
+    const int rated = a.rated[i];
+    bool need = rated < 0 || a.stamp[i] > rated;
+    for (int s = lane; s < K && !need; s += 32) {
+        const int nb = a.codes[static_cast<size_t>(i) * K + s];
+        need = nb >= 0 && a.stamp[nb / 3] > rated;
+    }
+    if (!__any_sync(0xffffffffu, need)) return;
     const bool act = a.active[i] != 0;
     const double meas = a.measure[i];
     const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
@@ -395,6 +410,7 @@ __global__ void __launch_bounds__(128, 4) k_bath_rate(Model m, RateArgs a) {
         a.rate[i] = rate_w[0];
         a.change[i] = change_w[0];
         a.second[i] = second_w[0];
+        a.rated[i] = a.publish;
     }
 }
 
@@ -1162,6 +1178,10 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
     GD_TRY_CUDA(c.complete.alloc(n));
     GD_TRY_CUDA(c.env.alloc(static_cast<size_t>(n) * 8));
     GD_TRY_CUDA(c.cached.alloc(static_cast<size_t>(n) * 4));
+    GD_TRY_CUDA(c.stamp.alloc(n));
+    GD_TRY_CUDA(c.rated.alloc(n));
+    GD_TRY_CUDA(cudaMemset(c.stamp.ptr, 0, sizeof(int) * n));
+    GD_TRY_CUDA(cudaMemset(c.rated.ptr, 0xff, sizeof(int) * n));
     GD_TRY_CUDA(c.ids.alloc(n));
     GD_TRY_CUDA(c.queue.alloc(n));
     GD_TRY_CUDA(c.group_sorted.alloc(n));
@@ -1235,10 +1255,16 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         ++c.launches;
         k_group_fill<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, spatial, at<int>(c.small, L.gcursor), c.group_sorted.ptr);
         GD_TRY_CUDA(cudaGetLastError());
+        // new neighbour lists and measures: no stored rate stands
+        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, s));
         c.local_geometry_valid = true;
     }
 
     const double lambda0 = n / static_cast<double>(K) / total_dust_mass;
+    if (lambda0 != c.rated_lambda0) {
+        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, s));
+        c.rated_lambda0 = lambda0;
+    }
     const Env *env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
     const size_t rate_smem = static_cast<size_t>(4) * (4 * 8 + 4) * K;
     if (rate_smem > 48 * 1024)
@@ -1256,9 +1282,10 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
 
     auto initialize = [&](const int *idp, int count) {
         ++c.launches;
+        ++c.publish;
         k_bath_init<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, c.size_old.ptr, c.numr_old.ptr, c.time.ptr,
                                                             c.events.ptr, c.complete.ptr, c.hazard.ptr, c.jump1.ptr,
-                                                            c.jump2.ptr, c.jumpmax.ptr);
+                                                            c.jump2.ptr, c.jumpmax.ptr, c.stamp.ptr, c.publish);
     };
     // rates, size bins and merged rate bins, then one copy of binmap + rate bins to the host
     auto rates_and_bins = [&](const int *idp, int count, int &merged) -> Status {
@@ -1287,6 +1314,9 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         ra.change = c.change_rate.ptr;
         ra.second = c.second_rate.ptr;
         ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
+        ra.stamp = c.stamp.ptr;
+        ra.rated = c.rated.ptr;
+        ra.publish = c.publish;
         ++c.launches;
         k_bath_rate<<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, s));

@@ -70,6 +70,14 @@ struct Collider {
     DevBuf<double> size_old, numr_old, time, hazard, jump1, jump2, jumpmax, rate, change_rate, second_rate;
     DevBuf<int> events, error;
     DevBuf<unsigned char> complete;
+    // Reuse of bath-start rates: stamp[j] = publish wave at which particle j's reservoir value last
+    // changed; rated[i] = publish wave at which owner i's rates were last evaluated (-1: never on
+    // this geometry).  Rates depend only on the reservoir of the owner and its neighbours, the
+    // neighbour list, measure, positions and lambda0, so an owner whose inputs are unchanged keeps
+    // bit-identical stored rates.
+    DevBuf<int> stamp, rated;
+    int publish = 0;
+    double rated_lambda0 = 0.0;
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
     DevBuf<int> ids, queue, group_sorted, spatial;
