@@ -12,7 +12,7 @@
 // implicit complete binary tree of axis-aligned boxes.  A query warp owns one bucket: each lane
 // is one owner, the warp walks the tree once for all 32 owners, and every candidate bucket is
 // staged once in shared memory and read by all 32 lanes, so one 512-byte tile load serves 1024
-// distance tests.  Each lane keeps its exact top-K as a max-heap of packed (d^2 bits, code) keys
+// distance tests.  Each lane keeps its exact top-K as a 4-ary max-heap of packed (d^2 bits, code) keys
 // in shared memory, the same key the reference heap uses (kdtree/index_heap.cuh:59-69), so the
 // kept set is the reference's set; a final in-place heap sort yields ascending (d^2, code), the
 // order of the reference Morton search (morton_types.cuh:68-72).
@@ -304,39 +304,53 @@ struct QueryArgs {
     unsigned long long *stats;  // optional counters: leaves scanned, nodes tested, offers, fallbacks
 };
 
-__device__ __forceinline__ void heap_sift(unsigned long long *h, int lane, unsigned long long key, int slot, int n) {
+// Per-lane 4-ary max-heaps of 64-bit keys (d^2 bits << 32 | code).  Lane-major: lane l's n
+// entries start at entry l * heap_stride(K).  The root (slot 0) has children 1..3, every other slot
+// i has children 4i..4i+3, so a node's children form one 32-byte aligned group that two 16-byte
+// loads fetch.  A depth-3 heap holds 64 entries.  heap_stride keeps the stride an odd number of 16-byte
+// chunks, so eight lanes reading the same slot group hit eight different bank groups.
+__host__ __device__ constexpr int heap_stride(int K) { return ((K + 3) & ~3) + 2; }
+
+// Sifts `key` down from slot i of a heap of n entries.
+__device__ __forceinline__ void heap_sift(unsigned long long *hp, unsigned long long key, int i, int n) {
     while (true) {
-        int child = 2 * slot + 1;
-        if (child >= n) break;
-        unsigned long long cv = h[child * 32 + lane];
-        if (child + 1 < n) {
-            unsigned long long rv = h[(child + 1) * 32 + lane];
-            if (rv > cv) {
-                cv = rv;
-                ++child;
+        const int c0 = i ? 4 * i : 1;  // first child
+        if (c0 >= n) break;
+        const int gb = c0 & ~3;        // the group holding the children (the root's holds the root too)
+        const ulonglong2 lo = *reinterpret_cast<const ulonglong2 *>(hp + gb);
+        const ulonglong2 hi = *reinterpret_cast<const ulonglong2 *>(hp + gb + 2);
+        const unsigned long long v[4] = {lo.x, lo.y, hi.x, hi.y};
+        unsigned long long bv = 0;
+        int bj = -1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int sl = gb + j;
+            if (sl >= c0 && sl < n && (bj < 0 || v[j] > bv)) {
+                bv = v[j];
+                bj = sl;
             }
         }
-        if (cv < key) break;
-        h[slot * 32 + lane] = cv;
-        slot = child;
+        if (bv < key) break;
+        hp[i] = bv;
+        i = bj;
     }
-    h[slot * 32 + lane] = key;
+    hp[i] = key;
 }
 
-// Floyd heap construction over the first n entries of one lane's column
-__device__ __forceinline__ void heap_build(unsigned long long *h, int lane, int n) {
-    for (int s = n / 2 - 1; s >= 0; --s) heap_sift(h, lane, h[s * 32 + lane], s, n);
+// Floyd heap construction over the first n entries of one lane's heap
+__device__ __forceinline__ void heap_build(unsigned long long *hp, int n) {
+    for (int i = (n - 1) / 4; i >= 0 && n > 1; --i) heap_sift(hp, hp[i], i, n);
 }
 
 __device__ __forceinline__ float key_d2(unsigned long long k) { return __uint_as_float(static_cast<unsigned int>(k >> 32)); }
 
-// Per-warp shared memory of k_knn_query: K-entry heaps of 32 lanes, a 32-site tile (also the
-// breadth-first frontier staging, kFrontier ints), and the leaf list / depth-first stack.
+// Per-warp shared memory of k_knn_query: the heaps of 32 lanes (heap_stride(K) entries each), a
+// 32-site tile (also the breadth-first frontier staging, kFrontier ints), and the leaf list /
+// depth-first stack.
 constexpr int kFrontier = 128;   // internal nodes of one breadth-first level
 constexpr int kListInts = 352;   // leaves of the breadth-first walk (also the depth-first stack)
-__host__ __device__ constexpr size_t knn_warp_bytes(int K) {
-    return static_cast<size_t>(K) * 32 * 8 + 32 * 16 + kListInts * 4;
-}
+__host__ __device__ constexpr size_t knn_heap_bytes(int K) { return static_cast<size_t>(heap_stride(K)) * 32 * 8; }
+__host__ __device__ constexpr size_t knn_warp_bytes(int K) { return knn_heap_bytes(K) + 32 * 16 + kListInts * 4; }
 
 // Loads of one leaf: this lane's site of the 32-site tile and the four 8-site sub-boxes.
 struct LeafLoad {
@@ -350,12 +364,12 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                                            int kcap) {
     const int lane = threadIdx.x & 31;
     const int K = a.k;
-    unsigned long long *heap = reinterpret_cast<unsigned long long *>(wbase);
-    float4 *tile = reinterpret_cast<float4 *>(wbase + static_cast<size_t>(kcap) * 32 * 8);
+    unsigned long long *hp = reinterpret_cast<unsigned long long *>(wbase) + lane * heap_stride(K);
+    float4 *tile = reinterpret_cast<float4 *>(wbase + knn_heap_bytes(kcap));
     // the breadth-first walk stages its next frontier in the tile buffer (no leaf is scanned then)
     int *staging = reinterpret_cast<int *>(tile);
     // leaf list of the breadth-first walk; the depth-first walk's stack (never live together)
-    int *stack = reinterpret_cast<int *>(wbase + static_cast<size_t>(kcap) * 32 * 8 + 32 * 16);
+    int *stack = reinterpret_cast<int *>(wbase + knn_heap_bytes(kcap) + 32 * 16);
     int *leaf_list = stack;
 
     const int n_act = a.counters[0];
@@ -432,16 +446,16 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
             const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
             if (d2 <= cut) {
                 ++st_offers;
-                heap[cnt * 32 + lane] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                                        static_cast<unsigned int>(__float_as_int(p.w));
+                hp[cnt] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                          static_cast<unsigned int>(__float_as_int(p.w));
                 ++cnt;
             }
         }
         const bool build_now = cnt == K && !built;
         if (__any_sync(0xffffffffu, build_now)) {
             if (build_now) {
-                heap_build(heap, lane, K);
-                cut = key_d2(heap[lane]);
+                heap_build(hp, K);
+                cut = key_d2(hp[0]);
                 built = true;
             }
         }
@@ -455,9 +469,9 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 ++st_offers;
                 const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
                                                static_cast<unsigned int>(__float_as_int(p.w));
-                if (key < heap[lane]) {
-                    heap_sift(heap, lane, key, 0, K);
-                    cut = key_d2(heap[lane]);
+                if (key < hp[0]) {
+                    heap_sift(hp, key, 0, K);
+                    cut = key_d2(hp[0]);
                 }
             }
         }
@@ -688,12 +702,12 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     }
 
     // ascending (d^2 bits, code): heap sort of the cnt real entries
-    if (cnt < K) heap_build(heap, lane, cnt);
+    if (cnt < K) heap_build(hp, cnt);
     for (int end = cnt - 1; end > 0; --end) {
-        const unsigned long long top = heap[lane];
-        const unsigned long long last = heap[end * 32 + lane];
-        heap[end * 32 + lane] = top;
-        heap_sift(heap, lane, last, 0, end);
+        const unsigned long long top = hp[0];
+        const unsigned long long last = hp[end];
+        hp[end] = top;
+        heap_sift(hp, last, 0, end);
     }
     if (a.stats && lane == 0) {
         atomicAdd(&a.stats[0], static_cast<unsigned long long>(st_leaves));
@@ -706,21 +720,24 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     }
     if (!valid) return;
 
-    const float maxd2 = cnt > 0 ? key_d2(heap[(cnt - 1) * 32 + lane]) : 0.f;
+    const float maxd2 = cnt > 0 ? key_d2(hp[cnt - 1]) : 0.f;
     int32_t *row = a.codes ? a.codes + static_cast<size_t>(idx) * K : nullptr;
     if (row) {
         if ((K & 3) == 0) {
             for (int s = 0; s < K; s += 4) {
+                // slots s..s+3 are one 32-byte aligned group of this lane's heap
+                const ulonglong2 lo = *reinterpret_cast<const ulonglong2 *>(hp + s);
+                const ulonglong2 hi = *reinterpret_cast<const ulonglong2 *>(hp + s + 2);
                 int4 v;
-                int *vp = &v.x;
-#pragma unroll
-                for (int t = 0; t < 4; ++t)
-                    vp[t] = (s + t < cnt) ? static_cast<int>(static_cast<unsigned int>(heap[(s + t) * 32 + lane])) : -1;
+                v.x = (s < cnt) ? static_cast<int>(static_cast<unsigned int>(lo.x)) : -1;
+                v.y = (s + 1 < cnt) ? static_cast<int>(static_cast<unsigned int>(lo.y)) : -1;
+                v.z = (s + 2 < cnt) ? static_cast<int>(static_cast<unsigned int>(hi.x)) : -1;
+                v.w = (s + 3 < cnt) ? static_cast<int>(static_cast<unsigned int>(hi.y)) : -1;
                 reinterpret_cast<int4 *>(row)[s >> 2] = v;
             }
         } else {
             for (int s = 0; s < K; ++s)
-                row[s] = (s < cnt) ? static_cast<int>(static_cast<unsigned int>(heap[s * 32 + lane])) : -1;
+                row[s] = (s < cnt) ? static_cast<int>(static_cast<unsigned int>(hp[s])) : -1;
         }
     }
     if (a.kth) a.kth[idx] = maxd2;
