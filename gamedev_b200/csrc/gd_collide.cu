@@ -341,8 +341,14 @@ struct RateArgs {
     int publish;       // the current publish wave
 };
 
-// col_bath_rate (col_bath_rate.cu:13-130): one warp per owner
-__global__ void __launch_bounds__(128, 4) k_bath_rate(Model m, RateArgs a) {
+// col_bath_rate (col_bath_rate.cu:13-130): one warp per owner.  kCached selects, at compile time,
+// the physical kernel on the cached environment (owner terms hoisted); the other instantiation
+// serves the synthetic kernels and the uncached physical one.  Each lane takes slots s and s + 32
+// and issues the gathers of both before the pair arithmetic, so their latencies overlap.  The
+// FP64 pair arithmetic is latency-bound: 8 blocks per SM (64 registers, a few spilled) beat 4
+// blocks at 128 registers without spills by a fifth on the c3 shapes.
+template <bool kCached>
+__global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -367,30 +373,41 @@ __global__ void __launch_bounds__(128, 4) k_bath_rate(Model m, RateArgs a) {
     const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
     const double size_i = a.size_old[i];
     // the physical kernel on the cached environment: owner terms once per owner
-    const bool cached = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m) && a.env;
     PairOwner po{0.0, 0.0, 0.0};
-    if (cached) po = cached_owner_terms(m, o.env, size_i);
-    for (int s = lane; s < K; s += 32) {
-        double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
-        const int nb = a.codes[static_cast<size_t>(i) * K + s];
-        if (act && nb >= 0 && meas > 0.0) {
-            const int j = nb / 3;
-            const double size_j = a.size_old[j];
-            double vrel;
-            double pr = cached ? pair_rate_cached(m, o, po, size_i, size_j, a.numr_old[j], a.part, j, vrel)
-                               : pair_rate(m, o, size_i, size_j, a.numr_old[j], a.part, j, vrel);
-            double mean = 0.0, sec = 0.0, maxi = 0.0;
-            pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
-            mx = pr > 0.0 ? maxi : 0.0;
-            c = pr * mean;
-            sc = pr * sec;
-            r = pr;
+    if (kCached) po = cached_owner_terms(m, o.env, size_i);
+    const int32_t *row = a.codes + static_cast<size_t>(i) * K;
+    for (int s0 = lane; s0 < K; s0 += 64) {
+        const int s1 = s0 + 32;
+        const int nb0 = row[s0];
+        const int nb1 = s1 < K ? row[s1] : -1;
+        const bool use0 = act && nb0 >= 0 && meas > 0.0, use1 = act && nb1 >= 0 && meas > 0.0;
+        const double sj0 = use0 ? a.size_old[nb0 / 3] : 0.0, nj0 = use0 ? a.numr_old[nb0 / 3] : 0.0;
+        const double sj1 = use1 ? a.size_old[nb1 / 3] : 0.0, nj1 = use1 ? a.numr_old[nb1 / 3] : 0.0;
+#pragma unroll 1
+        for (int t = 0; t < 2; ++t) {
+            const int s = t ? s1 : s0;
+            if (s >= K) break;
+            const bool use = t ? use1 : use0;
+            const int j = (t ? nb1 : nb0) / 3;
+            const double size_j = t ? sj1 : sj0, numr_j = t ? nj1 : nj0;
+            double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
+            if (use) {
+                double vrel;
+                double pr = kCached ? pair_rate_cached(m, o, po, size_i, size_j, numr_j, a.part, j, vrel)
+                                    : pair_rate(m, o, size_i, size_j, numr_j, a.part, j, vrel);
+                double mean = 0.0, sec = 0.0, maxi = 0.0;
+                pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+                mx = pr > 0.0 ? maxi : 0.0;
+                c = pr * mean;
+                sc = pr * sec;
+                r = pr;
+            }
+            rate_w[s] = r;
+            change_w[s] = c;
+            second_w[s] = sc;
+            max_w[s] = mx;
+            valid_w[s] = isfinite(r) && r >= 0.0;
         }
-        rate_w[s] = r;
-        change_w[s] = c;
-        second_w[s] = sc;
-        max_w[s] = mx;
-        valid_w[s] = isfinite(r) && r >= 0.0;
     }
     __syncwarp();
     warp_fold(K, lane, [&](int j, int h) {
@@ -1267,8 +1284,13 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
     }
     const Env *env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
     const size_t rate_smem = static_cast<size_t>(4) * (4 * 8 + 4) * K;
-    if (rate_smem > 48 * 1024)
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rate_smem)));
+    if (rate_smem > 48 * 1024) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(rate_smem)));
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(rate_smem)));
+    }
+    const bool rate_cached = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m) && env;
     const size_t chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
     if (chain_smem > 48 * 1024)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(chain_smem)));
@@ -1318,7 +1340,10 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         ra.rated = c.rated.ptr;
         ra.publish = c.publish;
         ++c.launches;
-        k_bath_rate<<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
+        if (rate_cached)
+            k_bath_rate<true><<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
+        else
+            k_bath_rate<false><<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, s));
         ++c.launches;
         k_count_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, at<int>(c.small, L.counts), part, spatial,
