@@ -794,19 +794,19 @@ struct AuditArgs {
 // so a warp mostly feeds one or two bins): one atomic per bin and warp instead of one per owner.
 constexpr int kAuditTerms = 13;  // staged doubles per owner besides the two maxima
 constexpr int kAuditTPB = 256;   // threads per block of k_audit_bin
-__global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
-    __shared__ double terms[kAuditTPB / 32][32][kAuditTerms + 2];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+// The audit terms of the owner at `slot` (-1: none): whether it is an active owner (`on`), whether
+// its terms are valid, its start and stop bins, and the staged terms t.
+__device__ __forceinline__ void audit_owner(const Model &m, const AuditArgs &a, int slot, bool &on, bool &valid,
+                                            int &start, int &stop, double t[kAuditTerms + 2]) {
     int i = 0;
-    bool on = slot < a.count;
+    on = slot >= 0 && slot < a.count;
     if (on) {
         i = owner_at(a.ids, slot);
         on = a.active[i] != 0;
     }
-    int start = -1, stop = -1;
-    bool valid = false;
-    double t[kAuditTerms + 2];
+    start = -1;
+    stop = -1;
+    valid = false;
 #pragma unroll
     for (int f = 0; f < kAuditTerms + 2; ++f) t[f] = 0.0;
     if (on) {
@@ -840,6 +840,15 @@ __global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
             t[14] = weight * a.jumpmax[i];   // maximum weighted jump
         }
     }
+}
+
+__global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
+    __shared__ double terms[kAuditTPB / 32][32][kAuditTerms + 2];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    bool on, valid;
+    int start, stop;
+    double t[kAuditTerms + 2];
+    audit_owner(m, a, blockIdx.x * blockDim.x + threadIdx.x, on, valid, start, stop, t);
 #pragma unroll
     for (int f = 0; f < kAuditTerms + 2; ++f) terms[wib][lane][f] = t[f];
     const unsigned int on_mask = __ballot_sync(0xffffffffu, on);
@@ -883,6 +892,104 @@ __global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
         double em = 0.0;
         for (unsigned int pm = speers; pm; pm &= pm - 1) em += terms[wib][__ffs(pm) - 1][10];
         atomicAdd(&a.bin[stop].end_mass, em);
+    }
+}
+
+// The same audit with a second level of aggregation: a block covers kAuditSpan consecutive
+// owners (one or two spatial groups, so a handful of bins) and its warps add their per-bin sums
+// into a shared-memory copy of the bins; the block then adds each touched bin to global memory
+// once.  Used when the raw bin count fits in shared memory (kAuditSmemBins); it turns the
+// contended global atomics of the per-warp kernel (all warps hitting the same few hundred bins)
+// into about one per bin and block.
+constexpr int kAuditPerThread = 16;                          // owners per thread
+constexpr int kAuditSpan = kAuditTPB * kAuditPerThread;      // owners per block
+constexpr int kAuditSmemBins = 512;
+constexpr int kAuditSums = 11;  // the ten start-bin sums, then the end mass
+__host__ __device__ constexpr size_t audit_blocked_smem(int bins) {
+    return sizeof(double) * (kAuditTPB / 32) * 32 * (kAuditTerms + 2) +
+           static_cast<size_t>(bins) * (sizeof(double) * kAuditSums + sizeof(unsigned long long) * 2 + sizeof(int) * 3);
+}
+__global__ void __launch_bounds__(kAuditTPB) k_audit_bin_blocked(Model m, AuditArgs a, int bins) {
+    extern __shared__ __align__(16) double sa[];
+    double(*terms)[32][kAuditTerms + 2] = reinterpret_cast<double(*)[32][kAuditTerms + 2]>(sa);
+    double *bsum = sa + (kAuditTPB / 32) * 32 * (kAuditTerms + 2);                              // [bins][kAuditSums]
+    unsigned long long *bmax = reinterpret_cast<unsigned long long *>(bsum + bins * kAuditSums);  // [bins][2]
+    int *bcnt = reinterpret_cast<int *>(bmax + bins * 2);  // [bins][3]: owners, invalid owners, end-mass adds
+    for (int k = threadIdx.x; k < bins * kAuditSums; k += blockDim.x) bsum[k] = 0.0;
+    for (int k = threadIdx.x; k < bins * 2; k += blockDim.x) bmax[k] = 0ull;
+    for (int k = threadIdx.x; k < bins * 3; k += blockDim.x) bcnt[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long first = static_cast<long long>(blockIdx.x) * kAuditSpan;
+    for (int it = 0; it < kAuditPerThread && first + it * kAuditTPB < a.count; ++it) {
+        const long long sl = first + it * kAuditTPB + threadIdx.x;
+        bool on, valid;
+        int start, stop;
+        double t[kAuditTerms + 2];
+        audit_owner(m, a, sl < a.count ? static_cast<int>(sl) : -1, on, valid, start, stop, t);
+#pragma unroll
+        for (int f = 0; f < kAuditTerms + 2; ++f) terms[wib][lane][f] = t[f];
+        const unsigned int on_mask = __ballot_sync(0xffffffffu, on);
+        const unsigned int valid_mask = __ballot_sync(0xffffffffu, valid);
+        __syncwarp();
+        if (on) {
+            const unsigned int peers = __match_any_sync(on_mask, start);
+            if (lane == __ffs(peers) - 1) {
+                double sum[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+                double mw = 0.0, mg = 0.0;
+                for (unsigned int pm = peers & valid_mask; pm; pm &= pm - 1) {
+                    const int l = __ffs(pm) - 1;
+#pragma unroll
+                    for (int f = 0; f < 10; ++f) sum[f] += terms[wib][l][f];
+                    mw = fmax(mw, terms[wib][l][13]);
+                    mg = fmax(mg, terms[wib][l][14]);
+                }
+                atomicAdd(&bcnt[start * 3], __popc(peers));
+                atomicAdd(&bcnt[start * 3 + 1], __popc(peers & ~valid_mask));
+                if (peers & valid_mask) {
+#pragma unroll
+                    for (int f = 0; f < 10; ++f) atomicAdd(&bsum[start * kAuditSums + f], sum[f]);
+                    // non-negative doubles order like their bit patterns
+                    atomicMax(&bmax[start * 2], static_cast<unsigned long long>(__double_as_longlong(mw)));
+                    atomicMax(&bmax[start * 2 + 1], static_cast<unsigned long long>(__double_as_longlong(mg)));
+                }
+            }
+        }
+        if (valid) {
+            const unsigned int speers = __match_any_sync(valid_mask, stop);
+            if (lane == __ffs(speers) - 1) {
+                double em = 0.0;
+                for (unsigned int pm = speers; pm; pm &= pm - 1) em += terms[wib][__ffs(pm) - 1][10];
+                atomicAdd(&bsum[stop * kAuditSums + 10], em);
+                atomicAdd(&bcnt[stop * 3 + 2], 1);
+            }
+        }
+        __syncwarp();  // the staged terms are rewritten by the next owner
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+        const int owners = bcnt[b * 3], invalid = bcnt[b * 3 + 1], ends = bcnt[b * 3 + 2];
+        AuditBin *g = a.bin + b;
+        if (owners) {
+            atomicAdd(&g->owner_count, owners);
+            if (invalid) atomicAdd(&g->invalid_count, invalid);
+        }
+        if (owners > invalid) {
+            const double *v = bsum + b * kAuditSums;
+            atomicAdd(&g->mass, v[0]);
+            atomicAdd(&g->predicted_f, v[1]);
+            atomicAdd(&g->predicted_e, v[2]);
+            atomicAdd(&g->predicted_var_f, v[3]);
+            atomicAdd(&g->predicted_var_e, v[4]);
+            atomicAdd(&g->predicted_g, v[5]);
+            atomicAdd(&g->predicted_var_g, v[6]);
+            atomic_max_double(&g->maximum_weight, __longlong_as_double(static_cast<long long>(bmax[b * 2])));
+            atomic_max_double(&g->maximum_g_jump, __longlong_as_double(static_cast<long long>(bmax[b * 2 + 1])));
+            atomicAdd(&g->touched, v[7]);
+            atomicAdd(&g->event_weight, v[8]);
+            atomicAdd(&g->growth, v[9]);
+        }
+        if (ends) atomicAdd(&g->end_mass, bsum[b * kAuditSums + 10]);
     }
 }
 
@@ -1291,6 +1398,9 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
                                          static_cast<int>(rate_smem)));
     }
     const bool rate_cached = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m) && env;
+    if (R <= kAuditSmemBins)
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(audit_blocked_smem(R))));
     const size_t chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
     if (chain_smem > 48 * 1024)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(chain_smem)));
@@ -1472,7 +1582,10 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         aa.lower = lower;
         aa.upper = upper;
         ++c.launches;
-        k_audit_bin<<<(count + kAuditTPB - 1) / kAuditTPB, kAuditTPB, 0, s>>>(m, aa);
+        if (R <= kAuditSmemBins)
+            k_audit_bin_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, audit_blocked_smem(R), s>>>(m, aa, R);
+        else
+            k_audit_bin<<<(count + kAuditTPB - 1) / kAuditTPB, kAuditTPB, 0, s>>>(m, aa);
         GD_TRY_CUDA(cudaGetLastError());
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small, c.small.ptr, L.binmap, cudaMemcpyDeviceToHost, s));
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.audit, c.small.ptr + L.audit, sizeof(AuditBin) * merged,
