@@ -993,6 +993,175 @@ __global__ void __launch_bounds__(kAuditTPB) k_audit_bin_blocked(Model m, AuditA
     }
 }
 
+// Blocked forms of the three controller scans, with the aggregation of k_audit_bin_blocked: a block
+// covers kAuditSpan consecutive owners, its warps combine per group or bin in shared memory, and
+// the block adds each touched entry to global memory once.  The host uses them while the groups
+// or bins fit in the default 48 KB of shared memory (kScanSmemEntries).
+constexpr int kScanSmemEntries = 1024;
+
+__global__ void __launch_bounds__(kAuditTPB) k_size_scan_blocked(const int *__restrict__ ids, int count,
+                                                                const gd_particle *__restrict__ part,
+                                                                const int32_t *__restrict__ spatial,
+                                                                const unsigned char *__restrict__ active, int G,
+                                                                unsigned long long *mmin, unsigned long long *mmax) {
+    extern __shared__ __align__(16) unsigned long long smm[];  // [G] minima, [G] maxima (double bits)
+    unsigned long long *smin = smm, *smax = smm + G;
+    for (int k = threadIdx.x; k < G; k += blockDim.x) {
+        smin[k] = ~0ull;
+        smax[k] = 0ull;
+    }
+    __syncthreads();
+    const long long first = static_cast<long long>(blockIdx.x) * kAuditSpan;
+    for (int it = 0; it < kAuditPerThread && first + it * kAuditTPB < count; ++it) {
+        const long long slot = first + it * kAuditTPB + threadIdx.x;
+        bool on = slot < count;
+        int g = 0;
+        unsigned long long bits = 0;
+        if (on) {
+            const int i = owner_at(ids, static_cast<int>(slot));
+            const double size = part[i].par_size;
+            on = active[i] && size > 0 && isfinite(size);
+            if (on) {
+                g = spatial[i];
+                bits = static_cast<unsigned long long>(__double_as_longlong(size));
+            }
+        }
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, g);
+            unsigned long long lo = bits, hi = bits;
+            for (unsigned int pm = peers; pm; pm &= pm - 1) {
+                const unsigned long long v = __shfl_sync(peers, bits, __ffs(pm) - 1);
+                lo = v < lo ? v : lo;
+                hi = v > hi ? v : hi;
+            }
+            if ((peers & lanes_below()) == 0) {
+                atomicMin(&smin[g], lo);
+                atomicMax(&smax[g], hi);
+            }
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        if (smax[g] != 0ull) {  // touched: positive sizes have non-zero bits
+            atomicMin(&mmin[g], smin[g]);
+            atomicMax(&mmax[g], smax[g]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kAuditTPB) k_count_bin_blocked(Model m, const int *__restrict__ ids, int count,
+                                                                int *__restrict__ counts,
+                                                                const gd_particle *__restrict__ part,
+                                                                const int32_t *__restrict__ spatial,
+                                                                const unsigned char *__restrict__ active,
+                                                                const double *lower, const double *upper, int R) {
+    extern __shared__ int scnt[];  // [R]
+    for (int k = threadIdx.x; k < R; k += blockDim.x) scnt[k] = 0;
+    __syncthreads();
+    const long long first = static_cast<long long>(blockIdx.x) * kAuditSpan;
+    for (int it = 0; it < kAuditPerThread && first + it * kAuditTPB < count; ++it) {
+        const long long slot = first + it * kAuditTPB + threadIdx.x;
+        bool on = slot < count;
+        int key = 0;
+        if (on) {
+            const int i = owner_at(ids, static_cast<int>(slot));
+            on = active[i] != 0;
+            if (on) {
+                const int g = spatial[i];
+                key = g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g);
+            }
+        }
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, key);
+            if ((peers & lanes_below()) == 0) atomicAdd(&scnt[key], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < R; k += blockDim.x)
+        if (scnt[k]) atomicAdd(counts + k, scnt[k]);
+}
+
+__global__ void __launch_bounds__(kAuditTPB) k_rate_bins_blocked(Model m, const int *__restrict__ ids, int count,
+                                                                RateBin *__restrict__ bin,
+                                                                const gd_particle *__restrict__ part,
+                                                                const double *__restrict__ rate,
+                                                                const double *__restrict__ change,
+                                                                const double *__restrict__ second,
+                                                                const int32_t *__restrict__ spatial,
+                                                                const int *__restrict__ binmap,
+                                                                const unsigned char *__restrict__ active,
+                                                                const double *lower, const double *upper, int R) {
+    extern __shared__ __align__(16) double srb[];  // [R][4] sums, then [R][2] owner / invalid counts
+    int *sct = reinterpret_cast<int *>(srb + 4 * R);
+    for (int k = threadIdx.x; k < 4 * R; k += blockDim.x) srb[k] = 0.0;
+    for (int k = threadIdx.x; k < 2 * R; k += blockDim.x) sct[k] = 0;
+    __syncthreads();
+    const long long first = static_cast<long long>(blockIdx.x) * kAuditSpan;
+    for (int it = 0; it < kAuditPerThread && first + it * kAuditTPB < count; ++it) {
+        const long long slot = first + it * kAuditTPB + threadIdx.x;
+        bool on = slot < count;
+        int b = 0;
+        bool valid = false;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+        if (on) {
+            const int i = owner_at(ids, static_cast<int>(slot));
+            on = active[i] != 0;
+            if (on) {
+                const int g = spatial[i];
+                b = binmap[g * m.col_bin_s + size_bin(m, part[i].par_size, lower, upper, g)];
+                const double weight = part[i].par_numr * grain_mass(m, part[i].par_size);
+                valid = !(!isfinite(weight) || !(weight > 0.0) || !isfinite(rate[i]) || rate[i] < 0.0 ||
+                          !isfinite(change[i]) || change[i] < 0 || !isfinite(second[i]) || second[i] < 0);
+                if (valid) {
+                    t0 = weight;
+                    t1 = weight * rate[i];
+                    t2 = weight * change[i];
+                    t3 = weight * second[i];
+                }
+            }
+        }
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        const unsigned int vmask = __ballot_sync(0xffffffffu, valid);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, b);
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (unsigned int pm = peers; pm; pm &= pm - 1) {
+                const int l = __ffs(pm) - 1;
+                s0 += __shfl_sync(peers, t0, l);
+                s1 += __shfl_sync(peers, t1, l);
+                s2 += __shfl_sync(peers, t2, l);
+                s3 += __shfl_sync(peers, t3, l);
+            }
+            if ((peers & lanes_below()) == 0) {
+                atomicAdd(&sct[2 * b], __popc(peers));
+                const int invalid = __popc(peers & ~vmask);
+                if (invalid) atomicAdd(&sct[2 * b + 1], invalid);
+                if (peers & vmask) {
+                    atomicAdd(&srb[4 * b], s0);
+                    atomicAdd(&srb[4 * b + 1], s1);
+                    atomicAdd(&srb[4 * b + 2], s2);
+                    atomicAdd(&srb[4 * b + 3], s3);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < R; k += blockDim.x) {
+        const int owners = sct[2 * k], invalid = sct[2 * k + 1];
+        if (!owners) continue;
+        atomicAdd(&bin[k].owner_count, owners);
+        if (invalid) atomicAdd(&bin[k].invalid_count, invalid);
+        if (owners > invalid) {
+            atomicAdd(&bin[k].mass, srb[4 * k]);
+            atomicAdd(&bin[k].weighted_rate, srb[4 * k + 1]);
+            atomicAdd(&bin[k].weighted_change, srb[4 * k + 2]);
+            atomicAdd(&bin[k].weighted_second, srb[4 * k + 3]);
+        }
+    }
+}
+
 // owner lists per spatial group (_col_chain.cuh:162-167) by a device counting sort
 __global__ void k_group_count(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcount) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1425,9 +1594,14 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         k_size_zero<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
                                                          at<unsigned long long>(c.small, L.mmax));
         ++c.launches;
-        k_size_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, spatial, active,
-                                                             at<unsigned long long>(c.small, L.mmin),
-                                                             at<unsigned long long>(c.small, L.mmax));
+        if (G <= kScanSmemEntries)
+            k_size_scan_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(unsigned long long) * 2 * G,
+                                  s>>>(idp, count, part, spatial, active, G, at<unsigned long long>(c.small, L.mmin),
+                                       at<unsigned long long>(c.small, L.mmax));
+        else
+            k_size_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, spatial, active,
+                                                                 at<unsigned long long>(c.small, L.mmin),
+                                                                 at<unsigned long long>(c.small, L.mmax));
         ++c.launches;
         k_size_bnds<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
                                                          at<unsigned long long>(c.small, L.mmax), lower, upper);
@@ -1456,14 +1630,25 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
             k_bath_rate<false><<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, s));
         ++c.launches;
-        k_count_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, at<int>(c.small, L.counts), part, spatial,
-                                                             active, lower, upper);
+        if (R <= kScanSmemEntries)
+            k_count_bin_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(int) * R, s>>>(
+                m, idp, count, at<int>(c.small, L.counts), part, spatial, active, lower, upper, R);
+        else
+            k_count_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, at<int>(c.small, L.counts), part,
+                                                                 spatial, active, lower, upper);
         GD_TRY_CUDA(cudaMemsetAsync(ratebin, 0, sizeof(RateBin) * R, s));
         ++c.launches;
         k_binmap<<<1, 1, 0, s>>>(m, at<int>(c.small, L.counts), binmap, at<int>(c.small, L.merged), ratebin);
         ++c.launches;
-        k_rate_bins<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, ratebin, part, c.rate.ptr, c.change_rate.ptr,
-                                                             c.second_rate.ptr, spatial, binmap, active, lower, upper);
+        if (R <= kScanSmemEntries)
+            k_rate_bins_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB,
+                                  (sizeof(double) * 4 + sizeof(int) * 2) * R, s>>>(
+                m, idp, count, ratebin, part, c.rate.ptr, c.change_rate.ptr, c.second_rate.ptr, spatial, binmap,
+                active, lower, upper, R);
+        else
+            k_rate_bins<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, ratebin, part, c.rate.ptr,
+                                                                 c.change_rate.ptr, c.second_rate.ptr, spatial, binmap,
+                                                                 active, lower, upper);
         GD_TRY_CUDA(cudaGetLastError());
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.merged, c.small.ptr + L.merged, 4, cudaMemcpyDeviceToHost, s));
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.binmap, c.small.ptr + L.binmap, L.audit - L.binmap,
