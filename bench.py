@@ -568,7 +568,9 @@ def run_ours(args):
             for label, fn in (("plain", swarm_step), ("learned", swarm_step_learned)):
                 fn()
                 barrier(world)
+                torch.cuda.nvtx.range_push(f"swarm_step_{label}")
                 a, b = _timed(stream, lambda: [fn() for _ in range(st_steps)])
+                torch.cuda.nvtx.range_pop()
                 barrier(world)
                 timings[label] = reduce_max(a.elapsed_time(b), world) / st_steps
             s_ms = timings["learned"]
