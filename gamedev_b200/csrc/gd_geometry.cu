@@ -351,6 +351,14 @@ constexpr int kFrontier = 128;   // internal nodes of one breadth-first level
 constexpr int kListInts = 352;   // leaves of the breadth-first walk (also the depth-first stack)
 __host__ __device__ constexpr size_t knn_heap_bytes(int K) { return static_cast<size_t>(heap_stride(K)) * 32 * 8; }
 __host__ __device__ constexpr size_t knn_warp_bytes(int K) { return knn_heap_bytes(K) + 32 * 16 + kListInts * 4; }
+// Entries a lane may hold.  Inside a well-proposed radius a lane finds a little more than K sites
+// (about 1.2 K at c3); a radius-bounded lane gets 3K/8 extra slots (rounded up to 8), appends them
+// all and selects the K nearest once at the end, instead of building its heap mid-walk (in as many
+// batches as the warp has fill times) and sifting every later candidate.  At K = 64: 88 slots;
+// 72, 80 and 96 were slower (fewer spare slots build more heaps, more cost residency).
+__host__ __device__ constexpr int knn_capacity(int K, bool bounded) {
+    return bounded ? K + (((3 * K) / 8 + 7) & ~7) : K;
+}
 
 // Loads of one leaf: this lane's site of the 32-site tile and the four 8-site sub-boxes.
 struct LeafLoad {
@@ -364,7 +372,8 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                                            int kcap) {
     const int lane = threadIdx.x & 31;
     const int K = a.k;
-    unsigned long long *hp = reinterpret_cast<unsigned long long *>(wbase) + lane * heap_stride(K);
+    const int cap = knn_capacity(K, a.radius != nullptr);  // entries a lane may hold (<= kcap)
+    unsigned long long *hp = reinterpret_cast<unsigned long long *>(wbase) + lane * heap_stride(cap);
     float4 *tile = reinterpret_cast<float4 *>(wbase + knn_heap_bytes(kcap));
     // the breadth-first walk stages its next frontier in the tile buffer (no leaf is scanned then)
     int *staging = reinterpret_cast<int *>(tile);
@@ -399,7 +408,7 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
 
     const int depth_leaves = a.leaf_slots;  // leaves under the root (a power of two)
 
-    bool built = false;  // this lane's K entries have been arranged into a max-heap
+    bool built = false;  // this lane's cap entries have been arranged into a max-heap
 
     auto load_leaf = [&](int lf, LeafLoad &L) {
         L.site = a.sorted[lf * kLeaf + lane];
@@ -436,10 +445,10 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
             }
             st_leaves += 1;
         }
-        // Fill phase: a lane with fewer than K entries appends without ordering work.  A lane
-        // that reaches K stops and keeps the rest of its mask; the lanes that filled up in this
+        // Fill phase: a lane with fewer than cap entries appends without ordering work.  A lane
+        // that reaches cap stops and keeps the rest of its mask; the lanes that filled up in this
         // leaf then build their heaps together (in step, instead of one lane after another).
-        while (mask && cnt < K) {
+        while (mask && cnt < cap) {
             const int c = __ffs(mask) - 1;
             mask &= mask - 1;
             const float4 p = tile[c];
@@ -451,10 +460,10 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 ++cnt;
             }
         }
-        const bool build_now = cnt == K && !built;
+        const bool build_now = cnt == cap && !built;
         if (__any_sync(0xffffffffu, build_now)) {
             if (build_now) {
-                heap_build(hp, K);
+                heap_build(hp, cap);
                 cut = key_d2(hp[0]);
                 built = true;
             }
@@ -470,7 +479,7 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
                                                static_cast<unsigned int>(__float_as_int(p.w));
                 if (key < hp[0]) {
-                    heap_sift(hp, key, 0, K);
+                    heap_sift(hp, key, 0, cap);
                     cut = key_d2(hp[0]);
                 }
             }
@@ -701,8 +710,10 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
         }
     }
 
-    // ascending (d^2 bits, code): heap sort of the cnt real entries
-    if (cnt < K) heap_build(hp, cnt);
+    // the K nearest of the held entries, ascending (d^2 bits, code): drop the largest beyond K,
+    // then heap sort
+    if (!built) heap_build(hp, cnt);
+    for (; cnt > K; --cnt) heap_sift(hp, hp[cnt - 1], 0, cnt - 1);
     for (int end = cnt - 1; end > 0; --end) {
         const unsigned long long top = hp[0];
         const unsigned long long last = hp[end];
@@ -751,7 +762,8 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
 __global__ void k_knn_query(Model m, QueryArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int wib = threadIdx.x >> 5;
-    knn_bucket(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(a.k), a.k);
+    const int kcap = knn_capacity(a.k, a.radius != nullptr);
+    knn_bucket(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(kcap), kcap);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1039,8 +1051,9 @@ int knn_block_warps(int K, const Tuning &tune, int *resident) {
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
                  float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats, const Tuning &tune) {
     const int K = m.n_k;
-    const size_t per_warp = knn_smem_per_warp(K);
-    const int warps = knn_block_warps(K, tune, nullptr);
+    const int kcap = knn_capacity(K, radius != nullptr);
+    const size_t per_warp = knn_smem_per_warp(kcap);
+    const int warps = knn_block_warps(kcap, tune, nullptr);
     if (warps == 0) return Status{GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory", 0};
     const size_t smem = per_warp * warps;
     // raise the kernel's shared-memory limit only when a larger one is needed, so that a step
