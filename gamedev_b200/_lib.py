@@ -107,6 +107,7 @@ SIGNATURES = {
     "gd_radius_model_gradient": (C.c_int, [_P, _P, _P, C.c_int, _P, C.POINTER(C.c_float), _P]),
     "gd_radius_model_calibrate": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.POINTER(C.c_float), _P]),
     "gd_radius_model_predict": (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    "gd_radius_model_check": (C.c_int, [_P]),
     "gd_radius_model_get": (C.c_int, [_P, _P, _P]),
     "gd_radius_model_set": (C.c_int, [_P, _P, _P]),
     "gd_get_cache": (C.c_int, [_P, _P, _P]),

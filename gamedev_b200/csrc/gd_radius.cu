@@ -57,6 +57,7 @@ struct RadiusModel {
     DevBuf<float> norm;                          // mean[8], inv_scale[8], margin, target_mean
     DevBuf<double> acc;                          // reductions: loss, stats
     DevBuf<unsigned int> hist;                   // residual histogram
+    DevBuf<int> err;                             // set by a tensor-core forward whose wait timed out
 };
 
 }  // namespace gd
@@ -226,25 +227,6 @@ __device__ __forceinline__ void load_x(const float *feat, size_t r, const float 
     for (int k = 0; k < kF; ++k) x[k] = (raw[k] - norm[k]) * norm[kF + k];
 }
 
-// forward of one row with weights in shared memory; h1 out (64 registers)
-__device__ __forceinline__ float forward(const float *sw, const float x[kF], float h1[kH]) {
-#pragma unroll 8
-    for (int j = 0; j < kH; ++j) {
-        float a = sw[oB1 + j];
-#pragma unroll
-        for (int k = 0; k < kF; ++k) a = fmaf(sw[oW1 + j * kF + k], x[k], a);
-        h1[j] = gelu(a);
-    }
-    float y = sw[oB3];
-    for (int o = 0; o < kH; ++o) {
-        float a = sw[oB2 + o];
-#pragma unroll
-        for (int j = 0; j < kH; ++j) a = fmaf(sw[oW2 + o * kH + j], h1[j], a);
-        y = fmaf(sw[oW3 + o], gelu(a), y);
-    }
-    return y;
-}
-
 // Forward and backward of one tile of rows; accumulates the summed gradient of
 // (1/norm_count) * sum (y - t)^2 into grad and the summed squared error into acc[0].
 // rows: sample_mode 0 -> rows base..base+kTile-1 (bounded by n); 1 -> hashed uniform draws.
@@ -360,34 +342,214 @@ __global__ void k_adam(float *params, float *grad, float *m1, float *m2, __nv_bf
     grad[p] = 0.0f;
 }
 
-__global__ void k_predict(const float *__restrict__ params, const __nv_bfloat16 *__restrict__ wq,
-                          const float *__restrict__ norm, const float *__restrict__ feat, int n, double R_0,
-                          float *__restrict__ radius) {
-    extern __shared__ __align__(16) float sw[];
-    load_net(sw, params, wq);
-    __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    float x[kF], h1[kH];
-    load_x(feat, static_cast<size_t>(r), norm, x);
-    const float y = forward(sw, x, h1) + norm[2 * kF];
-    radius[r] = static_cast<float>(R_0 * exp(static_cast<double>(y)));
+// ---------------------------------------------------------------------------------------------
+// Tensor-core forward on sm_100a (tcgen05).  One block of 128 threads per 128-row tile (a
+// persistent loop over tiles); thread t owns row t of the tile.
+//   1. Layer 1 (8 -> 64) and GELU on the CUDA cores.  Each FP32 activation h is split into two
+//      BF16 parts, hi = bf16(h) and lo = bf16(h - hi), stored in shared memory as two A operands
+//      (K-major, no swizzle): hi + lo carries about 16 significant bits, so the tensor-core layer
+//      matches the FP32 forward to ~1e-5 instead of the ~1e-3 that BF16 activations alone give.
+//   2. Layer 2 (64 x 64) as eight tcgen05.mma.kind::f16 (M = 128, N = 64, K = 16 each; hi and lo
+//      times the same B): B = W2 (BF16 weights, exact), stored once per block, FP32 accumulator in
+//      64 TMEM columns, issued by one thread and committed to an mbarrier.
+//   3. Every warp reads its 32 accumulator rows (tcgen05.ld 32x32b, lane = row), adds b2, applies
+//      GELU and the 64 -> 1 output layer on the CUDA cores.
+// The waits are bounded: a commit that does not arrive within about a second stops the block,
+// which sets *err, frees its TMEM and returns (gd_radius_model_check reports it).
+// Operand layout (SWIZZLE_NONE canonical K-major): element (row, k) of a 64-column BF16 operand
+// lies at (row / 8) * 1024 + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2 bytes: 8-row x 16-byte
+// core matrices, K-adjacent ones 128 B apart (leading byte offset), 8-row groups 1024 B apart
+// (stride byte offset).  One MMA consumes two K-adjacent core matrices (K = 16), so step ks starts
+// 256 * ks bytes in.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTcRows = 128;  // rows per tile = threads per block = TMEM lanes
+constexpr int kTcCols = 64;   // TMEM columns of the FP32 accumulator (N)
+// instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A and B BF16 (bits 7-9,
+// 10-12 = 1), both K-major (bits 15, 16 = 0), N / 8 in bits 17-22, M / 16 in bits 24-28
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr int kTcB = 0;                           // W2 (N = 64 rows x K = 64), 8 KB
+constexpr int kTcA = 8192;                        // activations, hi part (128 rows x K = 64), 16 KB
+constexpr int kTcAlo = kTcA + 16384;              // activations, lo part, 16 KB
+constexpr int kTcW = kTcAlo + 16384;              // floats: W1 [512], b1 [64], b2 [64], W3 [64], b3, margin
+constexpr int kTcWFloats = kH * kF + 3 * kH + 2;
+constexpr int kTcBar = kTcW + ((kTcWFloats * 4 + 15) & ~15);  // mbarrier (8 B), TMEM address (4 B)
+constexpr int kTcSmem = kTcBar + 16;
+
+__host__ __device__ constexpr int tc_offset(int row, int k) {
+    return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-__global__ void k_residual_hist(const float *__restrict__ params, const __nv_bfloat16 *__restrict__ wq,
-                                const float *__restrict__ norm, const float *__restrict__ feat,
-                                const float *__restrict__ kth, int n, double R_0, unsigned int *hist) {
-    extern __shared__ __align__(16) float sw[];
-    load_net(sw, params, wq);
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: start address, leading byte offset 128, stride byte offset
+// 1024 (all in 16-byte units), descriptor version 1 (bit 46), base offset 0, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3fffu) | (static_cast<uint64_t>(128 >> 4) << 16) |
+           (static_cast<uint64_t>(1024 >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// waits for the completion of phase `parity` of the mbarrier at `bar`, for at most ~2^31 cycles
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+}
+
+// 64 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_load64(uint32_t taddr, uint32_t v[64]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kTcRows, 4) k_mlp_tc(const float *__restrict__ params,
+                                                       const __nv_bfloat16 *__restrict__ wq,
+                                                       const float *__restrict__ norm, const float *__restrict__ feat,
+                                                       int n, double R_0, float *__restrict__ radius,
+                                                       const float *__restrict__ kth, unsigned int *hist, int *err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int t = threadIdx.x, warp = t >> 5;
+    float *sw = reinterpret_cast<float *>(smem + kTcW);
+    float *w1 = sw, *b1 = sw + kH * kF, *b2 = b1 + kH, *w3 = b2 + kH;
+    for (int p = t; p < kH * kF; p += kTcRows) w1[p] = __bfloat162float(wq[oW1 + p]);
+    for (int j = t; j < kH; j += kTcRows) {
+        b1[j] = params[oB1 + j];
+        b2[j] = params[oB2 + j];
+        w3[j] = __bfloat162float(wq[oW3 + j]);
+    }
+    if (t == 0) {
+        w3[kH] = params[oB3];
+        w3[kH + 1] = norm[2 * kF];  // margin
+    }
+    for (int p = t; p < kH * kH; p += kTcRows)  // W2[o][j]: row o of B (N), column j (K)
+        *reinterpret_cast<__nv_bfloat16 *>(smem + kTcB + tc_offset(p / kH, p % kH)) = wq[oW2 + p];
+    const uint32_t bar = smem_u32(smem + kTcBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kTcBar + 8);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // W2 was written through the generic proxy: make it visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n || !(kth[r] > 0.0f)) return;
-    float x[kF], h1[kH];
-    load_x(feat, static_cast<size_t>(r), norm, x);
-    const float res = target_of(kth[r], R_0) - forward(sw, x, h1);
-    int b = static_cast<int>(floorf((res - kHistLo) / (kHistHi - kHistLo) * kHistBins));
-    b = b < 0 ? 0 : (b >= kHistBins ? kHistBins + 1 : b + 1);  // [0] underflow, [bins+1] overflow
-    atomicAdd(&hist[b], 1u);
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t a_addr = smem_u32(smem + kTcA), alo_addr = smem_u32(smem + kTcAlo), b_addr = smem_u32(smem + kTcB);
+    const float b3 = w3[kH], margin = w3[kH + 1];
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    uint32_t parity = 0;
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int r = tile * kTcRows + t;
+        float x[kF];
+#pragma unroll
+        for (int k = 0; k < kF; ++k) x[k] = 0.0f;
+        if (r < n) load_x(feat, static_cast<size_t>(r), norm, x);
+#pragma unroll 1
+        for (int kc = 0; kc < kH / 8; ++kc) {
+            uint32_t ph[4], pl[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                float hi2[2], lo2[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int j = kc * 8 + h * 2 + e;
+                    float a = b1[j];
+#pragma unroll
+                    for (int k = 0; k < kF; ++k) a = fmaf(w1[j * kF + k], x[k], a);
+                    const float v = gelu(a);
+                    hi2[e] = __bfloat162float(__float2bfloat16_rn(v));
+                    lo2[e] = v - hi2[e];  // exact in FP32
+                }
+                const __nv_bfloat162 bh = __floats2bfloat162_rn(hi2[0], hi2[1]);
+                const __nv_bfloat162 bl = __floats2bfloat162_rn(lo2[0], lo2[1]);
+                ph[h] = *reinterpret_cast<const uint32_t *>(&bh);
+                pl[h] = *reinterpret_cast<const uint32_t *>(&bl);
+            }
+            *reinterpret_cast<uint4 *>(smem + kTcA + tc_offset(t, kc * 8)) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+            *reinterpret_cast<uint4 *>(smem + kTcAlo + tc_offset(t, kc * 8)) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < kH / 16; ++ks) {
+                tc_mma(tmem, tc_desc(a_addr + 256 * ks), tc_desc(b_addr + 256 * ks), kTcIdesc, ks > 0 ? 1u : 0u);
+                tc_mma(tmem, tc_desc(alo_addr + 256 * ks), tc_desc(b_addr + 256 * ks), kTcIdesc, 1u);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        const bool ok = tc_wait(bar, parity);
+        parity ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        tc_fence_after();
+        uint32_t acc[kTcCols];
+        tc_load64(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
+        float y = b3;
+#pragma unroll
+        for (int o = 0; o < kH; ++o) y = fmaf(w3[o], gelu(__uint_as_float(acc[o]) + b2[o]), y);
+        if (r < n) {
+            if (hist) {
+                if (kth[r] > 0.0f) {
+                    const float res = target_of(kth[r], R_0) - y;
+                    int b = static_cast<int>(floorf((res - kHistLo) / (kHistHi - kHistLo) * kHistBins));
+                    b = b < 0 ? 0 : (b >= kHistBins ? kHistBins + 1 : b + 1);  // [0] under, [bins+1] over
+                    atomicAdd(&hist[b], 1u);
+                }
+            } else {
+                radius[r] = static_cast<float>(R_0 * exp(static_cast<double>(y + margin)));
+            }
+        }
+        // every row's accumulator is read before the next tile's MMA overwrites it
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (failed && t == 0) atomicExch(err, 1);
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
 static size_t tile_smem() {
@@ -397,6 +559,30 @@ static size_t tile_smem() {
 }  // namespace gd
 
 using gd::RadiusModel;
+
+namespace {
+
+// The tensor-core forward over n rows: radii into `radius`, or (with `hist`) the residual histogram
+// against kth.  A persistent grid of up to 4 blocks per SM (the launch bound; 4 x 64 TMEM columns).
+cudaError_t launch_mlp(RadiusModel &m, const float *feat, int n, float *radius, const float *kth, unsigned int *hist,
+                       cudaStream_t s) {
+    static int sms[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!sms[dev]) {
+        e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    const int tiles = (n + gd::kTcRows - 1) / gd::kTcRows;
+    const int grid = tiles < 4 * sms[dev] ? tiles : 4 * sms[dev];
+    gd::k_mlp_tc<<<grid, gd::kTcRows, gd::kTcSmem, s>>>(m.params.ptr, m.wq.ptr, m.norm.ptr, feat, n, m.R_0, radius, kth,
+                                                       hist, m.err.ptr);
+    return cudaGetLastError();
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -416,6 +602,8 @@ gd_status gd_radius_model_create(unsigned long long seed, double R_0, gd_radius_
     if (e == cudaSuccess) e = m.norm.alloc(2 * gd::kF + 2);
     if (e == cudaSuccess) e = m.acc.alloc(32);
     if (e == cudaSuccess) e = m.hist.alloc(gd::kHistBins + 2);
+    if (e == cudaSuccess) e = m.err.alloc(1);
+    if (e == cudaSuccess) e = cudaMemset(m.err.ptr, 0, sizeof(int));
     if (e == cudaSuccess) {
         std::vector<float> norm(2 * gd::kF + 2, 0.0f);
         for (int k = 0; k < gd::kF; ++k) norm[gd::kF + k] = 1.0f;
@@ -516,14 +704,13 @@ gd_status gd_radius_model_calibrate(gd_radius_model *h, const float *dev_feature
     if (st != GD_OK) return st;
     if (cudaMemsetAsync(m.hist.ptr, 0, sizeof(unsigned int) * (gd::kHistBins + 2), s) != cudaSuccess)
         return GD_ERR_CUDA;
-    const size_t smem = sizeof(float) * gd::kNP;
-    gd::k_residual_hist<<<(n + 255) / 256, 256, smem, s>>>(m.params.ptr, m.wq.ptr, m.norm.ptr, dev_features, dev_kth_d2,
-                                                           n, m.R_0, m.hist.ptr);
+    if (launch_mlp(m, dev_features, n, nullptr, dev_kth_d2, m.hist.ptr, s) != cudaSuccess) return GD_ERR_CUDA;
     std::vector<unsigned int> hist(gd::kHistBins + 2);
     if (cudaMemcpyAsync(hist.data(), m.hist.ptr, sizeof(unsigned int) * hist.size(), cudaMemcpyDeviceToHost, s) !=
             cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return GD_ERR_CUDA;
+    if (gd_radius_model_check(h) != GD_OK) return GD_ERR_CUDA;
     unsigned long long total = 0;
     for (unsigned int v : hist) total += v;
     if (total == 0) return GD_ERR_INVALID_ARGUMENT;
@@ -553,10 +740,14 @@ gd_status gd_radius_model_predict(gd_radius_model *h, const float *dev_features,
     if (!h || !dev_features || !dev_radius || n <= 0) return GD_ERR_INVALID_ARGUMENT;
     RadiusModel &m = h->m;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t smem = sizeof(float) * gd::kNP;
-    gd::k_predict<<<(n + 255) / 256, 256, smem, s>>>(m.params.ptr, m.wq.ptr, m.norm.ptr, dev_features, n, m.R_0,
-                                                     dev_radius);
-    return cudaGetLastError() == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+    return launch_mlp(m, dev_features, n, dev_radius, nullptr, nullptr, s) == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+gd_status gd_radius_model_check(gd_radius_model *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    int e = 0;
+    if (cudaMemcpy(&e, h->m.err.ptr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return GD_ERR_CUDA;
+    return e ? GD_ERR_CUDA : GD_OK;
 }
 
 gd_status gd_radius_model_get(const gd_radius_model *h, float *params, float *norm17) {

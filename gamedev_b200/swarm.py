@@ -280,6 +280,10 @@ class RadiusModel:
                     "gd_radius_model_predict")
         return out
 
+    def check(self):
+        """Synchronise and raise if a tensor-core forward stopped at a timed-out wait."""
+        self._check(self.lib.gd_radius_model_check(self.h), "gd_radius_model_check")
+
     def get(self):
         p = np.zeros(self.N_PARAMS, np.float32)
         norm = np.zeros(17, np.float32)

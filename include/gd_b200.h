@@ -232,9 +232,15 @@ gd_status gd_radius_model_gradient(gd_radius_model *m, const float *dev_features
 gd_status gd_radius_model_calibrate(gd_radius_model *m, const float *dev_features, const float *dev_kth_d2, int n,
                                     double quantile, float *margin, void *stream);
 
-/* Proposed radius R_0 exp(prediction + margin) per row into dev_radius [n] (float32). */
+/* Proposed radius R_0 exp(prediction + margin) per row into dev_radius [n] (float32).  The hidden
+ * 64 x 64 layer runs on the tensor cores (tcgen05, BF16 operands, FP32 accumulation); asynchronous
+ * on `stream`, so a failure of its bounded waits is reported by gd_radius_model_check. */
 gd_status gd_radius_model_predict(gd_radius_model *m, const float *dev_features, int n, float *dev_radius,
                                   void *stream);
+
+/* Synchronous check of the model's device error flag: GD_ERR_CUDA when a tensor-core forward
+ * stopped at a timed-out wait (its radii are then incomplete), else GD_OK. */
+gd_status gd_radius_model_check(gd_radius_model *m);
 
 /* Copy the FP32 master parameters (and standardisation: 8 means, 8 scales, margin) out of or into
  * the model; host buffers of GD_RADIUS_PARAMS and 17 floats. */

@@ -3,7 +3,8 @@
 Bars:
   * gradient of the device backward kernel vs the float64 oracle on the same BF16 weights:
     |g_dev - g_ref| <= 2e-3 * max|g_ref| per parameter block (FP32 accumulation over 4096 rows);
-  * device forward vs oracle: log-radius within 1e-4 absolute;
+  * device forward (hidden layer on the tensor cores, activations split into BF16 hi + lo) vs
+    oracle: log-radius within 1e-4 absolute;
   * features: log(y/R_0), log(size/S_0) within 1e-6 relative of float32 numpy, Morton-cell
     occupancies equal to a numpy recount on the same quantisation;
   * a trained and calibrated model seeds gd_knn_bounded with neighbour lists bit-identical to the
@@ -69,6 +70,7 @@ def test_radius_forward_matches_oracle(gd, cuda):
     model.train(feats, kth, iterations=50, batch=4096, lr=3e-3)
     r = model.predict(feats)
     torch.cuda.synchronize()
+    model.check()  # no bounded wait of the tensor-core forward timed out
     params, norm = model.get()
     ref = mlp.predict_log(params, norm, feats[:2000].cpu().numpy()) + norm[16]
     got = np.log(r[:2000].cpu().numpy().astype(np.float64) / cfg.R_0)
