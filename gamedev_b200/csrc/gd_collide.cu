@@ -1163,45 +1163,116 @@ __global__ void __launch_bounds__(kAuditTPB) k_rate_bins_blocked(Model m, const 
 }
 
 // owner lists per spatial group (_col_chain.cuh:162-167) by a device counting sort
-__global__ void k_group_count(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcount) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool on = i < n;
-    const int g = on ? spatial[i] : 0;
-    const unsigned int mask = __ballot_sync(0xffffffffu, on);
-    if (!on) return;
-    const unsigned int peers = __match_any_sync(mask, g);
-    if ((peers & lanes_below()) == 0) atomicAdd(&gcount[g], __popc(peers));
-}
-// each group's lanes reserve consecutive slots with one atomic and write at their rank
-__global__ void k_group_fill(int n, const int32_t *__restrict__ spatial, int *__restrict__ gcursor,
-                             int *__restrict__ sorted) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool on = i < n;
-    const int g = on ? spatial[i] : 0;
-    const unsigned int mask = __ballot_sync(0xffffffffu, on);
-    if (!on) return;
-    const unsigned int peers = __match_any_sync(mask, g);
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if ((threadIdx.x & 31) == leader) base = atomicAdd(&gcursor[g], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    sorted[base + __popc(peers & lanes_below())] = i;
+// Owner lists per spatial group by a counting sort, and the group dependency graph.  Particles
+// come in index order, where neighbouring indices belong to unrelated groups, so warp matching
+// rarely merges their atomics.  Each block covers kAuditSpan consecutive particles and gathers
+// its counts, slot reservations and edges in shared memory first: one global atomic per touched
+// group (or edge word) and block instead of one per particle.
+constexpr int kGroupTPB = 256;
+constexpr int kGroupPerThread = 16;
+constexpr int kGroupSpan = kGroupTPB * kGroupPerThread;
+
+__global__ void __launch_bounds__(kGroupTPB) k_group_count(int n, int G, const int32_t *__restrict__ spatial,
+                                                          int *__restrict__ gcount) {
+    __shared__ int cnt[kMaxGroups];
+    for (int g = threadIdx.x; g < G; g += blockDim.x) cnt[g] = 0;
+    __syncthreads();
+    const long long first = static_cast<long long>(blockIdx.x) * kGroupSpan;
+    for (int it = 0; it < kGroupPerThread && first + it * kGroupTPB < n; ++it) {
+        const long long i = first + it * kGroupTPB + threadIdx.x;
+        const bool on = i < n;
+        const int g = on ? spatial[i] : 0;
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, g);
+            if ((peers & lanes_below()) == 0) atomicAdd(&cnt[g], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x)
+        if (cnt[g]) atomicAdd(&gcount[g], cnt[g]);
 }
 
-// col_dep_graph (col_dep_graph.cu:43-59): edge c->d when an owner in c has a neighbour in d
-__global__ void k_dep_graph(int n, int K, int words, unsigned int *__restrict__ edges, const int32_t *__restrict__ spatial,
-                            const int32_t *__restrict__ codes, const unsigned char *__restrict__ active) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !active[i]) return;
-    unsigned int bits[kMaxGroups / 32] = {};
-    for (int k = 0; k < K; ++k) {
-        int e = codes[static_cast<size_t>(i) * K + k];
-        if (e < 0) continue;
-        int c = spatial[e / 3];
-        bits[c >> 5] |= 1u << (c & 31);
+// Each block reserves one consecutive range per group it touches, then writes its particles
+// there at their rank within the block.
+__global__ void __launch_bounds__(kGroupTPB) k_group_fill(int n, int G, const int32_t *__restrict__ spatial,
+                                                         int *__restrict__ gcursor, int *__restrict__ sorted) {
+    __shared__ int cnt[kMaxGroups];
+    __shared__ int base[kMaxGroups];
+    for (int g = threadIdx.x; g < G; g += blockDim.x) cnt[g] = 0;
+    __syncthreads();
+    const long long first = static_cast<long long>(blockIdx.x) * kGroupSpan;
+    for (int it = 0; it < kGroupPerThread && first + it * kGroupTPB < n; ++it) {
+        const long long i = first + it * kGroupTPB + threadIdx.x;
+        const bool on = i < n;
+        const int g = on ? spatial[i] : 0;
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, g);
+            if ((peers & lanes_below()) == 0) atomicAdd(&cnt[g], __popc(peers));
+        }
     }
-    for (int wd = 0; wd < words; ++wd)
-        if (bits[wd]) atomicOr(edges + spatial[i] * words + wd, bits[wd]);
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        base[g] = cnt[g] ? atomicAdd(&gcursor[g], cnt[g]) : 0;
+        cnt[g] = 0;  // reused as the block's cursor per group
+    }
+    __syncthreads();
+    for (int it = 0; it < kGroupPerThread && first + it * kGroupTPB < n; ++it) {
+        const long long i = first + it * kGroupTPB + threadIdx.x;
+        const bool on = i < n;
+        const int g = on ? spatial[i] : 0;
+        const unsigned int mask = __ballot_sync(0xffffffffu, on);
+        if (on) {
+            const unsigned int peers = __match_any_sync(mask, g);
+            const int leader = __ffs(peers) - 1;
+            int off = 0;
+            if ((threadIdx.x & 31) == leader) off = atomicAdd(&cnt[g], __popc(peers));
+            off = __shfl_sync(peers, off, leader);
+            sorted[base[g] + off + __popc(peers & lanes_below())] = static_cast<int>(i);
+        }
+    }
+}
+
+// col_dep_graph (col_dep_graph.cu:43-59): edge c->d when an owner in c has a neighbour in d.  A
+// warp takes its particles one at a time: the lanes read the owner's codes (coalesced), look up
+// the neighbours' groups, and OR-reduce the group bitset across the warp.
+__global__ void __launch_bounds__(kGroupTPB) k_dep_graph(int n, int K, int G, int words,
+                                                        unsigned int *__restrict__ edges,
+                                                        const int32_t *__restrict__ spatial,
+                                                        const int32_t *__restrict__ codes,
+                                                        const unsigned char *__restrict__ active) {
+    __shared__ unsigned int se[kMaxGroups * (kMaxGroups / 32)];
+    for (int k = threadIdx.x; k < G * words; k += blockDim.x) se[k] = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long first = static_cast<long long>(blockIdx.x) * kGroupSpan;
+    const long long last = first + kGroupSpan < n ? first + kGroupSpan : n;
+    for (long long i = first + wib; i < last; i += kGroupTPB / 32) {
+        if (!active[i]) continue;  // warp-uniform: one particle per warp
+        unsigned int bits[kMaxGroups / 32];
+#pragma unroll
+        for (int wd = 0; wd < kMaxGroups / 32; ++wd) bits[wd] = 0u;
+        for (int k = lane; k < K; k += 32) {
+            const int e = codes[static_cast<size_t>(i) * K + k];
+            if (e >= 0) {
+                const int c = spatial[e / 3];
+#pragma unroll
+                for (int wd = 0; wd < kMaxGroups / 32; ++wd)
+                    if ((c >> 5) == wd) bits[wd] |= 1u << (c & 31);
+            }
+        }
+        const int gi = spatial[i];
+#pragma unroll
+        for (int wd = 0; wd < kMaxGroups / 32; ++wd) {
+            if (wd >= words) break;
+            const unsigned int b = __reduce_or_sync(0xffffffffu, bits[wd]);
+            if (lane == 0 && b) atomicOr(&se[gi * words + wd], b);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < G * words; k += blockDim.x)
+        if (se[k]) atomicOr(edges + k, se[k]);
 }
 
 struct WaveTable {
@@ -1533,9 +1604,10 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.gcount, 0, 4 * G, s));
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.graph, 0, 4 * G * W, s));
         ++c.launches;
-        k_group_count<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, spatial, at<int>(c.small, L.gcount));
+        k_group_count<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, G, spatial, at<int>(c.small, L.gcount));
         ++c.launches;
-        k_dep_graph<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, K, W, at<unsigned int>(c.small, L.graph), spatial, codes, active);
+        k_dep_graph<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, K, G, W, at<unsigned int>(c.small, L.graph),
+                                                                             spatial, codes, active);
         GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.graph, c.small.ptr + L.graph, L.gcursor - L.graph,
                                     cudaMemcpyDeviceToHost, s));
         GD_TRY_CUDA(cudaStreamSynchronize(s));
@@ -1546,7 +1618,8 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         c.edges.assign(gr, gr + G * W);
         GD_TRY_CUDA(cudaMemcpyAsync(c.small.ptr + L.gcursor, c.group_start.data(), 4 * G, cudaMemcpyHostToDevice, s));
         ++c.launches;
-        k_group_fill<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(n, spatial, at<int>(c.small, L.gcursor), c.group_sorted.ptr);
+        k_group_fill<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, G, spatial, at<int>(c.small, L.gcursor),
+                                                                              c.group_sorted.ptr);
         GD_TRY_CUDA(cudaGetLastError());
         // new neighbour lists and measures: no stored rate stands
         GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, s));
