@@ -1679,7 +1679,7 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         k_size_bnds<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
                                                          at<unsigned long long>(c.small, L.mmax), lower, upper);
         RateArgs ra;
-        ra.ids = idp;
+        ra.ids = count == n ? nullptr : idp;  // every particle once: index order (per-owner results)
         ra.count = count;
         ra.part = part;
         ra.codes = codes;
@@ -1784,7 +1784,9 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         GD_TRY_CUDA(cudaMemcpyAsync(dt, steps.data(), sizeof(double) * G, cudaMemcpyHostToDevice, s));
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, s));  // error_flag, queued, head
         ChainArgs ca;
-        ca.ids = ids;
+        // A wave of every group holds every particle once: the skip scan (whose queue order the chain
+        // does not depend on) then walks them in index order, with coalesced per-particle loads.
+        ca.ids = count == n ? nullptr : ids;
         ca.count = count;
         ca.rng = rng;
         ca.active = active;
