@@ -120,6 +120,37 @@ def test_gpu_large_sample_parity(gd, cuda, oracle_lib):
     assert np.array_equal(g["kth"][sample].view(np.uint32), kth.view(np.uint32))
 
 
+@pytest.mark.parametrize("K", [1, 7, 20, 33, 100])
+def test_gpu_radius_bounded_query_other_k(gd, cuda, K):
+    """Radius-bounded lanes hold K + 3K/8 entries (rounded up to 8) before they heapify; for K
+    from 1 (no spare slot) to 100, odd K (scalar row stores) and K not a multiple of 4, mixed short
+    and long proposals give rows bit-identical to the plain query."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = 1 << 16
+    cfg = workloads.config("c3_learned_3d")
+    cfg.n_k = K
+    p = workloads.particles("c3_learned_3d", n=n, seed=5)
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    gen = torch.Generator(device="cuda").manual_seed(K)
+    u = torch.rand(n, device="cuda", generator=gen)
+    factor = torch.where(u < 0.2, 0.7 + 0.25 * u, 1.0 + 2.0 * u)  # short, near and far proposals
+    radius = (kth.double().sqrt() * factor.double()).float()
+    codes_b = torch.empty_like(codes)
+    measure_b = torch.empty_like(measure)
+    kth_b = torch.empty_like(kth)
+    sw.col_cache_get_bounded(dp, radius, codes_b, measure_b, kth_b, None)
+    torch.cuda.synchronize()
+    assert torch.equal(codes, codes_b), K
+    assert torch.equal(measure.view(torch.int64), measure_b.view(torch.int64)), K
+    assert torch.equal(kth.view(torch.int32), kth_b.view(torch.int32)), K
+    sw.close()
+
+
 def test_gpu_radius_bounded_query_is_exact(gd, cuda):
     """gd_knn_bounded is exact by construction: with proposed radii below the true K-th distance
     (owners must fall back) and above it (owners finish inside the radius) the output equals the
