@@ -617,6 +617,10 @@ def run_batched(args):
     stream = torch.cuda.current_stream()
     dp = gd.particles_to_device(p)
     batch = gd.SwarmBatch(cfg, sizes, ks)
+    # the key length the single-swarm autotuner picks at c3: the top 16 Morton bits per dimension
+    # (6 radix passes in 3D instead of 8); the rows are exact for any key order
+    sort_bits = 16 * (3 if cfg.n_z > 1 else 2)
+    batch.set_tuning(sort_bits=sort_bits)
     codes, measure, kth = batch.outputs()
     side = torch.cuda.Stream()
     side.wait_stream(stream)
@@ -633,7 +637,9 @@ def run_batched(args):
     for _ in range(args.warmup):
         graph.replay()
     barrier(world)
+    torch.cuda.nvtx.range_push("c2_step")
     a, b = _timed(stream, lambda: [graph.replay() for _ in range(args.steps)])
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     batch.check()
     b_ms = reduce_max(a.elapsed_time(b) / args.steps, world)
@@ -669,6 +675,7 @@ def run_batched(args):
         "config": {"workload": "c2_batched", "swarms": len(sizes), "particles": int(sum(sizes)),
                    "n_range": [min(sizes), max(sizes)], "k_choices": [16, 32, 64],
                    "step": "per-swarm geometry on 8 streams + one persistent top-K launch, one CUDA graph replay",
+                   "sort_bits": sort_bits,
                    "parallelism": f"replicas x{world}"},
         "kernels_per_step": kernels,
         "one_handle_at_a_time": {"ms_per_step": solo_ms, "queries_per_s": queries / (solo_ms / 1e3)},
