@@ -25,6 +25,8 @@ STATUS_NAMES = {
     8: "GD_ERR_CONTROLLER",
     9: "GD_ERR_NOT_READY",
     10: "GD_ERR_OUT_OF_MEMORY",
+    11: "GD_ERR_TIMEOUT",
+    12: "GD_ERR_IO",
 }
 GD_SEARCH_KDTREE, GD_SEARCH_MORTON = 0, 1
 GD_KERNEL_CONSTANT, GD_KERNEL_LINEAR, GD_KERNEL_PRODUCT, GD_KERNEL_CUSTOM = 0, 1, 2, 3
@@ -108,6 +110,11 @@ SIGNATURES = {
     "gd_radius_model_calibrate": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, C.POINTER(C.c_float), _P]),
     "gd_radius_model_predict": (C.c_int, [_P, _P, C.c_int, _P, _P]),
     "gd_radius_model_check": (C.c_int, [_P]),
+    "gd_frame_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
+    "gd_particles_to_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),
+    "gd_particles_from_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),
+    "gd_save_checkpoint": (C.c_int, [C.POINTER(GdConfig), C.c_char_p, C.c_int, C.c_int, _P, C.c_int, _P]),
+    "gd_load_checkpoint": (C.c_int, [C.POINTER(GdConfig), C.c_char_p, C.c_int, C.c_int, _P, C.c_int, _P]),
     "gd_radius_model_get": (C.c_int, [_P, _P, _P]),
     "gd_radius_model_set": (C.c_int, [_P, _P, _P]),
     "gd_get_cache": (C.c_int, [_P, _P, _P]),

@@ -710,7 +710,8 @@ gd_status gd_radius_model_calibrate(gd_radius_model *h, const float *dev_feature
             cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return GD_ERR_CUDA;
-    if (gd_radius_model_check(h) != GD_OK) return GD_ERR_CUDA;
+    const gd_status chk = gd_radius_model_check(h);
+    if (chk != GD_OK) return chk;
     unsigned long long total = 0;
     for (unsigned int v : hist) total += v;
     if (total == 0) return GD_ERR_INVALID_ARGUMENT;
@@ -747,7 +748,7 @@ gd_status gd_radius_model_check(gd_radius_model *h) {
     if (!h) return GD_ERR_INVALID_ARGUMENT;
     int e = 0;
     if (cudaMemcpy(&e, h->m.err.ptr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return GD_ERR_CUDA;
-    return e ? GD_ERR_CUDA : GD_OK;
+    return e ? GD_ERR_TIMEOUT : GD_OK;
 }
 
 gd_status gd_radius_model_get(const gd_radius_model *h, float *params, float *norm17) {

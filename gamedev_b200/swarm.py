@@ -329,6 +329,54 @@ def particles_to_device(arr: np.ndarray, device="cuda:0"):
     return torch.from_numpy(a.copy()).to(device)
 
 
+def _io_check(status: int, what: str):
+    if status != 0:
+        raise GdError(status, what, 0)
+
+
+def frame_name(idx_file: int, save_max: int) -> str:
+    """The frame number of the reference's file names: idx_file zero padded to max(5, digits of
+    save_max)."""
+    buf = C.create_string_buffer(32)
+    _io_check(_lib.load().gd_frame_name(int(idx_file), int(save_max), buf, len(buf)), "gd_frame_name")
+    return buf.value.decode()
+
+
+def particles_to_file_layout(cfg: GdConfig, arr: np.ndarray) -> np.ndarray:
+    """Host particle records (n, 8) float64 in the internal layout -> a new array in the layout of
+    the reference's particle files (linear azimuthal and polar speeds)."""
+    a = np.ascontiguousarray(arr, np.float64).reshape(-1, 8).copy()
+    _io_check(_lib.load().gd_particles_to_file_layout(C.byref(cfg), C.c_void_p(a.ctypes.data), a.shape[0]),
+              "gd_particles_to_file_layout")
+    return a
+
+
+def particles_from_file_layout(cfg: GdConfig, arr: np.ndarray) -> np.ndarray:
+    """The inverse of particles_to_file_layout, as the reference converts after reading a file."""
+    a = np.ascontiguousarray(arr, np.float64).reshape(-1, 8).copy()
+    _io_check(_lib.load().gd_particles_from_file_layout(C.byref(cfg), C.c_void_p(a.ctypes.data), a.shape[0]),
+              "gd_particles_from_file_layout")
+    return a
+
+
+def save_checkpoint(cfg: GdConfig, prefix: str, idx_file: int, particles, rng=None, save_max: int = 0):
+    """Write <prefix>particle_<frame>.dat (and rngstate_<frame>.dat when rng is given) from device
+    tensors, in the reference's formats."""
+    _io_check(_lib.load().gd_save_checkpoint(C.byref(cfg), str(prefix).encode(), int(idx_file), int(save_max),
+                                             C.c_void_p(particles.data_ptr()), int(particles.shape[0]),
+                                             C.c_void_p(rng.data_ptr() if rng is not None else None)),
+              "gd_save_checkpoint")
+
+
+def load_checkpoint(cfg: GdConfig, prefix: str, idx_file: int, particles, rng=None, save_max: int = 0):
+    """Read a frame written by the reference (or by save_checkpoint) into device tensors of the
+    right sizes; raises GdError(GD_ERR_IO) on a missing file or a size mismatch."""
+    _io_check(_lib.load().gd_load_checkpoint(C.byref(cfg), str(prefix).encode(), int(idx_file), int(save_max),
+                                             C.c_void_p(particles.data_ptr()), int(particles.shape[0]),
+                                             C.c_void_p(rng.data_ptr() if rng is not None else None)),
+              "gd_load_checkpoint")
+
+
 STATIC_MAX_PARTICLES = 1 << 16  # gd_knn_static's fixed scratch
 
 

@@ -42,7 +42,10 @@ typedef enum gd_status {
     GD_ERR_TIME_RESOLUTION = 7,    /* scheduler needed more than 2^52 subdivisions             */
     GD_ERR_CONTROLLER = 8,         /* invalid rate or audit state seen by the bath controller   */
     GD_ERR_NOT_READY = 9,          /* geometry or model used before it was built               */
-    GD_ERR_OUT_OF_MEMORY = 10
+    GD_ERR_OUT_OF_MEMORY = 10,
+    GD_ERR_TIMEOUT = 11,           /* a bounded device wait gave up (the kernel stopped cleanly) */
+    GD_ERR_IO = 12                 /* a checkpoint file could not be opened, read or written,
+                                      or its size is not the expected one                       */
 } gd_status;
 
 /* Search structure requested by the model (Makefile COLLISION_SEARCH=kdtree|morton).  Both
@@ -238,7 +241,7 @@ gd_status gd_radius_model_calibrate(gd_radius_model *m, const float *dev_feature
 gd_status gd_radius_model_predict(gd_radius_model *m, const float *dev_features, int n, float *dev_radius,
                                   void *stream);
 
-/* Synchronous check of the model's device error flag: GD_ERR_CUDA when a tensor-core forward
+/* Synchronous check of the model's device error flag: GD_ERR_TIMEOUT when a tensor-core forward
  * stopped at a timed-out wait (its radii are then incomplete), else GD_OK. */
 gd_status gd_radius_model_check(gd_radius_model *m);
 
@@ -368,6 +371,26 @@ long long gd_batch_launch_count(const gd_batch *b);
 gd_status gd_knn_static(const gd_config *cfg, const gd_particle *dev_particle, int n_p, int32_t *dev_codes,
                         double *dev_measure, float *dev_kth_d2, void *stream, long long *detail, char *msg,
                         size_t msg_len);
+
+/* ---- Checkpoints in the reference's on-disk formats (inc/swarm/swarm_host.cuh:776-914, 1142-1205) --
+ * <prefix>particle_<frame>.dat holds n 64-byte records with the azimuthal and polar velocities as
+ * linear speeds (save_sam_as_velocity); <prefix>rngstate_<frame>.dat holds the n raw 48-byte
+ * cuRAND states.  <frame> is idx_file zero padded to max(5, digits of save_max) (frame_num).
+ * `prefix` is prepended as is (the reference's PATH ends with '/').  Synchronous. */
+gd_status gd_frame_name(int idx_file, int save_max, char *buf, size_t len);
+
+/* In-place conversion of host particle records between the internal layout (angular velocities)
+ * and the file layout, exactly as the reference converts them before writing and after reading. */
+gd_status gd_particles_to_file_layout(const gd_config *cfg, gd_particle *host, int n);
+gd_status gd_particles_from_file_layout(const gd_config *cfg, gd_particle *host, int n);
+
+/* SAVE_PARTICLE_TO_FILE / LOAD_PARTICLE_TO_VRAM: particles (and, when dev_rng is not NULL, the
+ * RNG states) of n particles in device memory to / from the frame's files.  A load checks the
+ * exact file sizes first and returns GD_ERR_IO on any mismatch. */
+gd_status gd_save_checkpoint(const gd_config *cfg, const char *prefix, int idx_file, int save_max,
+                             const gd_particle *dev_particle, int n, const void *dev_rng);
+gd_status gd_load_checkpoint(const gd_config *cfg, const char *prefix, int idx_file, int save_max,
+                             gd_particle *dev_particle, int n, void *dev_rng);
 
 #ifdef __cplusplus
 }
