@@ -513,6 +513,17 @@ gd_status gd_reset_controller(gd_handle *h) {
     return GD_OK;
 }
 
+size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len) {
+    if (!h) return 0;
+    const std::string text = h->col.summary.json();
+    if (buf && len) {
+        const size_t k = text.size() < len - 1 ? text.size() : len - 1;
+        std::memcpy(buf, text.data(), k);
+        buf[k] = '\0';
+    }
+    return text.size();
+}
+
 gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *dev_rng, double duration,
                                 double total_dust_mass) {
     if (!h || !dev_particle || !dev_rng) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");

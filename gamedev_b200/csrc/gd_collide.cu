@@ -26,8 +26,11 @@
 #include <math_constants.h>
 
 #include <cfloat>
+#include <algorithm>
 #include <climits>
 #include <cmath>
+#include <iomanip>
+#include <sstream>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -1561,6 +1564,72 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
 
 void collider_reset_state(Collider &c) {
     for (auto &s : c.state) s = BathState();
+    c.summary = ControllerSummary();  // swarm_runtime.cu:490-496 resets both at an output boundary
+}
+
+// _record_col_bath (_col_bound.cuh:219-238)
+void ControllerSummary::record(const BathRecord &r) {
+    const BathResult &res = r.result;
+    bath_count++;
+    continuation_launches += r.continuation_launches;
+    activity_overshoots += res.activity_overshoot ? 1 : 0;
+    distribution_overshoots += res.distribution_overshoot ? 1 : 0;
+    persistent_overshoots += res.persistent_overshoot ? 1 : 0;
+    minimum_duration = std::min(minimum_duration, r.duration);
+    maximum_duration = std::max(maximum_duration, r.duration);
+    minimum_limit_scale = std::min(minimum_limit_scale, r.limit_after);
+    maximum_f = std::max(maximum_f, res.max_f);
+    maximum_e = std::max(maximum_e, res.max_e);
+    maximum_touched = std::max(maximum_touched, res.max_touched);
+    maximum_events = std::max(maximum_events, res.max_events);
+    maximum_g = std::max(maximum_g, res.max_g);
+    maximum_g_upper = std::max(maximum_g_upper, res.max_g_upper);
+    maximum_d_bath = std::max(maximum_d_bath, res.d_bath);
+    baths.push_back(r);
+}
+
+// The text save_col_controller writes (_col_bound.cuh:242-299): schema 2, 17 significant digits.
+std::string ControllerSummary::json() const {
+    std::ostringstream f;
+    const double min_dur = std::isfinite(minimum_duration) ? minimum_duration : 0.0;
+    f << std::setprecision(17);
+    f << "{\n"
+      << "  \"schema\": 2,\n"
+      << "  \"operator_count\": " << operator_count << ",\n"
+      << "  \"bath_count\": " << bath_count << ",\n"
+      << "  \"wave_count\": " << wave_count << ",\n"
+      << "  \"continuation_launches\": " << continuation_launches << ",\n"
+      << "  \"activity_overshoots\": " << activity_overshoots << ",\n"
+      << "  \"distribution_overshoots\": " << distribution_overshoots << ",\n"
+      << "  \"persistent_overshoots\": " << persistent_overshoots << ",\n"
+      << "  \"minimum_duration\": " << min_dur << ",\n"
+      << "  \"maximum_duration\": " << maximum_duration << ",\n"
+      << "  \"minimum_limit_scale\": " << minimum_limit_scale << ",\n"
+      << "  \"maximum_f\": " << maximum_f << ",\n"
+      << "  \"maximum_e\": " << maximum_e << ",\n"
+      << "  \"maximum_touched\": " << maximum_touched << ",\n"
+      << "  \"maximum_events\": " << maximum_events << ",\n"
+      << "  \"maximum_g\": " << maximum_g << ",\n"
+      << "  \"maximum_g_upper\": " << maximum_g_upper << ",\n"
+      << "  \"maximum_d_bath\": " << maximum_d_bath << ",\n"
+      << "  \"baths\": [\n";
+    for (size_t k = 0; k < baths.size(); ++k) {
+        const BathRecord &r = baths[k];
+        const BathResult &res = r.result;
+        f << "    {\"operator\": " << r.operator_index << ", \"group\": " << r.group_index
+          << ", \"bath\": " << r.bath_index << ", \"merged_bins\": " << r.merged_bins
+          << ", \"continuation_launches\": " << r.continuation_launches << ", \"duration\": " << r.duration
+          << ", \"limit_before\": " << r.limit_before << ", \"limit_after\": " << r.limit_after
+          << ", \"max_f\": " << res.max_f << ", \"max_e\": " << res.max_e << ", \"max_touched\": " << res.max_touched
+          << ", \"max_events\": " << res.max_events << ", \"max_g\": " << res.max_g
+          << ", \"max_g_upper\": " << res.max_g_upper << ", \"d_bath\": " << res.d_bath
+          << ", \"activity_overshoot\": " << (res.activity_overshoot ? "true" : "false")
+          << ", \"distribution_overshoot\": " << (res.distribution_overshoot ? "true" : "false")
+          << ", \"persistent_overshoot\": " << (res.persistent_overshoot ? "true" : "false") << "}"
+          << ((k + 1 < baths.size()) ? "," : "") << "\n";
+    }
+    f << "  ]\n}\n";
+    return f.str();
 }
 
 static int chain_grid(const Model &m, size_t smem) {
@@ -1739,6 +1808,9 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         return choose_bath(m, h_ratebin + first, last - first, duration, c.state[g].limit_scale, out, nullptr);
     };
 
+    c.summary.operator_count++;
+    const int operator_index = c.summary.operator_count;
+    int bath_index = 0;
     // tick zero: every group starts from the same published reservoir
     initialize(nullptr, n);
     int merged = 0;
@@ -1871,9 +1943,22 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
             }
             if (!(mass > 0)) continue;
             BathResult res;
+            const double before = c.state[g].limit_scale;
             GD_TRY(finish_bath(m, h_audit + first, last - first, c.state[g], res));
             passed[g] = !(res.activity_overshoot || res.distribution_overshoot || res.persistent_overshoot);
+            BathRecord rec;
+            rec.group_index = g;
+            rec.operator_index = operator_index;
+            rec.bath_index = ++bath_index;
+            rec.merged_bins = last - first;
+            rec.duration = steps[g];
+            rec.limit_before = before;
+            rec.limit_after = c.state[g].limit_scale;
+            rec.result = res;
+            c.summary.record(rec);
         }
+        c.summary.continuation_launches += 1;  // the persistent chain: one launch per wave
+        c.summary.wave_count++;
         for (int g : groups) {
             c.stats.min_duration = std::min(c.stats.min_duration, steps[g]);
             c.stats.max_duration = std::max(c.stats.max_duration, steps[g]);

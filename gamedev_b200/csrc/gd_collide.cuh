@@ -4,7 +4,9 @@
 
 #include <curand_kernel.h>
 
+#include <cmath>
 #include <cstdint>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -33,6 +35,27 @@ struct BathState {
 struct BathResult {
     double max_f = 0, max_e = 0, max_touched = 0, max_events = 0, max_g = 0, max_g_upper = 0, d_bath = 0;
     bool activity_overshoot = false, distribution_overshoot = false, persistent_overshoot = false;
+};
+
+// Controller diagnostics of one output interval (col_bath_record / col_controller_summary,
+// inc/swarm/_col_types.cuh:87-120): one record per finished group bath and the running extrema,
+// kept by _record_col_bath (_col_bound.cuh:219-238) and written as save_col_controller writes them
+// (:242-299).  continuation_launches counts chain launches per wave; this build's chain is
+// persistent, so that is one per wave where the reference relaunches capped chains.
+struct BathRecord {
+    int group_index = -1, operator_index = 0, bath_index = 0, merged_bins = 0, continuation_launches = 0;
+    double duration = 0.0, limit_before = 1.0, limit_after = 1.0;
+    BathResult result;
+};
+struct ControllerSummary {
+    int operator_count = 0, bath_count = 0, wave_count = 0, continuation_launches = 0;
+    int activity_overshoots = 0, distribution_overshoots = 0, persistent_overshoots = 0;
+    double minimum_duration = HUGE_VAL, maximum_duration = 0.0, minimum_limit_scale = 1.0;
+    double maximum_f = 0.0, maximum_e = 0.0, maximum_touched = 0.0, maximum_events = 0.0, maximum_g = 0.0,
+           maximum_g_upper = 0.0, maximum_d_bath = 0.0;
+    std::vector<BathRecord> baths;
+    void record(const BathRecord &r);
+    std::string json() const;
 };
 
 // Power-of-two group scheduler on a 2^52-tick lattice (local_schedule, _col_sched.cuh:17-183).
@@ -89,6 +112,7 @@ struct Collider {
     std::vector<int> group_start;     // [groups + 1] offsets into group_sorted
     std::vector<unsigned int> edges;  // dependency rows, LOCAL_WORDS per group
     std::vector<BathState> state;
+    ControllerSummary summary;        // reset with `state` at output boundaries
     bool local_geometry_valid = false;
     gd_operator_stats stats{};
     long long launches = 0;           // kernels launched by the operator (reported by the ABI)

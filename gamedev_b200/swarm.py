@@ -158,6 +158,16 @@ class SwarmCollision:
     def reset_controller(self):
         self._check(self.lib.gd_reset_controller(self.h))
 
+    def controller_summary(self) -> dict:
+        """COL_DIAGNOSTICS controller summary of the current output interval (gd_controller_summary),
+        parsed from the JSON the reference's save_col_controller writes."""
+        import json
+
+        n = self.lib.gd_controller_summary(self.h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        self.lib.gd_controller_summary(self.h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
     # ---- collision operator ---------------------------------------------------------------
     def evolve_local_collisions(self, particles, rng, duration: float, total_dust_mass: float):
         self.lib.gd_set_stream(self.h, _stream())

@@ -273,6 +273,14 @@ gd_status gd_invalidate_geometry(gd_handle *h);
  * output boundary (swarm_runtime.cu:490-496). */
 gd_status gd_reset_controller(gd_handle *h);
 
+/* COL_DIAGNOSTICS controller summary of the current output interval (since the handle was created
+ * or gd_reset_controller last ran), as the JSON text save_col_controller writes
+ * (inc/swarm/_col_bound.cuh:242-299, schema 2): per finished group bath its duration, limit scale
+ * before and after and the audit result, and the running extrema.  Copies up to len - 1 bytes and a
+ * terminating NUL into buf (buf may be NULL) and returns the full text length.  Chain launches per
+ * wave are 1 (the persistent chain) where the reference counts its relaunches. */
+size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len);
+
 /* evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539): advance every owner through one
  * fixed-position frozen-bath collision operator of length `duration`, mutating par_size and
  * par_numr of dev_particle and the RNG states in dev_rng.  Uses the neighbour cache built by

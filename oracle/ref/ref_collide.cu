@@ -6,10 +6,12 @@
 // TEST INFRASTRUCTURE ONLY: it pins the B200 collision operator against the reference's CUDA
 // build (statistically, and per particle where the neighbour order is the same) and times it.
 //
-//   ref_collide <in.bin> <out.bin> <seed> <duration> <total_dust_mass> <operators>
+//   ref_collide <in.bin> <out.bin> <seed> <duration> <total_dust_mass> <operators> [<summary.json>]
 //   in.bin : int32 n (= N_P), then n particle records (the 64 B struct swarm)
 //   out.bin: the n records after `operators` calls of evolve_collisions(duration) on one geometry
 //   stdout : one JSON line {"n", "operators", "geometry_ms", "operator_ms": [...], "total_ms"}
+//   summary.json (builds with COL_DIAGNOSTICS only): the controller summary of the operators as
+//            the reference's save_col_controller writes it (_col_bound.cuh:242-299)
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -52,7 +54,8 @@ void check_bad(int *dev_bad_part) {
 
 int main(int argc, char **argv) {
     try {
-        if (argc != 7) throw std::runtime_error("usage: ref_collide <in> <out> <seed> <duration> <mass> <operators>");
+        if (argc != 7 && argc != 8)
+            throw std::runtime_error("usage: ref_collide <in> <out> <seed> <duration> <mass> <operators> [<summary>]");
         static_assert(sizeof(swarm) == 64, "MULTISIZE particle record");
         std::ifstream in(argv[1], std::ios::binary);
         int n = 0;
@@ -115,6 +118,10 @@ int main(int argc, char **argv) {
         bool local_geometry_valid = false;
         real clock_dyn = 0.0, dt_col = 0.0;
         int count_col = 0;
+#ifdef COL_DIAGNOSTICS
+        col_controller_summary col_summary;
+        const real clock_sim = 0.0;
+#endif
 
         gpuEvent_t a, b;
         check(gpuEventCreate(&a), "event");
@@ -168,7 +175,11 @@ int main(int argc, char **argv) {
                                     dev_col_unfinished, dev_col_active, dev_col_complete, dev_size_old,
                                     dev_numr_old, dev_col_time, dev_col_rate, dev_col_hazard, dev_col_jump1_int,
                                     dev_col_jump2_int, dev_col_jumpmax_int, dev_col_measure, dev_col_ratebin,
-                                    dev_col_audit);
+                                    dev_col_audit
+#ifdef COL_DIAGNOSTICS
+                                    , clock_sim, col_summary
+#endif
+            );
             check(gpuEventRecord(b, 0), "record");
             check(gpuEventSynchronize(b), "operator");
             float ms = 0.0f;
@@ -176,6 +187,10 @@ int main(int argc, char **argv) {
             op_ms.push_back(ms);
         }
         check(gpuMemcpy(particle.data(), dev_particle, sizeof(swarm) * N_P, gpuMemcpyDeviceToHost), "copy back");
+#ifdef COL_DIAGNOSTICS
+        if (argc == 8 && !save_col_controller(argv[7], col_summary))
+            throw std::runtime_error("cannot write the controller summary");
+#endif
         std::ofstream out(argv[2], std::ios::binary);
         out.write(reinterpret_cast<const char *>(&n), 4);
         out.write(reinterpret_cast<const char *>(particle.data()), sizeof(swarm) * N_P);

@@ -16,17 +16,19 @@ import numpy as np
 REF_DIR = Path(__file__).resolve().parents[1] / "_ref"
 
 
-def binary(model: str, n: int) -> Path:
-    return REF_DIR / f"collide_{model}_{n}" / "ref_collide"
+def binary(model: str, n: int, diagnostics: bool = False) -> Path:
+    return REF_DIR / f"collide{'_diag' if diagnostics else ''}_{model}_{n}" / "ref_collide"
 
 
-def available(model: str, n: int) -> bool:
-    return binary(model, n).exists()
+def available(model: str, n: int, diagnostics: bool = False) -> bool:
+    return binary(model, n, diagnostics).exists()
 
 
 def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dust_mass: float,
-        operators: int = 1, timeout: float = 1800):
-    """-> (particles after `operators` evolve_collisions(duration) calls on one geometry, info)"""
+        operators: int = 1, timeout: float = 1800, diagnostics: bool = False):
+    """-> (particles after `operators` evolve_collisions(duration) calls on one geometry, info).
+    With diagnostics (the COL_DIAGNOSTICS build), info["summary"] holds the controller summary the
+    reference's save_col_controller wrote, parsed, and info["summary_text"] its text."""
     p = np.ascontiguousarray(particles, dtype=np.float64).reshape(-1, 8)
     n = len(p)
     with tempfile.TemporaryDirectory() as d:
@@ -34,12 +36,18 @@ def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dus
         with open(src, "wb") as f:
             np.array([n], dtype=np.int32).tofile(f)
             p.tofile(f)
-        r = subprocess.run([str(binary(model, n)), str(src), str(dst), str(int(seed)), repr(float(duration)),
-                            repr(float(total_dust_mass)), str(int(operators))],
-                           capture_output=True, text=True, timeout=timeout)
+        summary = Path(d) / "summary.json"
+        args = [str(binary(model, n, diagnostics)), str(src), str(dst), str(int(seed)), repr(float(duration)),
+                repr(float(total_dust_mass)), str(int(operators))]
+        if diagnostics:
+            args.append(str(summary))
+        r = subprocess.run(args, capture_output=True, text=True, timeout=timeout, cwd=d)
         if r.returncode != 0:
             raise RuntimeError(f"ref_collide failed ({r.returncode}): {r.stderr.strip()[-2000:]}")
         info = json.loads(r.stdout.strip().splitlines()[-1])
+        if diagnostics:
+            info["summary_text"] = summary.read_text()
+            info["summary"] = json.loads(info["summary_text"])
         raw = np.fromfile(dst, dtype=np.uint8)
         out = raw[4:].view(np.float64).reshape(n, 8).copy()
         return out, info

@@ -142,3 +142,54 @@ def test_kd_operator_matches_reference_cuda_statistically(gd, cuda):
     assert mannwhitneyu(m2o, m2r).pvalue > 0.01, (m2o, m2r)
     dstat, pval = _weighted_ks(np.concatenate(xo), np.concatenate(wo), np.concatenate(xr), np.concatenate(wr))
     assert pval > 0.01, (dstat, pval)
+
+
+def test_morton_controller_summary_matches_reference(gd, cuda):
+    """COL_DIAGNOSTICS: over two operators on the Morton shapes (the same event chains as the
+    reference), the controller summary gd_controller_summary returns equals the one the reference's
+    COL_DIAGNOSTICS build writes (save_col_controller): operator, bath and wave counts, overshoot
+    counts and flags, every bath's group, merged bins, duration and limit scale before and after
+    exactly; the audit maxima, sums of FP64 atomics in either build, to 1e-9 relative (1e-12
+    absolute where they cancel).  Chain
+    launches per wave are not compared: this build's chain is persistent (one launch per wave)
+    where the reference relaunches chains capped at COL_EVENT_CAP events."""
+    from gamedev_b200 import workloads
+
+    refcollide = _refc()
+    model = "c1_multisize_2d"
+    if not refcollide.available(model, N, diagnostics=True):
+        pytest.skip("oracle/_ref reference COL_DIAGNOSTICS build absent (reference tree not mounted at build time)")
+    cfg = workloads.config(model)
+    p = workloads.particles(model, n=N, seed=11)
+    d = _duration(gd, cfg, p, 2000.0)
+    import torch
+
+    sw = gd.SwarmCollision(cfg, N)
+    dp = gd.particles_to_device(p)
+    rng = gd.rngstate_init(N, seed=1)
+    for _ in range(2):
+        sw.evolve_collisions(dp, rng, d, _mass(p))
+    torch.cuda.synchronize()
+    ours = sw.controller_summary()
+    sw.close()
+    _, info = refcollide.run(model, p, 1, d, _mass(p), 2, timeout=600, diagnostics=True)
+    ref = info["summary"]
+    exact = ["schema", "operator_count", "bath_count", "wave_count", "activity_overshoots",
+             "distribution_overshoots", "persistent_overshoots", "minimum_duration", "maximum_duration",
+             "minimum_limit_scale"]
+    for key in exact:
+        assert ours[key] == ref[key], (key, ours[key], ref[key])
+    close = ["maximum_f", "maximum_e", "maximum_touched", "maximum_events", "maximum_g", "maximum_g_upper",
+             "maximum_d_bath"]
+    for key in close:
+        assert math.isclose(ours[key], ref[key], rel_tol=1e-9, abs_tol=1e-12), (key, ours[key], ref[key])
+    assert ours["bath_count"] > 2 and ours["wave_count"] >= 2
+    assert len(ours["baths"]) == len(ref["baths"])
+    for a, b in zip(ours["baths"], ref["baths"]):
+        for key in ("operator", "group", "bath", "merged_bins", "duration", "limit_before", "limit_after",
+                    "activity_overshoot", "distribution_overshoot", "persistent_overshoot"):
+            assert a[key] == b[key], (key, a, b)
+        for key in ("max_f", "max_e", "max_touched", "max_events", "max_g", "max_g_upper", "d_bath"):
+            # d_bath is a difference of audit sums: where it cancels, the residual is ~1e-17 in one
+            # summation order and 0 in another
+            assert math.isclose(a[key], b[key], rel_tol=1e-9, abs_tol=1e-12), (key, a, b)
