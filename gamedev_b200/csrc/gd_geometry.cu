@@ -448,15 +448,26 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
         // Fill phase: a lane with fewer than cap entries appends without ordering work.  A lane
         // that reaches cap stops and keeps the rest of its mask; the lanes that filled up in this
         // leaf then build their heaps together (in step, instead of one lane after another).
+        // two candidates per pass: half the divergent trips, two independent distance chains
         while (mask && cnt < cap) {
-            const int c = __ffs(mask) - 1;
+            const int c0 = __ffs(mask) - 1;
             mask &= mask - 1;
-            const float4 p = tile[c];
-            const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
-            if (d2 <= cut) {
+            const bool two = mask && cnt + 1 < cap;
+            const int c1 = two ? __ffs(mask) - 1 : c0;
+            if (two) mask &= mask - 1;
+            const float4 p0 = tile[c0], p1 = tile[c1];
+            const float d0 = dist2(qp, make_float3(p0.x, p0.y, p0.z));
+            const float d1 = dist2(qp, make_float3(p1.x, p1.y, p1.z));
+            if (d0 <= cut) {
                 ++st_offers;
-                hp[cnt] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                          static_cast<unsigned int>(__float_as_int(p.w));
+                hp[cnt] = (static_cast<unsigned long long>(__float_as_uint(d0)) << 32) |
+                          static_cast<unsigned int>(__float_as_int(p0.w));
+                ++cnt;
+            }
+            if (two && d1 <= cut) {
+                ++st_offers;
+                hp[cnt] = (static_cast<unsigned long long>(__float_as_uint(d1)) << 32) |
+                          static_cast<unsigned int>(__float_as_int(p1.w));
                 ++cnt;
             }
         }
