@@ -250,3 +250,71 @@ def test_pair_rates_match_oracle(gd, cuda, oracle_lib, idx):
             lines.append("  gpu    " + " ".join(f"{v:.17g}" for v in g))
             lines.append("  oracle " + " ".join(f"{v:.17g}" for v in w))
         pytest.fail("\n".join(lines))
+
+
+def _controller_valid(data: dict) -> bool:
+    """The checks the reference's validator applies to an archived controller summary
+    (val/swarm/src/run_chain.py:99-170, validate_controller), restated."""
+    numeric = ("minimum_duration", "maximum_duration", "minimum_limit_scale", "maximum_f", "maximum_e",
+               "maximum_touched", "maximum_events", "maximum_g", "maximum_g_upper", "maximum_d_bath")
+    baths = data.get("baths", [])
+    finite = all(math.isfinite(float(data.get(k, math.nan))) for k in numeric)
+    complete = (data.get("schema") == 2 and data.get("bath_count") == len(baths) and data.get("bath_count", 0) > 0
+                and data.get("operator_count", 0) > 0 and data.get("wave_count", 0) > 0
+                and data.get("persistent_overshoots") == 0)
+    continuation = data.get("continuation_launches", 0) > 0
+    bath_numeric = ("duration", "limit_before", "limit_after", "max_f", "max_e", "max_touched", "max_events",
+                    "max_g", "max_g_upper", "d_bath")
+    records = all(r.get("operator", 0) > 0 and r.get("bath", 0) > 0 and r.get("merged_bins", 0) > 0
+                  and r.get("group", -1) >= 0 and r.get("duration", 0.0) > 0.0
+                  and 0.25 <= r.get("limit_before", 0.0) <= 1.0 and 0.25 <= r.get("limit_after", 0.0) <= 1.0
+                  and all(math.isfinite(float(r.get(k, math.nan))) for k in bath_numeric)
+                  and all(r.get(k, -1.0) >= 0.0 for k in bath_numeric if k != "limit_before")
+                  and not r.get("persistent_overshoot", True) for r in baths)
+    return finite and complete and continuation and records
+
+
+def _controller_equivalent(a, b) -> bool:
+    """The validator's repeat comparison (run_chain.py:64-96): equal keys and structure, numbers
+    within 1e-12 relative or absolute (atomic-sum roundoff)."""
+    if isinstance(a, dict):
+        return isinstance(b, dict) and a.keys() == b.keys() and all(_controller_equivalent(a[k], b[k]) for k in a)
+    if isinstance(a, list):
+        return isinstance(b, list) and len(a) == len(b) and all(_controller_equivalent(x, y) for x, y in zip(a, b))
+    if isinstance(a, (int, float)) and not isinstance(a, bool):
+        return (isinstance(b, (int, float)) and not isinstance(b, bool)
+                and math.isclose(float(a), float(b), rel_tol=1e-12, abs_tol=1e-12))
+    return a == b
+
+
+def test_controller_summary_passes_reference_validator(gd, cuda):
+    """COL_DIAGNOSTICS summary (gd_controller_summary) of a multi-wave run: accepted by the checks of
+    the reference's run_chain.py validator, repeat-consistent under its comparison, and cleared by
+    gd_reset_controller as at an output boundary."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    cfg = workloads.config("c1_multisize_2d")
+    p = workloads.particles("c1_multisize_2d", n=20000)
+    mass = _total_mass(p)
+    summaries = []
+    for _ in range(2):
+        sw, dp, rng, *_ = _setup(gd, cfg, p, seed=5)
+        sw.evolve_local_collisions(dp, rng, 1.0e-9 * workloads.orbital_time(), mass)
+        rate_max = float(sw.owner_state()[0][:, 0].max().item())
+        sw.reset_controller()
+        dp.copy_(gd.particles_to_device(p))
+        rng = gd.rngstate_init(len(p), seed=5)
+        for _ in range(3):
+            sw.evolve_local_collisions(dp, rng, 20.0 / rate_max, mass)
+        torch.cuda.synchronize()
+        summaries.append(sw.controller_summary())
+        sw.reset_controller()
+        empty = sw.controller_summary()
+        assert empty["operator_count"] == 0 and empty["baths"] == []
+        sw.close()
+    a, b = summaries
+    assert a["operator_count"] == 3 and a["wave_count"] > 3 and a["bath_count"] > 3
+    assert _controller_valid(a)
+    assert _controller_equivalent(a, b)

@@ -108,5 +108,6 @@ def test_resume_from_checkpoint_is_exact(gd, cuda, tmp_path, model):
     # the file layout pins inactive coordinates and round-trips velocities through R; the collision
     # path reads positions, sizes and numbers only, which the files carry unchanged
     assert torch.equal(da[:, 6:8], db[:, 6:8])
-    assert torch.equal(ra, rb)
+    # RNG states compared as streams (member-wise state copies need not keep struct padding)
+    assert torch.equal(gd.rng_uniforms(ra, n, 4), gd.rng_uniforms(rb, n, 4))
     sw2.close()
