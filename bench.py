@@ -613,7 +613,7 @@ def run_ours(args):
 
 def run_batched(args):
     """The batched configuration (256 c0-shaped swarms, log-uniform sizes on [2^10, 2^18], K from
-    {16, 32, 64}): per-swarm geometry + one persistent top-K launch, captured as one CUDA graph,
+    {16, 32, 64}): segmented geometry + one persistent top-K launch, captured as one CUDA graph,
     against the same swarms searched one handle at a time.  Every swarm is checked bit-exact
     against its one-swarm result."""
     import torch
@@ -683,7 +683,7 @@ def run_batched(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "c2_batched", "swarms": len(sizes), "particles": int(sum(sizes)),
                    "n_range": [min(sizes), max(sizes)], "k_choices": [16, 32, 64],
-                   "step": "per-swarm geometry on 8 streams + one persistent top-K launch, one CUDA graph replay",
+                   "step": "segmented geometry (one launch per stage for all swarms) + one persistent top-K launch, one CUDA graph replay",
                    "sort_bits": sort_bits,
                    "parallelism": f"replicas x{world}"},
         "kernels_per_step": kernels,

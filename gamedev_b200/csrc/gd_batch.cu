@@ -1,12 +1,12 @@
 // Batched neighbour search: many independent swarms of uneven size (and K) per call.  No
 // counterpart in the reference, which runs one swarm per process.
 //
-// Each swarm keeps its own geometry (site init, Morton radix sort, bucket tree: the one-swarm
-// kernels, enqueued on a few internal streams so that small swarms build side by side), and one
-// persistent launch then runs the top-K of every bucket of every swarm (knn_batch_query).  The
-// non-finite screen is deferred to gd_batch_check, so a call makes no host synchronisation and
-// can be captured into a CUDA graph (the internal streams fork from and join back to the batch's
-// stream).
+// One BatchGeometry indexes every swarm with one launch per stage: site init over the
+// concatenated particles, one radix sort of (swarm id, Morton) keys (each swarm's sites come out
+// contiguous), gather, leaf bounds and one launch per tree level across swarms.  One persistent
+// launch then runs the top-K of every bucket of every swarm (knn_batch_query).  The non-finite
+// screen is deferred to gd_batch_check, so a call makes no host synchronisation and can be
+// captured into a CUDA graph: about fifty kernels per call, whatever the number of swarms.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -25,30 +25,19 @@ struct gd_batch {
     long long n_total = 0, codes_total = 0;
     int kcap = 0;
     std::vector<gd::Model> models;
-    std::vector<std::unique_ptr<gd::Geometry>> geo;
+    gd::BatchGeometry geo;
     gd::DevBuf<gd::BatchSwarm> tab;
     gd::DevBuf<int> leaf_prefix;
     gd::DevBuf<long long> part_prefix;
     gd::DevBuf<int> next;
     cudaStream_t stream = nullptr;
-    std::vector<cudaStream_t> workers;
-    std::vector<cudaEvent_t> done;
-    cudaEvent_t start = nullptr;
     long long launches = 0;
     gd::Tuning tune;
     std::string err;
     long long detail = 0;
-
-    ~gd_batch() {
-        for (cudaStream_t w : workers) cudaStreamDestroy(w);
-        for (cudaEvent_t e : done) cudaEventDestroy(e);
-        if (start) cudaEventDestroy(start);
-    }
 };
 
 namespace {
-
-constexpr int kBatchStreams = 8;  // internal streams for the per-swarm geometry builds
 
 gd_status batch_fail(gd_batch *b, const gd::Status &s) {
     if (b) {
@@ -79,7 +68,6 @@ gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int
     b->S = S;
     b->n.assign(n_p, n_p + S);
     b->k.assign(n_k, n_k + S);
-    std::vector<gd::BatchSwarm> tab(S);
     std::vector<int> leaf_prefix(S + 1, 0);
     std::vector<long long> part_prefix(S + 1, 0);
     for (int s = 0; s < S; ++s) {
@@ -93,27 +81,27 @@ gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int
         b->n_total += n_p[s];
         b->codes_total += static_cast<long long>(n_p[s]) * n_k[s];
         b->kcap = n_k[s] > b->kcap ? n_k[s] : b->kcap;
-        std::unique_ptr<gd::Geometry> g(new (std::nothrow) gd::Geometry());
-        if (!g) return GD_ERR_OUT_OF_MEMORY;
-        gd::Status st = gd::geometry_alloc(*g, b->models.back(), n_p[s]);
-        if (!st) return st.code;
-        g->deferred_check = true;
-        gd::BatchSwarm &t = tab[s];
-        t.sorted = g->sorted.ptr;
-        t.lo = g->node_lo.ptr;
-        t.hi = g->node_hi.ptr;
-        t.sub_lo = g->sub_lo.ptr;
-        t.sub_hi = g->sub_hi.ptr;
-        t.qrad = g->q.ptr;
-        t.active = g->active.ptr;
-        t.counters = g->counters.ptr;
-        t.leaf_slots = g->leaf_slots;
-        t.k = n_k[s];
-        t.part_off = b->part_off.back();
-        t.codes_off = b->codes_off.back();
         leaf_prefix[s + 1] = leaf_prefix[s] + (n_p[s] + gd::kLeaf - 1) / gd::kLeaf;
         part_prefix[s + 1] = b->n_total;
-        b->geo.push_back(std::move(g));
+    }
+    gd::Status st = gd::batch_geometry_alloc(b->geo, b->models[0], S, n_p, b->tune.sort_bits);
+    if (!st) return st.code;
+    gd::BatchGeometry &g = b->geo;
+    std::vector<gd::BatchSwarm> tab(S);
+    for (int s = 0; s < S; ++s) {
+        gd::BatchSwarm &t = tab[s];
+        t.sorted = g.sorted.ptr + g.h_leaf_prefix[s] * gd::kLeaf;
+        t.lo = g.node_lo.ptr + g.h_node_off[s];
+        t.hi = g.node_hi.ptr + g.h_node_off[s];
+        t.sub_lo = g.sub_lo.ptr + g.h_leaf_prefix[s] * gd::kSubs;
+        t.sub_hi = g.sub_hi.ptr + g.h_leaf_prefix[s] * gd::kSubs;
+        t.qrad = g.q.ptr + b->part_off[s];
+        t.active = g.active.ptr + b->part_off[s];
+        t.counters = g.counters.ptr + 2 * s;
+        t.leaf_slots = g.leaf_slots[s];
+        t.k = n_k[s];
+        t.part_off = b->part_off[s];
+        t.codes_off = b->codes_off[s];
     }
     if (b->tab.alloc(S) != cudaSuccess || b->leaf_prefix.alloc(S + 1) != cudaSuccess ||
         b->part_prefix.alloc(S + 1) != cudaSuccess || b->next.alloc(1) != cudaSuccess)
@@ -124,16 +112,6 @@ gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int
         cudaMemcpy(b->part_prefix.ptr, part_prefix.data(), sizeof(long long) * (S + 1), cudaMemcpyHostToDevice) !=
             cudaSuccess)
         return GD_ERR_CUDA;
-    const int W = S < kBatchStreams ? S : kBatchStreams;
-    for (int w = 0; w < W; ++w) {
-        cudaStream_t st;
-        cudaEvent_t ev;
-        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GD_ERR_CUDA;
-        b->workers.push_back(st);
-        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return GD_ERR_CUDA;
-        b->done.push_back(ev);
-    }
-    if (cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming) != cudaSuccess) return GD_ERR_CUDA;
     *out = b.release();
     return GD_OK;
 }
@@ -150,30 +128,13 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
                        float *dev_kth_d2) {
     if (!b || !dev_particle || !dev_codes || !dev_measure || !dev_kth_d2)
         return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "null batch, particle or output pointer");
-    // fork: every internal stream starts after the work already queued on the batch's stream
-    if (cudaEventRecord(b->start, b->stream) != cudaSuccess)
-        return batch_fail(b, gd::cuda_status(cudaGetLastError(), "fork batch streams"));
-    const int W = static_cast<int>(b->workers.size());
-    for (int w = 0; w < W; ++w)
-        if (cudaStreamWaitEvent(b->workers[w], b->start, 0) != cudaSuccess)
-            return batch_fail(b, gd::cuda_status(cudaGetLastError(), "fork batch streams"));
-    for (int s = 0; s < b->S; ++s) {
-        gd::Geometry &g = *b->geo[s];
-        g.sort_bits = b->tune.sort_bits;
-        const long long before = g.launches;
-        gd::Status st = gd::geometry_build(g, b->models[s], dev_particle + b->part_off[s], b->workers[s % W]);
-        b->launches += g.launches - before;
-        if (!st) return batch_fail(b, st);
-    }
-    // join
-    for (int w = 0; w < W; ++w) {
-        if (cudaEventRecord(b->done[w], b->workers[w]) != cudaSuccess ||
-            cudaStreamWaitEvent(b->stream, b->done[w], 0) != cudaSuccess)
-            return batch_fail(b, gd::cuda_status(cudaGetLastError(), "join batch streams"));
-    }
-    gd::Status st = gd::knn_batch_query(b->models[0], b->tab.ptr, b->leaf_prefix.ptr, b->part_prefix.ptr, b->S,
-                                        b->n_total, b->kcap, b->next.ptr, dev_particle, dev_codes, dev_measure,
-                                        dev_kth_d2, b->stream, &b->launches, b->tune);
+    const long long before = b->geo.launches;
+    gd::Status st = gd::batch_geometry_build(b->geo, b->models[0], dev_particle, b->stream);
+    b->launches += b->geo.launches - before;
+    if (!st) return batch_fail(b, st);
+    st = gd::knn_batch_query(b->models[0], b->tab.ptr, b->leaf_prefix.ptr, b->part_prefix.ptr, b->S, b->n_total,
+                             b->kcap, b->next.ptr, dev_particle, dev_codes, dev_measure, dev_kth_d2, b->stream,
+                             &b->launches, b->tune);
     if (!st) return batch_fail(b, st);
     b->err.clear();
     b->detail = 0;
@@ -182,17 +143,9 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
 
 gd_status gd_batch_check(gd_batch *b) {
     if (!b) return GD_ERR_INVALID_ARGUMENT;
-    for (int s = 0; s < b->S; ++s) {
-        gd::Status st = gd::geometry_check(*b->geo[s], b->stream);
-        if (!st) {
-            if (st.code == GD_ERR_NONFINITE) {
-                st.detail += b->part_off[s];  // index in the concatenated particle array
-                st.msg = "non-finite particle state before collision search at particle " +
-                         std::to_string(st.detail) + " (swarm " + std::to_string(s) + ")";
-            }
-            return batch_fail(b, st);
-        }
-    }
+    int swarm = -1;
+    gd::Status st = gd::batch_geometry_check(b->geo, b->stream, &swarm);
+    if (!st) return batch_fail(b, st);
     b->err.clear();
     b->detail = 0;
     return GD_OK;
@@ -212,6 +165,13 @@ gd_status gd_batch_set_tuning(gd_batch *b, const gd_tuning *t) {
     u.sort_bits = t->sort_bits;
     if (u.warps > 0 && gd::knn_block_warps(b->kcap, u, nullptr) == 0)
         return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory");
+    // the Morton bits the next build keeps under the swarm id
+    const int key_bits = 21 * dim;
+    int mbits = (u.sort_bits > 0 && u.sort_bits < key_bits) ? u.sort_bits : key_bits;
+    if (u.sort_bits == 0 && mbits + b->geo.sbits > 64) mbits = 64 - b->geo.sbits;
+    if (mbits + b->geo.sbits > 64) return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "too many swarms for the sort key");
+    b->geo.mbits = mbits;
+    b->geo.mshift = key_bits - mbits;
     b->tune = u;
     return GD_OK;
 }

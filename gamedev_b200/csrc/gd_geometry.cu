@@ -1020,6 +1020,302 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     return Status::ok();
 }
 
+// ------------------------------------------------------------------------------------------------
+// Batched geometry (BatchGeometry): every stage of geometry_build once over all swarms.
+// ------------------------------------------------------------------------------------------------
+// the last s in [0, S) with prefix[s] <= x (prefix[0] = 0, ascending)
+__device__ __forceinline__ int segment_of(const long long *__restrict__ prefix, int S, long long x) {
+    int lo = 0, hi = S - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_batch_counters_reset(int S, int *counters) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 2 * S) counters[t] = (t & 1) ? INT_MAX : 0;
+}
+
+// k_site_init over the batch: key = swarm id above the top `mbits` Morton bits; an inactive or
+// non-finite site carries an all-ones Morton field, so it sorts after its swarm's active sites
+__global__ void k_batch_site_init(Model m, int S, const long long *__restrict__ part_prefix, long long n_total,
+                                  long long n_sort, const gd_particle *__restrict__ part, float4 *__restrict__ site,
+                                  float *__restrict__ qrad, unsigned char *__restrict__ active,
+                                  unsigned long long *__restrict__ key, unsigned int *__restrict__ val, int mbits,
+                                  int mshift, int *__restrict__ counters) {
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n_sort) return;
+    if (g >= n_total) {  // sort padding: after every swarm
+        key[g] = ~0ull;
+        val[g] = static_cast<unsigned int>(g);
+        return;
+    }
+    const int sw = segment_of(part_prefix, S, g);
+    const int i = static_cast<int>(g - part_prefix[sw]);
+    const double2 *rec = reinterpret_cast<const double2 *>(part + g);
+    const double2 a = rec[0], b = rec[1], c = rec[2], d = rec[3];
+    const bool finite = isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y) && isfinite(c.x) &&
+                        isfinite(c.y) && isfinite(d.x) && isfinite(d.y);
+    const unsigned long long ones = (mbits >= 64) ? ~0ull : ((1ull << mbits) - 1ull);
+    unsigned long long field = ones;
+    float4 st = make_float4(0.f, 0.f, 0.f, __int_as_float(3 * i));
+    float qi = 0.f;
+    bool act = false;
+    if (!finite) {
+        atomicMin(&counters[2 * sw + 1], i);
+    } else {
+        const double x = a.x, y = a.y, z = b.x;
+        act = site_active(m, y, z);
+        const double R = cyl_R(m, y, z);
+        const double Z = cyl_Z(m, y, z);
+        const float3 pt = (m.n_x == 1 && m.n_z == 1)
+                              ? make_float3(static_cast<float>(R), 0.0f, 0.0f)
+                              : make_float3(static_cast<float>(R * cos(x)), static_cast<float>(R * sin(x)),
+                                            static_cast<float>(Z));
+        st.x = pt.x;
+        st.y = pt.y;
+        st.z = pt.z;
+        if (act) {
+            qi = static_cast<float>(m.h_search * get_hg(m, R) * R);
+            field = morton_key(m, pt) >> mshift;
+            if (field == ones) field = ones - 1;  // strictly before the swarm's inactive sites
+        }
+    }
+    site[g] = st;
+    qrad[g] = qi;
+    active[g] = act ? 1 : 0;
+    key[g] = (static_cast<unsigned long long>(sw) << mbits) | field;
+    val[g] = static_cast<unsigned int>(g);
+    // one atomic per swarm present among the warp's active lanes
+    const unsigned int am = __ballot_sync(__activemask(), act);
+    if (act) {
+        const unsigned int peers = __match_any_sync(am, sw);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counters[2 * sw], __popc(peers));
+    }
+}
+
+// k_gather_sorted over the batch: global sorted slot j of swarm s is its slot j - 32 * leaf_prefix[s]
+__global__ void k_batch_gather(int S, long long n_slots, const long long *__restrict__ leaf_prefix,
+                               const long long *__restrict__ part_prefix, const int *__restrict__ counters,
+                               const unsigned int *__restrict__ val, const float4 *__restrict__ site,
+                               float4 *__restrict__ sorted) {
+    const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n_slots) return;
+    const int sw = segment_of(leaf_prefix, S, j / kLeaf);
+    const long long l = j - leaf_prefix[sw] * kLeaf;
+    const int n_act = counters[2 * sw];
+    const long long n_pad = (n_act + kLeaf - 1) / kLeaf * kLeaf;
+    if (l >= n_pad) return;
+    sorted[j] = (l < n_act) ? site[val[part_prefix[sw] + l]]
+                            : make_float4(CUDART_INF_F_, CUDART_INF_F_, CUDART_INF_F_, __int_as_float(-1));
+}
+
+// k_leaf_bounds over the batch: one warp per leaf slot of every swarm
+__global__ void k_batch_leaf_bounds(int S, long long n_leaves, const long long *__restrict__ leaf_prefix,
+                                    const long long *__restrict__ node_off, const int *__restrict__ counters,
+                                    const float4 *__restrict__ sorted, float4 *__restrict__ lo, float4 *__restrict__ hi,
+                                    float4 *__restrict__ sub_lo, float4 *__restrict__ sub_hi) {
+    const long long L = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (L >= n_leaves) return;
+    const int sw = segment_of(leaf_prefix, S, L);
+    const long long leaf = L - leaf_prefix[sw];
+    const long long slots = leaf_prefix[sw + 1] - leaf_prefix[sw];
+    const int n_act = counters[2 * sw];
+    const long long i = leaf * kLeaf + lane;
+    float3 a = make_float3(CUDART_INF_F_, CUDART_INF_F_, CUDART_INF_F_);
+    float3 b = make_float3(-CUDART_INF_F_, -CUDART_INF_F_, -CUDART_INF_F_);
+    if (i < n_act) {
+        const float4 st = sorted[leaf_prefix[sw] * kLeaf + i];
+        a = make_float3(st.x, st.y, st.z);
+        b = a;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        if (off == kSub && (lane & (kSub - 1)) == 0) {
+            sub_lo[L * kSubs + lane / kSub] = make_float4(a.x, a.y, a.z, 0.f);
+            sub_hi[L * kSubs + lane / kSub] = make_float4(b.x, b.y, b.z, 0.f);
+        }
+        a.x = fminf(a.x, __shfl_xor_sync(0xffffffffu, a.x, off));
+        a.y = fminf(a.y, __shfl_xor_sync(0xffffffffu, a.y, off));
+        a.z = fminf(a.z, __shfl_xor_sync(0xffffffffu, a.z, off));
+        b.x = fmaxf(b.x, __shfl_xor_sync(0xffffffffu, b.x, off));
+        b.y = fmaxf(b.y, __shfl_xor_sync(0xffffffffu, b.y, off));
+        b.z = fmaxf(b.z, __shfl_xor_sync(0xffffffffu, b.z, off));
+    }
+    if (lane == 0) {
+        const long long node = node_off[sw] + slots - 1 + leaf;
+        lo[node] = make_float4(a.x, a.y, a.z, 0.f);
+        hi[node] = make_float4(b.x, b.y, b.z, 0.f);
+    }
+}
+
+// k_tree_level over the batch: rows (node offset, first node, count, running count) of one level
+__global__ void k_batch_tree_level(const int4 *__restrict__ rows, int n_rows, int n_nodes, float4 *__restrict__ lo,
+                                   float4 *__restrict__ hi) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_nodes) return;
+    int r0 = 0, r1 = n_rows - 1;
+    while (r0 < r1) {
+        const int mid = (r0 + r1 + 1) >> 1;
+        if (rows[mid].w <= t) r0 = mid;
+        else r1 = mid - 1;
+    }
+    const int4 row = rows[r0];
+    const long long base = row.x;
+    const int node = row.y + (t - row.w);
+    const float4 l0 = lo[base + 2 * node + 1], l1 = lo[base + 2 * node + 2];
+    const float4 h0 = hi[base + 2 * node + 1], h1 = hi[base + 2 * node + 2];
+    lo[base + node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.f);
+    hi[base + node] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.f);
+}
+
+Status batch_geometry_alloc(BatchGeometry &g, const Model &m, int S, const int *n_p, int sort_bits) {
+    g.S = S;
+    g.h_part_prefix.assign(S + 1, 0);
+    g.h_leaf_prefix.assign(S + 1, 0);
+    g.h_node_off.assign(S + 1, 0);
+    g.leaf_slots.assign(S, 0);
+    for (int s = 0; s < S; ++s) {
+        const int leaves = (n_p[s] + kLeaf - 1) / kLeaf;
+        g.leaf_slots[s] = next_pow2(leaves < 1 ? 1 : leaves);
+        g.h_part_prefix[s + 1] = g.h_part_prefix[s] + n_p[s];
+        g.h_leaf_prefix[s + 1] = g.h_leaf_prefix[s] + g.leaf_slots[s];
+        g.h_node_off[s + 1] = g.h_node_off[s] + 2 * static_cast<long long>(g.leaf_slots[s]);
+    }
+    g.n_total = g.h_part_prefix[S];
+    if (g.n_total >= 0xffffffffLL || g.h_node_off[S] >= 0x7fffffffLL)
+        return Status{GD_ERR_INVALID_ARGUMENT, "batch too large for 32-bit site and node indices", 0};
+    g.n_sort = (g.n_total + kRadixTile - 1) / kRadixTile * kRadixTile;
+    const int key_bits = 21 * m.dim;
+    g.sbits = 0;
+    while ((1LL << g.sbits) < S) ++g.sbits;
+    if (g.sbits > 32) return Status{GD_ERR_INVALID_ARGUMENT, "too many swarms for the sort key", 0};
+    // by default the top Morton bits that fit beside the swarm id (the lists are exact for any key)
+    g.mbits = (sort_bits > 0 && sort_bits < key_bits) ? sort_bits : key_bits;
+    if (sort_bits == 0 && g.mbits + g.sbits > 64) g.mbits = 64 - g.sbits;
+    g.mshift = key_bits - g.mbits;
+    if (g.mbits + g.sbits > 64) return Status{GD_ERR_INVALID_ARGUMENT, "too many swarms for the sort key", 0};
+    const long long tiles = g.n_sort / kRadixTile;
+    const size_t hist_len = static_cast<size_t>(256) * tiles;
+    const size_t chunks = (hist_len + kScanChunk - 1) / kScanChunk;
+    const long long L = g.h_leaf_prefix[S];
+    GD_TRY_CUDA(g.site.alloc(g.n_total));
+    GD_TRY_CUDA(g.q.alloc(g.n_total));
+    GD_TRY_CUDA(g.active.alloc(g.n_total));
+    GD_TRY_CUDA(g.key_a.alloc(g.n_sort));
+    GD_TRY_CUDA(g.key_b.alloc(g.n_sort));
+    GD_TRY_CUDA(g.val_a.alloc(g.n_sort));
+    GD_TRY_CUDA(g.val_b.alloc(g.n_sort));
+    GD_TRY_CUDA(g.hist.alloc(hist_len + (chunks > 1 ? chunks : 0)));
+    GD_TRY_CUDA(g.sorted.alloc(static_cast<size_t>(L) * kLeaf));
+    GD_TRY_CUDA(g.node_lo.alloc(g.h_node_off[S]));
+    GD_TRY_CUDA(g.node_hi.alloc(g.h_node_off[S]));
+    GD_TRY_CUDA(g.sub_lo.alloc(static_cast<size_t>(L) * kSubs));
+    GD_TRY_CUDA(g.sub_hi.alloc(static_cast<size_t>(L) * kSubs));
+    GD_TRY_CUDA(g.counters.alloc(2 * static_cast<size_t>(S)));
+    GD_TRY_CUDA(g.part_prefix.alloc(S + 1));
+    GD_TRY_CUDA(g.leaf_prefix.alloc(S + 1));
+    GD_TRY_CUDA(g.node_off.alloc(S + 1));
+    GD_TRY_CUDA(cudaMemcpy(g.part_prefix.ptr, g.h_part_prefix.data(), sizeof(long long) * (S + 1),
+                           cudaMemcpyHostToDevice));
+    GD_TRY_CUDA(cudaMemcpy(g.leaf_prefix.ptr, g.h_leaf_prefix.data(), sizeof(long long) * (S + 1),
+                           cudaMemcpyHostToDevice));
+    GD_TRY_CUDA(cudaMemcpy(g.node_off.ptr, g.h_node_off.data(), sizeof(long long) * (S + 1), cudaMemcpyHostToDevice));
+    // tree level rows: level t covers the nodes t levels above each swarm's leaves
+    int depth_max = 0;
+    for (int s = 0; s < S; ++s) {
+        int d = 0;
+        while ((1 << d) < g.leaf_slots[s]) ++d;
+        depth_max = d > depth_max ? d : depth_max;
+    }
+    std::vector<int4> rows;
+    g.level_row0.assign(depth_max + 1, 0);
+    g.level_rows.assign(depth_max + 1, 0);
+    g.level_nodes.assign(depth_max + 1, 0);
+    for (int t = 1; t <= depth_max; ++t) {
+        g.level_row0[t] = static_cast<int>(rows.size());
+        int run = 0;
+        for (int s = 0; s < S; ++s) {
+            const int count = g.leaf_slots[s] >> t;
+            if (count < 1) continue;
+            rows.push_back(make_int4(static_cast<int>(g.h_node_off[s]), count - 1, count, run));
+            run += count;
+        }
+        g.level_rows[t] = static_cast<int>(rows.size()) - g.level_row0[t];
+        g.level_nodes[t] = run;
+    }
+    GD_TRY_CUDA(g.level_tab.alloc(rows.size()));
+    if (!rows.empty())
+        GD_TRY_CUDA(cudaMemcpy(g.level_tab.ptr, rows.data(), sizeof(int4) * rows.size(), cudaMemcpyHostToDevice));
+    return Status::ok();
+}
+
+Status batch_geometry_build(BatchGeometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
+    const int S = g.S;
+    g.launches += 2;
+    k_batch_counters_reset<<<(2 * S + 255) / 256, 256, 0, s>>>(S, g.counters.ptr);
+    k_batch_site_init<<<static_cast<unsigned int>((g.n_sort + 255) / 256), 256, 0, s>>>(
+        m, S, g.part_prefix.ptr, g.n_total, g.n_sort, dev_particle, g.site.ptr, g.q.ptr, g.active.ptr, g.key_a.ptr,
+        g.val_a.ptr, g.mbits, g.mshift, g.counters.ptr);
+    GD_TRY_CUDA(cudaGetLastError());
+    // one LSD radix sort over the swarm id and the kept Morton bits
+    const int tiles = static_cast<int>(g.n_sort / kRadixTile);
+    const int passes = (g.mbits + g.sbits + 7) / 8;
+    unsigned long long *kin = g.key_a.ptr, *kout = g.key_b.ptr;
+    unsigned int *vin = g.val_a.ptr, *vout = g.val_b.ptr;
+    const int hist_len = 256 * tiles;
+    const int chunks = (hist_len + kScanChunk - 1) / kScanChunk;
+    unsigned int *part = chunks > 1 ? g.hist.ptr + hist_len : nullptr;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        g.launches += part ? 4 : 3;
+        k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, shift, tiles, g.hist.ptr);
+        k_scan_chunks<<<chunks, kRadixThreads, 0, s>>>(g.hist.ptr, hist_len, part);
+        if (part) k_scan_parts<<<1, kRadixThreads, 0, s>>>(part, chunks);
+        k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, kout, vout, shift, tiles, g.hist.ptr, part);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    const long long L = g.h_leaf_prefix[S];
+    const long long slots = L * kLeaf;
+    g.launches += 2;
+    k_batch_gather<<<static_cast<unsigned int>((slots + 255) / 256), 256, 0, s>>>(
+        S, slots, g.leaf_prefix.ptr, g.part_prefix.ptr, g.counters.ptr, vin, g.site.ptr, g.sorted.ptr);
+    k_batch_leaf_bounds<<<static_cast<unsigned int>((L * 32 + 255) / 256), 256, 0, s>>>(
+        S, L, g.leaf_prefix.ptr, g.node_off.ptr, g.counters.ptr, g.sorted.ptr, g.node_lo.ptr, g.node_hi.ptr,
+        g.sub_lo.ptr, g.sub_hi.ptr);
+    for (size_t t = 1; t < g.level_rows.size(); ++t) {
+        if (g.level_nodes[t] == 0) continue;
+        g.launches += 1;
+        k_batch_tree_level<<<(g.level_nodes[t] + 255) / 256, 256, 0, s>>>(
+            g.level_tab.ptr + g.level_row0[t], g.level_rows[t], g.level_nodes[t], g.node_lo.ptr, g.node_hi.ptr);
+    }
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
+Status batch_geometry_check(BatchGeometry &g, cudaStream_t s, int *swarm) {
+    std::vector<int> c(2 * static_cast<size_t>(g.S));
+    GD_TRY_CUDA(cudaMemcpyAsync(c.data(), g.counters.ptr, sizeof(int) * c.size(), cudaMemcpyDeviceToHost, s));
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < g.S; ++k) {
+        if (c[2 * k + 1] != INT_MAX) {
+            if (swarm) *swarm = k;
+            Status st;
+            st.code = GD_ERR_NONFINITE;
+            st.detail = g.h_part_prefix[k] + c[2 * k + 1];
+            st.msg = "non-finite particle state before collision search at particle " + std::to_string(st.detail) +
+                     " (swarm " + std::to_string(k) + ")";
+            return st;
+        }
+    }
+    return Status::ok();
+}
+
 Status geometry_check(Geometry &g, cudaStream_t s) {
     int cnt[2];
     GD_TRY(read_counters(g, s, cnt));

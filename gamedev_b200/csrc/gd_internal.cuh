@@ -166,6 +166,38 @@ struct BatchSwarm {
     long long part_off;
     long long codes_off;
 };
+// The geometry of many swarms built together: one launch per stage for all of them.  Sites are
+// concatenated in swarm order (particle g of the batch is particle g - part_prefix[s] of swarm s);
+// one LSD radix sort orders (swarm id, top Morton bits) keys, so each swarm's sites come out
+// contiguous and Morton-ordered; per-swarm sorted tiles, trees and sub-boxes sit at the offsets
+// below, and the BatchSwarm table points into them.
+struct BatchGeometry {
+    int S = 0;
+    long long n_total = 0, n_sort = 0;
+    int mbits = 0, mshift = 0, sbits = 0;  // Morton bits kept, low Morton bits dropped, swarm id bits
+    DevBuf<float4> site;                   // [n_total], w = code bits of the swarm-local index
+    DevBuf<float> q;
+    DevBuf<unsigned char> active;
+    DevBuf<unsigned long long> key_a, key_b;
+    DevBuf<unsigned int> val_a, val_b, hist;
+    DevBuf<float4> sorted, node_lo, node_hi, sub_lo, sub_hi;
+    DevBuf<int> counters;                  // [2S]: active count, first non-finite local index
+    DevBuf<long long> part_prefix, leaf_prefix, node_off;  // [S+1] particles, leaf slots; [S] nodes
+    std::vector<long long> h_part_prefix, h_leaf_prefix, h_node_off;
+    std::vector<int> leaf_slots;           // per swarm, a power of two
+    // tree levels bottom-up: level t holds, for each swarm with at least t levels, the nodes t
+    // levels above its leaves as (node offset, first node, count, running count) rows; the rows of
+    // all levels are concatenated in level_tab, level t's starting at level_row0[t]
+    DevBuf<int4> level_tab;
+    std::vector<int> level_row0, level_rows, level_nodes;
+    long long launches = 0;
+};
+Status batch_geometry_alloc(BatchGeometry &g, const Model &m, int S, const int *n_p, int sort_bits);
+Status batch_geometry_build(BatchGeometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s);
+// The non-finite screen of the last build: GD_ERR_NONFINITE with the smallest bad index of the
+// first swarm that has one (as a batch index); synchronises the stream.
+Status batch_geometry_check(BatchGeometry &g, cudaStream_t s, int *swarm);
+
 // Top-K of every swarm of a batch in one persistent launch (plus the inactive rows): dev_tab[S],
 // dev_leaf_prefix[S + 1] (buckets of swarm s are items leaf_prefix[s] ..), dev_part_prefix[S + 1],
 // kcap = the largest K.  dev_next is a device counter the call resets.
