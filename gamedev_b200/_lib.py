@@ -111,6 +111,8 @@ SIGNATURES = {
     "gd_radius_model_predict": (C.c_int, [_P, _P, C.c_int, _P, _P]),
     "gd_radius_model_check": (C.c_int, [_P]),
     "gd_controller_summary": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "gd_set_diagnostics": (C.c_int, [_P, C.c_int]),
+    "gd_event_totals": (C.c_int, [_P, _P, _P]),
     "gd_frame_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
     "gd_particles_to_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),
     "gd_particles_from_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),

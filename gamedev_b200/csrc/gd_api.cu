@@ -513,6 +513,24 @@ gd_status gd_reset_controller(gd_handle *h) {
     return GD_OK;
 }
 
+gd_status gd_set_diagnostics(gd_handle *h, int on) {
+    if (!h || (on != 0 && on != 1)) return GD_ERR_INVALID_ARGUMENT;
+    h->col.diagnostics = on != 0;
+    return GD_OK;
+}
+
+gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_mass) {
+    if (!h || !counts || !log_mass) return GD_ERR_INVALID_ARGUMENT;
+    if (!h->col.diagnostics) return fail(h, GD_ERR_NOT_READY, "diagnostics are off (gd_set_diagnostics)");
+    if (cudaMemcpyAsync(counts, h->col.event_count.ptr, sizeof(unsigned long long) * gd::kEventCategories,
+                        cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(log_mass, h->col.event_log_mass.ptr, sizeof(double) * gd::kEventCategories,
+                        cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return fail(h, GD_ERR_CUDA, "copy of the event totals");
+    return GD_OK;
+}
+
 size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len) {
     if (!h) return 0;
     const std::string text = h->col.summary.json();

@@ -570,6 +570,8 @@ struct ChainRun {
     int *error_flag;
     int *head;
     unsigned long long *events_total;
+    unsigned long long *event_count;  // [7] per outcome category (COL_DIAGNOSTICS), or null
+    double *event_log_mass;           // [7]
 };
 
 // col_chain_run (col_chain_run.cu:21-404): persistent warps, one owner at a time
@@ -732,6 +734,13 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
             const bool high_speed = vrel >= m.v_frag;
             const double sample = high_speed ? col_uniform(&rng) : 0.0;
             const double size_new = sample_outcome(m, size_i, size_j, high_speed, sample);
+            if (r.event_count && lane == 0) {
+                int cat;
+                double lm;
+                outcome_category(m, size_i, size_j, high_speed, sample, size_new, cat, lm);
+                atomicAdd(&r.event_count[cat], 1ull);
+                atomicAdd(&r.event_log_mass[cat], lm);
+            }
             numr_i = mass_before / (size_new * size_new * size_new);
             size_i = size_new;
             time_i = event_time;
@@ -1559,6 +1568,8 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
     GD_TRY_CUDA(cudaMemset(c.error.ptr, 0, sizeof(int) * n));
     GD_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&c.host_small), L.total));
     c.state.assign(m.local_groups, BathState());
+    GD_TRY_CUDA(c.event_count.alloc(kEventCategories));
+    GD_TRY_CUDA(c.event_log_mass.alloc(kEventCategories));
     return Status::ok();
 }
 
@@ -1810,6 +1821,10 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
 
     c.summary.operator_count++;
     const int operator_index = c.summary.operator_count;
+    if (c.diagnostics) {
+        GD_TRY_CUDA(cudaMemsetAsync(c.event_count.ptr, 0, sizeof(unsigned long long) * kEventCategories, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.event_log_mass.ptr, 0, sizeof(double) * kEventCategories, s));
+    }
     int bath_index = 0;
     // tick zero: every group starts from the same published reservoir
     initialize(nullptr, n);
@@ -1889,6 +1904,8 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         cr.error_flag = at<int>(c.small, L.error_flag);
         cr.head = at<int>(c.small, L.head);
         cr.events_total = at<unsigned long long>(c.small, L.events);
+        cr.event_count = c.diagnostics ? c.event_count.ptr : nullptr;
+        cr.event_log_mass = c.diagnostics ? c.event_log_mass.ptr : nullptr;
         const int blocks = std::min(grid_chain, (count + kChainWarps - 1) / kChainWarps);
         ++c.launches;
         k_chain<<<blocks, kChainWarps * 32, chain_smem, s>>>(m, ca, cr);

@@ -42,6 +42,8 @@ struct BathResult {
 // kept by _record_col_bath (_col_bound.cuh:219-238) and written as save_col_controller writes them
 // (:242-299).  continuation_launches counts chain launches per wave; this build's chain is
 // persistent, so that is one per wave where the reference relaunches capped chains.
+constexpr int kEventCategories = 7;  // EVENT_CATEGORIES (inc/swarm/_col_types.cuh:32)
+
 struct BathRecord {
     int group_index = -1, operator_index = 0, bath_index = 0, merged_bins = 0, continuation_launches = 0;
     double duration = 0.0, limit_before = 1.0, limit_after = 1.0;
@@ -113,6 +115,11 @@ struct Collider {
     std::vector<unsigned int> edges;  // dependency rows, LOCAL_WORDS per group
     std::vector<BathState> state;
     ControllerSummary summary;        // reset with `state` at output boundaries
+    // COL_DIAGNOSTICS event bookkeeping of the last operator (when `diagnostics` is on): events
+    // and summed log mass change per outcome category (event_work, _col_types.cuh:32-33)
+    bool diagnostics = false;
+    DevBuf<unsigned long long> event_count;
+    DevBuf<double> event_log_mass;
     bool local_geometry_valid = false;
     gd_operator_stats stats{};
     long long launches = 0;           // kernels launched by the operator (reported by the ABI)

@@ -304,6 +304,35 @@ __device__ __forceinline__ double outcome_moments(const Model &m, double si, dou
     return 1.0;
 }
 
+// The COL_DIAGNOSTICS bookkeeping of one sampled outcome (_sample_erosion_outcome and
+// _record_event_work, inc/swarm/_col_event.cuh:9-13, :306-336): category 0..3 sticking with
+// q <= 1e-6, 1e-4, 1e-2 or above, 4 catastrophic fragmentation, 5 remnant erosion, 6 debris; and
+// the event's log mass change.  si is the owner's diameter before the event, size_new after it.
+__device__ __forceinline__ void outcome_category(const Model &m, double si, double sj, bool high_speed, double u,
+                                                 double size_new, int &category, double &log_mass) {
+    (void)m;
+    const double q = mass_ratio(si, sj);
+    const double G = sticking_packet(q);
+    if (!high_speed) {
+        category = q <= 1.0e-06 ? 0 : q <= 1.0e-04 ? 1 : q <= 1.0e-02 ? 2 : 3;
+        log_mass = log1p(G * q);
+        return;
+    }
+    if (q <= 0.1) {
+        const double factor = (1.0 - q) / G + q;
+        if (u < q / factor) {
+            category = 6;
+            log_mass = log(q);
+        } else {
+            category = 5;
+            log_mass = log1p(-G * q);
+        }
+        return;
+    }
+    category = 4;
+    log_mass = 3.0 * log(size_new / si);
+}
+
 // _sample_erosion_outcome (inc/swarm/_col_event.cuh:306-336): the new owner diameter
 __device__ __forceinline__ double sample_outcome(const Model &m, double si, double sj, bool high_speed, double u) {
     double q = mass_ratio(si, sj);

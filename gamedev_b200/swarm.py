@@ -158,6 +158,18 @@ class SwarmCollision:
     def reset_controller(self):
         self._check(self.lib.gd_reset_controller(self.h))
 
+    def set_diagnostics(self, on: bool = True):
+        """COL_DIAGNOSTICS event bookkeeping per operator (gd_set_diagnostics)."""
+        self._check(self.lib.gd_set_diagnostics(self.h, 1 if on else 0))
+
+    def event_totals(self):
+        """(counts [7] uint64, log_mass [7] float64) of the last operator's events per outcome
+        category (gd_event_totals)."""
+        counts = np.zeros(7, np.uint64)
+        log_mass = np.zeros(7, np.float64)
+        self._check(self.lib.gd_event_totals(self.h, C.c_void_p(counts.ctypes.data), C.c_void_p(log_mass.ctypes.data)))
+        return counts, log_mass
+
     def controller_summary(self) -> dict:
         """COL_DIAGNOSTICS controller summary of the current output interval (gd_controller_summary),
         parsed from the JSON the reference's save_col_controller writes."""

@@ -281,6 +281,14 @@ gd_status gd_reset_controller(gd_handle *h);
  * wave are 1 (the persistent chain) where the reference counts its relaunches. */
 size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len);
 
+/* COL_DIAGNOSTICS event bookkeeping (event_work / col_event_sum, inc/swarm/_col_event.cuh:9-13,
+ * _col_chain.cuh:519-535).  With diagnostics on (off by default), each collision operator counts
+ * its events and sums their log mass change per outcome category: 0..3 sticking with mass ratio
+ * q <= 1e-6, 1e-4, 1e-2 or above; 4 catastrophic fragmentation; 5 remnant erosion; 6 debris.
+ * gd_event_totals copies the last operator's 7 counts and 7 sums to host arrays (synchronous). */
+gd_status gd_set_diagnostics(gd_handle *h, int on);
+gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_mass);
+
 /* evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539): advance every owner through one
  * fixed-position frozen-bath collision operator of length `duration`, mutating par_size and
  * par_numr of dev_particle and the RNG states in dev_rng.  Uses the neighbour cache built by

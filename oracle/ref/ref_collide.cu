@@ -11,7 +11,9 @@
 //   out.bin: the n records after `operators` calls of evolve_collisions(duration) on one geometry
 //   stdout : one JSON line {"n", "operators", "geometry_ms", "operator_ms": [...], "total_ms"}
 //   summary.json (builds with COL_DIAGNOSTICS only): the controller summary of the operators as
-//            the reference's save_col_controller writes it (_col_bound.cuh:242-299)
+//            the reference's save_col_controller writes it (_col_bound.cuh:242-299); those builds
+//            also write their per-operator log, collision_local_<stamp>.jsonl, to the working
+//            directory
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -114,7 +116,8 @@ int main(int argc, char **argv) {
             image_dist_min = _get_image_dist_min(static_cast<float>(X_MIN), static_cast<float>(X_MAX),
                                                  static_cast<float>(Y_MIN), static_cast<float>(Z_MIN),
                                                  static_cast<float>(Z_MAX));
-        local_workspace local("/tmp/");
+        // the COL_DIAGNOSTICS build writes its per-operator log (collision_local_<stamp>.jsonl) here
+        local_workspace local("./");
         bool local_geometry_valid = false;
         real clock_dyn = 0.0, dt_col = 0.0;
         int count_col = 0;

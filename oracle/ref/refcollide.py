@@ -28,7 +28,8 @@ def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dus
         operators: int = 1, timeout: float = 1800, diagnostics: bool = False):
     """-> (particles after `operators` evolve_collisions(duration) calls on one geometry, info).
     With diagnostics (the COL_DIAGNOSTICS build), info["summary"] holds the controller summary the
-    reference's save_col_controller wrote, parsed, and info["summary_text"] its text."""
+    reference's save_col_controller wrote, parsed, info["summary_text"] its text, and
+    info["operator_log"] the parsed lines of its per-operator log."""
     p = np.ascontiguousarray(particles, dtype=np.float64).reshape(-1, 8)
     n = len(p)
     with tempfile.TemporaryDirectory() as d:
@@ -48,6 +49,9 @@ def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dus
         if diagnostics:
             info["summary_text"] = summary.read_text()
             info["summary"] = json.loads(info["summary_text"])
+            logs = sorted(Path(d).glob("collision_local_*.jsonl"))
+            info["operator_log"] = [json.loads(line) for f in logs for line in f.read_text().splitlines()
+                                    if line.strip()]
         raw = np.fromfile(dst, dtype=np.uint8)
         out = raw[4:].view(np.float64).reshape(n, 8).copy()
         return out, info

@@ -193,3 +193,39 @@ def test_morton_controller_summary_matches_reference(gd, cuda):
             # d_bath is a difference of audit sums: where it cancels, the residual is ~1e-17 in one
             # summation order and 0 in another
             assert math.isclose(a[key], b[key], rel_tol=1e-9, abs_tol=1e-12), (key, a, b)
+
+
+def test_morton_event_categories_match_reference(gd, cuda):
+    """COL_DIAGNOSTICS event bookkeeping: per operator, the events per outcome category and their
+    summed log mass change (gd_event_totals) equal the event_counts and event_log_mass_sums of the
+    reference's per-operator diagnostics log, on the Morton shapes where the event chains are the
+    same: counts exactly, log-mass sums to 1e-9 relative (summation order)."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    refcollide = _refc()
+    model = "c1_multisize_2d"
+    if not refcollide.available(model, N, diagnostics=True):
+        pytest.skip("oracle/_ref reference COL_DIAGNOSTICS build absent (reference tree not mounted at build time)")
+    cfg = workloads.config(model)
+    p = workloads.particles(model, n=N, seed=11)
+    d = _duration(gd, cfg, p, 2000.0)
+    sw = gd.SwarmCollision(cfg, N)
+    sw.set_diagnostics(True)
+    dp = gd.particles_to_device(p)
+    rng = gd.rngstate_init(N, seed=1)
+    ours = []
+    for _ in range(2):
+        sw.evolve_collisions(dp, rng, d, _mass(p))
+        torch.cuda.synchronize()
+        ours.append(sw.event_totals())
+    sw.close()
+    _, info = refcollide.run(model, p, 1, d, _mass(p), 2, timeout=600, diagnostics=True)
+    log = info["operator_log"]
+    assert len(log) == 2
+    for (counts, lm), line in zip(ours, log):
+        assert [int(c) for c in counts] == [int(c) for c in line["event_counts"]], (counts, line["event_counts"])
+        assert int(counts.sum()) > 1000
+        for a, b in zip(lm, line["event_log_mass_sums"]):
+            assert math.isclose(float(a), float(b), rel_tol=1e-9, abs_tol=1e-12), (lm, line["event_log_mass_sums"])
