@@ -88,6 +88,14 @@ class Clocks:
                  "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi takes a few hundred ms to start: wait (bounded) for its first row so that the
+        # samples cover the region that follows
+        t_end = time.monotonic() + 5.0
+        while time.monotonic() < t_end and self.proc.poll() is None:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -386,6 +394,9 @@ def run_ours(args):
         graph_body()
     graph_launches = sw.launch_count() - launches_g0 + 1  # + the radius model's MLP kernel
     graph_ev, graph_exact = [], 0
+    # clocks from the timed replays through one more window of at least 2 s of the same replays
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
     for s_ in range(args.warmup + args.steps):
         sw.drift_keplerian(dp, drift_dt)  # outside the timed region
         if s_ >= args.warmup:
@@ -406,13 +417,16 @@ def run_ours(args):
     knn_alone = []
     for _ in range(args.steps):
         knn_alone.append(_timed(stream, lambda: sw.col_cache_get_bounded(dp, radius, codes, measure, kth, None)))
-    # clocks over one more timed window of graph-replayed learned steps
-    clocks = Clocks(torch.cuda.current_device())
     barrier(world)
-    clocks.start()
-    for _ in range(args.steps):
+    t_end = time.monotonic() + 2.0
+    done = 0
+    while done < args.steps or time.monotonic() < t_end:
         sw.drift_keplerian(dp, drift_dt)
         graph.replay()
+        done += 1
+        if done % 8 == 0:
+            stream.synchronize()
+    stream.synchronize()
     barrier(world)
     clk = clocks.stop()
     sw.check_geometry()
@@ -646,10 +660,18 @@ def run_batched(args):
     for _ in range(args.warmup):
         graph.replay()
     barrier(world)
+    # clocks over the timed replays and at least 2 s of the same replays after them
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    t_end = time.monotonic() + 2.0
     torch.cuda.nvtx.range_push("c2_step")
     a, b = _timed(stream, lambda: [graph.replay() for _ in range(args.steps)])
     torch.cuda.nvtx.range_pop()
+    while time.monotonic() < t_end:
+        graph.replay()
+        stream.synchronize()
     barrier(world)
+    clk = clocks.stop()
     batch.check()
     b_ms = reduce_max(a.elapsed_time(b) / args.steps, world)
     # the same swarms one handle at a time (geometry + top-K per swarm, eager)
@@ -690,6 +712,7 @@ def run_batched(args):
         "one_handle_at_a_time": {"ms_per_step": solo_ms, "queries_per_s": queries / (solo_ms / 1e3)},
         "speedup_vs_one_at_a_time": solo_ms / b_ms,
         "bit_exact_swarms": f"{exact}/{len(sizes)}",
+        "clocks": clk,
     }
     if exact != len(sizes):
         line["error"] = "batched rows differ from the one-swarm results"
