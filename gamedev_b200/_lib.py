@@ -98,6 +98,9 @@ SIGNATURES = {
     "gd_autotune": (C.c_int, [_P, _P, _P, C.c_int, C.POINTER(GdTuning), C.POINTER(C.c_double)]),
     "gd_check_geometry": (C.c_int, [_P]),
     "gd_get_sites": (C.c_int, [_P, _P, _P, _P]),
+    "gd_site_count": (C.c_int, [_P]),
+    "gd_wedge_info": (C.c_int, [C.POINTER(GdConfig), C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                C.POINTER(C.c_float)]),
     "gd_knn_bounded": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "gd_drift_keplerian": (C.c_int, [_P, _P, C.c_double]),
     "gd_pair_rates": (C.c_int, [_P, _P, _P, C.c_int, C.c_double, _P]),

@@ -60,6 +60,18 @@ Model make_model(const gd_config &c) {
     m.dim = (c.n_z > 1) ? 3 : 2;
     m.local_groups = ((c.n_x > 1) ? c.col_bin_x : 1) * c.col_bin_y * ((c.n_z > 1) ? c.col_bin_z : 1);
     m.raw_bins = m.local_groups * c.col_bin_s;
+    // X_WEDGE (const_defs.cuh:56-57) and _get_image_dist_min (param_grid.cuh:86-89, evaluated on
+    // the host as swarm_runtime.cu:334-339 does)
+    const float fx_min = static_cast<float>(c.x_min), fx_max = static_cast<float>(c.x_max);
+    m.wedge = (c.n_x > 1 && fx_max - fx_min < 6.28318530717958647692f - 1.0e-06f) ? 1 : 0;
+    m.morton_images = (c.search == GD_SEARCH_MORTON) ? 1 : 0;
+    m.wedge_width = m.morton_images ? fx_max - fx_min : static_cast<float>(c.x_max - c.x_min);
+    m.image_dist_min = -1.0f;
+    if (m.wedge) {
+        const float y_min = static_cast<float>(c.y_min), z_min = static_cast<float>(c.z_min),
+                    z_max = static_cast<float>(c.z_max);
+        m.image_dist_min = 2.0f * y_min * fminf(sinf(z_min), sinf(z_max)) * fabsf(sinf(0.5f * (fx_max - fx_min)));
+    }
     return m;
 }
 
@@ -155,10 +167,6 @@ static std::string validate(const gd_config &c, int n) {
     if (c.coag_kernel < 0 || c.coag_kernel > 3) return "coag_kernel must be 0..3";
     if (c.col_bin_x < 1 || c.col_bin_y < 1 || c.col_bin_z < 1 || c.col_bin_s < 1) return "controller bins must be positive";
     if (c.search != GD_SEARCH_KDTREE && c.search != GD_SEARCH_MORTON) return "unknown search";
-    // a wedge (azimuth shorter than 2 pi) needs periodic images, which this build does not create
-    const bool wedge = c.n_x > 1 && static_cast<float>(c.x_max) - static_cast<float>(c.x_min) <
-                                        6.28318530717958647692f - 1.0e-06f;
-    if (wedge) return "azimuthal wedges (periodic images) are not supported";
     return std::string();
 }
 
@@ -461,12 +469,24 @@ gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned ch
     if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "geometry not built");
     cudaError_t e = cudaSuccess;
     if (dev_site4)
-        e = cudaMemcpyAsync(dev_site4, h->geo.site.ptr, sizeof(float4) * h->n, cudaMemcpyDeviceToDevice, h->stream);
+        e = cudaMemcpyAsync(dev_site4, h->geo.site.ptr, sizeof(float4) * h->geo.n_sites, cudaMemcpyDeviceToDevice,
+                            h->stream);
     if (e == cudaSuccess && dev_q)
         e = cudaMemcpyAsync(dev_q, h->geo.q.ptr, sizeof(float) * h->n, cudaMemcpyDeviceToDevice, h->stream);
     if (e == cudaSuccess && dev_active)
         e = cudaMemcpyAsync(dev_active, h->geo.active.ptr, h->n, cudaMemcpyDeviceToDevice, h->stream);
     if (e != cudaSuccess) return fail(h, gd::cuda_status(e, "copy sites"));
+    return GD_OK;
+}
+
+int gd_site_count(const gd_handle *h) { return h ? h->geo.n_sites : 0; }
+
+gd_status gd_wedge_info(const gd_config *cfg, int *wedge, float *width, float *image_dist_min) {
+    if (!cfg) return GD_ERR_INVALID_ARGUMENT;
+    const gd::Model m = gd::make_model(*cfg);
+    if (wedge) *wedge = m.wedge;
+    if (width) *width = m.wedge ? m.wedge_width : 0.0f;
+    if (image_dist_min) *image_dist_min = m.image_dist_min;
     return GD_OK;
 }
 
@@ -694,6 +714,7 @@ struct BorrowedGeometry {
     Geometry g;
     BorrowedGeometry(const Model &m, int n, unsigned char *base) {
         g.n = n;
+        g.n_sites = n;  // gd_knn_static rejects wedges
         g.n_sort = (n + kRadixTile - 1) / kRadixTile * kRadixTile;
         const int leaves = (n + kLeaf - 1) / kLeaf;
         int slots = 1;
@@ -770,6 +791,8 @@ extern "C" gd_status gd_knn_static(const gd_config *cfg, const gd_particle *dev_
         return gd::static_fail(st, detail, msg, msg_len);
     }
     std::string why = validate(*cfg, n_p);
+    if (why.empty() && gd::make_model(*cfg).wedge)
+        why = "azimuthal wedges (three sites per particle) need gd_create/gd_geometry_build/gd_knn";
     if (!why.empty()) {
         st.code = GD_ERR_INVALID_ARGUMENT;
         st.msg = "gd_knn_static: " + why;

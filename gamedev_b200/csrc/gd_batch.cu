@@ -68,6 +68,8 @@ gd_status gd_batch_create(const gd_config *cfg, int S, const int *n_p, const int
     b->S = S;
     b->n.assign(n_p, n_p + S);
     b->k.assign(n_k, n_k + S);
+    // the segmented geometry holds one site per particle: wedges (three) take the one-swarm path
+    if (gd::make_model(*cfg).wedge) return GD_ERR_INVALID_ARGUMENT;
     std::vector<int> leaf_prefix(S + 1, 0);
     std::vector<long long> part_prefix(S + 1, 0);
     for (int s = 0; s < S; ++s) {

@@ -27,17 +27,21 @@ namespace gd {
 
 // ------------------------------------------------------------------------------------------------
 // col_site_init (col_site_init.cu:17-55 / 78-118) fused with the Morton key generation
-// (morton_keygen, morton_index.cuh:41-60).  One thread per particle.
+// (morton_keygen, morton_index.cuh:41-60).  One thread per particle; threads past the sites write
+// the sort padding.  Site i is particle i; with a wedge, sites n + i and 2n + i are its images
+// rotated by -width (image 1) and +width (image 2), active when the particle is.
 // ------------------------------------------------------------------------------------------------
-__global__ void k_site_init(Model m, int n, const gd_particle *__restrict__ part,
+__global__ void k_site_init(Model m, int n, int n_sites, const gd_particle *__restrict__ part,
                             float4 *__restrict__ site, float *__restrict__ qrad,
                             unsigned char *__restrict__ active, unsigned long long *__restrict__ key,
                             unsigned int *__restrict__ val, int n_sort, int *__restrict__ counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_sort) return;
-    if (i >= n) {  // sort padding: sorts after every active site
-        key[i] = ~0ull;
-        val[i] = static_cast<unsigned int>(i);
+    if (i >= n) {
+        if (i >= n_sites) {  // sort padding: sorts after every active site
+            key[i] = ~0ull;
+            val[i] = static_cast<unsigned int>(i);
+        }
         return;
     }
     const double2 *rec = reinterpret_cast<const double2 *>(part + i);
@@ -72,9 +76,42 @@ __global__ void k_site_init(Model m, int n, const gd_particle *__restrict__ part
     active[i] = act ? 1 : 0;
     key[i] = k;
     val[i] = static_cast<unsigned int>(i);
+    if (m.wedge) {
+        // both rotated images, rounded as each search's reference kernel rounds them (KD:
+        // col_site_init.cu:58-76; Morton ghosts: morton_ghost.cuh:60-82).  Which product of each
+        // coordinate the reference's compiled code fuses was measured against its records, so the
+        // Morton forms are written out; the KD loop keeps the reference kernel's own expression.
+        float sin_width, cos_width;
+        sincosf(m.wedge_width, &sin_width, &cos_width);
+        float3 img[2];
+        if (!m.morton_images) {
+            for (int image = 0; image < 2; image++) {
+                float sin_angle = (image == 0) ? -sin_width : sin_width;
+                img[image] = make_float3(cos_width * s.x - sin_angle * s.y, sin_angle * s.x + cos_width * s.y, s.z);
+            }
+        } else {
+            // image 2 (+width): x' = cos x - sin y, y' = sin x + cos y
+            img[1] = make_float3(__fmaf_rn(cos_width, s.x, -__fmul_rn(sin_width, s.y)),
+                                 __fmaf_rn(sin_width, s.x, __fmul_rn(cos_width, s.y)), s.z);
+            // image 1 (-width): x' = cos x + sin y, y' = -sin x + cos y
+            img[0] = make_float3(__fmaf_rn(cos_width, s.x, __fmul_rn(sin_width, s.y)),
+                                 __fmaf_rn(cos_width, s.y, -__fmul_rn(sin_width, s.x)), s.z);
+        }
+#pragma unroll
+        for (int image = 0; image < 2; ++image) {
+            const int t = (image + 1) * n + i;
+            site[t] = make_float4(img[image].x, img[image].y, img[image].z, __int_as_float(3 * i + image + 1));
+            key[t] = act ? morton_key(m, img[image]) : ~0ull;
+            val[t] = static_cast<unsigned int>(t);
+        }
+        // the largest search radius, for the Morton search's one dedup decision
+        // (swarm_runtime.cu:413-415); q >= 0, so its bits order as the values do
+        if (act) atomicMax(&counters[2], __float_as_int(qi));
+    }
     // count active sites with one atomic per warp
     unsigned int ballot = __ballot_sync(__activemask(), act);
-    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot) atomicAdd(&counters[0], __popc(ballot));
+    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot)
+        atomicAdd(&counters[0], __popc(ballot) * (m.wedge ? 3 : 1));
 }
 
 // colstate_flag (colstate_flag.cu:13-29): non-finite screen when the geometry is reused.
@@ -366,8 +403,20 @@ struct LeafLoad {
     float4 sl[kSubs], sh[kSubs];
 };
 
+// The slot of this lane's entry for the same particle as code `code` among its first `len` entries,
+// or -1: the duplicate-image scan of idx_old_heap::processCandidate (kdtree/index_heap.cuh:118-131).
+__device__ __forceinline__ int same_particle(const unsigned long long *hp, int len, int code) {
+    const int base = code - code % 3;  // 3 * particle
+    for (int j = 0; j < len; ++j)
+        if (static_cast<unsigned int>(static_cast<int>(static_cast<unsigned int>(hp[j])) - base) < 3u) return j;
+    return -1;
+}
+
 // The exact top-K of the 32 owners of bucket (leaf) `leaf` of one swarm, by one warp.  `wbase` is
-// the warp's shared memory laid out for up to kcap neighbours (knn_warp_bytes(kcap)).
+// the warp's shared memory laid out for up to kcap neighbours (knn_warp_bytes(kcap)).  kImages: the
+// sites include wedge images, so only image-0 lanes are owners, and an owner whose search ball can
+// reach two images of one particle keeps only the nearer (the dedup of index_heap.cuh:118-136).
+template <bool kImages>
 __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, int leaf, unsigned char *wbase,
                                            int kcap) {
     const int lane = threadIdx.x & 31;
@@ -386,12 +435,20 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     if (leaf >= n_leaves) return;
 
     const int i = leaf * kLeaf + lane;
-    const bool valid = i < n_act;
     const float4 me = a.sorted[i];
     const float3 qp = make_float3(me.x, me.y, me.z);
     const int code = __float_as_int(me.w);
+    // with wedge images only the physical sites (image 0) query (_col_cache.cuh:22)
+    const bool valid = i < n_act && (!kImages || code % 3 == 0);
     const int idx = valid ? code / 3 : 0;
     const float qr = valid ? a.qrad[idx] : 0.f;
+    // dedup_needed = !unique_ids (_col_cache.cuh:38-39 per owner for KD; the largest q for Morton,
+    // swarm_runtime.cu:413-415)
+    bool dd = false;
+    if (kImages && valid) {
+        const float qd = m.morton_images ? __int_as_float(a.counters[2]) : qr;
+        dd = !(m.image_dist_min < 0.0f || m.image_dist_min > 2.0f * qd);
+    }
     // Reference acceptance: key < (q^2 bits, 0xffffffff), i.e. d^2 <= q^2 with the float q^2 the
     // reference heap is seeded with (kdtree/index_heap.cuh:58-61, morton_index.cuh:276).
     const float q2 = qr * qr;
@@ -448,8 +505,26 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
         // Fill phase: a lane with fewer than cap entries appends without ordering work.  A lane
         // that reaches cap stops and keeps the rest of its mask; the lanes that filled up in this
         // leaf then build their heaps together (in step, instead of one lane after another).
+        if constexpr (kImages) {
+            // one candidate per pass; a second image of a held particle replaces it when nearer
+            while (mask && cnt < cap) {
+                const int c = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const float4 p = tile[c];
+                const float d2 = dist2(qp, make_float3(p.x, p.y, p.z));
+                if (d2 <= cut) {
+                    ++st_offers;
+                    const int cc = __float_as_int(p.w);
+                    const unsigned long long key =
+                        (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned int>(cc);
+                    const int slot = dd ? same_particle(hp, cnt, cc) : -1;
+                    if (slot < 0) hp[cnt++] = key;
+                    else if (key < hp[slot]) hp[slot] = key;
+                }
+            }
+        }
         // two candidates per pass: half the divergent trips, two independent distance chains
-        while (mask && cnt < cap) {
+        while (!kImages && mask && cnt < cap) {
             const int c0 = __ffs(mask) - 1;
             mask &= mask - 1;
             const bool two = mask && cnt + 1 < cap;
@@ -479,7 +554,8 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 built = true;
             }
         }
-        // heap phase: a candidate below the heap's largest key replaces it
+        // heap phase: a candidate below the heap's largest key replaces it (with images: a nearer
+        // image of a held particle replaces that particle's entry instead, index_heap.cuh:133-141)
         while (mask) {
             const int c = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -489,7 +565,13 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
                 ++st_offers;
                 const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
                                                static_cast<unsigned int>(__float_as_int(p.w));
-                if (key < hp[0]) {
+                const int slot = (kImages && dd) ? same_particle(hp, cap, __float_as_int(p.w)) : -1;
+                if (slot >= 0) {
+                    if (key < hp[slot]) {
+                        heap_sift(hp, key, slot, cap);
+                        cut = key_d2(hp[0]);
+                    }
+                } else if (key < hp[0]) {
                     heap_sift(hp, key, 0, cap);
                     cut = key_d2(hp[0]);
                 }
@@ -770,11 +852,12 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     }
 }
 
+template <bool kImages>
 __global__ void k_knn_query(Model m, QueryArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int wib = threadIdx.x >> 5;
     const int kcap = knn_capacity(a.k, a.radius != nullptr);
-    knn_bucket(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(kcap), kcap);
+    knn_bucket<kImages>(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(kcap), kcap);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -822,7 +905,7 @@ __global__ void k_knn_batch(Model m, const BatchSwarm *__restrict__ tab, const i
         a.stats = nullptr;
         a.prescan = prescan;
         a.bfs = bfs;
-        knn_bucket(m, a, item - leaf_prefix[lo], wbase, kcap);
+        knn_bucket<false>(m, a, item - leaf_prefix[lo], wbase, kcap);
         __syncwarp();
     }
 }
@@ -935,12 +1018,13 @@ static int next_pow2(int v) {
 
 Status geometry_alloc(Geometry &g, const Model &m, int n) {
     g.n = n;
-    g.n_sort = (n + kRadixTile - 1) / kRadixTile * kRadixTile;
-    int leaves = (n + kLeaf - 1) / kLeaf;
+    g.n_sites = m.wedge ? 3 * n : n;
+    g.n_sort = (g.n_sites + kRadixTile - 1) / kRadixTile * kRadixTile;
+    int leaves = (g.n_sites + kLeaf - 1) / kLeaf;
     g.leaf_slots = next_pow2(leaves < 1 ? 1 : leaves);
     g.key_bits = 21 * m.dim;
     int tiles = g.n_sort / kRadixTile;
-    GD_TRY_CUDA(g.site.alloc(n));
+    GD_TRY_CUDA(g.site.alloc(g.n_sites));
     GD_TRY_CUDA(g.q.alloc(n));
     GD_TRY_CUDA(g.active.alloc(n));
     GD_TRY_CUDA(g.key_a.alloc(g.n_sort));
@@ -975,8 +1059,9 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
     const int n = g.n;
     g.launches += 2;
     k_counters_reset<<<1, 32, 0, s>>>(g.counters.ptr);
-    k_site_init<<<(g.n_sort + 255) / 256, 256, 0, s>>>(m, n, dev_particle, g.site.ptr, g.q.ptr, g.active.ptr,
-                                                        g.key_a.ptr, g.val_a.ptr, g.n_sort, g.counters.ptr);
+    k_site_init<<<(g.n_sort + 255) / 256, 256, 0, s>>>(m, n, g.n_sites, dev_particle, g.site.ptr, g.q.ptr,
+                                                        g.active.ptr, g.key_a.ptr, g.val_a.ptr, g.n_sort,
+                                                        g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
     // the reference stops on the first non-finite particle before building (swarm_runtime.cu:382-393);
     // a deferred screen is read by geometry_check instead (non-finite particles are inactive and
@@ -1365,13 +1450,14 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     const size_t smem = per_warp * warps;
     // raise the kernel's shared-memory limit only when a larger one is needed, so that a step
     // enqueued under stream capture after a first eager call makes no attribute call
-    static int smem_set[64] = {};
+    static int smem_set[2][64] = {};
     int dev = 0;
     GD_TRY_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64 || smem_set[dev] < static_cast<int>(smem)) {
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_query, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
-        if (dev >= 0 && dev < 64) smem_set[dev] = static_cast<int>(smem);
+    const int wi = m.wedge ? 1 : 0;
+    if (dev < 0 || dev >= 64 || smem_set[wi][dev] < static_cast<int>(smem)) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(m.wedge ? k_knn_query<true> : k_knn_query<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        if (dev >= 0 && dev < 64) smem_set[wi][dev] = static_cast<int>(smem);
     }
     QueryArgs qa;
     qa.sorted = g.sorted.ptr;
@@ -1391,10 +1477,11 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     qa.stats = stats;
     qa.prescan = tune.prescan;
     qa.bfs = tune.bfs;
-    const int max_leaves = (g.n + kLeaf - 1) / kLeaf;
+    const int max_leaves = (g.n_sites + kLeaf - 1) / kLeaf;
     const int blocks = (max_leaves + warps - 1) / warps;
     g.launches += 2;
-    k_knn_query<<<blocks, warps * 32, smem, s>>>(m, qa);
+    if (m.wedge) k_knn_query<true><<<blocks, warps * 32, smem, s>>>(m, qa);
+    else k_knn_query<false><<<blocks, warps * 32, smem, s>>>(m, qa);
     k_inactive_rows<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, K, g.active.ptr, codes, measure, kth_d2);
     GD_TRY_CUDA(cudaGetLastError());
     return Status::ok();

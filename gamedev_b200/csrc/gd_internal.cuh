@@ -55,6 +55,13 @@ struct Model {
     int dim;          // 2 when the polar direction is collapsed, else 3
     int local_groups; // spatial controller groups (_col_types.cuh:463)
     int raw_bins;     // local_groups * col_bin_s (_col_bound.cuh:223-229)
+    // Azimuthal wedge: X_WEDGE (const_defs.cuh:56-57), n_x > 1 and an azimuth shorter than 2 pi.
+    // Every particle then has two more sites, rotated by -width (image 1) and +width (image 2).
+    int wedge;
+    int morton_images;     // 1: the Morton search's rotation, width and dedup decision; 0: KD's
+    float wedge_width;     // KD: float(x_max - x_min) (col_site_init.cu:60);
+                           // Morton: float(x_max) - float(x_min) (morton_ghost.cuh:62)
+    float image_dist_min;  // _get_image_dist_min (param_grid.cuh:86-89); -1 without a wedge
 };
 
 Model make_model(const gd_config &c);
@@ -107,10 +114,11 @@ struct DevBuf {
 // Geometry (index) state of one swarm.
 struct Geometry {
     int n = 0;              // particles
-    int n_sort = 0;         // n rounded up to the sort tile
+    int n_sites = 0;        // sites: n, or 3n with wedge images (site n*image + i)
+    int n_sort = 0;         // n_sites rounded up to the sort tile
     int leaf_slots = 0;     // power of two >= ceil(n / kLeaf)
     int key_bits = 0;       // Morton bits sorted (3*21 or 2*21)
-    DevBuf<float4> site;    // by particle index
+    DevBuf<float4> site;    // by site index
     DevBuf<float> q;        // search radius by particle index
     DevBuf<unsigned char> active;
     DevBuf<unsigned long long> key_a, key_b;
@@ -119,7 +127,8 @@ struct Geometry {
     DevBuf<float4> sorted;        // [leaf_slots*kLeaf] Morton-ordered sites, w = code bits
     DevBuf<float4> node_lo, node_hi;  // implicit tree, 2*leaf_slots-1 nodes
     DevBuf<float4> sub_lo, sub_hi;    // four 8-site sub-boxes per leaf, [leaf_slots*4]
-    DevBuf<int> counters;         // [0] active count, [1] first bad index (INT_MAX if none)
+    DevBuf<int> counters;         // [0] active sites, [1] first bad index (INT_MAX if none),
+                                  // [2] bits of the largest q (wedges only)
     unsigned int *sorted_val = nullptr;  // points into val_a or val_b after the sort
     unsigned long long *sorted_key = nullptr;  // points into key_a or key_b after the sort
     long long launches = 0;              // kernels launched by this geometry (reported by the ABI)

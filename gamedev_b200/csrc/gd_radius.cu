@@ -109,10 +109,12 @@ __global__ void k_features(Model m, int slots, const int *__restrict__ counters,
     if (i >= slots) return;  // whole warps: slots is a multiple of 32
     const int n_act = counters[0];
     const bool valid = i < n_act;
-    int idx = 0;
+    int idx = 0, image = 0;
     double w = 0.0, y = 0.0, z = 0.0, size = 1.0;
     if (valid) {
-        idx = __float_as_int(sorted[i].w) / 3;
+        const int code = __float_as_int(sorted[i].w);
+        idx = code / 3;
+        image = code % 3;
         y = part[idx].position[1];
         z = part[idx].position[2];
         size = part[idx].par_size;
@@ -125,7 +127,7 @@ __global__ void k_features(Model m, int slots, const int *__restrict__ counters,
         wsum += __shfl_xor_sync(0xffffffffu, wsum, off);
         cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
     }
-    if (!valid) return;
+    if (!valid || image != 0) return;  // a wedge image's particle row is written by its own site
     float f[kF];
 #pragma unroll
     for (int l = 0; l < 3; ++l) {

@@ -133,10 +133,11 @@ class SwarmCollision:
         self.col_cache_get(particles)
 
     def get_sites(self):
-        """Site-init outputs of the last geometry build: (site4 float32 [n,4], q [n], active [n])."""
+        """Site-init outputs of the last geometry build: (site4 float32 [sites,4], q [n], active [n]);
+        sites = n, or 3n for an azimuthal wedge (images n..2n-1 at -width, 2n..3n-1 at +width)."""
         torch = _torch()
         dev = torch.device("cuda", torch.cuda.current_device())
-        site4 = torch.empty((self.n_p, 4), dtype=torch.float32, device=dev)
+        site4 = torch.empty((self.lib.gd_site_count(self.h), 4), dtype=torch.float32, device=dev)
         q = torch.empty(self.n_p, dtype=torch.float32, device=dev)
         active = torch.empty(self.n_p, dtype=torch.uint8, device=dev)
         self._check(self.lib.gd_get_sites(self.h, C.c_void_p(site4.data_ptr()), C.c_void_p(q.data_ptr()),
@@ -321,6 +322,16 @@ class RadiusModel:
 
 def rng_state_bytes() -> int:
     return int(_lib.load().gd_rng_state_bytes())
+
+
+def wedge_info(cfg):
+    """(wedge, width, image_dist_min) the search uses for cfg (gd_wedge_info): X_WEDGE, the images'
+    rotation angle and _get_image_dist_min (-1 without a wedge)."""
+    w, width, idm = C.c_int(), C.c_float(), C.c_float()
+    r = _lib.load().gd_wedge_info(C.byref(cfg), C.byref(w), C.byref(width), C.byref(idm))
+    if r != _lib.GD_OK:
+        raise GdError(r, "gd_wedge_info failed", 0)
+    return bool(w.value), float(width.value), float(idm.value)
 
 
 def rngstate_init(n: int, seed: int = 1, device="cuda:0"):

@@ -19,6 +19,10 @@ Config names:
   c3_learned_3d    3D, N = 10^7, K = 64, c0 positions, radii log-uniform on [1e-4, 10] cm
   c4_production_3d as c3 (its collision operator; transport, diffusion and radiation are not in
                    this build)
+  w0_wedge_3d      3D wedge (azimuth [-0.6, 0.6)), N = 65,536, K = 32, KD search, with periodic
+                   images
+  w1_narrow_2d     radial-azimuthal 0.05 rad wedge, N = 65,536, K = 32, Morton search, with periodic
+                   images
 """
 
 from __future__ import annotations
@@ -79,6 +83,13 @@ CONFIGS = {
                           sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=3),
     "c4_production_3d": dict(n=10_000_000, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
                              sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=4),
+    # azimuthal wedges (periodic images): a 1.2 rad wedge searched by the KD tree, whose owners
+    # beyond ~4 au can reach two images of one particle, and a 0.05 rad sliver searched by the
+    # Morton index, where every owner can
+    "w0_wedge_3d": dict(n=65536, k=32, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                        sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=7, x_range=(-0.6, 0.6)),
+    "w1_narrow_2d": dict(n=65536, k=32, three_d=False, search=GD_SEARCH_MORTON, v_frag=100.0,
+                         sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=8, x_range=(0.0, 0.05)),
 }
 
 
@@ -88,6 +99,8 @@ def config(name: str, n: int | None = None, k: int | None = None):
     smin = sizes[1]
     smax = sizes[1] if sizes[0] == "mono" else sizes[2]
     cfg = _base_config(k or spec["k"], spec["three_d"], spec["search"], spec["v_frag"], smin, smax)
+    if "x_range" in spec:
+        cfg.x_min, cfg.x_max = spec["x_range"]
     return cfg
 
 
@@ -110,7 +123,8 @@ def particles(name: str, n: int | None = None, seed: int | None = None) -> np.nd
     spec = CONFIGS[name]
     n = int(n or spec["n"])
     rng = np.random.Generator(np.random.PCG64(spec["seed"] if seed is None else seed))
-    phi = rng.uniform(0.0, 2.0 * math.pi, n)
+    x_lo, x_hi = spec.get("x_range", (-math.pi, math.pi))
+    phi = rng.uniform(0.0, x_hi - x_lo, n)
     r_au = _radius_samples(rng, n, spec["radial"])
     if spec["three_d"]:
         h = 0.05 * r_au ** 0.25
@@ -127,7 +141,7 @@ def particles(name: str, n: int | None = None, seed: int | None = None) -> np.nd
     y = r_au * AU
     R = y * np.sin(theta)
     out = np.empty((n, 8), np.float64)
-    out[:, 0] = phi - math.pi  # azimuth in [-pi, pi)
+    out[:, 0] = phi + x_lo  # azimuth in [x_min, x_max)
     out[:, 1] = y
     out[:, 2] = theta
     out[:, 3] = np.sqrt(G_CGS * MSUN * R)  # Keplerian l_phi

@@ -251,10 +251,25 @@ gd_status gd_radius_model_get(const gd_radius_model *m, float *params, float *no
 gd_status gd_radius_model_set(gd_radius_model *m, const float *params, const float *norm17);
 
 /* Copy the site-init outputs of the last gd_geometry_build to caller device buffers (any may be
- * NULL): sites [n_p] x (x, y, z, code bits) as float4, search radius q [n_p] (0 when inactive),
- * active flags [n_p] (the reference's dev_kdtree_node cartesian / dev_search_dist /
- * dev_col_active, col_site_init.cu:44-55, 106-117). */
+ * NULL): sites [gd_site_count(h)] x (x, y, z, code bits) as float4, search radius q [n_p] (0 when
+ * inactive), active flags [n_p] (the reference's dev_kdtree_node cartesian / dev_search_dist /
+ * dev_col_active, col_site_init.cu:44-76, 106-117).  Sites 0..n_p-1 are the particles; with an
+ * azimuthal wedge, sites n_p + i and 2 n_p + i are particle i's periodic images rotated by -width
+ * (code 3i + 1) and +width (code 3i + 2), as the reference's N_T = 3 N_P tree nodes are. */
 gd_status gd_get_sites(gd_handle *h, float *dev_site4, float *dev_q, unsigned char *dev_active);
+
+/* Sites of the handle's geometry: n_p, or 3 n_p for an azimuthal wedge (N_T, const_defs.cuh:240). */
+int gd_site_count(const gd_handle *h);
+
+/* The periodic-image parameters the search uses for cfg (no device work): *wedge = X_WEDGE
+ * (n_x > 1 and float(x_max) - float(x_min) < 2 pi - 1e-6, const_defs.cuh:56-57); *width = the
+ * rotation angle of the images (KD: float(x_max - x_min), col_site_init.cu:60; Morton:
+ * float(x_max) - float(x_min), morton_ghost.cuh:62), 0 without a wedge; *image_dist_min =
+ * _get_image_dist_min (param_grid.cuh:86-89), -1 without a wedge.  An owner keeps one image per
+ * particle (the nearer) when image_dist_min <= 2 q, with q its own search distance for the KD
+ * search (_col_cache.cuh:38-39) and the largest one for the Morton search (swarm_runtime.cu:413-415).
+ * Any output may be NULL. */
+gd_status gd_wedge_info(const gd_config *cfg, int *wedge, float *width, float *image_dist_min);
 
 /* Copy the handle's neighbour cache (codes, measures) to caller device buffers. */
 gd_status gd_get_cache(gd_handle *h, int32_t *dev_codes, double *dev_measure);

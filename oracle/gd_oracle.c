@@ -184,6 +184,70 @@ void gdo_knn_brute(int n, const float *site4, const float *q, const unsigned cha
     }
 }
 
+/* replace slot `slot` by the smaller cand and sift it down (index_heap.cuh:133-174) */
+static void heap_replace_at(uint64_t *h, int K, int slot, uint64_t cand) {
+    for (;;) {
+        int child = 2 * slot + 1;
+        if (child >= K) break;
+        uint64_t cv = h[child];
+        if (child + 1 < K && h[child + 1] > cv) {
+            cv = h[child + 1];
+            ++child;
+        }
+        if (cv < cand) break;
+        h[slot] = cv;
+        slot = child;
+    }
+    h[slot] = cand;
+}
+
+void gdo_knn_brute_images(int n, int n_sites, const float *site4, const float *q, const unsigned char *active,
+                          int K, float image_dist_min, float q_dedup, int32_t *codes, float *d2, int threads) {
+#pragma omp parallel num_threads(threads > 0 ? threads : 1)
+    {
+        uint64_t *h = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)K);
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < n; ++i) {
+            int32_t *crow = codes + (size_t)i * K;
+            float *drow = d2 ? d2 + (size_t)i * K : NULL;
+            if (!active[i]) {
+                empty_row(K, crow, drow);
+                continue;
+            }
+            /* unique_ids (_col_cache.cuh:38-39; swarm_runtime.cu:413-415 with q_dedup = max q) */
+            const float qd = q_dedup >= 0.f ? q_dedup : q[i];
+            const int dedup = !(image_dist_min < 0.f || image_dist_min > 2.0f * qd);
+            heap_init(h, K, q[i]);
+            const float *qp = site4 + 4 * (size_t)i;
+            for (int j = 0; j < n_sites; ++j) {
+                const uint32_t code = site_code(site4 + 4 * (size_t)j);
+                const uint32_t idx_old = code / 3u;
+                if (!active[idx_old]) continue;
+                const uint64_t cand = make_key(gdo_dist2(qp, site4 + 4 * (size_t)j), code);
+                /* processCandidate (index_heap.cuh:112-176) */
+                int slot = -1;
+                if (dedup)
+                    for (int s = 0; s < K; ++s) {
+                        const uint32_t old = (uint32_t)h[s];
+                        if (old == 0xffffffffu || old / 3u != idx_old) continue;
+                        slot = s;
+                        break;
+                    }
+                if (slot >= 0) {
+                    if (cand >= h[slot]) continue;
+                } else {
+                    if (cand >= h[0]) continue;
+                    slot = 0;
+                }
+                heap_replace_at(h, K, slot, cand);
+            }
+            qsort(h, (size_t)K, sizeof(uint64_t), cmp_u64);
+            write_row(h, K, crow, drow);
+        }
+        free(h);
+    }
+}
+
 /* ---- KD tree: widest-dimension median splits over active sites ----------------------------- */
 typedef struct {
     float lo[3], hi[3];

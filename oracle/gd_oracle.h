@@ -37,6 +37,15 @@ void gdo_knn_brute(int n, const float *site4, const float *q, const unsigned cha
 void gdo_knn_kdtree(int n, const float *site4, const float *q, const unsigned char *active, int K, int32_t *codes,
                     float *d2, int threads, int first, int count);
 
+/* The same top-K over sites that include azimuthal-wedge images (col_site_init.cu:58-76): owners
+ * are sites 0..n-1 (image 0); every one of the n_sites sites (code = 3 * particle + image) is a
+ * candidate, active when its particle is.  An owner with image_dist_min <= 2 q keeps one image per
+ * particle, the one with the smaller key (the dedup of kdtree/index_heap.cuh:118-141); q is the
+ * owner's own q_i (KD search, _col_cache.cuh:38-39) or q_dedup >= 0 (Morton search: the largest
+ * q, swarm_runtime.cu:413-415).  image_dist_min < 0: no dedup. */
+void gdo_knn_brute_images(int n, int n_sites, const float *site4, const float *q, const unsigned char *active,
+                          int K, float image_dist_min, float q_dedup, int32_t *codes, float *d2, int threads);
+
 /* The pinned single-precision squared distance. */
 float gdo_dist2(const float *a, const float *b);
 

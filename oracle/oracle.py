@@ -38,6 +38,9 @@ def load():
         lib.gdo_site_init.argtypes = [P, P, C.c_int, P, P, P]
         lib.gdo_knn_brute.restype = None
         lib.gdo_knn_brute.argtypes = [C.c_int, P, P, P, C.c_int, P, P, C.c_int]
+        lib.gdo_knn_brute_images.restype = None
+        lib.gdo_knn_brute_images.argtypes = [C.c_int, C.c_int, P, P, P, C.c_int, C.c_float, C.c_float, P, P,
+                                             C.c_int]
         lib.gdo_knn_kdtree.restype = None
         lib.gdo_knn_kdtree.argtypes = [C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_int]
         lib.gdo_kdtree_build.restype = P
@@ -107,6 +110,20 @@ def knn_brute(site4, q, active, k: int, threads: int | None = None):
     codes = np.empty((n, k), np.int32)
     d2 = np.empty((n, k), np.float32)
     load().gdo_knn_brute(n, _p(site4), _p(q), _p(active), k, _p(codes), _p(d2), threads or os.cpu_count())
+    return codes, d2
+
+
+def knn_brute_images(site4, n: int, q, active, k: int, image_dist_min: float, q_dedup: float = -1.0,
+                     threads: int | None = None):
+    """Top-K of owners 0..n-1 over every site of `site4` (wedge images included), with the duplicate
+    image dedup of the reference heap (gdo_knn_brute_images)."""
+    site4 = np.ascontiguousarray(site4, np.float32)
+    q = np.ascontiguousarray(q, np.float32)
+    active = np.ascontiguousarray(active, np.uint8)
+    codes = np.empty((n, k), np.int32)
+    d2 = np.empty((n, k), np.float32)
+    load().gdo_knn_brute_images(n, site4.shape[0], _p(site4), _p(q), _p(active), k, float(image_dist_min),
+                                float(q_dedup), _p(codes), _p(d2), threads or os.cpu_count())
     return codes, d2
 
 

@@ -10,12 +10,17 @@
 //   in.bin : int32 n (= N_P), then n particle records (the 64 B struct swarm)
 //   out.bin: the n records after `operators` calls of evolve_collisions(duration) on one geometry
 //   stdout : one JSON line {"n", "operators", "geometry_ms", "operator_ms": [...], "total_ms"}
+//   GD_REF_SITES=<file> (environment): also writes the search's records (KD nodes, or the Morton
+//            index's points and periodic ghosts), int32 count, count x (float32 x, y, z, int32 code)
+//   GD_REF_NEIGHBOURS=<file> (environment): also writes the neighbour cache of the geometry,
+//            int32 n, int32 K, int32 codes[n][K] (col_cache_get's order), float64 measure[n]
 //   summary.json (builds with COL_DIAGNOSTICS only): the controller summary of the operators as
 //            the reference's save_col_controller writes it (_col_bound.cuh:242-299); those builds
 //            also write their per-operator log, collision_local_<stamp>.jsonl, to the working
 //            directory
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <stdexcept>
 #include <string>
@@ -169,6 +174,52 @@ int main(int argc, char **argv) {
         check(gpuEventRecord(b, 0), "record");
         check(gpuEventSynchronize(b), "geometry");
         check(gpuEventElapsedTime(&geometry_ms, a, b), "elapsed");
+        // the search's records (KD tree nodes, or the Morton index's points with its periodic ghosts),
+        // when GD_REF_SITES names a file: int32 count, then count x (float x, y, z, int32 code)
+        if (const char *path = std::getenv("GD_REF_SITES")) {
+            std::vector<float> rec;
+#ifdef COLLISION_KDTREE
+            std::vector<kdtree_node> node(N_T);
+            check(gpuMemcpy(node.data(), dev_kdtree_node, sizeof(kdtree_node) * N_T, gpuMemcpyDeviceToHost),
+                  "copy kd nodes");
+            for (const kdtree_node &t : node) {
+                const int code = _encode_col_neighbor(t.idx_old, t.image);
+                float c;
+                std::memcpy(&c, &code, 4);
+                rec.insert(rec.end(), {t.cartesian.x, t.cartesian.y, t.cartesian.z, c});
+            }
+#else
+            const morton_view view = morton_owner.view();
+            std::vector<morton_point> pts(view.point_count);
+            check(gpuMemcpy(pts.data(), view.dev_point, sizeof(morton_point) * pts.size(), gpuMemcpyDeviceToHost),
+                  "copy Morton points");
+            for (const morton_point &t : pts) {
+                float c;
+                std::memcpy(&c, &t.idx_old, 4);
+                rec.insert(rec.end(), {t.cartesian.x, t.cartesian.y, t.cartesian.z, c});
+            }
+#endif
+            std::ofstream sf(path, std::ios::binary);
+            const int count = static_cast<int>(rec.size() / 4);
+            sf.write(reinterpret_cast<const char *>(&count), 4);
+            sf.write(reinterpret_cast<const char *>(rec.data()), sizeof(float) * rec.size());
+            if (!sf) throw std::runtime_error("cannot write the search records");
+        }
+        // the neighbour cache col_cache_get wrote, when GD_REF_NEIGHBOURS names a file
+        if (const char *path = std::getenv("GD_REF_NEIGHBOURS")) {
+            std::vector<int> codes(static_cast<std::size_t>(N_P) * N_K);
+            std::vector<real> measure(N_P);
+            check(gpuMemcpy(codes.data(), dev_col_neighbor, sizeof(int) * codes.size(), gpuMemcpyDeviceToHost),
+                  "copy neighbours");
+            check(gpuMemcpy(measure.data(), dev_col_measure, sizeof(real) * N_P, gpuMemcpyDeviceToHost),
+                  "copy measures");
+            std::ofstream nb(path, std::ios::binary);
+            const int header[2] = {N_P, N_K};
+            nb.write(reinterpret_cast<const char *>(header), sizeof(header));
+            nb.write(reinterpret_cast<const char *>(codes.data()), sizeof(int) * codes.size());
+            nb.write(reinterpret_cast<const char *>(measure.data()), sizeof(real) * measure.size());
+            if (!nb) throw std::runtime_error("cannot write the neighbour cache");
+        }
 
         for (int op = 0; op < operators; ++op) {
             check(gpuEventRecord(a, 0), "record");

@@ -66,7 +66,6 @@ def test_rng_state_is_curand_xorwow_size(gd):
         ({"n_k": 0}, 100),
         ({"n_k": 257}, 100),
         ({"coag_kernel": 4}, 100),
-        ({"x_min": -0.1, "x_max": 0.1}, 100),  # wedge: periodic images unsupported
         ({}, 800_000_000),  # 3*N overflows int32 neighbour codes
     ],
 )
@@ -77,6 +76,20 @@ def test_create_rejects_invalid_models_without_a_device(gd, overrides, n):
     h = C.c_void_p()
     st = gd.load().gd_create(C.byref(cfg), n, C.byref(h))
     assert st == 1 and not h.value  # GD_ERR_INVALID_ARGUMENT, no handle
+
+
+def test_wedges_are_rejected_by_the_one_site_per_particle_paths(gd):
+    """A wedge (n_x > 1, azimuth shorter than 2 pi) has three sites per particle: the batch and the
+    fixed-scratch search refuse it before any device work; gd_create accepts it."""
+    lib = gd.load()
+    cfg = gd.default_config(n_x=64, x_min=-0.1, x_max=0.1)
+    b = C.c_void_p()
+    n_p, n_k = (C.c_int * 1)(1024), (C.c_int * 1)(16)
+    assert lib.gd_batch_create(C.byref(cfg), 1, n_p, n_k, C.byref(b)) == 1 and not b.value
+    msg = C.create_string_buffer(256)
+    fake = C.c_void_p(256)  # never dereferenced: the call returns before any device work
+    st = lib.gd_knn_static(C.byref(cfg), fake, 1024, fake, fake, fake, None, None, msg, 256)
+    assert st == 1 and b"wedge" in msg.value
 
 
 def test_null_arguments_are_rejected(gd):

@@ -1,0 +1,117 @@
+"""Azimuthal wedges on the host: the periodic-image parameters and the oracle's duplicate-image dedup.
+
+In a wedge (n_x > 1, azimuth shorter than 2 pi) the reference gives every particle two images
+rotated by -width and +width (src/swarm/col_site_init.cu:58-76).  An owner whose search ball can
+reach two images of one particle (image_dist_min <= 2 q) keeps only the nearer one, by
+(d^2 bits, code) (kdtree/index_heap.cuh:118-141; the Morton search's id sort,
+morton/morton_query.cuh:18-58 and 62-140, keeps the same one).
+"""
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+
+def _wedge_sites(n, width, seed):
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(1.0, 2.0, n)
+    phi = rng.uniform(0.0, width, n)
+    base = np.stack([r * np.cos(phi), r * np.sin(phi), rng.normal(0.0, 0.05, n)], 1)
+    sites = np.zeros((3 * n, 4), np.float32)
+    for img, ang in ((0, 0.0), (1, -width), (2, width)):
+        c, s = math.cos(ang), math.sin(ang)
+        blk = sites[img * n:(img + 1) * n]
+        blk[:, 0] = c * base[:, 0] - s * base[:, 1]
+        blk[:, 1] = s * base[:, 0] + c * base[:, 1]
+        blk[:, 2] = base[:, 2]
+        blk[:, 3] = (3 * np.arange(n, dtype=np.int32) + img).view(np.float32)
+    return sites
+
+
+def _first_per_particle(row, k):
+    """The first entry of each particle along an ascending row, up to k (the dedup's result)."""
+    out, seen = [], set()
+    for c in row:
+        if c < 0:
+            break
+        if c // 3 in seen:
+            continue
+        seen.add(c // 3)
+        out.append(c)
+        if len(out) == k:
+            break
+    return out + [-1] * (k - len(out))
+
+
+def test_oracle_dedup_keeps_the_nearest_image_of_each_particle():
+    from oracle import oracle
+
+    n, K, width = 400, 40, 0.05  # a sliver: the K nearest reach across the seams
+    sites = _wedge_sites(n, width, seed=11)
+    q = np.full(n, 0.4, np.float32)
+    active = np.ones(n, np.uint8)
+    active[::17] = 0
+    # every candidate of every owner, ascending (K = all sites, no dedup)
+    all_codes, _ = oracle.knn_brute_images(sites, n, q, active, 3 * n, -1.0)
+    # image_dist_min = 0.1 <= 2 q: every owner deduplicates
+    codes, d2 = oracle.knn_brute_images(sites, n, q, active, K, 0.1)
+    plain, _ = oracle.knn_brute_images(sites, n, q, active, K, -1.0)
+    repeats = 0
+    for i in range(n):
+        if not active[i]:
+            assert (codes[i] == -1).all()
+            continue
+        assert codes[i].tolist() == _first_per_particle(all_codes[i], K), i
+        assert plain[i].tolist() == all_codes[i][:K].tolist(), i
+        kept = plain[i][plain[i] >= 0] // 3
+        repeats += int(len(kept) != len(set(kept.tolist())))
+    assert repeats > 0  # the case holds owners that see two images of one particle
+    # the Morton search's decision uses the largest q: 2 * 0.01 < 0.1, no owner deduplicates
+    morton_off, _ = oracle.knn_brute_images(sites, n, q, active, K, 0.1, q_dedup=0.01)
+    assert np.array_equal(morton_off, plain)
+    # image_dist_min > 2 q: unique identifiers, the plain top-K
+    unique, _ = oracle.knn_brute_images(sites, n, q, active, K, 0.81)
+    assert np.array_equal(unique, plain)
+
+
+def _libm_sinf():
+    libm = ctypes.CDLL("libm.so.6")
+    libm.sinf.restype = ctypes.c_float
+    libm.sinf.argtypes = [ctypes.c_float]
+    return lambda x: np.float32(libm.sinf(np.float32(x)))
+
+
+@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d", "c0_plain_small", "c1_multisize_2d"])
+def test_wedge_info_restates_x_wedge_and_image_dist_min(gd, workload):
+    from gamedev_b200 import GD_SEARCH_MORTON, workloads
+
+    cfg = workloads.config(workload)
+    wedge, width, idm = gd.wedge_info(cfg)
+    f = np.float32
+    x_min, x_max = f(cfg.x_min), f(cfg.x_max)
+    # X_WEDGE (const_defs.cuh:56-57)
+    assert wedge == bool(cfg.n_x > 1 and x_max - x_min < f(6.28318530717958647692) - f(1.0e-06))
+    assert wedge == workload.startswith("w")
+    if not wedge:
+        assert width == 0.0 and idm == -1.0
+        return
+    # the image rotation angle of each search (col_site_init.cu:60, morton_ghost.cuh:62)
+    want = (x_max - x_min) if cfg.search == GD_SEARCH_MORTON else f(cfg.x_max - cfg.x_min)
+    assert f(width) == want
+    # _get_image_dist_min (param_grid.cuh:86-89) with the host's sinf
+    sinf = _libm_sinf()
+    y_min, z_min, z_max = f(cfg.y_min), f(cfg.z_min), f(cfg.z_max)
+    expect = f(2.0) * y_min * min(sinf(z_min), sinf(z_max)) * abs(sinf(f(0.5) * (x_max - x_min)))
+    assert f(idm).view(np.uint32) == f(expect).view(np.uint32)
+
+
+@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d"])
+def test_wedge_swarms_lie_inside_the_wedge(workload):
+    from gamedev_b200 import workloads
+
+    cfg = workloads.config(workload)
+    p = workloads.particles(workload, n=4096)
+    assert (p[:, 0] >= cfg.x_min).all() and (p[:, 0] < cfg.x_max).all()
+    assert cfg.n_x > 1 and cfg.x_max - cfg.x_min < 2.0 * math.pi

@@ -1,0 +1,168 @@
+"""Azimuthal wedges on the B200: periodic images, the duplicate-image dedup, and parity with the
+reference's own CUDA build of the same wedge models.
+
+Bars:
+  * the device's sites: particle i at site i (code 3i); its images at sites n + i and 2n + i
+    (codes 3i + 1 and 3i + 2), the physical site rotated by -width and +width (col_site_init.cu:58-76)
+    to 1e-6 of the radius;
+  * every neighbour row bit-identical to the oracle's restatement of the reference heap with its
+    dedup (gdo_knn_brute_images, index_heap.cuh:112-176) over the device's own sites, and the kept
+    K-th d^2 bit-identical; the radius-bounded search gives the same rows;
+  * against the reference's CUDA build of the same model (oracle/_ref/collide_w*_65536: its
+    col_site_init with images, its KD tree or Morton ghost index, and col_cache_get):
+      - every image coordinate bit-identical to the reference's KD node or Morton ghost record of
+        the same code, and every physical site too;
+      - the KD rows as sets (the reference writes heap order), the Morton rows in order, every
+        measure to 1e-12 relative;
+      - on the Morton wedge, the collision operator leaves every particle as the reference's does
+        (grain size and count to 1e-12 relative).
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+WEDGES = ["w0_wedge_3d", "w1_narrow_2d"]
+
+
+def _run(gd, cfg, p, radius_scale=None):
+    import torch
+
+    sw = gd.SwarmCollision(cfg, len(p))
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    site4, q, active = (t.cpu().numpy() for t in sw.get_sites())
+    bounded = None
+    if radius_scale is not None:
+        radius = torch.from_numpy(q * np.float32(radius_scale)).to(dp.device)
+        bc = torch.empty_like(codes)
+        bk = torch.empty_like(kth)
+        sw.col_cache_get_bounded(dp, radius, bc, None, bk, None)
+        bounded = (bc.cpu().numpy(), bk.cpu().numpy())
+    torch.cuda.synchronize()
+    out = codes.cpu().numpy(), measure.cpu().numpy(), kth.cpu().numpy(), site4, q, active, bounded
+    sw.close()
+    return out
+
+
+@pytest.mark.parametrize("workload", WEDGES)
+def test_wedge_sites_and_rows_match_the_oracle(gd, cuda, workload):
+    from gamedev_b200 import GD_SEARCH_MORTON, workloads
+    from oracle import oracle
+
+    n = 16384
+    cfg = workloads.config(workload)
+    p = workloads.particles(workload, n=n)
+    codes, _, kth, site4, q, active, bounded = _run(gd, cfg, p, radius_scale=0.35)
+    wedge, width, idm = gd.wedge_info(cfg)
+    assert wedge and site4.shape == (3 * n, 4)
+    code = site4[:, 3].view(np.int32)
+    i = np.arange(n)
+    for img in range(3):
+        assert np.array_equal(code[img * n:(img + 1) * n], 3 * i + img)
+    for img, ang in ((1, -width), (2, width)):
+        c, s = math.cos(ang), math.sin(ang)
+        x, y = site4[:n, 0].astype(np.float64), site4[:n, 1].astype(np.float64)
+        blk = site4[img * n:(img + 1) * n].astype(np.float64)
+        r = np.hypot(x, y)
+        assert np.abs(blk[:, 0] - (c * x - s * y)).max() <= 1e-6 * r.max()
+        assert np.abs(blk[:, 1] - (s * x + c * y)).max() <= 1e-6 * r.max()
+        assert np.array_equal(blk[:, 2], site4[:n, 2])
+    q_dedup = float(q.max()) if cfg.search == GD_SEARCH_MORTON else -1.0
+    want, wd2 = oracle.knn_brute_images(site4, n, q, active, cfg.n_k, idm, q_dedup)
+    bad = np.nonzero((want != codes).any(axis=1))[0]
+    assert bad.size == 0, (workload, int(bad.size), int(bad[0]), want[bad[0]][:8], codes[bad[0]][:8])
+    act = active.astype(bool)
+    kth_want = np.where(want >= 0, wd2, 0.0).max(axis=1).astype(np.float32)
+    assert np.array_equal(kth_want[act].view(np.uint32), kth[act].view(np.uint32))
+    # the rows reach images; some owners deduplicate (on the 1.2 rad wedge their K nearest rarely
+    # hold two images of one particle; on the sliver the dedup changes rows)
+    assert (codes[act] % 3 != 0).any()
+    assert np.any(2.0 * (q_dedup if q_dedup >= 0 else q[act]) >= idm)
+    if workload == "w1_narrow_2d":
+        plain, _ = oracle.knn_brute_images(site4, n, q, active, cfg.n_k, -1.0)
+        assert (plain != want).any(axis=1).sum() > 0
+    # the radius-bounded search (walk first out to 0.35 q) gives the same rows
+    assert np.array_equal(bounded[0], codes)
+    assert np.array_equal(bounded[1].view(np.uint32), kth.view(np.uint32))
+
+
+def _refc(workload, n):
+    from oracle.ref import refcollide
+
+    if not refcollide.available(workload, n):
+        pytest.skip("oracle/_ref reference collision build absent (reference tree not mounted at build time)")
+    return refcollide
+
+
+def _mass(p):
+    return float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+
+
+@pytest.mark.parametrize("workload", WEDGES)
+def test_wedge_images_and_rows_match_the_reference_build(gd, cuda, workload):
+    from gamedev_b200 import GD_SEARCH_MORTON, workloads
+
+    n = 65536
+    refcollide = _refc(workload, n)
+    cfg = workloads.config(workload)
+    p = workloads.particles(workload, n=n)
+    codes, measure, _, site4, _, active, _ = _run(gd, cfg, p)
+    _, info = refcollide.run(workload, p, 1, 1.0, _mass(p), 0, timeout=600, neighbours=True, records=True)
+    # every reference record (KD nodes; Morton points and ghosts) against our site of the same code
+    rec = info["records"]
+    rcode = rec[:, 3].view(np.int32)
+    pos = np.empty(3 * n, np.int64)
+    pos[site4[:, 3].view(np.int32)] = np.arange(3 * n)
+    ours = site4[pos[rcode], :3]
+    same_site = (ours.view(np.uint32) == rec[:, :3].view(np.uint32)).all(axis=1)
+    assert same_site.all(), (workload, int((~same_site).sum()), rcode[~same_site][:4])
+    assert (rcode % 3 != 0).sum() > n // 10  # images are present in the reference's records
+    # the neighbour cache
+    rc, rm = info["codes"], info["measure"]
+    if cfg.search == GD_SEARCH_MORTON:
+        same = (rc == codes).all(axis=1)
+    else:
+        same = (np.sort(rc, axis=1) == np.sort(codes, axis=1)).all(axis=1)
+    bad = np.nonzero(~same)[0]
+    assert bad.size == 0, (workload, int(bad.size), int(bad[0]), np.sort(rc[bad[0]])[:8],
+                           np.sort(codes[bad[0]])[:8])
+    assert (codes[active.astype(bool)] % 3 != 0).any()
+    assert np.allclose(measure, rm, rtol=1e-12, atol=0)
+
+
+def test_morton_wedge_operator_matches_the_reference_per_particle(gd, cuda):
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = 65536
+    workload = "w1_narrow_2d"
+    refcollide = _refc(workload, n)
+    cfg = workloads.config(workload)
+    p = workloads.particles(workload, n=n, seed=21)
+    # an operator giving the fastest owner about 2000 expected events at bath start
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    rng = gd.rngstate_init(n, seed=1)
+    sw.evolve_collisions(dp, rng, 1.0e-12 * workloads.orbital_time(), _mass(p))
+    rates = sw.owner_state()[0][:, 0].cpu().numpy()
+    sw.close()
+    duration = 2000.0 / rates.max()
+    for seed in (1, 2):
+        sw = gd.SwarmCollision(cfg, n)
+        dp = gd.particles_to_device(p)
+        rng = gd.rngstate_init(n, seed=seed)
+        sw.evolve_collisions(dp, rng, duration, _mass(p))
+        torch.cuda.synchronize()
+        ours = dp.cpu().numpy()
+        events = sw.last_operator_stats()
+        sw.close()
+        ref, _ = refcollide.run(workload, p, seed, duration, _mass(p), 1, timeout=600)
+        same = (np.isclose(ours[:, 6], ref[:, 6], rtol=1e-12, atol=0)
+                & np.isclose(ours[:, 7], ref[:, 7], rtol=1e-12, atol=0))
+        assert same.all(), (seed, int((~same).sum()), events)
+        assert (ours[:, 6] != p[:, 6]).any()  # the operator changed grains
