@@ -78,14 +78,43 @@ def test_wedge_sites_and_rows_match_the_oracle(gd, cuda, workload):
     act = active.astype(bool)
     kth_want = np.where(want >= 0, wd2, 0.0).max(axis=1).astype(np.float32)
     assert np.array_equal(kth_want[act].view(np.uint32), kth[act].view(np.uint32))
-    # the rows reach images; some owners deduplicate (on the 1.2 rad wedge their K nearest rarely
-    # hold two images of one particle; on the sliver the dedup changes rows)
+    # the rows reach images, and some owners have the dedup on (their K nearest here never hold two
+    # images of one particle: test_dedup_replaces_a_held_image covers that)
     assert (codes[act] % 3 != 0).any()
     assert np.any(2.0 * (q_dedup if q_dedup >= 0 else q[act]) >= idm)
-    if workload == "w1_narrow_2d":
-        plain, _ = oracle.knn_brute_images(site4, n, q, active, cfg.n_k, -1.0)
-        assert (plain != want).any(axis=1).sum() > 0
     # the radius-bounded search (walk first out to 0.35 q) gives the same rows
+    assert np.array_equal(bounded[0], codes)
+    assert np.array_equal(bounded[1].view(np.uint32), kth.view(np.uint32))
+
+
+@pytest.mark.parametrize("search", ["kd", "morton"])
+def test_dedup_replaces_a_held_image(gd, cuda, search):
+    """A 0.002 rad sliver of 4096 particles: an owner's 32 nearest span several wedge widths, so
+    two or three images of one particle fall inside its ball and the dedup must keep the nearer."""
+    from gamedev_b200 import GD_SEARCH_KDTREE, GD_SEARCH_MORTON, workloads
+    from oracle import oracle
+
+    n, width = 4096, 0.002
+    cfg = workloads.config("w1_narrow_2d")
+    cfg.search = GD_SEARCH_KDTREE if search == "kd" else GD_SEARCH_MORTON
+    cfg.x_min, cfg.x_max = 0.0, width
+    p = workloads.particles("w1_narrow_2d", n=n)
+    p[:, 0] *= width / 0.05  # azimuths into [0, width)
+    codes, _, kth, site4, q, active, bounded = _run(gd, cfg, p, radius_scale=0.5)
+    wedge, _, idm = gd.wedge_info(cfg)
+    assert wedge
+    q_dedup = float(q.max()) if search == "morton" else -1.0
+    want, wd2 = oracle.knn_brute_images(site4, n, q, active, cfg.n_k, idm, q_dedup)
+    bad = np.nonzero((want != codes).any(axis=1))[0]
+    assert bad.size == 0, (search, int(bad.size), int(bad[0]), want[bad[0]][:8], codes[bad[0]][:8])
+    act = active.astype(bool)
+    kth_want = np.where(want >= 0, wd2, 0.0).max(axis=1).astype(np.float32)
+    assert np.array_equal(kth_want[act].view(np.uint32), kth[act].view(np.uint32))
+    # no row holds two images of one particle, and without the dedup many rows would
+    kept = np.where(codes >= 0, codes // 3, -1 - np.arange(cfg.n_k)[None, :])
+    assert all(len(set(r.tolist())) == cfg.n_k for r in kept[act])
+    plain, _ = oracle.knn_brute_images(site4, n, q, active, cfg.n_k, -1.0)
+    assert (plain != want).any(axis=1).sum() > n // 10
     assert np.array_equal(bounded[0], codes)
     assert np.array_equal(bounded[1].view(np.uint32), kth.view(np.uint32))
 
