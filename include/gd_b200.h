@@ -168,9 +168,10 @@ gd_status gd_set_tuning(gd_handle *h, const gd_tuning *t);
 
 /* Autotuner: times the search on the caller's own particles (and proposed radii, or NULL for the
  * plain query) over the sort order (if tune_sort), the walk and prescan depth, then the block width
- * (greedy, best of two runs each), checks that every setting reproduces the starting setting's
- * codes and kept d^2 bit for bit (GD_ERR_CONTROLLER otherwise), keeps the fastest in the handle and
- * leaves the geometry built with it.  *out_best / *out_ms (may be NULL) receive the setting and its
+ * (greedy, best of three runs each; a setting replaces the current one only when at least 2%
+ * faster), checks that every setting reproduces the starting setting's codes and kept d^2 bit for
+ * bit (GD_ERR_CONTROLLER otherwise), keeps the fastest in the handle and leaves the geometry built
+ * with it.  *out_best / *out_ms (may be NULL) receive the setting and its
  * query time.  Synchronises the stream; not for use under stream capture. */
 gd_status gd_autotune(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int tune_sort,
                       gd_tuning *out_best, double *out_ms);
