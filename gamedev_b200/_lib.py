@@ -58,6 +58,19 @@ class GdConfig(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class GdRunInfo(C.Structure):
+    """gd_run_info: the model-directory settings variables.txt records beyond gd_config."""
+
+    _fields_ = [
+        ("multisize", C.c_int), ("transport", C.c_int), ("diffusion", C.c_int), ("radiation", C.c_int),
+        ("pr_effect", C.c_int), ("visc_flow", C.c_int), ("importgas", C.c_int), ("log_output", C.c_int),
+        ("save_max", C.c_int), ("out_base", C.c_int), ("col_bath_tpb", C.c_int),
+        ("metal_z", C.c_double), ("schmidt_x", C.c_double), ("schmidt_r", C.c_double), ("schmidt_z", C.c_double),
+        ("beta_0", C.c_double), ("kappa_0", C.c_double), ("t_beta", C.c_double), ("c_light", C.c_double),
+        ("dt_out", C.c_double), ("dt_max", C.c_double), ("cfl_dyn", C.c_double),
+    ]
+
+
 class GdTuning(C.Structure):
     _fields_ = [("warps_per_block", C.c_int), ("prescan", C.c_int), ("walk_breadth_first", C.c_int),
                 ("sort_bits", C.c_int)]
@@ -120,6 +133,7 @@ SIGNATURES = {
     "gd_particles_to_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),
     "gd_particles_from_file_layout": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int]),
     "gd_save_checkpoint": (C.c_int, [C.POINTER(GdConfig), C.c_char_p, C.c_int, C.c_int, _P, C.c_int, _P]),
+    "gd_save_variables": (C.c_int, [C.POINTER(GdConfig), C.POINTER(GdRunInfo), C.c_int, C.c_double, C.c_char_p]),
     "gd_load_checkpoint": (C.c_int, [C.POINTER(GdConfig), C.c_char_p, C.c_int, C.c_int, _P, C.c_int, _P]),
     "gd_radius_model_get": (C.c_int, [_P, _P, _P]),
     "gd_radius_model_set": (C.c_int, [_P, _P, _P]),

@@ -410,6 +410,13 @@ def load_checkpoint(cfg: GdConfig, prefix: str, idx_file: int, particles, rng=No
               "gd_load_checkpoint")
 
 
+def save_variables(cfg: GdConfig, run, n_p: int, total_dust_mass: float, path: str):
+    """Write the run's variables.txt as the reference's save_variable does (gd_save_variables);
+    `run` is a GdRunInfo with the model directory's other settings."""
+    _io_check(_lib.load().gd_save_variables(C.byref(cfg), C.byref(run), int(n_p), float(total_dust_mass),
+                                            str(path).encode()), "gd_save_variables")
+
+
 STATIC_MAX_PARTICLES = 1 << 16  # gd_knn_static's fixed scratch
 
 

@@ -104,6 +104,24 @@ def config(name: str, n: int | None = None, k: int | None = None):
     return cfg
 
 
+def run_info(name: str):
+    """The model directory's settings outside gd_config (a GdRunInfo): the compile flags
+    mod/make_models.py writes for `name` (COLLISION and MULTISIZE; TRANSPORT and DIFFUSION in 3D;
+    linear output) and the constants those flags bring in.  variables.txt records them."""
+    from ._lib import GdRunInfo
+
+    three_d = CONFIGS[name]["three_d"]
+    r = GdRunInfo()
+    r.multisize = 1
+    r.transport = r.diffusion = int(three_d)
+    r.radiation = r.pr_effect = r.visc_flow = r.importgas = r.log_output = 0
+    r.save_max, r.out_base, r.col_bath_tpb = 10, 1, 64
+    r.metal_z, r.schmidt_x, r.schmidt_r, r.schmidt_z = 1.0e-02, 1.0, 1.0, 1.0
+    r.beta_0, r.kappa_0, r.t_beta, r.c_light = 1.0e+01, 1.0, 2.0 * math.pi, 1.0e+04
+    r.dt_out, r.dt_max, r.cfl_dyn = 0.5 * orbital_time(), 0.05 * orbital_time(), 0.45
+    return r
+
+
 def _radius_samples(rng, n: int, kind: str) -> np.ndarray:
     if kind == "loguniform":
         return np.exp(rng.uniform(math.log(R_IN_AU), math.log(R_OUT_AU), n))

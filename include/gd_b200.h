@@ -424,6 +424,26 @@ gd_status gd_save_checkpoint(const gd_config *cfg, const char *prefix, int idx_f
 gd_status gd_load_checkpoint(const gd_config *cfg, const char *prefix, int idx_file, int save_max,
                              gd_particle *dev_particle, int n, void *dev_rng);
 
+/* ---- variables.txt (save_variable, inc/swarm/swarm_host.cuh:989-1143) ------------------------------
+ * The parameter file a GameDev run writes beside its output (swarm_runtime.cu:290-291), which the
+ * reference's analysis scripts read.  The collision constants come from cfg.  The rest of a model
+ * directory's settings, most of them outside the collision path, come in gd_run_info: its
+ * compile-time flags and the constants those flags bring in.  Without a flag, its constants are
+ * not written, as in the reference.  The search written is cfg->search. */
+typedef struct gd_run_info {
+    int multisize, transport, diffusion, radiation, pr_effect, visc_flow, importgas;
+    int log_output;     /* LOGTIMING or LOGOUTPUT: writes LOG_BASE = out_base, else LIN_BASE */
+    int save_max, out_base;
+    int col_bath_tpb;   /* COL_BATH_TPB of the model (the reference's bath-rate block width) */
+    double metal_z, schmidt_x, schmidt_r, schmidt_z;
+    double beta_0, kappa_0, t_beta, c_light;
+    double dt_out, dt_max, cfl_dyn;
+} gd_run_info;
+/* Writes `path` as save_variable(path, total_dust_mass) does for a model with N_P = n_p, byte for
+ * byte.  Host only.  GD_ERR_IO when the file cannot be written. */
+gd_status gd_save_variables(const gd_config *cfg, const gd_run_info *run, int n_p, double total_dust_mass,
+                            const char *path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,9 @@
 //   ref_io load  <in.dat> <out.bin>   a particle file read as LOAD_PARTICLE_TO_VRAM reads it
 //                                     (size-checked), back in the internal layout, int32 n first
 //   ref_io frame <idx>                prints frame_num(idx)
+//   ref_io variables <out.txt> <total_dust_mass>
+//                                     the run's parameter file as save_variable writes it
+//                                     (swarm_host.cuh:989-1143)
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -24,8 +27,10 @@ int main(int argc, char **argv) {
         std::printf("%s\n", frame_num(std::atoi(argv[2])).c_str());
         return 0;
     }
+    if (argc == 4 && std::string(argv[1]) == "variables")
+        return save_variable(argv[2], std::strtod(argv[3], nullptr)) ? 0 : 4;
     if (argc != 4) {
-        std::fprintf(stderr, "usage: ref_io save|load <in> <out> | ref_io frame <idx>\n");
+        std::fprintf(stderr, "usage: ref_io save|load <in> <out> | ref_io frame <idx> | ref_io variables <out> <mass>\n");
         return 2;
     }
     const std::string mode = argv[1];

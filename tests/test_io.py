@@ -7,8 +7,11 @@ configuration (oracle/ref/Makefile).  Bars:
   * frame names equal frame_num for indices below, at and above the 5-digit width and save_max;
   * the particle file the library's layout conversion produces is byte-identical to the file the
     reference writes for the same particles (random velocities, plus owners at R = 0 and y = 0);
-  * reading a reference file back gives the reference's internal records bit for bit.
-The c0 shapes are 3D (polar velocities converted), the c1 shapes 2D (polar pinned to pi/2).
+  * reading a reference file back gives the reference's internal records bit for bit;
+  * variables.txt from gd_save_variables is byte-identical to the one save_variable writes for the
+    same model (the model header's constants come from workloads.config and workloads.run_info).
+The c0 shapes are 3D (polar velocities converted; KD search, transport and diffusion flags), the c1
+shapes 2D (polar pinned to pi/2; Morton search).
 """
 
 import re
@@ -85,3 +88,19 @@ def test_reference_reader_rejects_wrong_size(gd, tmp_path):
     (tmp_path / "short.dat").write_bytes(b"\0" * (64 * N - 64))
     r = subprocess.run([str(exe), "load", str(tmp_path / "short.dat"), str(tmp_path / "x.bin")])
     assert r.returncode != 0  # the size check the library's reader restates (GD_ERR_IO)
+
+
+@pytest.mark.parametrize("model", MODELS)
+def test_variables_file_matches_reference(gd, model, tmp_path):
+    from gamedev_b200 import workloads
+
+    exe = _ref_io(model)
+    mass = 1.0e-4 * workloads.MSUN * 0.731  # any positive total dust mass
+    ref, ours = tmp_path / "ref_variables.txt", tmp_path / "variables.txt"
+    subprocess.run([str(exe), "variables", str(ref), repr(mass)], check=True)
+    gd.save_variables(workloads.config(model), workloads.run_info(model), N, mass, str(ours))
+    want = ref.read_bytes()
+    assert b"[SWARM_DTYPE]" in want and b"LAMBDA_0" in want
+    assert ours.read_bytes() == want, "\n".join(
+        f"{a!r} != {b!r}" for a, b in zip(ours.read_text().splitlines(), ref.read_text().splitlines()) if a != b)
+
