@@ -22,17 +22,22 @@ PROGRAM = r"""
 #include <gd_bridge.cuh>
 int main() {
     gd_config c = gd_bridge_config();
+    int wedge = -1;
+    gd_wedge_info(&c, &wedge, nullptr, nullptr);
     std::printf("{\"n_p\": %d, \"n_k\": %d, \"n_x\": %d, \"n_z\": %d, \"coag_kernel\": %d, \"search\": %d, "
                 "\"G\": %.17g, \"y_max\": %.17g, \"sigma_0\": %.17g, \"stokes_0\": %.17g, \"v_frag\": %.17g, "
-                "\"col_bath_max\": %.17g, \"init_smin\": %.17g, \"code_unit\": %d, \"alpha\": %.17g}\n",
+                "\"col_bath_max\": %.17g, \"init_smin\": %.17g, \"code_unit\": %d, \"alpha\": %.17g, "
+                "\"x_min\": %.17g, \"x_max\": %.17g, \"x_wedge\": %d, \"gd_wedge\": %d}\n",
                 N_P, c.n_k, c.n_x, c.n_z, c.coag_kernel, c.search, c.G, c.y_max, c.sigma_0, c.stokes_0,
-                c.v_frag, c.col_bath_max, c.init_smin, c.code_unit, c.alpha);
+                c.v_frag, c.col_bath_max, c.init_smin, c.code_unit, c.alpha, c.x_min, c.x_max,
+                static_cast<int>(X_WEDGE), wedge);
     return 0;
 }
 """
 
 
-@pytest.mark.parametrize("model", ["c0_plain_small", "c1_multisize_2d", "c3_learned_3d"])
+@pytest.mark.parametrize("model", ["c0_plain_small", "c1_multisize_2d", "c3_learned_3d", "w0_wedge_3d",
+                                   "w1_narrow_2d"])
 def test_bridge_maps_model_constants(gd, tmp_path, model):
     if not (REF / "inc" / "gpu.cuh").exists():
         pytest.skip("reference tree not mounted (gpu.cuh)")
@@ -59,5 +64,8 @@ def test_bridge_maps_model_constants(gd, tmp_path, model):
     assert got["n_p"] == workloads.CONFIGS[model]["n"]
     for key in ("n_k", "n_x", "n_z", "coag_kernel", "search", "code_unit"):
         assert got[key] == getattr(cfg, key), key
-    for key in ("G", "y_max", "sigma_0", "stokes_0", "v_frag", "col_bath_max", "init_smin", "alpha"):
+    for key in ("G", "y_max", "sigma_0", "stokes_0", "v_frag", "col_bath_max", "init_smin", "alpha", "x_min",
+                "x_max"):
         assert got[key] == getattr(cfg, key), key
+    # the library's wedge decision for the bridged configuration is the model's own X_WEDGE
+    assert got["gd_wedge"] == got["x_wedge"] == int(model.startswith("w"))
