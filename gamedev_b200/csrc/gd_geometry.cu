@@ -1487,10 +1487,16 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
     return Status::ok();
 }
 
+// clears only the first-bad-index counter: the screen keeps the built geometry's active-site count
+// and largest q, which a later query on the same geometry reads
+__global__ void k_bad_index_reset(int *counters) {
+    if (threadIdx.x == 0) counters[1] = INT_MAX;
+}
+
 Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle, cudaStream_t s) {
     (void)m;
     g.launches += 2;
-    k_counters_reset<<<1, 32, 0, s>>>(g.counters.ptr);
+    k_bad_index_reset<<<1, 32, 0, s>>>(g.counters.ptr);
     k_state_screen<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, dev_particle, g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
     int cnt[2];

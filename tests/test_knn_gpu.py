@@ -191,3 +191,35 @@ def test_gpu_radius_bounded_query_is_exact(gd, cuda):
     torch.cuda.synchronize()
     assert torch.equal(codes, codes_p) and int(stats0[3].item()) == 0
     assert int(stats0[0].item()) > 0
+
+
+def test_query_after_the_collision_screen_reuses_the_geometry(gd, cuda):
+    """gd_evolve_collisions on a valid geometry and cache only screens the particles for non-finite
+    state (colstate_flag).  The geometry stays valid, so a later query on it must give the rows it
+    gave before the operator: collisions change grain sizes and counts, not positions."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = 4096
+    cfg = workloads.config("c0_plain_small")
+    p = workloads.particles("c0_plain_small", n=n)
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    sw.build_cache(dp)  # geometry + the handle's own cache: the operator's screen path applies
+    out = []
+    for step in range(2):
+        codes = torch.full((n, cfg.n_k), -7, dtype=torch.int32, device=dp.device)
+        kth = torch.full((n,), -7.0, dtype=torch.float32, device=dp.device)
+        sw.col_cache_get(dp, codes, None, kth)
+        torch.cuda.synchronize()
+        out.append((codes.cpu().numpy(), kth.cpu().numpy()))
+        if step == 0:
+            mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+            rng = gd.rngstate_init(n, seed=3)
+            sw.evolve_collisions(dp, rng, 1.0e-12 * workloads.orbital_time(), mass)
+            sw.evolve_collisions(dp, rng, 1.0e-12 * workloads.orbital_time(), mass)  # the screen path
+    sw.close()
+    assert (out[0][0] >= 0).any() and not (out[0][0] == -7).any()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
