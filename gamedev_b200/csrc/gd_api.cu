@@ -167,6 +167,10 @@ static std::string validate(const gd_config &c, int n) {
     if (c.coag_kernel < 0 || c.coag_kernel > 3) return "coag_kernel must be 0..3";
     if (c.col_bin_x < 1 || c.col_bin_y < 1 || c.col_bin_z < 1 || c.col_bin_s < 1) return "controller bins must be positive";
     if (c.search != GD_SEARCH_KDTREE && c.search != GD_SEARCH_MORTON) return "unknown search";
+    // the index addresses at most 2^30 sites (its leaf slots times 32 in int); a wedge has three per
+    // particle
+    if (gd::make_model(c).wedge && 3LL * n > (1LL << 30))
+        return "a wedge's three sites per particle exceed the 2^30 sites the index addresses";
     return std::string();
 }
 

@@ -67,6 +67,7 @@ def test_rng_state_is_curand_xorwow_size(gd):
         ({"n_k": 257}, 100),
         ({"coag_kernel": 4}, 100),
         ({}, 800_000_000),  # 3*N overflows int32 neighbour codes
+        ({"n_x": 64, "x_min": -0.1, "x_max": 0.1}, 357_913_942),  # a wedge: 3N sites above 2^30
     ],
 )
 def test_create_rejects_invalid_models_without_a_device(gd, overrides, n):
