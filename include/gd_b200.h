@@ -112,7 +112,10 @@ void gd_config_default(gd_config *cfg);
 
 /* Create a handle for n_p particles (const_defs.cuh:39 N_P) on the current CUDA device.
  * Allocates the index, neighbour cache, controller workspace (the reference's local_workspace,
- * _col_chain.cuh:36-96) and the caches the reference allocates in swarm_runtime.cu:120-184. */
+ * _col_chain.cuh:36-96) and the caches the reference allocates in swarm_runtime.cu:120-184.
+ * Limits (GD_ERR_INVALID_ARGUMENT, before any device work): 3 n_p <= INT_MAX (packed neighbour
+ * codes, _col_image.cuh:14-15); in an azimuthal wedge, whose index holds three sites per particle,
+ * 3 n_p <= 2^30. */
 gd_status gd_create(const gd_config *cfg, int n_p, gd_handle **out);
 void      gd_destroy(gd_handle *h);
 
