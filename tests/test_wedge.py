@@ -115,3 +115,44 @@ def test_wedge_swarms_lie_inside_the_wedge(workload):
     p = workloads.particles(workload, n=4096)
     assert (p[:, 0] >= cfg.x_min).all() and (p[:, 0] < cfg.x_max).all()
     assert cfg.n_x > 1 and cfg.x_max - cfg.x_min < 2.0 * math.pi
+
+
+def _morton_ghost_rows(all_codes, all_d2, k, unique_ids):
+    """_morton_ghost_topk's selection (morton/morton_query.cuh:62-140) from an owner's ascending
+    candidate list: without unique ids, the 3K nearest records, sorted by (particle, d^2, code),
+    the first of each particle kept, then the K nearest of those; with unique ids, the K nearest."""
+    rows = []
+    for codes, d2 in zip(all_codes, all_d2):
+        keep = codes >= 0
+        cand = list(zip(d2[keep].view(np.uint32).tolist(), codes[keep].tolist()))  # ascending keys
+        if not unique_ids:
+            cand = sorted(cand[:3 * k], key=lambda t: (t[1] // 3, t[0], t[1]))
+            cand = [t for j, t in enumerate(cand) if j == 0 or t[1] // 3 != cand[j - 1][1] // 3]
+            cand.sort()
+        row = [c for _, c in cand[:k]]
+        rows.append(row + [-1] * (k - len(row)))
+    return np.array(rows, np.int32)
+
+
+def test_morton_ghost_selection_equals_the_heap_dedup():
+    """The Morton search keeps only the 3K nearest records before removing duplicate images.  That
+    loses nothing: the K nearest particles by their nearest image lie among the 3K - 2 nearest
+    records, since each particle has at most three.  So its rows equal the KD heap's in-place dedup
+    (gdo_knn_brute_images), for every K, with the decision taken from the largest q."""
+    from oracle import oracle
+
+    n, width = 200, 0.05
+    sites = _wedge_sites(n, width, seed=23)
+    rng = np.random.default_rng(5)
+    q = rng.uniform(0.05, 0.5, n).astype(np.float32)
+    active = np.ones(n, np.uint8)
+    active[::13] = 0
+    act = active.astype(bool)
+    all_codes, all_d2 = oracle.knn_brute_images(sites, n, q, active, 3 * n, -1.0)
+    all_codes, all_d2 = all_codes[act], all_d2[act]
+    for k in (1, 5, 17, 40):
+        for idm in (0.1, 2.0):  # dedup on (image_dist_min <= 2 q_max) and off
+            unique = not (idm <= 2.0 * float(q.max()))
+            want = _morton_ghost_rows(all_codes, all_d2, k, unique)
+            got, _ = oracle.knn_brute_images(sites, n, q, active, k, idm, q_dedup=float(q.max()))
+            assert np.array_equal(got[act], want), (k, idm)
