@@ -90,6 +90,13 @@ CONFIGS = {
                         sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=7, x_range=(-0.6, 0.6)),
     "w1_narrow_2d": dict(n=65536, k=32, three_d=False, search=GD_SEARCH_MORTON, v_frag=100.0,
                          sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=8, x_range=(0.0, 0.05)),
+    # a radial-only model in code units with a constant viscosity, radiation pressure, viscous flow and
+    # logarithmic output: the settings the other models leave off, so that every branch of the run's
+    # parameter file (variables.txt) has a model that writes it
+    "v0_radial_units": dict(n=4096, k=16, three_d=False, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                            sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=9, n_x=1,
+                            units=dict(const_nu=1, nu=1.0e-5, code_unit=1, reynolds_0=1.0e8),
+                            flags=dict(radiation=1, pr_effect=1, visc_flow=1, log_output=1)),
 }
 
 
@@ -101,13 +108,18 @@ def config(name: str, n: int | None = None, k: int | None = None):
     cfg = _base_config(k or spec["k"], spec["three_d"], spec["search"], spec["v_frag"], smin, smax)
     if "x_range" in spec:
         cfg.x_min, cfg.x_max = spec["x_range"]
+    if "n_x" in spec:
+        cfg.n_x = spec["n_x"]
+    for key, value in spec.get("units", {}).items():
+        setattr(cfg, key, value)
     return cfg
 
 
 def run_info(name: str):
     """The model directory's settings outside gd_config (a GdRunInfo): the compile flags
     mod/make_models.py writes for `name` (COLLISION and MULTISIZE; TRANSPORT and DIFFUSION in 3D;
-    linear output) and the constants those flags bring in.  variables.txt records them."""
+    linear output unless the config asks for others) and the constants those flags bring in.
+    variables.txt records them."""
     from ._lib import GdRunInfo
 
     three_d = CONFIGS[name]["three_d"]
@@ -115,7 +127,9 @@ def run_info(name: str):
     r.multisize = 1
     r.transport = r.diffusion = int(three_d)
     r.radiation = r.pr_effect = r.visc_flow = r.importgas = r.log_output = 0
-    r.save_max, r.out_base, r.col_bath_tpb = 10, 1, 64
+    for key, value in CONFIGS[name].get("flags", {}).items():
+        setattr(r, key, value)
+    r.save_max, r.out_base, r.col_bath_tpb = 10, (10 if r.log_output else 1), 64
     r.metal_z, r.schmidt_x, r.schmidt_r, r.schmidt_z = 1.0e-02, 1.0, 1.0, 1.0
     r.beta_0, r.kappa_0, r.t_beta, r.c_light = 1.0e+01, 1.0, 2.0 * math.pi, 1.0e+04
     r.dt_out, r.dt_max, r.cfl_dyn = 0.5 * orbital_time(), 0.05 * orbital_time(), 0.45

@@ -9,7 +9,9 @@ configuration (oracle/ref/Makefile).  Bars:
     reference writes for the same particles (random velocities, plus owners at R = 0 and y = 0);
   * reading a reference file back gives the reference's internal records bit for bit;
   * variables.txt from gd_save_variables is byte-identical to the one save_variable writes for the
-    same model (the model header's constants come from workloads.config and workloads.run_info).
+    same model (the model header's constants come from workloads.config and workloads.run_info),
+    also for v0_radial_units, the radial model with the other branches of the file: code units, a
+    constant viscosity, radiation with the PR effect, viscous flow, logarithmic output.
 The c0 shapes are 3D (polar velocities converted; KD search, transport and diffusion flags), the c1
 shapes 2D (polar pinned to pi/2; Morton search).
 """
@@ -26,8 +28,8 @@ N = 65536
 MODELS = ["c0_plain_small", "c1_multisize_2d"]
 
 
-def _ref_io(model):
-    exe = ROOT / "oracle" / "_ref" / f"io_{model}_{N}" / "ref_io"
+def _ref_io(model, n=N):
+    exe = ROOT / "oracle" / "_ref" / f"io_{model}_{n}" / "ref_io"
     if not exe.exists():
         pytest.skip("oracle/_ref reference I/O build absent (reference tree not mounted at build time)")
     return exe
@@ -90,15 +92,16 @@ def test_reference_reader_rejects_wrong_size(gd, tmp_path):
     assert r.returncode != 0  # the size check the library's reader restates (GD_ERR_IO)
 
 
-@pytest.mark.parametrize("model", MODELS)
+@pytest.mark.parametrize("model", MODELS + ["v0_radial_units"])
 def test_variables_file_matches_reference(gd, model, tmp_path):
     from gamedev_b200 import workloads
 
-    exe = _ref_io(model)
+    n = workloads.CONFIGS[model]["n"] if model not in MODELS else N
+    exe = _ref_io(model, n)
     mass = 1.0e-4 * workloads.MSUN * 0.731  # any positive total dust mass
     ref, ours = tmp_path / "ref_variables.txt", tmp_path / "variables.txt"
     subprocess.run([str(exe), "variables", str(ref), repr(mass)], check=True)
-    gd.save_variables(workloads.config(model), workloads.run_info(model), N, mass, str(ours))
+    gd.save_variables(workloads.config(model), workloads.run_info(model), n, mass, str(ours))
     want = ref.read_bytes()
     assert b"[SWARM_DTYPE]" in want and b"LAMBDA_0" in want
     assert ours.read_bytes() == want, "\n".join(
