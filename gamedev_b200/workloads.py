@@ -97,6 +97,10 @@ CONFIGS = {
                             sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=9, n_x=1,
                             units=dict(const_nu=1, nu=1.0e-5, code_unit=1, reynolds_0=1.0e8),
                             flags=dict(radiation=1, pr_effect=1, visc_flow=1, log_output=1)),
+    # radial-polar (no azimuth) with an imported gas density: the last two branches of that file
+    "v1_polar_gas": dict(n=4096, k=16, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                         sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=10, n_x=1,
+                         flags=dict(importgas=1)),
 }
 
 

@@ -11,7 +11,8 @@ configuration (oracle/ref/Makefile).  Bars:
   * variables.txt from gd_save_variables is byte-identical to the one save_variable writes for the
     same model (the model header's constants come from workloads.config and workloads.run_info),
     also for v0_radial_units, the radial model with the other branches of the file: code units, a
-    constant viscosity, radiation with the PR effect, viscous flow, logarithmic output.
+    constant viscosity, radiation with the PR effect, viscous flow, logarithmic output; and for
+    v1_polar_gas, radial-polar with an imported gas density.
 The c0 shapes are 3D (polar velocities converted; KD search, transport and diffusion flags), the c1
 shapes 2D (polar pinned to pi/2; Morton search).
 """
@@ -92,7 +93,7 @@ def test_reference_reader_rejects_wrong_size(gd, tmp_path):
     assert r.returncode != 0  # the size check the library's reader restates (GD_ERR_IO)
 
 
-@pytest.mark.parametrize("model", MODELS + ["v0_radial_units"])
+@pytest.mark.parametrize("model", MODELS + ["v0_radial_units", "v1_polar_gas"])
 def test_variables_file_matches_reference(gd, model, tmp_path):
     from gamedev_b200 import workloads
 
