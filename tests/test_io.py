@@ -41,12 +41,20 @@ def _save_max(model):
     return int(re.search(r"SAVE_MAX\s*=\s*(\d+)", defs).group(1))
 
 
+def _n(model):
+    """Particles of the model's reference I/O build: N for the benchmark shapes, else the config's."""
+    from gamedev_b200 import workloads
+
+    return N if model in MODELS else workloads.CONFIGS[model]["n"]
+
+
 def _particles(model, seed=7):
     from gamedev_b200 import workloads
 
-    p = workloads.particles(model, n=N, seed=seed).copy()
+    n = _n(model)
+    p = workloads.particles(model, n=n, seed=seed).copy()
     rng = np.random.default_rng(seed)
-    p[:, 3:6] = rng.normal(size=(N, 3)) * 1e-3  # angular velocities of both signs
+    p[:, 3:6] = rng.normal(size=(n, 3)) * 1e-3  # angular velocities of both signs
     p[5, 1] = 0.0          # y = 0: R = 0 and no polar speed
     p[9, 2] = 0.0          # on the pole: R = y sin z = 0 in 3D
     return p
@@ -68,11 +76,13 @@ def test_frame_names_match_reference(gd, model):
     assert gd.frame_name(3, 1234567) == "0000003"  # width follows the digits of save_max
 
 
-@pytest.mark.parametrize("model", MODELS)
+@pytest.mark.parametrize("model", MODELS + ["v0_radial_units", "v1_polar_gas"])
 def test_particle_file_bytes_match_reference(gd, model, tmp_path):
+    """Also on the radial (N_X = N_Z = 1) and radial-polar (N_X = 1) models, where the azimuth is
+    pinned to the domain centre on both sides of the conversion."""
     from gamedev_b200 import workloads
 
-    exe = _ref_io(model)
+    exe = _ref_io(model, _n(model))
     cfg = workloads.config(model)
     p = _particles(model)
     _write_records(tmp_path / "in.bin", p)
@@ -97,7 +107,7 @@ def test_reference_reader_rejects_wrong_size(gd, tmp_path):
 def test_variables_file_matches_reference(gd, model, tmp_path):
     from gamedev_b200 import workloads
 
-    n = workloads.CONFIGS[model]["n"] if model not in MODELS else N
+    n = _n(model)
     exe = _ref_io(model, n)
     mass = 1.0e-4 * workloads.MSUN * 0.731  # any positive total dust mass
     ref, ours = tmp_path / "ref_variables.txt", tmp_path / "variables.txt"
