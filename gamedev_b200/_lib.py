@@ -8,6 +8,7 @@ CUDA kernels.
 from __future__ import annotations
 
 import ctypes as C
+import math
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libgd_b200.so"
@@ -189,6 +190,32 @@ class GdError(RuntimeError):
         self.status = status
         self.message = message
         self.detail = detail
+
+
+# gd_config_default's values (gamedev_b200/csrc/gd_api.cu), restated so that a configuration can be
+# built without loading the library (the reference arm of the benchmark must not map it);
+# tests/test_abi.py checks that the two agree field by field
+CONFIG_DEFAULTS = {
+    "G": 1.0, "M_S": 1.0, "R_0": 1.0, "S_0": 1.0, "n_x": 100, "n_y": 100, "n_z": 1,
+    "x_min": -math.pi, "x_max": math.pi, "y_min": 0.5, "y_max": 1.5, "z_min": 0.5 * math.pi,
+    "z_max": 0.5 * math.pi, "sigma_0": 1.0e-2, "aspr_0": 0.05, "idx_p": -1.0, "idx_q": -0.4,
+    "const_nu": 0, "nu": 1.0e-5, "alpha": 1.0e-4, "code_unit": 0, "reynolds_0": 1.0e8,
+    "m_mol": 2.3 * 1.66054e-24, "x_sec": 2.0e-15, "half_disk": 0, "const_st": 0, "stokes_0": 1.0e-3,
+    "rho_0": 1.0, "coag_kernel": GD_KERNEL_CONSTANT, "n_k": 200, "h_search": 1.0, "v_frag": 1.0,
+    "col_event_cap": 32, "col_bin_x": 8, "col_bin_y": 4, "col_bin_z": 2, "col_bin_s": 8, "col_bin_min": 64,
+    "col_bath_max": 0.05, "col_bath_eps": 0.02, "col_bath_alpha": 1.0e-3, "init_smin": 1.0, "init_smax": 1.0,
+    "search": GD_SEARCH_KDTREE, "morton_leaf_target": 128, "morton_max_level": 20,
+}
+
+
+def config_defaults(**overrides) -> GdConfig:
+    """gd_config_default's configuration built in Python, without loading libgd_b200.so."""
+    cfg = GdConfig()
+    for k, v in {**CONFIG_DEFAULTS, **overrides}.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
 
 
 def default_config(**overrides) -> GdConfig:

@@ -677,6 +677,11 @@ constexpr size_t kOffSubHi = kOffSubLo + round256(sizeof(float4) * kStaticLeafSl
 constexpr size_t kOffCounters = kOffSubHi + round256(sizeof(float4) * kStaticLeafSlots * kSubs);
 constexpr size_t kStaticBytes = kOffCounters + round256(sizeof(int) * 4);  // 4,407,552 bytes
 static_assert(kStaticBytes == 4407552, "scratch size stated in gd_b200.h");
+// The histogram region holds the [digit][tile] counts of one scan chunk and no chunk totals:
+// geometry_build's chunked scan needs a chunk-total area only when the counts span more than one
+// chunk, which this bound rules out for every swarm that fits the scratch.
+static_assert(256 * (kStaticSort / kRadixTile) <= kScanChunk,
+              "raising kStaticParticles past one scan chunk needs room for the chunk totals");
 
 constexpr int kStaticMaxDevices = 64;
 
@@ -692,7 +697,9 @@ std::mutex g_scratch_mu;
 unsigned char *g_scratch_addr[kStaticMaxDevices] = {};
 
 // Device address of g_knn_scratch on the current device, resolved once per device with that device
-// current (the first call on a device may load this library's device code there).
+// current (the first call on a device may load this library's device code there).  The address is
+// kept for the life of the process: after the host resets a device (cudaDeviceReset) this entry
+// point must not be called on it again.
 Status static_scratch(unsigned char **out) {
     int dev = -1;
     GD_TRY_CUDA(cudaGetDevice(&dev));

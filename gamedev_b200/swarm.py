@@ -426,7 +426,16 @@ def knn_static(cfg: GdConfig, particles, codes, measure, kth):
     a time loop that cannot take the synchronisation an allocation can cause).  Its scratch is a
     fixed 4.4 MB device array, so at most 65536 particles.  The caller provides the outputs; calls
     whose GPU work overlaps on one device race on the shared scratch."""
+    torch = _torch()
     n = int(particles.shape[0])
+    want = ((codes, torch.int32, (n, int(cfg.n_k))), (measure, torch.float64, (n,)), (kth, torch.float32, (n,)))
+    for t, dtype, shape in want:
+        if (t.dtype != dtype or tuple(t.shape) != shape or not t.is_contiguous()
+                or t.device != particles.device):
+            raise ValueError(f"knn_static output must be a contiguous {dtype} tensor of shape {shape} on "
+                             f"{particles.device}, got {t.dtype} {tuple(t.shape)} on {t.device}")
+    if not particles.is_cuda or not particles.is_contiguous():
+        raise ValueError("knn_static particles must be a contiguous device tensor")
     detail = C.c_longlong(0)
     msg = C.create_string_buffer(512)
     r = _lib.load().gd_knn_static(C.byref(cfg), C.c_void_p(particles.data_ptr()), n, C.c_void_p(codes.data_ptr()),

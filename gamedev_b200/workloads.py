@@ -31,7 +31,7 @@ import math
 
 import numpy as np
 
-from ._lib import GD_KERNEL_CUSTOM, GD_SEARCH_KDTREE, GD_SEARCH_MORTON, default_config
+from ._lib import GD_KERNEL_CUSTOM, GD_SEARCH_KDTREE, GD_SEARCH_MORTON, config_defaults
 
 AU = 1.495978707e13
 MSUN = 1.98847e33
@@ -47,7 +47,7 @@ def orbital_time() -> float:
 
 
 def _base_config(n_k: int, three_d: bool, search: int, v_frag: float, smin: float, smax: float):
-    cfg = default_config()
+    cfg = config_defaults()
     cfg.G, cfg.M_S, cfg.R_0, cfg.S_0 = G_CGS, MSUN, AU, 1.0
     cfg.n_x, cfg.n_y = 64, 64
     cfg.n_z = 32 if three_d else 1
@@ -117,6 +117,19 @@ def config(name: str, n: int | None = None, k: int | None = None):
     for key, value in spec.get("units", {}).items():
         setattr(cfg, key, value)
     return cfg
+
+
+# One collision half-operator of a swarm step, in seconds: at the c3/c4 shapes the fastest owner
+# expects about two events over it at bath start (its bath-start rate is 0.035 /s; the grain sizes
+# span five decades, so a fixed orbital fraction would ask the fastest owners for millions of
+# events).  Both benchmark arms use these lengths.
+SWARM_HALF_OPERATOR_S = {"c3_learned_3d": 57.0, "c4_production_3d": 57.0}
+
+
+def swarm_half_operator(name: str) -> float:
+    """The half-operator length of a swarm step of workload `name` (0.5/Omega(1 au) where none is
+    set)."""
+    return SWARM_HALF_OPERATOR_S.get(name, 0.5 * orbital_time())
 
 
 def run_info(name: str):

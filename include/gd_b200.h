@@ -398,8 +398,9 @@ long long gd_batch_launch_count(const gd_batch *b);
  *
  * The first call on each device, with that device current, looks up the scratch's device address
  * (this can load the library's device code on that device); make that first call before any stream
- * capture begins.  The call synchronises `stream` once (the non-finite screen) and returns with the
- * query enqueued on it.  All calls on one device share the one scratch: calls whose GPU work
+ * capture begins.  The address is kept for the life of the process, so after a cudaDeviceReset of a
+ * device this entry point must not be called on that device again.  The call synchronises `stream`
+ * once (the non-finite screen) and returns with the query enqueued on it.  All calls on one device share the one scratch: calls whose GPU work
  * overlaps (from several host threads, or on streams with no ordering between them) race and
  * corrupt each other's results; order them on one stream or serialise them.
  */

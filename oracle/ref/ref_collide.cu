@@ -14,6 +14,13 @@
 //            index's points and periodic ghosts), int32 count, count x (float32 x, y, z, int32 code)
 //   GD_REF_NEIGHBOURS=<file> (environment): also writes the neighbour cache of the geometry,
 //            int32 n, int32 K, int32 codes[n][K] (col_cache_get's order), float64 measure[n]
+//   GD_REF_STEPS=<s> (environment): repeat the whole sequence s times (default 1), as a swarm step
+//            of the reference's runtime does it (swarm_runtime.cu:504-601 without transport): rebuild
+//            the geometry (col_site_init, index, col_cache_get, col_space_bin; the owner lists are
+//            invalidated), then `operators` evolve_collisions(duration) calls, each after the first
+//            preceded by the colstate_flag screen the reference runs on a valid geometry
+//            (swarm_runtime.cu:361-373); stdout then also holds "steps": [[geometry_ms, op_ms...]...]
+//            and the dumps below describe the first step's geometry
 //   summary.json (builds with COL_DIAGNOSTICS only): the controller summary of the operators as
 //            the reference's save_col_controller writes it (_col_bound.cuh:242-299); those builds
 //            also write their per-operator log, collision_local_<stamp>.jsonl, to the working
@@ -136,8 +143,16 @@ int main(int argc, char **argv) {
         check(gpuEventCreate(&b), "event");
         float geometry_ms = 0.0f;
         std::vector<float> op_ms;
+        int steps = 1;
+        if (const char *env = std::getenv("GD_REF_STEPS")) steps = std::atoi(env);
+        if (steps < 1) throw std::runtime_error("GD_REF_STEPS must be positive");
+        std::vector<std::vector<float>> step_ms;
 
-        // geometry once (positions do not change between the operators)
+        for (int step = 0; step < steps; ++step) {
+        // geometry once per step (positions do not change between the operators of a step)
+        local_geometry_valid = false;
+        clock_dyn = 0.0;
+        count_col = 0;
         check(gpuDeviceSynchronize(), "setup");
         check(gpuEventRecord(a, 0), "record");
         check(gpuMemset(dev_bad_part, 0, sizeof(int)), "clear bad particle");
@@ -176,7 +191,8 @@ int main(int argc, char **argv) {
         check(gpuEventElapsedTime(&geometry_ms, a, b), "elapsed");
         // the search's records (KD tree nodes, or the Morton index's points with its periodic ghosts),
         // when GD_REF_SITES names a file: int32 count, then count x (float x, y, z, int32 code)
-        if (const char *path = std::getenv("GD_REF_SITES")) {
+        const char *sites_path = step == 0 ? std::getenv("GD_REF_SITES") : nullptr;
+        if (const char *path = sites_path) {
             std::vector<float> rec;
 #ifdef COLLISION_KDTREE
             std::vector<kdtree_node> node(N_T);
@@ -206,7 +222,8 @@ int main(int argc, char **argv) {
             if (!sf) throw std::runtime_error("cannot write the search records");
         }
         // the neighbour cache col_cache_get wrote, when GD_REF_NEIGHBOURS names a file
-        if (const char *path = std::getenv("GD_REF_NEIGHBOURS")) {
+        const char *neighbours_path = step == 0 ? std::getenv("GD_REF_NEIGHBOURS") : nullptr;
+        if (const char *path = neighbours_path) {
             std::vector<int> codes(static_cast<std::size_t>(N_P) * N_K);
             std::vector<real> measure(N_P);
             check(gpuMemcpy(codes.data(), dev_col_neighbor, sizeof(int) * codes.size(), gpuMemcpyDeviceToHost),
@@ -221,8 +238,16 @@ int main(int argc, char **argv) {
             if (!nb) throw std::runtime_error("cannot write the neighbour cache");
         }
 
+        std::vector<float> this_step{geometry_ms};
         for (int op = 0; op < operators; ++op) {
             check(gpuEventRecord(a, 0), "record");
+            if (op > 0) {
+                // the non-finite screen evolve_collisions runs when the geometry is still valid
+                check(gpuMemset(dev_bad_part, 0, sizeof(int)), "clear bad particle");
+                colstate_flag<<<NB_P, TPB>>>(dev_particle, dev_bad_part);
+                check(gpuGetLastError(), "colstate_flag");
+                check_bad(dev_bad_part);
+            }
             evolve_local_collisions(local, local_geometry_valid, duration, total_dust_mass, clock_dyn, dt_col,
                                     count_col, col_raw_count, dev_particle, dev_rngstate, dev_col_spatial,
                                     dev_col_neighbor, dev_col_events, dev_col_count, dev_col_binmap, dev_col_error,
@@ -238,7 +263,10 @@ int main(int argc, char **argv) {
             check(gpuEventSynchronize(b), "operator");
             float ms = 0.0f;
             check(gpuEventElapsedTime(&ms, a, b), "elapsed");
-            op_ms.push_back(ms);
+            this_step.push_back(ms);
+        }
+        if (step == 0) op_ms.assign(this_step.begin() + 1, this_step.end());
+        step_ms.push_back(this_step);
         }
         check(gpuMemcpy(particle.data(), dev_particle, sizeof(swarm) * N_P, gpuMemcpyDeviceToHost), "copy back");
 #ifdef COL_DIAGNOSTICS
@@ -249,14 +277,21 @@ int main(int argc, char **argv) {
         out.write(reinterpret_cast<const char *>(&n), 4);
         out.write(reinterpret_cast<const char *>(particle.data()), sizeof(swarm) * N_P);
         if (!out) throw std::runtime_error("cannot write output");
-        float total = geometry_ms;
+        float total = step_ms[0][0];
         std::string ops;
         for (std::size_t i = 0; i < op_ms.size(); ++i) {
             total += op_ms[i];
             ops += (i ? ", " : "") + std::to_string(op_ms[i]);
         }
-        std::printf("{\"n\": %d, \"operators\": %d, \"geometry_ms\": %.4f, \"operator_ms\": [%s], \"total_ms\": %.4f}\n",
-                    N_P, operators, geometry_ms, ops.c_str(), total);
+        std::string all;
+        for (std::size_t s = 0; s < step_ms.size(); ++s) {
+            all += s ? ", [" : "[";
+            for (std::size_t k = 0; k < step_ms[s].size(); ++k) all += (k ? ", " : "") + std::to_string(step_ms[s][k]);
+            all += "]";
+        }
+        std::printf("{\"n\": %d, \"operators\": %d, \"geometry_ms\": %.4f, \"operator_ms\": [%s], \"total_ms\": %.4f, "
+                    "\"steps\": [%s]}\n",
+                    N_P, operators, step_ms[0][0], ops.c_str(), total, all.c_str());
         return 0;
     } catch (const std::exception &e) {
         std::fprintf(stderr, "ref_collide: %s\n", e.what());

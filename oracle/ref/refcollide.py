@@ -27,14 +27,16 @@ def available(model: str, n: int, diagnostics: bool = False) -> bool:
 
 def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dust_mass: float,
         operators: int = 1, timeout: float = 1800, diagnostics: bool = False, neighbours: bool = False,
-        records: bool = False):
+        records: bool = False, steps: int = 1):
     """-> (particles after `operators` evolve_collisions(duration) calls on one geometry, info).
     With diagnostics (the COL_DIAGNOSTICS build), info["summary"] holds the controller summary the
     reference's save_col_controller wrote, parsed, info["summary_text"] its text, and
     info["operator_log"] the parsed lines of its per-operator log.  With neighbours,
     info["codes"] [n][K] and info["measure"] [n] hold the neighbour cache col_cache_get wrote; with
     records, info["records"] [count][4] float32 holds the search's records (x, y, z, code bits): the
-    KD nodes, or the Morton index's points with its periodic ghosts."""
+    KD nodes, or the Morton index's points with its periodic ghosts.  With steps > 1 the geometry and
+    the operators repeat `steps` times (a swarm step each: GD_REF_STEPS of ref_collide.cu) and
+    info["steps"] lists [geometry_ms, operator_ms...] per step; the dumps describe the first step."""
     p = np.ascontiguousarray(particles, dtype=np.float64).reshape(-1, 8)
     n = len(p)
     with tempfile.TemporaryDirectory() as d:
@@ -53,6 +55,7 @@ def run(model: str, particles: np.ndarray, seed: int, duration: float, total_dus
             env["GD_REF_NEIGHBOURS"] = str(nb)
         if records:
             env["GD_REF_SITES"] = str(rb)
+        env["GD_REF_STEPS"] = str(int(steps))
         r = subprocess.run(args, capture_output=True, text=True, timeout=timeout, cwd=d, env=env)
         if r.returncode != 0:
             raise RuntimeError(f"ref_collide failed ({r.returncode}): {r.stderr.strip()[-2000:]}")

@@ -188,7 +188,9 @@ def ref_host():
 
 
 if __name__ == "__main__":
-    reference = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    from oracle.ref import REFERENCE_ROOT
+
+    reference = Path(sys.argv[1]) if len(sys.argv) > 1 else REFERENCE_ROOT
     (HERE / "colphys_golden.json").write_text(json.dumps(colphys(reference)))
     (HERE / "ref_host_golden.json").write_text(json.dumps(ref_host()))
     print("written", [p.name for p in HERE.glob("*.json")])

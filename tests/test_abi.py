@@ -54,6 +54,31 @@ def test_config_defaults_match_reference_const_defs(gd):
     assert (cfg.morton_leaf_target, cfg.morton_max_level) == (128, 20)
 
 
+def test_python_config_defaults_equal_the_library_defaults(gd):
+    """config_defaults() builds gd_config_default's values without loading the library (the
+    benchmark's reference arm uses it); every field must agree bit for bit."""
+    from gamedev_b200 import _lib
+
+    native, py = gd.default_config(), _lib.config_defaults()
+    for name, _ in _lib.GdConfig._fields_:
+        a, b = getattr(native, name), getattr(py, name)
+        assert a == b and type(a) is type(b), (name, a, b)
+
+
+def test_workloads_do_not_load_the_library():
+    """The reference arm builds its configuration and particles through workloads: that must not
+    map libgd_b200.so."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r); from gamedev_b200 import workloads, _lib; "
+            "workloads.config('c3_learned_3d'); workloads.particles('c0_plain_small', n=64); "
+            "assert _lib._lib is None; "
+            "assert 'libgd_b200' not in open('/proc/self/maps').read()" % str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+
+
 def test_rng_state_is_curand_xorwow_size(gd):
     assert gd.rng_state_bytes() == 48
 

@@ -15,7 +15,7 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
-REF = Path(os.environ.get("GD_REFERENCE_ROOT", "/root/reference"))
+from oracle.ref import REFERENCE_ROOT as REF  # noqa: E402
 
 PROGRAM = r"""
 #include <const_defs.cuh>
