@@ -74,7 +74,7 @@ class GdRunInfo(C.Structure):
 
 class GdTuning(C.Structure):
     _fields_ = [("warps_per_block", C.c_int), ("prescan", C.c_int), ("walk_breadth_first", C.c_int),
-                ("sort_bits", C.c_int)]
+                ("sort_bits", C.c_int), ("range_query", C.c_int)]
 
 
 class GdOperatorStats(C.Structure):

@@ -243,7 +243,8 @@ static bool tuning_ok(const gd::Model &m, const gd_tuning &t) {
     const int full = 21 * m.dim;
     return t.warps_per_block >= 0 && t.warps_per_block <= 32 && t.prescan >= 0 && t.prescan <= 8 &&
            (t.walk_breadth_first == 0 || t.walk_breadth_first == 1) &&
-           (t.sort_bits == 0 || (t.sort_bits >= 16 * m.dim && t.sort_bits <= full));
+           (t.sort_bits == 0 || (t.sort_bits >= 16 * m.dim && t.sort_bits <= full)) &&
+           (t.range_query == 0 || t.range_query == 1);
 }
 
 static gd::Tuning to_tuning(const gd_tuning &t) {
@@ -252,6 +253,7 @@ static gd::Tuning to_tuning(const gd_tuning &t) {
     u.prescan = t.prescan;
     u.bfs = t.walk_breadth_first;
     u.sort_bits = t.sort_bits;
+    u.range = t.range_query;
     return u;
 }
 
@@ -261,6 +263,7 @@ static gd_tuning from_tuning(const gd::Tuning &u) {
     t.prescan = u.prescan;
     t.walk_breadth_first = u.bfs;
     t.sort_bits = u.sort_bits;
+    t.range_query = u.range;
     return t;
 }
 
@@ -363,6 +366,12 @@ gd_status gd_autotune(gd_handle *h, const gd_particle *dev_particle, const float
             if (t.bfs == best.bfs && t.prescan == best.prescan) continue;
             consider(t, false);
         }
+    if (st && dev_radius && gd::knn_range_eligible(h->m, h->m.n_k)) {
+        // the radius-bounded query: warp-per-owner range query or per-lane heaps
+        gd::Tuning t = best;
+        t.range = best.range ? 0 : 1;
+        consider(t, false);
+    }
     for (int w : {1, 2, 4, 8}) {
         if (!st) break;
         gd::Tuning t = best;

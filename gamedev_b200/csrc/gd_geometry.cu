@@ -418,7 +418,7 @@ __device__ __forceinline__ int same_particle(const unsigned long long *hp, int l
 // reach two images of one particle keeps only the nearer (the dedup of index_heap.cuh:118-136).
 template <bool kImages>
 __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, int leaf, unsigned char *wbase,
-                                           int kcap) {
+                                           int kcap, unsigned int lanes = 0xffffffffu) {
     const int lane = threadIdx.x & 31;
     const int K = a.k;
     const int cap = knn_capacity(K, a.radius != nullptr);  // entries a lane may hold (<= kcap)
@@ -439,7 +439,7 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     const float3 qp = make_float3(me.x, me.y, me.z);
     const int code = __float_as_int(me.w);
     // with wedge images only the physical sites (image 0) query (_col_cache.cuh:22)
-    const bool valid = i < n_act && (!kImages || code % 3 == 0);
+    const bool valid = i < n_act && (!kImages || code % 3 == 0) && ((lanes >> lane) & 1u);
     const int idx = valid ? code / 3 : 0;
     const float qr = valid ? a.qrad[idx] : 0.f;
     // dedup_needed = !unique_ids (_col_cache.cuh:38-39 per owner for KD; the largest q for Morton,
@@ -457,7 +457,7 @@ __device__ __forceinline__ void knn_bucket(const Model &m, const QueryArgs &a, i
     float lim2 = q2;
     if (a.radius && valid) {
         const float r = a.radius[idx];
-        if (r < qr) lim2 = r * r;
+        if (r >= 0.0f && r < qr) lim2 = r * r;  // a negative or NaN proposal bounds nothing
     }
     int cnt = 0;                              // real entries held by this lane (fill phase below K)
     float cut = valid ? lim2 : -1.0f;         // d^2 bound of an acceptable candidate
@@ -860,6 +860,22 @@ __global__ void k_knn_query(Model m, QueryArgs a) {
     knn_bucket<kImages>(m, a, blockIdx.x * (blockDim.x >> 5) + wib, smem + wib * knn_warp_bytes(kcap), kcap);
 }
 
+// The owners the range query (k_knn_range) left over: the listed buckets, only the listed lanes of
+// each, by the per-lane heap query with the full q.  A persistent grid walks the list, whose
+// length the range query left in device memory.
+__global__ void k_knn_fallback(Model m, QueryArgs a, const int *__restrict__ fb_count, const int *__restrict__ fb_leaf,
+                               const unsigned int *__restrict__ fb_mask) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int wib = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const int kcap = knn_capacity(a.k, false);
+    unsigned char *wbase = smem + wib * knn_warp_bytes(kcap);
+    const int total = *fb_count;
+    for (int w = blockIdx.x * warps + wib; w < total; w += gridDim.x * warps) {
+        knn_bucket<false>(m, a, fb_leaf[w], wbase, kcap, fb_mask[w]);
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Many swarms in one persistent launch.  Every warp takes (swarm, bucket) items from a device
 // counter until none is left and runs the same knn_bucket as the one-swarm kernel, so each swarm's
@@ -1041,6 +1057,9 @@ Status geometry_alloc(Geometry &g, const Model &m, int n) {
     GD_TRY_CUDA(g.sub_lo.alloc(static_cast<size_t>(g.leaf_slots) * kSubs));
     GD_TRY_CUDA(g.sub_hi.alloc(static_cast<size_t>(g.leaf_slots) * kSubs));
     GD_TRY_CUDA(g.counters.alloc(4));
+    GD_TRY_CUDA(g.fb_leaf.alloc(static_cast<size_t>(g.leaf_slots)));
+    GD_TRY_CUDA(g.fb_mask.alloc(static_cast<size_t>(g.leaf_slots)));
+    GD_TRY_CUDA(g.fb_count.alloc(1));
     return Status::ok();
 }
 
@@ -1440,9 +1459,60 @@ int knn_block_warps(int K, const Tuning &tune, int *resident) {
     return best;
 }
 
+Status knn_fallback(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
+                    float *kth_d2, cudaStream_t s, unsigned long long *stats, const Tuning &tune) {
+    const int K = m.n_k;
+    const int kcap = knn_capacity(K, false);
+    int resident = 0;
+    const int warps = knn_block_warps(kcap, tune, &resident);
+    if (warps == 0) return Status{GD_ERR_INVALID_ARGUMENT, "warps per block do not fit in shared memory", 0};
+    const size_t smem = knn_smem_per_warp(kcap) * warps;
+    static int smem_set[64] = {};
+    int dev = 0, sms = 0;
+    GD_TRY_CUDA(cudaGetDevice(&dev));
+    GD_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (dev < 0 || dev >= 64 || smem_set[dev] < static_cast<int>(smem)) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_knn_fallback, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+        if (dev >= 0 && dev < 64) smem_set[dev] = static_cast<int>(smem);
+    }
+    QueryArgs qa;
+    qa.sorted = g.sorted.ptr;
+    qa.lo = g.node_lo.ptr;
+    qa.hi = g.node_hi.ptr;
+    qa.sub_lo = g.sub_lo.ptr;
+    qa.sub_hi = g.sub_hi.ptr;
+    qa.qrad = g.q.ptr;
+    qa.counters = g.counters.ptr;
+    qa.part = dev_particle;
+    qa.leaf_slots = g.leaf_slots;
+    qa.k = K;
+    qa.codes = codes;
+    qa.measure = measure;
+    qa.kth = kth_d2;
+    qa.radius = nullptr;
+    qa.stats = stats;
+    qa.prescan = tune.prescan;
+    qa.bfs = tune.bfs;
+    // one block per SM's worth of resident warps: the list is short (owners whose proposal missed)
+    const int blocks = sms * (resident / warps > 0 ? resident / warps : 1);
+    g.launches += 1;
+    k_knn_fallback<<<blocks, warps * 32, smem, s>>>(m, qa, g.fb_count.ptr, g.fb_leaf.ptr, g.fb_mask.ptr);
+    GD_TRY_CUDA(cudaGetLastError());
+    return Status::ok();
+}
+
 Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
                  float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats, const Tuning &tune) {
     const int K = m.n_k;
+    if (radius && tune.range && knn_range_eligible(m, K)) {
+        // a proposed radius: the warp-per-owner range query (gd_range.cu), its leftovers by the heap query
+        GD_TRY(knn_range(g, m, dev_particle, codes, measure, kth_d2, s, radius, stats, tune));
+        g.launches += 1;
+        k_inactive_rows<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, K, g.active.ptr, codes, measure, kth_d2);
+        GD_TRY_CUDA(cudaGetLastError());
+        return Status::ok();
+    }
     const int kcap = knn_capacity(K, radius != nullptr);
     const size_t per_warp = knn_smem_per_warp(kcap);
     const int warps = knn_block_warps(kcap, tune, nullptr);

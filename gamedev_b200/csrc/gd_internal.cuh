@@ -136,6 +136,10 @@ struct Geometry {
     // and geometry_check reads it later (what stream capture into a CUDA graph needs).
     bool deferred_check = false;
     int sort_bits = 0;  // top Morton key bits the radix sort orders by (0: all)
+    // owners the radius-bounded range query leaves to the heap query: bucket, lanes, count
+    DevBuf<int> fb_leaf;
+    DevBuf<unsigned int> fb_mask;
+    DevBuf<int> fb_count;
 };
 
 // Speed-only settings of the neighbour search (every setting gives the same exact lists).
@@ -144,6 +148,7 @@ struct Tuning {
     int prescan = kPrescan;   // Morton-neighbour buckets scanned on each side before the walk
     int bfs = 1;              // breadth-first walk (1) or depth-first walk (0)
     int sort_bits = 0;        // top Morton key bits the radix sort orders by (0: all)
+    int range = 1;            // radius-bounded query: warp-per-owner range query (1) or per-lane heaps (0)
 };
 
 Status geometry_alloc(Geometry &g, const Model &m, int n);
@@ -163,6 +168,12 @@ Status knn_query(Geometry &g, const Model &m, const gd_particle *dev_particle, i
 // Warps per block of the top-K kernel for K neighbours under `tune` (0 when infeasible), and the
 // resident warps per SM it gives.
 int knn_block_warps(int K, const Tuning &tune, int *resident);
+// The radius-bounded range query (gd_range.cu) and the heap query over its leftover owners.
+bool knn_range_eligible(const Model &m, int K);
+Status knn_range(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
+                 float *kth_d2, cudaStream_t s, const float *radius, unsigned long long *stats, const Tuning &tune);
+Status knn_fallback(Geometry &g, const Model &m, const gd_particle *dev_particle, int32_t *codes, double *measure,
+                    float *kth_d2, cudaStream_t s, unsigned long long *stats, const Tuning &tune);
 // One swarm of a batch as the persistent batch query sees it: its geometry and the offsets of its
 // rows in the caller's concatenated particle (part_off) and code (codes_off) buffers.
 struct BatchSwarm {

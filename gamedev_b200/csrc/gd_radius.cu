@@ -1,6 +1,9 @@
 // Learned search-radius proposal: per-owner features, an 8 -> 64 -> 64 -> 1 GELU network with
 // BF16 weights and FP32 accumulation, its forward / backward / Adam kernels, residual calibration
-// and radius prediction.  The proposal only seeds gd_knn_bounded, whose fallback keeps the
+// and radius prediction.  The network predicts the CHANGE of the log K-th distance since the
+// previous step: the proposal is feature 7 (that previous log distance, raw) plus the network's
+// output, so an untrained network already proposes the previous distance and training only has
+// to learn how it moves (Keplerian shear, drift, growth).  The proposal only seeds gd_knn_bounded, whose fallback keeps the
 // neighbour lists identical to the plain query, so the network never changes a result.
 #include <cuda_bf16.h>
 
@@ -180,6 +183,8 @@ __global__ void k_quantise(const float *params, __nv_bfloat16 *wq) {
 __device__ __forceinline__ float target_of(float kth_d2, double R_0) {
     return static_cast<float>(0.5 * log(static_cast<double>(kth_d2)) - log(R_0));
 }
+// the skip term of the output: the raw previous log K-th distance (feature 7; 0 when unknown)
+__device__ __forceinline__ float base_of(const float *feat, size_t r) { return feat[r * kF + kF - 1]; }
 
 // feature and target moments over rows with a valid target: acc[0..7] sum, [8..15] sum sq,
 // [16] target sum, [17] count
@@ -195,7 +200,7 @@ __global__ void k_stats(const float *__restrict__ feat, const float *__restrict_
             loc[k] += x;
             loc[kF + k] += x * x;
         }
-        loc[16] += target_of(kth[r], R_0);
+        loc[16] += target_of(kth[r], R_0) - base_of(feat, static_cast<size_t>(r));
         loc[17] += 1.0;
     }
     for (int k = 0; k < 18; ++k) atomicAdd(&part[k], loc[k]);
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ p
                                    static_cast<unsigned long long>(n));
     }
     float x[kF] = {};
-    float target = 0.0f;
+    float target = 0.0f, base = 0.0f;
     bool valid = false;
     if (r >= 0) {
         const float d2 = kth[r];
@@ -266,6 +271,7 @@ __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ p
         if (valid) {
             load_x(feat, static_cast<size_t>(r), norm, x);
             target = target_of(d2, R_0);
+            base = base_of(feat, static_cast<size_t>(r));
         }
     }
     float *h1 = sh1 + t * (kH + 1), *d1 = sd1 + t * (kH + 1), *d2 = sd2 + t * (kH + 1), *h2 = sh2 + t * (kH + 1);
@@ -276,7 +282,7 @@ __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ p
         h1[j] = gelu(a);
         d1[j] = gelu_grad(a);  // holds gelu'(a1) until the backward pass
     }
-    float y = sw[oB3];
+    float y = sw[oB3] + base;
     for (int o = 0; o < kH; ++o) {
         float a = sw[oB2 + o];
         for (int j = 0; j < kH; ++j) a = fmaf(sw[oW2 + o * kH + j], h1[j], a);
@@ -481,7 +487,11 @@ __global__ void __launch_bounds__(kTcRows, 4) k_mlp_tc(const float *__restrict__
         float x[kF];
 #pragma unroll
         for (int k = 0; k < kF; ++k) x[k] = 0.0f;
-        if (r < n) load_x(feat, static_cast<size_t>(r), norm, x);
+        float base = 0.0f;
+        if (r < n) {
+            load_x(feat, static_cast<size_t>(r), norm, x);
+            base = base_of(feat, static_cast<size_t>(r));
+        }
 #pragma unroll 1
         for (int kc = 0; kc < kH / 8; ++kc) {
             uint32_t ph[4], pl[4];
@@ -528,7 +538,7 @@ __global__ void __launch_bounds__(kTcRows, 4) k_mlp_tc(const float *__restrict__
         tc_fence_after();
         uint32_t acc[kTcCols];
         tc_load64(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
-        float y = b3;
+        float y = b3 + base;
 #pragma unroll
         for (int o = 0; o < kH; ++o) y = fmaf(w3[o], gelu(__uint_as_float(acc[o]) + b2[o]), y);
         if (r < n) {

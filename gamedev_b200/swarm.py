@@ -509,7 +509,7 @@ class SwarmBatch:
         return t[int(self.part_off[s]):int(self.part_off[s + 1])]
 
     def set_tuning(self, warps_per_block=0, prescan=2, walk_breadth_first=1, sort_bits=0):
-        t = _lib.GdTuning(warps_per_block, prescan, walk_breadth_first, sort_bits)
+        t = _lib.GdTuning(warps_per_block, prescan, walk_breadth_first, sort_bits, 1)
         self._check(self.lib.gd_batch_set_tuning(self.h, C.byref(t)))
 
     def launch_count(self) -> int:

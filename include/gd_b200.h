@@ -162,9 +162,14 @@ gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const fl
  *   prescan             Morton-neighbour buckets scanned on each side before the tree walk (0..8)
  *   walk_breadth_first  1: breadth-first walk with a pipelined leaf list; 0: depth-first walk
  *   sort_bits           top Morton key bits the index sort orders by: 0 (all, 21 per axis) or
- *                       16..21 per axis (fewer radix passes, coarser buckets) */
+ *                       16..21 per axis (fewer radix passes, coarser buckets)
+ *   range_query         radius-bounded query (gd_knn_bounded) only: 1 (default) serves each owner
+ *                       with a whole warp, collecting the sites inside min(q, r) and sorting them
+ *                       with a warp-wide network, the owners it cannot serve going to the per-lane
+ *                       heap query; 0: the per-lane heap query for every owner.  Used for K <= 64
+ *                       outside wedges; elsewhere the heap query runs either way. */
 typedef struct gd_tuning {
-    int warps_per_block, prescan, walk_breadth_first, sort_bits;
+    int warps_per_block, prescan, walk_breadth_first, sort_bits, range_query;
 } gd_tuning;
 gd_status gd_get_tuning(const gd_handle *h, gd_tuning *out);
 gd_status gd_set_tuning(gd_handle *h, const gd_tuning *t);

@@ -3,8 +3,10 @@ the device uses).  TEST INFRASTRUCTURE ONLY: the checker for the device forward 
 kernels; the library never calls it.
 
 Layout of the 4801 parameters: W1 [64][8], b1 [64], W2 [64][64] (row = output unit), b2 [64],
-W3 [64], b3.  Inputs are standardised with the model's (mean, 1/scale); loss is the mean over all
-rows of (y - t)^2 with t = log(sqrt(kth_d2)/R_0) and rows with kth_d2 <= 0 contributing zero.
+W3 [64], b3.  Inputs are standardised with the model's (mean, 1/scale).  The output is the raw
+feature 7 (the previous step's log K-th distance) plus the network, y = f7 + net(x); loss is the
+mean over all rows of (y - t)^2 with t = log(sqrt(kth_d2)/R_0) and rows with kth_d2 <= 0
+contributing zero.
 """
 
 from __future__ import annotations
@@ -62,7 +64,8 @@ def loss_and_grad(params, norm, features, kth_d2, R_0):
     h1 = gelu(a1)
     a2 = h1 @ W2.T + b2
     h2 = gelu(a2)
-    y = h2 @ W3 + b3
+    base = np.where(valid, features[:, F - 1].astype(np.float64), 0.0)
+    y = h2 @ W3 + b3 + base
     err = np.where(valid, y - t, 0.0)
     loss = float((err ** 2).sum() / n)
     dy = 2.0 * err / n
@@ -81,4 +84,4 @@ def loss_and_grad(params, norm, features, kth_d2, R_0):
 def predict_log(params, norm, features):
     W1, b1, W2, b2, W3, b3 = unpack(params)
     x = (features.astype(np.float64) - norm[:F]) * norm[F:2 * F]
-    return gelu(gelu(x @ W1.T + b1) @ W2.T + b2) @ W3 + b3
+    return gelu(gelu(x @ W1.T + b1) @ W2.T + b2) @ W3 + b3 + features[:, F - 1].astype(np.float64)
