@@ -2,8 +2,10 @@
 // BF16 weights and FP32 accumulation, its forward / backward / Adam kernels, residual calibration
 // and radius prediction.  The network predicts the CHANGE of the log K-th distance since the
 // previous step: the proposal is feature 7 (that previous log distance, raw) plus the network's
-// output, so an untrained network already proposes the previous distance and training only has
-// to learn how it moves (Keplerian shear, drift, growth).  The proposal only seeds gd_knn_bounded, whose fallback keeps the
+// output.  Its output layer starts at zero, so an untrained network proposes the previous distance
+// itself.  It is trained with the pinball loss of the kQuantile quantile, so it learns an upper
+// bound per owner (how far that owner's K-th distance can move, which the local shear sets) rather
+// than the mean; calibration then adds one global margin for the 0.999 coverage.  The proposal only seeds gd_knn_bounded, whose fallback keeps the
 // neighbour lists identical to the plain query, so the network never changes a result.
 #include <cuda_bf16.h>
 
@@ -29,6 +31,7 @@ constexpr int oW3 = oB2 + kH;           // [kH]
 constexpr int oB3 = oW3 + kH;           // scalar
 static_assert(oB3 + 1 == kNP, "parameter layout");
 constexpr int kTile = 128;              // samples per training block
+constexpr float kQuantile = 0.99f;      // the quantile the pinball loss trains for
 constexpr int kHistBins = 8192;
 constexpr float kHistLo = -4.0f, kHistHi = 4.0f;
 // Morton levels of the occupancy features: cells of 2^-9, 2^-12 and 2^-15 of the root cube
@@ -161,7 +164,7 @@ __global__ void k_init_params(float *params, float *m1, float *m2, float *grad, 
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kNP) return;
     float v = 0.0f;
-    if (is_weight(p)) {
+    if (is_weight(p) && p < oW3) {  // the output layer W3 starts at zero
         const int fan_in = (p < oB1) ? kF : kH;
         // Box-Muller normal from two hashed uniforms, He-style scale
         const unsigned long long a = mix64(seed * 0x100000001b3ull + 2ull * p), b = mix64(a + 1ull);
@@ -235,7 +238,7 @@ __device__ __forceinline__ void load_x(const float *feat, size_t r, const float 
 }
 
 // Forward and backward of one tile of rows; accumulates the summed gradient of
-// (1/norm_count) * sum (y - t)^2 into grad and the summed squared error into acc[0].
+// (1/norm_count) * sum pinball(y - t) into grad and the summed pinball loss into acc[0].
 // rows: sample_mode 0 -> rows base..base+kTile-1 (bounded by n); 1 -> hashed uniform draws.
 __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ params, const __nv_bfloat16 *__restrict__ wq,
                                                      const float *__restrict__ norm, const float *__restrict__ feat,
@@ -291,8 +294,10 @@ __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ p
         d2[o] = gelu_grad(a);
         y = fmaf(sw[oW3 + o], g, y);
     }
+    // pinball loss of the kQuantile quantile: tau * (t - y) above the output, (1 - tau) * (y - t) below
     const float err = valid ? (y - target) : 0.0f;
-    const float dy = 2.0f * err * scale;
+    const float dy = valid ? (err >= 0.0f ? (1.0f - kQuantile) : -kQuantile) * scale : 0.0f;
+    const float pin = valid ? (err >= 0.0f ? (1.0f - kQuantile) * err : -kQuantile * err) : 0.0f;
     sdy[t] = dy;
     for (int o = 0; o < kH; ++o) d2[o] *= dy * sw[oW3 + o];
     for (int j = 0; j < kH; ++j) {
@@ -302,8 +307,8 @@ __global__ void __launch_bounds__(kTile) k_grad_tile(const float *__restrict__ p
     }
 #pragma unroll
     for (int k = 0; k < kF; ++k) sx[t * kF + k] = x[k];
-    // squared-error sum of the tile
-    float e2 = err * err;
+    // pinball-loss sum of the tile
+    float e2 = pin;
 #pragma unroll
     for (int off = 16; off; off >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, off);
     if ((t & 31) == 0) atomicAdd(&acc[0], static_cast<double>(e2));

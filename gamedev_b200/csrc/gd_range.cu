@@ -152,57 +152,70 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
     const float3 qp = make_float3(me.x, me.y, me.z);
     long long st_groups = 0, st_nodes = 0, st_cand = 0;
 
-    // 1. the bucket's union leaf list (breadth-first; the same conservative union box as the heap
-    //    query's walk, exact per-lane tests at the leaves)
-    bool list_ok = true;
-    int nleaf = 0;
-    {
-        const float rr = valid ? sqrtf(cut) * 1.0001f + (fabsf(qp.x) + fabsf(qp.y) + fabsf(qp.z)) * 1.0e-6f : 0.f;
-        float ulx = valid ? qp.x - rr : CUDART_INF_F_, uly = valid ? qp.y - rr : CUDART_INF_F_,
-              ulz = valid ? qp.z - rr : CUDART_INF_F_;
-        float uhx = valid ? qp.x + rr : -CUDART_INF_F_, uhy = valid ? qp.y + rr : -CUDART_INF_F_,
-              uhz = valid ? qp.z + rr : -CUDART_INF_F_;
+    // 1. Leaf lists by a breadth-first walk: internal boxes against an axis-aligned box around the
+    //    balls (the heap query's conservative inflation), leaf boxes exactly against each ball.
+    //    single < 0: the union of the 32 lanes' balls; single = o: owner o's ball of squared radius
+    //    sbound alone.  Returns the number of leaves written to out (at most cap), or -1 when a
+    //    level or the list outgrows its buffer.
+    const int levels = 31 - __clz(a.leaf_slots);
+    const int first_leaf = a.leaf_slots - 1;
+    auto walk = [&](int single, float sbound, int *out, int cap) -> int {
+        const float3 sq = single < 0 ? qp
+                                     : make_float3(__shfl_sync(0xffffffffu, qp.x, single),
+                                                   __shfl_sync(0xffffffffu, qp.y, single),
+                                                   __shfl_sync(0xffffffffu, qp.z, single));
+        const float scut = single < 0 ? cut : sbound;
+        const bool in_box = single < 0 ? valid : true;
+        const float rr = in_box ? sqrtf(scut) * 1.0001f + (fabsf(sq.x) + fabsf(sq.y) + fabsf(sq.z)) * 1.0e-6f : 0.f;
+        float ulx = in_box ? sq.x - rr : CUDART_INF_F_, uly = in_box ? sq.y - rr : CUDART_INF_F_,
+              ulz = in_box ? sq.z - rr : CUDART_INF_F_;
+        float uhx = in_box ? sq.x + rr : -CUDART_INF_F_, uhy = in_box ? sq.y + rr : -CUDART_INF_F_,
+              uhz = in_box ? sq.z + rr : -CUDART_INF_F_;
+        if (single < 0) {
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            ulx = fminf(ulx, __shfl_xor_sync(0xffffffffu, ulx, off));
-            uly = fminf(uly, __shfl_xor_sync(0xffffffffu, uly, off));
-            ulz = fminf(ulz, __shfl_xor_sync(0xffffffffu, ulz, off));
-            uhx = fmaxf(uhx, __shfl_xor_sync(0xffffffffu, uhx, off));
-            uhy = fmaxf(uhy, __shfl_xor_sync(0xffffffffu, uhy, off));
-            uhz = fmaxf(uhz, __shfl_xor_sync(0xffffffffu, uhz, off));
+            for (int off = 16; off > 0; off >>= 1) {
+                ulx = fminf(ulx, __shfl_xor_sync(0xffffffffu, ulx, off));
+                uly = fminf(uly, __shfl_xor_sync(0xffffffffu, uly, off));
+                ulz = fminf(ulz, __shfl_xor_sync(0xffffffffu, ulz, off));
+                uhx = fmaxf(uhx, __shfl_xor_sync(0xffffffffu, uhx, off));
+                uhy = fmaxf(uhy, __shfl_xor_sync(0xffffffffu, uhy, off));
+                uhz = fmaxf(uhz, __shfl_xor_sync(0xffffffffu, uhz, off));
+            }
         }
         auto overlaps = [&](const float4 &l, const float4 &h) {
             return l.x <= uhx && h.x >= ulx && l.y <= uhy && h.y >= uly && l.z <= uhz && h.z >= ulz;
         };
-        const int levels = 31 - __clz(a.leaf_slots);
-        const int first_leaf = a.leaf_slots - 1;
         if (levels == 0) {
-            sh.list[0] = 0;
-            nleaf = 1;
-        } else {
-            int fr[kRangeFrontier / 32];
-            fr[0] = 0;
-            int nf = 1;
-            for (int d = 0; d < levels && list_ok; ++d) {
-                const bool to_leaves = (d + 1 == levels);
-                int nnext = 0;
+            out[0] = 0;
+            return 1;
+        }
+        int fr[kRangeFrontier / 32];
+        fr[0] = 0;
+        int nf = 1, nl = 0;
+        for (int d = 0; d < levels; ++d) {
+            const bool to_leaves = (d + 1 == levels);
+            int nnext = 0;
 #pragma unroll
-                for (int r = 0; r < kRangeFrontier / 32; ++r) {
-                    if (r * 32 >= nf) break;
-                    const bool has = r * 32 + lane < nf;
-                    const int node = has ? fr[r] : 0;
-                    const int c0 = 2 * node + 1, c1 = c0 + 1;
-                    float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), h0 = l0, l1 = l0, h1 = l0;
-                    if (has) {
-                        l0 = a.lo[c0];
-                        h0 = a.hi[c0];
-                        l1 = a.lo[c1];
-                        h1 = a.hi[c1];
-                    }
-                    st_nodes += has ? 2 : 0;
-                    bool p0 = has && overlaps(l0, h0);
-                    bool p1 = has && overlaps(l1, h1);
-                    if (to_leaves && __any_sync(0xffffffffu, p0 || p1)) {
+            for (int r = 0; r < kRangeFrontier / 32; ++r) {
+                if (r * 32 >= nf) break;
+                const bool has = r * 32 + lane < nf;
+                const int node = has ? fr[r] : 0;
+                const int c0 = 2 * node + 1, c1 = c0 + 1;
+                float4 l0 = make_float4(0.f, 0.f, 0.f, 0.f), h0 = l0, l1 = l0, h1 = l0;
+                if (has) {
+                    l0 = a.lo[c0];
+                    h0 = a.hi[c0];
+                    l1 = a.lo[c1];
+                    h1 = a.hi[c1];
+                }
+                st_nodes += has ? 2 : 0;
+                bool p0 = has && overlaps(l0, h0);
+                bool p1 = has && overlaps(l1, h1);
+                if (to_leaves) {
+                    if (single >= 0) {
+                        p0 = p0 && box_dist2(sq, l0, h0) <= scut;
+                        p1 = p1 && box_dist2(sq, l1, h1) <= scut;
+                    } else if (__any_sync(0xffffffffu, p0 || p1)) {
                         // exact: some lane's own ball reaches the leaf box
                         bool e0 = false, e1 = false;
                         for (int o = 0; o < 32; ++o) {
@@ -216,110 +229,148 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
                         p0 = e0;
                         p1 = e1;
                     }
-                    const unsigned int b0 = __ballot_sync(0xffffffffu, p0), b1 = __ballot_sync(0xffffffffu, p1);
-                    const int tot = __popc(b0) + __popc(b1);
-                    int kk = __popc(b0 & lt) + __popc(b1 & lt);
-                    if (to_leaves) {
-                        if (nleaf + tot > kRangeList) {
-                            list_ok = false;
-                            break;
-                        }
-                        kk += nleaf;
-                        if (p0) sh.list[kk++] = c0 - first_leaf;
-                        if (p1) sh.list[kk] = c1 - first_leaf;
-                        nleaf += tot;
-                    } else {
-                        if (nnext + tot > kRangeFrontier) {
-                            list_ok = false;
-                            break;
-                        }
-                        kk += nnext;
-                        if (p0) sh.frontier[kk++] = c0;
-                        if (p1) sh.frontier[kk] = c1;
-                        nnext += tot;
-                    }
                 }
-                __syncwarp();
-                if (!to_leaves && list_ok) {
-#pragma unroll
-                    for (int r = 0; r < kRangeFrontier / 32; ++r)
-                        if (r * 32 + lane < nnext) fr[r] = sh.frontier[r * 32 + lane];
-                    nf = nnext;
-                    __syncwarp();
-                    if (nf == 0) break;
+                const unsigned int b0 = __ballot_sync(0xffffffffu, p0), b1 = __ballot_sync(0xffffffffu, p1);
+                const int tot = __popc(b0) + __popc(b1);
+                int kk = __popc(b0 & lt) + __popc(b1 & lt);
+                if (to_leaves) {
+                    if (nl + tot > cap) return -1;
+                    kk += nl;
+                    if (p0) out[kk++] = c0 - first_leaf;
+                    if (p1) out[kk] = c1 - first_leaf;
+                    nl += tot;
+                } else {
+                    if (nnext + tot > kRangeFrontier) return -1;
+                    kk += nnext;
+                    if (p0) sh.frontier[kk++] = c0;
+                    if (p1) sh.frontier[kk] = c1;
+                    nnext += tot;
                 }
             }
+            __syncwarp();
+            if (!to_leaves) {
+#pragma unroll
+                for (int r = 0; r < kRangeFrontier / 32; ++r)
+                    if (r * 32 + lane < nnext) fr[r] = sh.frontier[r * 32 + lane];
+                nf = nnext;
+                __syncwarp();
+                if (nf == 0) break;
+            }
         }
-    }
+        return nl;
+    };
+    // the bucket's union list, walked once for all 32 owners; when the bucket's sites lie far apart
+    // (a jump of the Morton curve) the union outgrows the buffers and each owner walks alone
+    const int union_leaves = walk(-1, 0.0f, sh.list, kRangeList);
+    const bool list_ok = union_leaves >= 0;
+    const int nleaf = list_ok ? union_leaves : 0;
+    __syncwarp();
 
     // 2-3. owner by owner
     const unsigned int valid_mask = __ballot_sync(0xffffffffu, valid);
-    unsigned int fb_mask = list_ok ? 0u : valid_mask;  // lanes left to the heap query
-    const int first_leaf_node = a.leaf_slots - 1;
-    for (unsigned int todo = list_ok ? valid_mask : 0u; todo; todo &= todo - 1) {
+    unsigned int fb_mask = 0u;  // lanes left to the heap query
+    for (unsigned int todo = valid_mask; todo; todo &= todo - 1) {
         const int o = __ffs(todo) - 1;
         const float oc = __shfl_sync(0xffffffffu, cut, o);
         const float oq2 = __shfl_sync(0xffffffffu, q2, o);
         const int oidx = __shfl_sync(0xffffffffu, idx, o);
         const float3 oq = make_float3(__shfl_sync(0xffffffffu, qp.x, o), __shfl_sync(0xffffffffu, qp.y, o),
                                       __shfl_sync(0xffffffffu, qp.z, o));
-        bool overflow = false;
-        // leaves of the union list the owner's ball reaches
-        int nown = 0;
-        for (int b = 0; b < nleaf; b += 32) {
-            const bool has = b + lane < nleaf;
-            const int lf = has ? sh.list[b + lane] : 0;
-            bool pass = false;
-            if (has) pass = box_dist2(oq, a.lo[first_leaf_node + lf], a.hi[first_leaf_node + lf]) <= oc;
-            const unsigned int bal = __ballot_sync(0xffffffffu, pass);
-            if (nown + __popc(bal) > kOwnLeaves) {
-                overflow = true;
-                break;
-            }
-            if (pass) sh.own_leaves[nown + __popc(bal & lt)] = lf;
-            nown += __popc(bal);
-        }
-        __syncwarp();
-        // their 8-site groups the ball reaches: eight leaves per pass, a lane per sub-box
         int ngroup = 0;
-        for (int b = 0; b < nown && !overflow; b += 8) {
-            const int li = b + (lane >> 2);
-            const bool has = li < nown;
-            const int g = has ? sh.own_leaves[li] * kSubs + (lane & 3) : 0;
-            const bool pass = has && box_dist2(oq, a.sub_lo[g], a.sub_hi[g]) <= oc;
-            const unsigned int bal = __ballot_sync(0xffffffffu, pass);
-            if (ngroup + __popc(bal) > kOwnGroups) {
-                overflow = true;
-                break;
+        // The leaves (into own_leaves) and then the 8-site groups (into own_groups) the owner's ball
+        // of squared radius `bound` reaches: from the bucket's union list when the first bound is
+        // the one that list was walked with, else by a walk of the owner's own.  False when a list
+        // outgrows its buffer.
+        auto gather = [&](float bound, bool from_union) -> bool {
+            int nown = 0;
+            if (from_union) {
+                for (int b = 0; b < nleaf; b += 32) {
+                    const bool has = b + lane < nleaf;
+                    const int lf = has ? sh.list[b + lane] : 0;
+                    const bool pass = has && box_dist2(oq, a.lo[first_leaf + lf], a.hi[first_leaf + lf]) <= bound;
+                    const unsigned int bal = __ballot_sync(0xffffffffu, pass);
+                    if (nown + __popc(bal) > kOwnLeaves) return false;
+                    if (pass) sh.own_leaves[nown + __popc(bal & lt)] = lf;
+                    nown += __popc(bal);
+                }
+            } else {
+                nown = walk(o, bound, sh.own_leaves, kOwnLeaves);
+                if (nown < 0) return false;
             }
-            if (pass) sh.own_groups[ngroup + __popc(bal & lt)] = g;
-            ngroup += __popc(bal);
-        }
-        __syncwarp();
-        // the groups' sites, four groups (32 sites) per pass: candidates inside the ball
-        int count = 0;
-        for (int b = 0; b < ngroup && !overflow; b += 4) {
-            const int gi = b + (lane >> 3);
-            bool in = false;
-            unsigned long long key = 0;
-            if (gi < ngroup) {
-                const float4 p = a.sorted[sh.own_groups[gi] * kSub + (lane & 7)];  // padding sites lie at +inf
-                const float d2 = dist2(oq, make_float3(p.x, p.y, p.z));
-                in = d2 <= oc;
-                key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                      static_cast<unsigned int>(__float_as_int(p.w));
+            __syncwarp();
+            // eight leaves per pass, a lane per sub-box
+            ngroup = 0;
+            for (int b = 0; b < nown; b += 8) {
+                const int li = b + (lane >> 2);
+                const bool has = li < nown;
+                const int g = has ? sh.own_leaves[li] * kSubs + (lane & 3) : 0;
+                const bool pass = has && box_dist2(oq, a.sub_lo[g], a.sub_hi[g]) <= bound;
+                const unsigned int bal = __ballot_sync(0xffffffffu, pass);
+                if (ngroup + __popc(bal) > kOwnGroups) return false;
+                if (pass) sh.own_groups[ngroup + __popc(bal & lt)] = g;
+                ngroup += __popc(bal);
             }
-            const unsigned int bal = __ballot_sync(0xffffffffu, in);
-            const int pos = count + __popc(bal & lt);
-            if (in && pos < kRangeCap) sh.cand[pos] = key;
-            count += __popc(bal);
+            __syncwarp();
+            return true;
+        };
+        // the groups' sites, four groups (32 sites) per pass: candidates with d^2 <= bound
+        auto collect = [&](float bound) {
+            int cnt = 0;
+            for (int b = 0; b < ngroup; b += 4) {
+                const int gi = b + (lane >> 3);
+                bool in = false;
+                unsigned long long key = 0;
+                if (gi < ngroup) {
+                    const float4 p = a.sorted[sh.own_groups[gi] * kSub + (lane & 7)];  // padding sites lie at +inf
+                    const float d2 = dist2(oq, make_float3(p.x, p.y, p.z));
+                    in = d2 <= bound;
+                    key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                          static_cast<unsigned int>(__float_as_int(p.w));
+                }
+                const unsigned int bal = __ballot_sync(0xffffffffu, in);
+                const int pos = cnt + __popc(bal & lt);
+                if (in && pos < kRangeCap) sh.cand[pos] = key;
+                cnt += __popc(bal);
+            }
+            __syncwarp();
+            st_groups += ngroup;
+            st_cand += cnt;
+            return cnt;
+        };
+        // More candidates than the network holds: the K-th smallest d^2 among the first kRangeCap
+        // collected is a bound that at least K sites meet, so the true K nearest lie inside it;
+        // rescan with it (a few rounds at most).
+        auto shrink = [&](int cnt) {
+            for (int round = 0; round < 3 && cnt > kRangeCap; ++round) {
+                unsigned long long v[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) v[j] = sh.cand[j * 32 + lane];
+                __syncwarp();
+                warp_bitonic<4>(v, lane);
+                const int e = K - 1;
+                unsigned long long sel = v[0];
+#pragma unroll
+                for (int j = 1; j < 4; ++j)
+                    if (j == (e >> 5)) sel = v[j];
+                const float bound =
+                    __uint_as_float(static_cast<unsigned int>(__shfl_sync(0xffffffffu, sel, e & 31) >> 32));
+                cnt = collect(bound);
+            }
+            return cnt;
+        };
+        float bound = oc;
+        bool ok = gather(bound, list_ok);
+        int count = ok ? shrink(collect(bound)) : 0;
+        if (ok && count < K && bound < oq2) {
+            // fewer than K inside a proposal below q: a short proposal, or an owner whose row is not
+            // full even at q (a sparse region).  Search the whole q ball, which the range query can
+            // hold when the region is sparse.
+            bound = oq2;
+            ok = gather(bound, false);
+            count = ok ? shrink(collect(bound)) : 0;
         }
-        st_groups += ngroup;
-        st_cand += count;
-        // fewer than K inside a radius below q (the rows beyond it are unknown here), or more than
-        // the network holds: the heap query takes this owner
-        if (overflow || count > kRangeCap || (count < K && oc < oq2)) {
-            fb_mask |= 1u << o;  // warp-uniform
+        if (!ok || count > kRangeCap) {
+            fb_mask |= 1u << o;  // warp-uniform: the heap query takes this owner
             __syncwarp();
             continue;
         }
@@ -328,7 +379,7 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
         float kth;
         // up to kTrim candidates above 64: drop the largest one at a time, then a 64-key network
         int len = count;
-        if (len > 64 && len <= 64 + kTrim && K <= 64) {
+        if (len > 64 && len <= 64 + kTrim) {
             for (; len > 64; --len) {
                 unsigned long long best = 0;
                 int where = -1;

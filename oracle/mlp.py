@@ -5,8 +5,9 @@ kernels; the library never calls it.
 Layout of the 4801 parameters: W1 [64][8], b1 [64], W2 [64][64] (row = output unit), b2 [64],
 W3 [64], b3.  Inputs are standardised with the model's (mean, 1/scale).  The output is the raw
 feature 7 (the previous step's log K-th distance) plus the network, y = f7 + net(x); loss is the
-mean over all rows of (y - t)^2 with t = log(sqrt(kth_d2)/R_0) and rows with kth_d2 <= 0
-contributing zero.
+mean over all rows of the pinball loss of the 0.99 quantile, tau (t - y) for t > y and
+(1 - tau)(y - t) otherwise, with t = log(sqrt(kth_d2)/R_0) and rows with kth_d2 <= 0 contributing
+zero.
 """
 
 from __future__ import annotations
@@ -16,6 +17,7 @@ import math
 import numpy as np
 
 F, H = 8, 64
+TAU = np.float64(np.float32(0.99))  # the quantile of the pinball loss (a float32 constant on the device)
 OW1, OB1 = 0, 512
 OW2, OB2 = 576, 576 + 4096
 OW3, OB3 = OB2 + 64, OB2 + 128
@@ -67,8 +69,9 @@ def loss_and_grad(params, norm, features, kth_d2, R_0):
     base = np.where(valid, features[:, F - 1].astype(np.float64), 0.0)
     y = h2 @ W3 + b3 + base
     err = np.where(valid, y - t, 0.0)
-    loss = float((err ** 2).sum() / n)
-    dy = 2.0 * err / n
+    above = err >= 0.0
+    loss = float(np.where(above, (1.0 - TAU) * err, -TAU * err).sum() / n)
+    dy = np.where(valid, np.where(above, 1.0 - TAU, -TAU), 0.0) / n
     g = np.zeros(len(params))
     g[OW3:OB3] = h2.T @ dy
     g[OB3] = dy.sum()

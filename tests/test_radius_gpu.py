@@ -1,7 +1,8 @@
 """Learned search-radius proposal on the GPU, checked against the CPU oracle (oracle/mlp.py).
 
 Bars:
-  * gradient of the device backward kernel vs the float64 oracle on the same BF16 weights:
+  * gradient of the device backward kernel (pinball loss of the 0.99 quantile) vs the float64
+    oracle on the same BF16 weights, after a few training steps:
     |g_dev - g_ref| <= 2e-3 * max|g_ref| per parameter block (FP32 accumulation over 4096 rows);
   * device forward (hidden layer on the tensor cores, activations split into BF16 hi + lo) vs
     oracle: log-radius within 1e-4 absolute;
@@ -46,6 +47,8 @@ def test_radius_gradient_matches_oracle(gd, cuda):
     f = feats[:rows].contiguous()
     k = kth[:rows].contiguous()
     model = gd.RadiusModel(cfg.R_0, seed=11)
+    # the output layer starts at zero (the hidden layers then get no gradient): train a little first
+    model.train(feats, kth, iterations=30, batch=4096, lr=3e-3)
     g, loss = model.gradient(f, k)
     torch.cuda.synchronize()
     params, norm = model.get()
@@ -139,12 +142,14 @@ def test_learned_radius_is_exact_and_scans_less(gd, cuda):
     """Online training over drifted steps, calibration, then a radius-bounded query: identical
     neighbour lists to the plain query, few fallbacks, and fewer candidate offers than both the
     plain walk and the method without the network, which proposes the previous step's K-th
-    distance times a margin calibrated the same way (the 0.999 quantile of its one-step change)."""
+    distance times a margin calibrated the same way (the 0.999 quantile of its one-step change).
+    At 2^20 owners every q-ball of the c3 disk holds more than K sites (no row is short), the
+    regime of the benchmark."""
     import torch
 
     from gamedev_b200 import workloads
 
-    n = 1 << 18
+    n = 1 << 20
     cfg, p, sw, dp, codes, kth, mass = _swarm(gd, n=n)
     model = gd.RadiusModel(cfg.R_0, seed=7)
     dt = 0.02 * workloads.orbital_time()
@@ -177,8 +182,8 @@ def test_learned_radius_is_exact_and_scans_less(gd, cuda):
     assert fallbacks <= 0.01 * n, (fallbacks, margin)
     offers = {name: int(v[2].item()) for name, v in st.items()}
     groups = {name: int(v[0].item()) for name, v in st.items()}
-    # what the trained network buys over the plain walk: fewer heap offers, no more leaf groups
+    # what the trained network buys over the plain walk: fewer candidates offered
     assert offers["learned"] < 0.9 * offers["plain"], offers
-    assert groups["learned"] <= groups["plain"], groups
-    # and over the method without it: fewer offers than the previous distance alone
+    # and over the method without it (the same bounded kernel): fewer candidates, no more groups
     assert offers["learned"] < offers["previous"], (offers, margin, heur_margin)
+    assert groups["learned"] <= groups["previous"], (groups, margin, heur_margin)

@@ -6,8 +6,9 @@ Bar: for every proposal below, the rows, the FP64 measures and the K-th d^2 equa
 bit for bit, with the range query on and off.  Proposals cover the cases the kernel branches on:
   * near the true K-th distance (the common case: a little more than K sites inside);
   * exactly the K-th distance (float rounding of r*r can leave K - 1 inside: a fallback);
-  * shorter (fewer than K inside: fallbacks) and much longer (more than the 128 candidates an owner
-    may hold: fallbacks);
+  * shorter (fewer than K inside: the whole q ball is searched, or the heap query takes the owner
+    when that ball is too large) and much longer (more than the 128 candidates an owner may hold: the
+    K-th nearest of the first 128 bounds a rescan);
   * r >= q, r = 0, r = inf, NaN and negative r (the bound falls back to q, or to nothing);
 on 3D, 2D and radial-only shapes, odd and small K, and a swarm of a single bucket.
 """
@@ -85,16 +86,16 @@ def test_range_query_equals_plain_rows(gd, cuda, workload, n, K):
         assert torch.equal(codes, c), (workload, K, rq, int((codes != c).any(dim=1).sum().item()))
         assert torch.equal(measure.view(torch.int64), m.view(torch.int64)), (workload, K, rq)
         assert torch.equal(kth.view(torch.int32), k.view(torch.int32)), (workload, K, rq)
-        assert int(st[3].item()) > 0  # the proposal kinds above force some fallbacks
     sw.close()
 
 
 def test_range_query_serves_good_proposals_without_fallback(gd, cuda):
     """With proposals a few per cent above the true K-th distance every owner is served by the range
-    query itself: no fallback, and about K candidates collected per owner."""
+    query itself: no fallback, and about K candidates collected per owner.  (At 2^20 owners every
+    q-ball of the c3 disk holds more than K sites, so no row is short.)"""
     import torch
 
-    n, K = 1 << 18, 64
+    n, K = 1 << 20, 64
     cfg, sw, dp, codes, measure, kth = _setup(gd, "c3_learned_3d", n, K)
     site4, q, active = sw.get_sites()
     radius = (kth.double().sqrt() * 1.02).float()
@@ -106,4 +107,30 @@ def test_range_query_serves_good_proposals_without_fallback(gd, cuda):
     assert int(st[3].item()) <= incomplete + n_act // 1000, (int(st[3].item()), incomplete)
     cand = int(st[2].item()) / n_act
     assert K <= cand < 1.3 * K, cand
+    sw.close()
+
+
+def test_range_query_hands_large_balls_to_the_heap_query(gd, cuda):
+    """A search radius q four times the default makes every q ball hold thousands of sites: owners
+    with short proposals then outgrow the range query's lists and go to the per-lane heap query.
+    Rows stay identical to the plain query's."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n, K = 1 << 18, 64
+    cfg = workloads.config("c3_learned_3d")
+    cfg.h_search = 4.0
+    p = workloads.particles("c3_learned_3d", n=n, seed=9)
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = sw.knn(dp)
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    u = torch.rand(n, device="cuda", generator=gen, dtype=torch.float64)
+    radius = (kth.double().sqrt() * torch.where(u < 0.5, 0.3 + 0.5 * u, 1.0 + 0.02 * u)).float()
+    c, m, k, st = _bounded(sw, dp, radius, codes, 1)
+    assert torch.equal(codes, c)
+    assert torch.equal(measure.view(torch.int64), m.view(torch.int64))
+    assert torch.equal(kth.view(torch.int32), k.view(torch.int32))
+    assert int(st[3].item()) > 0
     sw.close()
