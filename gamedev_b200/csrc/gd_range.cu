@@ -38,8 +38,8 @@ constexpr int kRangeWarps = 4;       // warps per block
 constexpr int kRangeCap = 128;       // candidates an owner may hold (the 128-key network)
 constexpr int kRangeFrontier = 128;  // internal nodes of one breadth-first level
 constexpr int kRangeList = 256;      // leaves of the bucket's union list
-constexpr int kOwnLeaves = 64;       // leaves of the union list an owner's ball reaches
-constexpr int kOwnGroups = 128;      // 8-site groups an owner's ball reaches
+constexpr int kOwnLeaves = 128;      // leaves an owner's ball reaches
+constexpr int kOwnGroups = 256;      // 8-site groups an owner's ball reaches
 constexpr int kTrim = 8;             // up to this many candidates above 64 are dropped one by one
 
 struct RangeShared {
@@ -125,7 +125,7 @@ struct RangeArgs {
     unsigned int *fb_mask;      // and which lanes
 };
 
-__global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeArgs a) {
+__global__ void __launch_bounds__(kRangeWarps * 32, 8) k_knn_range(Model m, RangeArgs a) {
     __shared__ RangeShared sh_all[kRangeWarps];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     RangeShared &sh = sh_all[wib];
@@ -211,24 +211,11 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
                 st_nodes += has ? 2 : 0;
                 bool p0 = has && overlaps(l0, h0);
                 bool p1 = has && overlaps(l1, h1);
-                if (to_leaves) {
-                    if (single >= 0) {
-                        p0 = p0 && box_dist2(sq, l0, h0) <= scut;
-                        p1 = p1 && box_dist2(sq, l1, h1) <= scut;
-                    } else if (__any_sync(0xffffffffu, p0 || p1)) {
-                        // exact: some lane's own ball reaches the leaf box
-                        bool e0 = false, e1 = false;
-                        for (int o = 0; o < 32; ++o) {
-                            const float oc = __shfl_sync(0xffffffffu, cut, o);
-                            const float3 oq = make_float3(__shfl_sync(0xffffffffu, qp.x, o),
-                                                          __shfl_sync(0xffffffffu, qp.y, o),
-                                                          __shfl_sync(0xffffffffu, qp.z, o));
-                            e0 = e0 || (p0 && box_dist2(oq, l0, h0) <= oc);
-                            e1 = e1 || (p1 && box_dist2(oq, l1, h1) <= oc);
-                        }
-                        p0 = e0;
-                        p1 = e1;
-                    }
+                // leaves: exact against a single owner's ball; the union list keeps every leaf the
+                // union box reaches, since each owner tests the listed leaves against its own ball
+                if (to_leaves && single >= 0) {
+                    p0 = p0 && box_dist2(sq, l0, h0) <= scut;
+                    p1 = p1 && box_dist2(sq, l1, h1) <= scut;
                 }
                 const unsigned int b0 = __ballot_sync(0xffffffffu, p0), b1 = __ballot_sync(0xffffffffu, p1);
                 const int tot = __popc(b0) + __popc(b1);
@@ -316,21 +303,25 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
         // the groups' sites, four groups (32 sites) per pass: candidates with d^2 <= bound
         auto collect = [&](float bound) {
             int cnt = 0;
-            for (int b = 0; b < ngroup; b += 4) {
-                const int gi = b + (lane >> 3);
-                bool in = false;
-                unsigned long long key = 0;
-                if (gi < ngroup) {
-                    const float4 p = a.sorted[sh.own_groups[gi] * kSub + (lane & 7)];  // padding sites lie at +inf
-                    const float d2 = dist2(oq, make_float3(p.x, p.y, p.z));
-                    in = d2 <= bound;
-                    key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                          static_cast<unsigned int>(__float_as_int(p.w));
-                }
-                const unsigned int bal = __ballot_sync(0xffffffffu, in);
-                const int pos = cnt + __popc(bal & lt);
-                if (in && pos < kRangeCap) sh.cand[pos] = key;
-                cnt += __popc(bal);
+            // eight groups (two sites per lane, both loads in flight) per pass
+            for (int b = 0; b < ngroup; b += 8) {
+                const int g0 = b + (lane >> 3), g1 = g0 + 4;
+                const float4 inf4 = make_float4(CUDART_INF_F_, CUDART_INF_F_, CUDART_INF_F_, 0.f);
+                const float4 p0 = g0 < ngroup ? a.sorted[sh.own_groups[g0] * kSub + (lane & 7)] : inf4;
+                const float4 p1 = g1 < ngroup ? a.sorted[sh.own_groups[g1] * kSub + (lane & 7)] : inf4;
+                // padding sites of a partly filled leaf lie at +inf too
+                const float d0 = dist2(oq, make_float3(p0.x, p0.y, p0.z));
+                const float d1 = dist2(oq, make_float3(p1.x, p1.y, p1.z));
+                const bool in0 = d0 <= bound, in1 = d1 <= bound;
+                const unsigned int bal0 = __ballot_sync(0xffffffffu, in0), bal1 = __ballot_sync(0xffffffffu, in1);
+                const int pos0 = cnt + __popc(bal0 & lt), pos1 = cnt + __popc(bal0) + __popc(bal1 & lt);
+                if (in0 && pos0 < kRangeCap)
+                    sh.cand[pos0] = (static_cast<unsigned long long>(__float_as_uint(d0)) << 32) |
+                                    static_cast<unsigned int>(__float_as_int(p0.w));
+                if (in1 && pos1 < kRangeCap)
+                    sh.cand[pos1] = (static_cast<unsigned long long>(__float_as_uint(d1)) << 32) |
+                                    static_cast<unsigned int>(__float_as_int(p1.w));
+                cnt += __popc(bal0) + __popc(bal1);
             }
             __syncwarp();
             st_groups += ngroup;
@@ -339,9 +330,9 @@ __global__ void __launch_bounds__(kRangeWarps * 32) k_knn_range(Model m, RangeAr
         };
         // More candidates than the network holds: the K-th smallest d^2 among the first kRangeCap
         // collected is a bound that at least K sites meet, so the true K nearest lie inside it;
-        // rescan with it (a few rounds at most).
+        // rescan with it (six rounds at most).
         auto shrink = [&](int cnt) {
-            for (int round = 0; round < 3 && cnt > kRangeCap; ++round) {
+            for (int round = 0; round < 6 && cnt > kRangeCap; ++round) {
                 unsigned long long v[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) v[j] = sh.cand[j * 32 + lane];
