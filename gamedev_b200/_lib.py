@@ -151,6 +151,11 @@ SIGNATURES = {
     "gd_get_owner_state": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "gd_knn_static": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int, _P, _P, _P, _P,
                                 C.POINTER(C.c_longlong), C.c_char_p, C.c_size_t]),
+    "gd_set_clock": (C.c_int, [_P, C.c_double, C.c_double, C.c_double]),
+    "gd_get_clock": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_int)]),
+    "gd_dynamics_step": (C.c_int, [_P, C.POINTER(GdRunInfo), _P, _P]),
+    "gd_step": (C.c_int, [_P, C.POINTER(GdRunInfo), _P, _P, C.c_double, _P]),
     # include/gd_b200_controller.h (host only)
     "gd_ctl_binmap": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P]),
     "gd_ctl_choose_bath": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int, C.c_double, C.c_double, _P, _P]),

@@ -19,7 +19,7 @@ LIB = PKG / "libgd_b200.so"
 OBJ = PKG / "_build"
 
 SOURCES = ["gd_geometry.cu", "gd_range.cu", "gd_collide.cu", "gd_controller.cu", "gd_radius.cu", "gd_api.cu",
-           "gd_batch.cu", "gd_io.cu"]
+           "gd_batch.cu", "gd_io.cu", "gd_transport.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I", str(ROOT / "include")]

@@ -8,6 +8,7 @@
 
 #include "gd_collide.cuh"
 #include "gd_internal.cuh"
+#include "gd_transport.cuh"
 
 namespace gd {
 
@@ -108,6 +109,10 @@ struct gd_handle {
     bool cache_valid = false;
     std::string err;
     long long detail = 0;
+    // the Strang step: device clocks and optical depth, and the learned proposal's buffers
+    gd::DynState dyn;
+    gd::DevBuf<float> step_features, step_radius, step_prev_kth;
+    bool step_prev_valid = false;  // step_prev_kth holds the last search's K-th d^2
 };
 
 static gd_status fail(gd_handle *h, const gd::Status &s) {
@@ -834,3 +839,144 @@ extern "C" gd_status gd_knn_static(const gd_config *cfg, const gd_particle *dev_
     if (!st) return gd::static_fail(st, detail, msg, msg_len);
     return GD_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// The Strang step of the reference's time loop (src/swarm/swarm_runtime.cu:504-601)
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+// The geometry and the handle's neighbour cache for the current positions: the plain query, or,
+// with a radius model and a previous search, the learned proposal seeded by the previous K-th
+// distances (the rows are the plain query's either way).
+gd::Status step_search(gd_handle *h, gd_particle *part, double total_mass, gd_radius_model *model) {
+    h->geom_valid = false;
+    h->cache_valid = false;
+    h->col.local_geometry_valid = false;
+    h->geo.sort_bits = h->tune.sort_bits;
+    GD_TRY(gd::geometry_build(h->geo, h->m, part, h->stream));
+    h->geom_valid = true;
+    const float *radius = nullptr;
+    if (model && h->step_prev_valid) {
+        GD_TRY(gd::radius_features(h->geo, h->m, part, h->step_prev_kth.ptr, total_mass, h->step_features.ptr,
+                                   h->stream));
+        if (gd_radius_model_predict(model, h->step_features.ptr, h->n, h->step_radius.ptr, h->stream) != GD_OK)
+            return gd::Status{GD_ERR_CUDA, "radius model prediction failed", 0};
+        radius = h->step_radius.ptr;
+    }
+    GD_TRY(gd::knn_query(h->geo, h->m, part, h->codes.ptr, h->measure.ptr, h->kth.ptr, h->stream, radius, nullptr,
+                         h->tune));
+    GD_TRY(gd::space_bin(h->m, part, h->n, h->spatial.ptr, h->stream));
+    if (h->step_prev_kth.ptr) {
+        GD_TRY_CUDA(cudaMemcpyAsync(h->step_prev_kth.ptr, h->kth.ptr, sizeof(float) * h->n, cudaMemcpyDeviceToDevice,
+                                    h->stream));
+        h->step_prev_valid = true;
+    }
+    h->cache_valid = true;
+    return gd::Status::ok();
+}
+
+void invalidate(gd_handle *h) {
+    h->geom_valid = false;
+    h->cache_valid = false;
+    h->col.local_geometry_valid = false;
+}
+
+gd::Status step_prepare(gd_handle *h, const gd_run_info *run, gd_particle *part, void *rng, gd::Dyn &d) {
+    if (!run || !part || !rng) return gd::Status{GD_ERR_INVALID_ARGUMENT, "null pointer", 0};
+    GD_TRY(gd::dyn_validate(h->m, *run));
+    d = gd::make_dyn(*run);
+    GD_TRY(gd::dyn_alloc(h->dyn, h->m));
+    return gd::Status::ok();
+}
+
+// the dynamics of one step: D(dt/2) T(dt) D(dt/2) on the step's device timestep
+gd::Status step_dynamics(gd_handle *h, const gd::Dyn &d, gd_particle *part, void *rng, long long *launches) {
+    curandState *st = static_cast<curandState *>(rng);
+    GD_TRY(gd::dyn_diffuse(h->dyn, h->m, d, h->n, part, st, h->stream, launches));
+    GD_TRY(gd::dyn_transport(h->dyn, h->m, d, h->n, part, h->stream, launches));
+    GD_TRY(gd::dyn_diffuse(h->dyn, h->m, d, h->n, part, st, h->stream, launches));
+    invalidate(h);
+    return gd::Status::ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+gd_status gd_set_clock(gd_handle *h, double clock_sim, double clock_out, double dt_out) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(clock_sim) || !std::isfinite(clock_out) || !(dt_out > 0) || !std::isfinite(dt_out))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "invalid clocks");
+    gd::Status s = gd::dyn_alloc(h->dyn, h->m);
+    if (s) s = gd::dyn_set_clock(h->dyn, clock_sim, clock_out, dt_out, h->stream);
+    return done(h, s);
+}
+
+gd_status gd_get_clock(gd_handle *h, double *clock_sim, double *clock_out, double *dt_last, int *steps) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    if (!h->dyn.clock.ptr) return fail(h, GD_ERR_NOT_READY, "gd_get_clock before gd_set_clock");
+    gd::StepClock c{};
+    gd::Status s = gd::dyn_read_clock(h->dyn, c, h->stream);
+    if (!s) return fail(h, s);
+    if (clock_sim) *clock_sim = c.clock_sim;
+    if (clock_out) *clock_out = c.clock_out;
+    if (dt_last) *dt_last = c.dt;
+    if (steps) *steps = c.count_dyn;
+    return done(h, s);
+}
+
+gd_status gd_dynamics_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    gd::Dyn d;
+    gd::Status s = step_prepare(h, run, dev_particle, dev_rng, d);
+    if (s && !h->dyn.clock.ptr) s = gd::Status{GD_ERR_NOT_READY, "gd_dynamics_step before gd_set_clock", 0};
+    long long launches = 0;
+    if (s) s = gd::dyn_timestep(h->dyn, h->m, d, h->n, dev_particle, h->stream, &launches);
+    if (s) s = step_dynamics(h, d, dev_particle, dev_rng, &launches);
+    if (s) s = gd::dyn_clock_advance(h->dyn, h->stream, &launches);
+    h->geo.launches += launches;
+    return done(h, s);
+}
+
+gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng,
+                  double total_dust_mass, gd_radius_model *radius_model) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    gd::Dyn d;
+    gd::Status s = step_prepare(h, run, dev_particle, dev_rng, d);
+    if (s && !h->dyn.clock.ptr) s = gd::Status{GD_ERR_NOT_READY, "gd_step before gd_set_clock", 0};
+    if (s && !(total_dust_mass > 0)) s = gd::Status{GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive", 0};
+    if (s && radius_model && !h->step_features.ptr) {
+        cudaError_t e = h->step_features.alloc(static_cast<size_t>(h->n) * GD_RADIUS_FEATURES);
+        if (e == cudaSuccess) e = h->step_radius.alloc(h->n);
+        if (e == cudaSuccess) e = h->step_prev_kth.alloc(h->n);
+        if (e != cudaSuccess) s = gd::cuda_status(e, "gd_step radius buffers");
+        h->step_prev_valid = false;
+    }
+    long long launches = 0;
+    // dt = min(DT_MAX, 1 / max rate, dt_out - clock_out), on the device
+    if (s) s = gd::dyn_timestep(h->dyn, h->m, d, h->n, dev_particle, h->stream, &launches);
+    gd::StepClock c{};
+    if (s) s = gd::dyn_read_clock(h->dyn, c, h->stream);
+    if (s && (!(c.dt > 0) || !std::isfinite(c.dt)))
+        s = gd::Status{GD_ERR_TIME_RESOLUTION, "invalid dynamics timestep", 0};
+    const double half = 0.5 * c.dt;
+    // C(dt/2): the geometry stays while the positions have not moved
+    if (s) {
+        if (h->geom_valid && h->cache_valid) s = gd::state_screen(h->geo, h->m, dev_particle, h->stream);
+        else s = step_search(h, dev_particle, total_dust_mass, radius_model);
+    }
+    if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
+                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, half,
+                                      total_dust_mass, h->stream);
+    // D(dt/2) T(dt) D(dt/2), then C(dt/2) on the moved positions
+    if (s) s = step_dynamics(h, d, dev_particle, dev_rng, &launches);
+    if (s) s = step_search(h, dev_particle, total_dust_mass, radius_model);
+    if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
+                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, half,
+                                      total_dust_mass, h->stream);
+    if (s) s = gd::dyn_clock_advance(h->dyn, h->stream, &launches);
+    h->geo.launches += launches;
+    return done(h, s);
+}
+
+}  // extern "C"

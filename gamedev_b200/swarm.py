@@ -229,6 +229,31 @@ class SwarmCollision:
         self.lib.gd_set_stream(self.h, _stream())
         self._check(self.lib.gd_drift_keplerian(self.h, C.c_void_p(_ptr(particles)), float(dt)))
 
+    # ---- the Strang step (gd_step) -------------------------------------------------------------
+    def set_clock(self, clock_sim: float = 0.0, clock_out: float = 0.0, dt_out: float = 1.0):
+        """gd_set_clock: the time loop's device clocks and the output interval."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_set_clock(self.h, float(clock_sim), float(clock_out), float(dt_out)))
+
+    def clock(self) -> dict:
+        """gd_get_clock: clock_sim, clock_out, the last step's dt and the steps taken."""
+        a, b, c, k = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_get_clock(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(k)))
+        return {"clock_sim": a.value, "clock_out": b.value, "dt": c.value, "steps": k.value}
+
+    def dynamics_step(self, run, particles, rng):
+        """gd_dynamics_step: the timestep and D(dt/2) T(dt) D(dt/2), without collisions."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_dynamics_step(self.h, C.byref(run), C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng))))
+
+    def step(self, run, particles, rng, total_dust_mass: float, radius_model=None):
+        """gd_step: one Strang step C(dt/2) D(dt/2) T(dt) D(dt/2) C(dt/2); radius_model (a
+        RadiusModel) seeds every geometry rebuild after the first with the learned proposal."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_step(self.h, C.byref(run), C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
+                                     float(total_dust_mass), radius_model.h if radius_model else None))
+
     def radius_features(self, particles, prev_kth_d2, total_mass: float, out=None):
         """Learned-radius features [n_p, 8] of the current geometry (gd_radius_features)."""
         torch = _torch()

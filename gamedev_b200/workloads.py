@@ -17,8 +17,9 @@ Config names:
   c1_multisize_2d  radial-azimuthal, N = 2^20, K = 64, Morton search, gap at 9-11 au, ring at 30 au,
                    radii log-uniform on [1e-4, 10] cm, fragmentation above 1 m/s
   c3_learned_3d    3D, N = 10^7, K = 64, c0 positions, radii log-uniform on [1e-4, 10] cm
-  c4_production_3d as c3 (its collision operator; transport, diffusion and radiation are not in
-                   this build)
+  c4_production_3d as c3, with the full Strang step: drag and gravity, radiation pressure with
+                   Poynting-Robertson drag, Ito diffusion and coagulation/fragmentation
+  t0_transport_3d  the c4 shapes at N = 65,536 with transport and diffusion but no radiation
   w0_wedge_3d      3D wedge (azimuth [-0.6, 0.6)), N = 65,536, K = 32, KD search, with periodic
                    images
   w1_narrow_2d     radial-azimuthal 0.05 rad wedge, N = 65,536, K = 32, Morton search, with periodic
@@ -81,8 +82,17 @@ CONFIGS = {
                             sizes=("loguniform", 2.0e-4, 20.0), radial="gap_ring", seed=2),
     "c3_learned_3d": dict(n=10_000_000, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
                           sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=3),
+    # the full production step: drag and gravity, radiation pressure with Poynting-Robertson drag
+    # through the radial optical depth, Ito diffusion and collisions.  Radiation constants in cgs:
+    # a 1 cm grain feels 1e-4 of the star's gravity, its gray opacity is its geometric cross section
+    # per mass (1.5 cm^2/g), the force ramps up over one orbit at 1 au
     "c4_production_3d": dict(n=10_000_000, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
-                             sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=4),
+                             sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=4,
+                             flags=dict(radiation=1, pr_effect=1),
+                             run=dict(beta_0=1.0e-4, kappa_0=1.5, t_beta="orbit", c_light=2.99792458e10)),
+    # the c4 shapes with the dynamics alone and no radiation field (ssa_transport + diffusion)
+    "t0_transport_3d": dict(n=65536, k=64, three_d=True, search=GD_SEARCH_KDTREE, v_frag=100.0,
+                            sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=11),
     # azimuthal wedges (periodic images): a 1.2 rad wedge searched by the KD tree, whose owners
     # beyond ~4 au can reach two images of one particle, and a 0.05 rad sliver searched by the
     # Morton index, where every owner can
@@ -150,6 +160,8 @@ def run_info(name: str):
     r.metal_z, r.schmidt_x, r.schmidt_r, r.schmidt_z = 1.0e-02, 1.0, 1.0, 1.0
     r.beta_0, r.kappa_0, r.t_beta, r.c_light = 1.0e+01, 1.0, 2.0 * math.pi, 1.0e+04
     r.dt_out, r.dt_max, r.cfl_dyn = 0.5 * orbital_time(), 0.05 * orbital_time(), 0.45
+    for key, value in CONFIGS[name].get("run", {}).items():
+        setattr(r, key, 2.0 * math.pi * orbital_time() if value == "orbit" else value)
     return r
 
 

@@ -453,6 +453,32 @@ typedef struct gd_run_info {
 gd_status gd_save_variables(const gd_config *cfg, const gd_run_info *run, int n_p, double total_dust_mass,
                             const char *path);
 
+/* ---------------------------------------------------------------------------------------------
+ * The Strang step of the reference's time loop (src/swarm/swarm_runtime.cu:504-601), for a model
+ * with TRANSPORT (and DIFFUSION in 3D, optionally RADIATION, PR_EFFECT and VISC_FLOW, analytic gas):
+ *     dt = min(DT_MAX, 1 / max rate, dt_out - clock_out)          dyn_rate_calc (dyn_rate_calc.cu)
+ *     C(dt/2)  D(dt/2)  T(dt)  D(dt/2)  C(dt/2)
+ * with C the collision operator (gd_evolve_collisions), D diffusion_pos (diffusion_pos.cu) and T
+ * ssa_transport, or with RADIATION ssa_substep_1, the optical depth (optdepth_*.cu) and
+ * ssa_substep_2.  The model's dynamics settings come in gd_run_info (transport, diffusion,
+ * radiation, pr_effect, visc_flow, schmidt_*, beta_0, kappa_0, t_beta, c_light, dt_max, cfl_dyn);
+ * importgas is not supported (GD_ERR_INVALID_ARGUMENT).  The clocks live on the device: each step
+ * advances clock_sim and clock_out by its dt. */
+
+/* Sets the device clocks: clock_sim (time since the start), clock_out (time into the current
+ * output interval) and the interval length dt_out.  Enqueued on the handle's stream. */
+gd_status gd_set_clock(gd_handle *h, double clock_sim, double clock_out, double dt_out);
+/* Reads the clocks, the last step's dt and the steps taken since gd_set_clock.  Synchronises. */
+gd_status gd_get_clock(gd_handle *h, double *clock_sim, double *clock_out, double *dt_last, int *steps);
+/* One step of the dynamics alone: the timestep, D(dt/2) T(dt) D(dt/2), the clocks advanced.  No
+ * host synchronisation.  Invalidates the geometry. */
+gd_status gd_dynamics_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng);
+/* One full step, collisions included.  With radius_model (may be NULL) each geometry rebuild after
+ * the first searches with the learned proposal seeded by the previous search's K-th distances; the
+ * rows are the plain query's either way.  Reads the step's dt back once. */
+gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng,
+                  double total_dust_mass, gd_radius_model *radius_model);
+
 #ifdef __cplusplus
 }
 #endif
