@@ -143,6 +143,7 @@ SIGNATURES = {
     "gd_space_bin": (C.c_int, [_P, _P, _P]),
     "gd_invalidate_geometry": (C.c_int, [_P]),
     "gd_reset_controller": (C.c_int, [_P]),
+    "gd_check_operator": (C.c_int, [_P]),
     "gd_collision_operator": (C.c_int, [_P, _P, _P, C.c_double, C.c_double]),
     "gd_evolve_collisions": (C.c_int, [_P, _P, _P, C.c_double, C.c_double]),
     "gd_last_operator_stats": (C.c_int, [_P, C.POINTER(GdOperatorStats)]),
@@ -156,6 +157,7 @@ SIGNATURES = {
                                C.POINTER(C.c_int)]),
     "gd_dynamics_step": (C.c_int, [_P, C.POINTER(GdRunInfo), _P, _P]),
     "gd_step": (C.c_int, [_P, C.POINTER(GdRunInfo), _P, _P, C.c_double, _P]),
+    "gd_check_step": (C.c_int, [_P]),
     # include/gd_b200_controller.h (host only)
     "gd_ctl_binmap": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P]),
     "gd_ctl_choose_bath": (C.c_int, [C.POINTER(GdConfig), _P, C.c_int, C.c_double, C.c_double, _P, _P]),

@@ -19,7 +19,10 @@ LIB = PKG / "libgd_b200.so"
 OBJ = PKG / "_build"
 
 SOURCES = ["gd_geometry.cu", "gd_range.cu", "gd_collide.cu", "gd_controller.cu", "gd_radius.cu", "gd_api.cu",
-           "gd_batch.cu", "gd_io.cu", "gd_transport.cu"]
+           "gd_batch.cu", "gd_io.cu", "gd_transport.cu", "gd_devctl.cu"]
+# The device controller compiles the host controller's arithmetic; without FMA contraction its
+# roundings are the host's, so the schedule and baths it picks are the host controller's, bit for bit.
+SOURCE_FLAGS = {"gd_devctl.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I", str(ROOT / "include")]
@@ -48,7 +51,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         o = OBJ / (s.stem + ".o")
         objs.append(o)
         if force or ptxas_info or _stale(o, [s] + headers):
-            cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc(), *ARCH, *FLAGS, *SOURCE_FLAGS.get(src, []), "-c", str(s), "-o", str(o)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             if verbose:

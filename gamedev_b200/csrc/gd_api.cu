@@ -113,6 +113,7 @@ struct gd_handle {
     gd::DynState dyn;
     gd::DevBuf<float> step_features, step_radius, step_prev_kth;
     bool step_prev_valid = false;  // step_prev_kth holds the last search's K-th d^2
+    gd::DevBuf<int> step_screen;   // first failed screen of the captured steps since the last check
 };
 
 static gd_status fail(gd_handle *h, const gd::Status &s) {
@@ -549,8 +550,12 @@ gd_status gd_invalidate_geometry(gd_handle *h) {
 
 gd_status gd_reset_controller(gd_handle *h) {
     if (!h) return GD_ERR_INVALID_ARGUMENT;
-    gd::collider_reset_state(h->col);
-    return GD_OK;
+    return done(h, gd::collider_reset_state(h->col, h->stream));
+}
+
+gd_status gd_check_operator(gd_handle *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    return done(h, gd::collider_check(h->col, h->stream));
 }
 
 gd_status gd_set_diagnostics(gd_handle *h, int on) {
@@ -941,10 +946,26 @@ gd_status gd_dynamics_step(gd_handle *h, const gd_run_info *run, gd_particle *de
 gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng,
                   double total_dust_mass, gd_radius_model *radius_model) {
     if (!h) return GD_ERR_INVALID_ARGUMENT;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess || cs == cudaStreamCaptureStatusInvalidated)
+        return fail(h, GD_ERR_CUDA, "the handle's stream capture is invalid");
+    const bool captured = cs == cudaStreamCaptureStatusActive;
+    // a captured step allocates nothing and reads nothing back: the buffers come from an eager step
+    if (captured && (!h->dyn.clock.ptr || !h->col.setup_done || !h->step_screen.ptr ||
+                     (radius_model && !h->step_features.ptr)))
+        return fail(h, GD_ERR_NOT_READY, "capture gd_step after one eager gd_step with the same radius model");
     gd::Dyn d;
     gd::Status s = step_prepare(h, run, dev_particle, dev_rng, d);
     if (s && !h->dyn.clock.ptr) s = gd::Status{GD_ERR_NOT_READY, "gd_step before gd_set_clock", 0};
     if (s && !(total_dust_mass > 0)) s = gd::Status{GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive", 0};
+    const bool deferred = h->geo.deferred_check;
+    if (captured) h->geo.deferred_check = true;  // the screens are read by gd_check_step
+    if (s && !h->step_screen.ptr) {
+        const int none = INT_MAX;
+        cudaError_t e = h->step_screen.alloc(1);
+        if (e == cudaSuccess) e = cudaMemcpy(h->step_screen.ptr, &none, sizeof(int), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) s = gd::cuda_status(e, "gd_step screen buffer");
+    }
     if (s && radius_model && !h->step_features.ptr) {
         cudaError_t e = h->step_features.alloc(static_cast<size_t>(h->n) * GD_RADIUS_FEATURES);
         if (e == cudaSuccess) e = h->step_radius.alloc(h->n);
@@ -953,30 +974,52 @@ gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particl
         h->step_prev_valid = false;
     }
     long long launches = 0;
-    // dt = min(DT_MAX, 1 / max rate, dt_out - clock_out), on the device
+    // dt = min(DT_MAX, 1 / max rate, dt_out - clock_out), on the device; the collision halves read
+    // dt / 2 there (the operator's controller rejects a non-positive or non-finite one)
     if (s) s = gd::dyn_timestep(h->dyn, h->m, d, h->n, dev_particle, h->stream, &launches);
-    gd::StepClock c{};
-    if (s) s = gd::dyn_read_clock(h->dyn, c, h->stream);
-    if (s && (!(c.dt > 0) || !std::isfinite(c.dt)))
-        s = gd::Status{GD_ERR_TIME_RESOLUTION, "invalid dynamics timestep", 0};
-    const double half = 0.5 * c.dt;
+    const double *dt_dev = h->dyn.clock.ptr ? &h->dyn.clock.ptr->dt : nullptr;
     // C(dt/2): the geometry stays while the positions have not moved
     if (s) {
         if (h->geom_valid && h->cache_valid) s = gd::state_screen(h->geo, h->m, dev_particle, h->stream);
         else s = step_search(h, dev_particle, total_dust_mass, radius_model);
     }
+    if (s && captured) s = gd::screen_keep(h->geo, h->step_screen.ptr, h->stream);
     if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
-                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, half,
-                                      total_dust_mass, h->stream);
+                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, 0.0,
+                                      total_dust_mass, h->stream, dt_dev, 0.5);
     // D(dt/2) T(dt) D(dt/2), then C(dt/2) on the moved positions
     if (s) s = step_dynamics(h, d, dev_particle, dev_rng, &launches);
     if (s) s = step_search(h, dev_particle, total_dust_mass, radius_model);
+    if (s && captured) s = gd::screen_keep(h->geo, h->step_screen.ptr, h->stream);
     if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
-                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, half,
-                                      total_dust_mass, h->stream);
+                                      h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, 0.0,
+                                      total_dust_mass, h->stream, dt_dev, 0.5);
     if (s) s = gd::dyn_clock_advance(h->dyn, h->stream, &launches);
     h->geo.launches += launches;
+    h->geo.deferred_check = deferred;
     return done(h, s);
+}
+
+gd_status gd_check_step(gd_handle *h) {
+    if (!h) return GD_ERR_INVALID_ARGUMENT;
+    // the operators' results (this also clears their accumulators), then the first failed
+    // non-finite screen of the steps, which the reference meets before the operator that follows it
+    gd::Status op = gd::collider_check(h->col, h->stream);
+    int first = INT_MAX;
+    if (h->step_screen.ptr) {
+        const int none = INT_MAX;
+        if (cudaMemcpyAsync(&first, h->step_screen.ptr, sizeof(int), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+            cudaMemcpyAsync(h->step_screen.ptr, &none, sizeof(int), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return fail(h, GD_ERR_CUDA, "read of the step screen");
+    }
+    if (first != INT_MAX) {
+        invalidate(h);
+        gd::Status st{GD_ERR_NONFINITE,
+                      "non-finite particle state before collision search at particle " + std::to_string(first), first};
+        return fail(h, st);
+    }
+    return done(h, op);
 }
 
 }  // extern "C"

@@ -33,9 +33,11 @@
 #include <sstream>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <string>
 
 #include "gd_collide.cuh"
+#include "gd_ctl_core.cuh"
 #include "gd_physics.cuh"
 
 namespace gd {
@@ -115,22 +117,26 @@ __global__ void k_env_cache(Model m, int n, const gd_particle *__restrict__ part
 }
 
 // col_bath_init (col_bath_init.cu:11-23) + col_comp_zero (col_comp_zero.cu:11-19)
-__global__ void k_bath_init(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
-                            double *__restrict__ size_old, double *__restrict__ numr_old, double *__restrict__ time,
-                            int *__restrict__ events, unsigned char *__restrict__ complete, double *__restrict__ hazard,
+__global__ void k_bath_init(const WaveInfo *__restrict__ w, const int *__restrict__ ids,
+                            const gd_particle *__restrict__ part, double *__restrict__ size_old,
+                            double *__restrict__ numr_old, double *__restrict__ time, int *__restrict__ events,
+                            unsigned char *__restrict__ complete, double *__restrict__ hazard,
                             double *__restrict__ jump1, double *__restrict__ jump2, double *__restrict__ jumpmax,
-                            int *__restrict__ stamp, int publish) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= count) return;
-    int i = owner_at(ids, slot);
-    const double size = part[i].par_size, numr = part[i].par_numr;
-    if (!(size_old[i] == size && numr_old[i] == numr)) stamp[i] = publish;  // the reservoir value changes
-    size_old[i] = size;
-    numr_old[i] = numr;
-    time[i] = 0.0;
-    events[i] = 0;
-    complete[i] = 0;
-    hazard[i] = jump1[i] = jump2[i] = jumpmax[i] = 0.0;
+                            int *__restrict__ stamp) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count, publish = w->publish;
+    if (w->full) ids = nullptr;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+        const int i = owner_at(ids, slot);
+        const double size = part[i].par_size, numr = part[i].par_numr;
+        if (!(size_old[i] == size && numr_old[i] == numr)) stamp[i] = publish;  // the reservoir value changes
+        size_old[i] = size;
+        numr_old[i] = numr;
+        time[i] = 0.0;
+        events[i] = 0;
+        complete[i] = 0;
+        hazard[i] = jump1[i] = jump2[i] = jumpmax[i] = 0.0;
+    }
 }
 
 __global__ void k_size_zero(int G, unsigned long long *mmin, unsigned long long *mmax) {
@@ -145,9 +151,13 @@ __global__ void k_size_zero(int G, unsigned long long *mmin, unsigned long long 
 // key combine their terms with shuffles inside their group and the lowest one updates memory.
 __device__ __forceinline__ unsigned int lanes_below() { return (1u << (threadIdx.x & 31)) - 1u; }
 
-__global__ void k_size_scan(const int *__restrict__ ids, int count, const gd_particle *__restrict__ part,
-                            const int32_t *__restrict__ spatial, const unsigned char *__restrict__ active,
-                            unsigned long long *mmin, unsigned long long *mmax) {
+__global__ void k_size_scan(const WaveInfo *__restrict__ w, const int *__restrict__ ids,
+                            const gd_particle *__restrict__ part, const int32_t *__restrict__ spatial,
+                            const unsigned char *__restrict__ active, unsigned long long *mmin,
+                            unsigned long long *mmax) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     bool on = slot < count;
     int g = 0;
@@ -192,9 +202,13 @@ __device__ __forceinline__ int size_bin(const Model &m, double size, const doubl
     return max(0, min(m.col_bin_s - 1, static_cast<int>(floor(fraction * m.col_bin_s))));
 }
 
-__global__ void k_count_bin(Model m, const int *__restrict__ ids, int count, int *__restrict__ counts,
-                            const gd_particle *__restrict__ part, const int32_t *__restrict__ spatial,
-                            const unsigned char *__restrict__ active, const double *lower, const double *upper) {
+__global__ void k_count_bin(Model m, const WaveInfo *__restrict__ w, const int *__restrict__ ids,
+                            int *__restrict__ counts, const gd_particle *__restrict__ part,
+                            const int32_t *__restrict__ spatial, const unsigned char *__restrict__ active,
+                            const double *lower, const double *upper) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     bool on = slot < count;
     int key = 0;
@@ -244,15 +258,20 @@ __host__ __device__ inline int binmap_compute(int groups, int bins, int bin_min,
     return merged;
 }
 
-__global__ void k_binmap(Model m, const int *counts, int *binmap, int *merged, RateBin *ratebin) {
+__global__ void k_binmap(Model m, const WaveInfo *__restrict__ w, const int *counts, int *binmap, int *merged) {
+    if (!w->go || !w->need_rates) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) *merged = binmap_compute(m.local_groups, m.col_bin_s, m.col_bin_min, counts, binmap);
 }
 
-__global__ void k_rate_bins(Model m, const int *__restrict__ ids, int count, RateBin *__restrict__ bin,
-                            const gd_particle *__restrict__ part, const double *__restrict__ rate,
-                            const double *__restrict__ change, const double *__restrict__ second,
-                            const int32_t *__restrict__ spatial, const int *__restrict__ binmap,
-                            const unsigned char *__restrict__ active, const double *lower, const double *upper) {
+__global__ void k_rate_bins(Model m, const WaveInfo *__restrict__ w, const int *__restrict__ ids,
+                            RateBin *__restrict__ bin, const gd_particle *__restrict__ part,
+                            const double *__restrict__ rate, const double *__restrict__ change,
+                            const double *__restrict__ second, const int32_t *__restrict__ spatial,
+                            const int *__restrict__ binmap, const unsigned char *__restrict__ active,
+                            const double *lower, const double *upper) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     bool on = slot < count;
     int b = 0;
@@ -328,7 +347,7 @@ __device__ __forceinline__ void warp_fold(int K, int lane, F &&combine) {
 
 struct RateArgs {
     const int *ids;
-    int count;
+    const WaveInfo *w;  // the wave's owner count and order, and its publish wave
     const gd_particle *part;
     const int32_t *codes;
     const double *measure;
@@ -341,7 +360,6 @@ struct RateArgs {
     RateMoments *cached;
     const int *stamp;  // publish wave of each particle's last reservoir change
     int *rated;        // publish wave of each owner's stored rates (-1: none)
-    int publish;       // the current publish wave
 };
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner.  kCached selects, at compile time,
@@ -355,13 +373,16 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int slot = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (slot >= a.count) return;
+    if (!a.w->go || !a.w->need_rates) return;
+    const int count = a.w->count, publish = a.w->publish;
+    const int *ids = a.w->full ? nullptr : a.ids;
+    // a persistent grid: each warp takes owners strided by the number of warps
+    for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < count; slot += gridDim.x * (blockDim.x >> 5)) {
     double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 4 * K;
     double *rate_w = w, *change_w = w + K, *second_w = w + 2 * K, *max_w = w + 3 * K;
     int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
                    static_cast<size_t>(wib) * K;
-    const int i = owner_at(a.ids, slot);
+    const int i = owner_at(ids, slot);
     // stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
     // since they were evaluated (same geometry and lambda0)
     const int rated = a.rated[i];
@@ -370,7 +391,7 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
         const int nb = a.codes[static_cast<size_t>(i) * K + s];
         need = nb >= 0 && a.stamp[nb / 3] > rated;
     }
-    if (!__any_sync(0xffffffffu, need)) return;
+    if (!__any_sync(0xffffffffu, need)) continue;
     const bool act = a.active[i] != 0;
     const double meas = a.measure[i];
     const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
@@ -430,7 +451,9 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
         a.rate[i] = rate_w[0];
         a.change[i] = change_w[0];
         a.second[i] = second_w[0];
-        a.rated[i] = a.publish;
+        a.rated[i] = publish;
+    }
+    __syncwarp();  // the warp's staging is rewritten by its next owner
     }
 }
 
@@ -494,7 +517,7 @@ __device__ __forceinline__ double col_uniform(curandState *st) {
 
 struct ChainArgs {
     const int *ids;
-    int count;
+    const WaveInfo *w;  // the wave's owner count and order
     curandState *rng;
     const unsigned char *active;
     const double *measure;
@@ -510,11 +533,16 @@ struct ChainArgs {
 
 // col_skip_scan (col_skip_scan.cu:13-59)
 __global__ void k_skip_scan(ChainArgs a) {
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!a.w->go) return;
+    const int count = a.w->count;
+    const int *ids = a.w->full ? nullptr : a.ids;
+    // a persistent grid; every warp of a block runs the same number of passes (ballots below)
+    for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    const int slot = base + threadIdx.x;
     bool enqueue = false;
     int i = 0;
-    if (slot < a.count) {
-        i = owner_at(a.ids, slot);
+    if (slot < count) {
+        i = owner_at(ids, slot);
         const double end = a.dt[a.spatial[i]];
         if (!a.active[i] || !(a.measure[i] > 0.0)) {
             a.time[i] = end;
@@ -552,10 +580,11 @@ __global__ void k_skip_scan(ChainArgs a) {
     const unsigned int mask = __ballot_sync(0xffffffffu, enqueue);
     if (mask) {
         const int lane = threadIdx.x & 31;
-        int base = 0;
-        if (lane == __ffs(mask) - 1) base = atomicAdd(a.queued, __popc(mask));
-        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
-        if (enqueue) a.queue[base + __popc(mask & ((1u << lane) - 1u))] = i;
+        int qbase = 0;
+        if (lane == __ffs(mask) - 1) qbase = atomicAdd(a.queued, __popc(mask));
+        qbase = __shfl_sync(0xffffffffu, qbase, __ffs(mask) - 1);
+        if (enqueue) a.queue[qbase + __popc(mask & ((1u << lane) - 1u))] = i;
+    }
     }
 }
 
@@ -787,8 +816,9 @@ __device__ __forceinline__ void atomic_max_double(double *address, double value)
 }
 
 struct AuditArgs {
-    const int *ids;
-    int count;
+    const int *ids;  // the wave's owners, grouped by spatial group (even when the wave holds every one)
+    const WaveInfo *w;
+    int count;       // set from the wave in the kernel
     AuditBin *bin;
     const gd_particle *part;
     const double *size_old, *numr_old, *rate, *hazard, *jump1, *jump2, *jumpmax;
@@ -854,7 +884,10 @@ __device__ __forceinline__ void audit_owner(const Model &m, const AuditArgs &a, 
     }
 }
 
-__global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a) {
+__global__ void __launch_bounds__(kAuditTPB) k_audit_bin(Model m, AuditArgs a_in) {
+    if (!a_in.w->go) return;
+    AuditArgs a = a_in;
+    a.count = a.w->count;
     __shared__ double terms[kAuditTPB / 32][32][kAuditTerms + 2];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     bool on, valid;
@@ -921,7 +954,11 @@ __host__ __device__ constexpr size_t audit_blocked_smem(int bins) {
     return sizeof(double) * (kAuditTPB / 32) * 32 * (kAuditTerms + 2) +
            static_cast<size_t>(bins) * (sizeof(double) * kAuditSums + sizeof(unsigned long long) * 2 + sizeof(int) * 3);
 }
-__global__ void __launch_bounds__(kAuditTPB) k_audit_bin_blocked(Model m, AuditArgs a, int bins) {
+__global__ void __launch_bounds__(kAuditTPB) k_audit_bin_blocked(Model m, AuditArgs a_in, int bins) {
+    if (!a_in.w->go) return;
+    AuditArgs a = a_in;
+    a.count = a.w->count;
+    if (static_cast<long long>(blockIdx.x) * kAuditSpan >= a.count) return;
     extern __shared__ __align__(16) double sa[];
     double(*terms)[32][kAuditTerms + 2] = reinterpret_cast<double(*)[32][kAuditTerms + 2]>(sa);
     double *bsum = sa + (kAuditTPB / 32) * 32 * (kAuditTerms + 2);                              // [bins][kAuditSums]
@@ -1011,11 +1048,15 @@ __global__ void __launch_bounds__(kAuditTPB) k_audit_bin_blocked(Model m, AuditA
 // or bins fit in the default 48 KB of shared memory (kScanSmemEntries).
 constexpr int kScanSmemEntries = 1024;
 
-__global__ void __launch_bounds__(kAuditTPB) k_size_scan_blocked(const int *__restrict__ ids, int count,
+__global__ void __launch_bounds__(kAuditTPB) k_size_scan_blocked(const WaveInfo *__restrict__ w, const int *__restrict__ ids,
                                                                 const gd_particle *__restrict__ part,
                                                                 const int32_t *__restrict__ spatial,
                                                                 const unsigned char *__restrict__ active, int G,
                                                                 unsigned long long *mmin, unsigned long long *mmax) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
+    if (static_cast<long long>(blockIdx.x) * kAuditSpan >= count) return;
     extern __shared__ __align__(16) unsigned long long smm[];  // [G] minima, [G] maxima (double bits)
     unsigned long long *smin = smm, *smax = smm + G;
     for (int k = threadIdx.x; k < G; k += blockDim.x) {
@@ -1062,12 +1103,17 @@ __global__ void __launch_bounds__(kAuditTPB) k_size_scan_blocked(const int *__re
     }
 }
 
-__global__ void __launch_bounds__(kAuditTPB) k_count_bin_blocked(Model m, const int *__restrict__ ids, int count,
+__global__ void __launch_bounds__(kAuditTPB) k_count_bin_blocked(Model m, const WaveInfo *__restrict__ w,
+                                                                const int *__restrict__ ids,
                                                                 int *__restrict__ counts,
                                                                 const gd_particle *__restrict__ part,
                                                                 const int32_t *__restrict__ spatial,
                                                                 const unsigned char *__restrict__ active,
                                                                 const double *lower, const double *upper, int R) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
+    if (static_cast<long long>(blockIdx.x) * kAuditSpan >= count) return;
     extern __shared__ int scnt[];  // [R]
     for (int k = threadIdx.x; k < R; k += blockDim.x) scnt[k] = 0;
     __syncthreads();
@@ -1095,7 +1141,8 @@ __global__ void __launch_bounds__(kAuditTPB) k_count_bin_blocked(Model m, const 
         if (scnt[k]) atomicAdd(counts + k, scnt[k]);
 }
 
-__global__ void __launch_bounds__(kAuditTPB) k_rate_bins_blocked(Model m, const int *__restrict__ ids, int count,
+__global__ void __launch_bounds__(kAuditTPB) k_rate_bins_blocked(Model m, const WaveInfo *__restrict__ w,
+                                                                const int *__restrict__ ids,
                                                                 RateBin *__restrict__ bin,
                                                                 const gd_particle *__restrict__ part,
                                                                 const double *__restrict__ rate,
@@ -1105,6 +1152,10 @@ __global__ void __launch_bounds__(kAuditTPB) k_rate_bins_blocked(Model m, const 
                                                                 const int *__restrict__ binmap,
                                                                 const unsigned char *__restrict__ active,
                                                                 const double *lower, const double *upper, int R) {
+    if (!w->go || !w->need_rates) return;
+    const int count = w->count;
+    if (w->full) ids = nullptr;
+    if (static_cast<long long>(blockIdx.x) * kAuditSpan >= count) return;
     extern __shared__ __align__(16) double srb[];  // [R][4] sums, then [R][2] owner / invalid counts
     int *sct = reinterpret_cast<int *>(srb + 4 * R);
     for (int k = threadIdx.x; k < 4 * R; k += blockDim.x) srb[k] = 0.0;
@@ -1287,28 +1338,8 @@ __global__ void __launch_bounds__(kGroupTPB) k_dep_graph(int n, int K, int G, in
         if (se[k]) atomicOr(edges + k, se[k]);
 }
 
-struct WaveTable {
-    int groups;
-    int start[kMaxGroups];
-    int len[kMaxGroups];
-    int out[kMaxGroups];
-};
-
-// concatenate the owner lists of the due groups into ids
-__global__ void k_wave_ids(WaveTable t, int total, const int *__restrict__ sorted, int *__restrict__ ids) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    int lo = 0, hi = t.groups - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (t.out[mid] <= p) lo = mid;
-        else hi = mid - 1;
-    }
-    ids[p] = sorted[t.start[lo] + (p - t.out[lo])];
-}
-
 // ------------------------------------------------------------------------------------------------
-// host controller: scheduler and bath bounds
+// host controller: the shared arithmetic of gd_ctl_core.cuh behind Status
 // ------------------------------------------------------------------------------------------------
 static Status err(gd_status code, const std::string &msg, long long detail = 0) {
     Status s;
@@ -1318,129 +1349,25 @@ static Status err(gd_status code, const std::string &msg, long long detail = 0) 
     return s;
 }
 
-Status Schedule::init(double h, const std::vector<double> &requested, const std::vector<unsigned int> &edges) {
-    horizon = h;
-    const int n = static_cast<int>(requested.size());
-    level.assign(n, 0);
-    step.assign(n, 0);
-    next.assign(n, 0);
-    links.clear();
-    if (!(h > 0) || !std::isfinite(h)) return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
-    const int words = (n + 31) / 32;
-    for (int c = 0; c < n; ++c) {
-        if (!(requested[c] > 0) || !std::isfinite(requested[c]))
-            return err(GD_ERR_CONTROLLER, "invalid local collision timestep");
-        double dt = h;
-        while (dt > requested[c]) {
-            if (++level[c] > 52) return err(GD_ERR_TIME_RESOLUTION, "local collision timestep exceeds time resolution");
-            dt *= 0.5;
-        }
+Status ctl_status(int code) {
+    switch (code) {
+    case kCtlOk: return Status::ok();
+    case kCtlBadHorizon: return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
+    case kCtlBadTimestep: return err(GD_ERR_CONTROLLER, "invalid local collision timestep");
+    case kCtlTimeResolution: return err(GD_ERR_TIME_RESOLUTION, "local collision timestep exceeds time resolution");
+    case kCtlBadAdaptStep: return err(GD_ERR_CONTROLLER, "invalid adaptive collision timestep");
+    case kCtlAdaptResolution: return err(GD_ERR_TIME_RESOLUTION, "adaptive collision time resolution exceeded");
+    case kCtlBadRateMoments: return err(GD_ERR_CONTROLLER, "invalid change-based rate moments");
+    case kCtlBadChangeInputs: return err(GD_ERR_CONTROLLER, "invalid change-based refresh inputs");
+    case kCtlChangeUnderflow: return err(GD_ERR_CONTROLLER, "change-based timestep underflow");
+    case kCtlBadAudit: return err(GD_ERR_CONTROLLER, "collision bath controller returned an invalid audit state");
+    case kCtlNoMass: return err(GD_ERR_CONTROLLER, "collision bath controller found no active represented mass");
+    case kCtlWaveLimit: return err(GD_ERR_CONTROLLER, "the collision scheduler found no owners in too many waves");
+    default: break;
     }
-    for (int c = 0; c < n; ++c)
-        for (int d = c + 1; d < n; ++d)
-            if ((edges[c * words + d / 32] & (1u << (d % 32))) || (edges[d * words + c / 32] & (1u << (c % 32))))
-                links.emplace_back(c, d);
-    bool changed;
-    do {
-        changed = false;
-        for (int c = 0; c < n; ++c)
-            for (int d = 0; d < n; ++d) {
-                if (!(edges[c * words + d / 32] & (1u << (d % 32)))) continue;
-                if (level[c] < level[d] - 4) {
-                    level[c] = level[d] - 4;
-                    changed = true;
-                }
-                if (level[d] < level[c] - 4) {
-                    level[d] = level[c] - 4;
-                    changed = true;
-                }
-            }
-    } while (changed);
-    end = std::uint64_t(1) << 52;
-    for (int c = 0; c < n; ++c) step[c] = std::uint64_t(1) << (52 - level[c]);
-    return Status::ok();
-}
-
-std::uint64_t Schedule::time() const {
-    std::uint64_t t = next[0];
-    for (auto v : next) t = v < t ? v : t;
-    return t;
-}
-
-std::vector<int> Schedule::due(std::uint64_t tick) const {
-    std::vector<int> out;
-    for (int c = 0; c < static_cast<int>(next.size()); ++c)
-        if (next[c] == tick) out.push_back(c);
-    return out;
-}
-
-Status Schedule::adapt(std::uint64_t tick, const std::vector<int> &groups, const std::vector<double> &requested,
-                       const std::vector<bool> &passed) {
-    const int n = static_cast<int>(level.size());
-    std::vector<bool> act(n, false);
-    for (int c : groups) act[c] = true;
-    std::vector<int> cap(n, 52), cand = level;
-    for (int c = 0; c < n; ++c)
-        if (!act[c]) cap[c] = level[c];
-    bool changed;
-    do {
-        changed = false;
-        for (const auto &e : links) {
-            int c = e.first, d = e.second;
-            if (act[c] && cap[c] > cap[d] + 4) {
-                cap[c] = cap[d] + 4;
-                changed = true;
-            }
-            if (act[d] && cap[d] > cap[c] + 4) {
-                cap[d] = cap[c] + 4;
-                changed = true;
-            }
-        }
-    } while (changed);
-    for (int c : groups) {
-        if (!(requested[c] > 0) || !std::isfinite(requested[c]))
-            return err(GD_ERR_CONTROLLER, "invalid adaptive collision timestep");
-        int want = 0;
-        double h = horizon;
-        while (h > requested[c]) {
-            if (++want > 52) return err(GD_ERR_TIME_RESOLUTION, "adaptive collision time resolution exceeded");
-            h *= 0.5;
-        }
-        cand[c] = passed[c] ? want : std::max(want, level[c]);
-        while (tick % (std::uint64_t(1) << (52 - cand[c]))) ++cand[c];
-        cand[c] = std::min(cand[c], cap[c]);
-    }
-    do {
-        changed = false;
-        for (const auto &e : links) {
-            int c = e.first, d = e.second;
-            if (act[c] && cand[c] < cand[d] - 4) {
-                cand[c] = cand[d] - 4;
-                changed = true;
-            }
-            if (act[d] && cand[d] < cand[c] - 4) {
-                cand[d] = cand[c] - 4;
-                changed = true;
-            }
-        }
-    } while (changed);
-    for (int c : groups) {
-        level[c] = cand[c];
-        step[c] = std::uint64_t(1) << (52 - level[c]);
-    }
-    return Status::ok();
-}
-
-// change_limit (inc/swarm/_col_bound.cuh:209-220)
-Status change_limit(double A, double B, double epsilon, double horizon, ChangeBound &out) {
-    if (!std::isfinite(A) || A < 0 || !std::isfinite(B) || B < 0 || !std::isfinite(epsilon) || !(epsilon > 0) ||
-        !std::isfinite(horizon) || !(horizon > 0))
-        return err(GD_ERR_CONTROLLER, "invalid change-based refresh inputs");
-    out = {horizon, 0};
-    if (A > 0 && epsilon / A < out.duration) out = {epsilon / A, 1};
-    if (B > 0 && epsilon * epsilon / B < out.duration) out = {epsilon * epsilon / B, 2};
-    if (!(out.duration > 0)) return err(GD_ERR_CONTROLLER, "change-based timestep underflow");
-    return Status::ok();
+    if (code == 100 + 7) return err(GD_ERR_CONTINUATION_LIMIT, "local collision continuation limit exceeded", 7);
+    if (code > 100) return err(GD_ERR_CHAIN, "local collision chain error " + std::to_string(code - 100), code - 100);
+    return err(GD_ERR_CONTROLLER, "unknown controller state " + std::to_string(code), code);
 }
 
 int build_binmap(const Model &m, const std::vector<int> &raw_count, std::vector<int> &raw_to_merged) {
@@ -1451,100 +1378,37 @@ int build_binmap(const Model &m, const std::vector<int> &raw_count, std::vector<
 // _choose_col_bath (inc/swarm/_col_bound.cuh:288-310)
 Status choose_bath(const Model &m, const RateBin *bins, int count, double remaining, double limit_scale, double &out,
                    int *binding) {
-    double duration = std::min(remaining, m.col_bath_max);
-    double tolerance = m.col_bath_eps * limit_scale;
-    int reason = 0;
-    for (int b = 0; b < count; ++b) {
-        const RateBin &v = bins[b];
-        if (v.invalid_count) return err(GD_ERR_CONTROLLER, "invalid change-based rate moments");
-        if (!(v.mass > 0)) continue;
-        ChangeBound bound;
-        GD_TRY(change_limit(v.weighted_change / v.mass, v.weighted_second / v.mass, tolerance, duration, bound));
-        if (bound.duration < duration) {
-            duration = bound.duration;
-            reason = bound.reason;
-        }
-    }
-    if (binding) *binding = reason;
-    out = duration;
-    return Status::ok();
+    return ctl_status(ctl_choose_bath(m, bins, count, remaining, limit_scale, out, binding));
 }
 
 // _finish_col_bath (inc/swarm/_col_bound.cuh:313-403)
 Status finish_bath(const Model &m, const AuditBin *bins, int count, BathState &state, BathResult &result) {
-    result = BathResult();
-    int active_count = 0;
-    double total_mass = 0.0;
-    for (int b = 0; b < count; ++b) {
-        if (bins[b].invalid_count != 0)
-            return err(GD_ERR_CONTROLLER, "collision bath controller returned an invalid audit state");
-        if (bins[b].mass > 0.0) active_count++;
-        total_mass += bins[b].mass;
-    }
-    if (!(total_mass > 0.0)) return err(GD_ERR_CONTROLLER, "collision bath controller found no active represented mass");
-    double confidence_log = std::log(2.0 * static_cast<double>(active_count) / m.col_bath_alpha);
-    double mass_difference = 0.0;
-    for (int b = 0; b < count; ++b) {
-        const AuditBin &v = bins[b];
-        mass_difference += std::abs(v.end_mass - v.mass);
-        if (!(v.mass > 0.0)) continue;
-        double mass_sq = v.mass * v.mass;
-        double predicted_f = v.predicted_f / v.mass;
-        double predicted_e = v.predicted_e / v.mass;
-        double predicted_g = v.predicted_g / v.mass;
-        double touched = v.touched / v.mass;
-        double events = v.event_weight / v.mass;
-        double growth = v.growth / v.mass;
-        double weight_max = v.maximum_weight / v.mass;
-        double jump_max = v.maximum_g_jump / v.mass;
-        double upper_f = std::min(1.0, predicted_f + std::sqrt(2.0 * v.predicted_var_f / mass_sq * confidence_log) +
-                                           weight_max * confidence_log / 3.0);
-        double upper_e = predicted_e + std::sqrt(2.0 * v.predicted_var_e / mass_sq * confidence_log) +
-                         weight_max * confidence_log / 3.0;
-        double upper_g = predicted_g + std::sqrt(2.0 * v.predicted_var_g / mass_sq * confidence_log) +
-                         jump_max * confidence_log / 3.0;
-        result.max_f = std::max(result.max_f, predicted_f);
-        result.max_e = std::max(result.max_e, predicted_e);
-        result.max_touched = std::max(result.max_touched, touched);
-        result.max_events = std::max(result.max_events, events);
-        result.max_g = std::max(result.max_g, growth);
-        result.max_g_upper = std::max(result.max_g_upper, upper_g);
-        result.activity_overshoot = result.activity_overshoot || std::min(touched, 1.0) > upper_f || events > upper_e;
-        result.distribution_overshoot = result.distribution_overshoot || growth > std::max(m.col_bath_eps, upper_g);
-    }
-    result.d_bath = mass_difference / (2.0 * total_mass);
-    result.distribution_overshoot = result.distribution_overshoot || result.d_bath > m.col_bath_eps;
-    bool issue = result.activity_overshoot || result.distribution_overshoot;
-    bool at_floor = state.limit_scale <= 0.25 * (1.0 + 8.0 * std::numeric_limits<double>::epsilon());
-    if (issue) {
-        state.activity_streak++;
-        state.quiet_streak = 0;
-        state.floor_streak = at_floor ? state.floor_streak + 1 : 0;
-    } else {
-        state.activity_streak = 0;
-        state.quiet_streak++;
-        state.floor_streak = 0;
-    }
-    if (result.distribution_overshoot || state.activity_streak >= 2) {
-        state.limit_scale = std::max(0.25, 0.5 * state.limit_scale);
-        state.activity_streak = 0;
-    } else if (state.quiet_streak >= 3) {
-        state.limit_scale = std::min(1.0, 1.25 * state.limit_scale);
-        state.quiet_streak = 0;
-    }
-    result.persistent_overshoot = state.floor_streak >= 2;
-    return Status::ok();
+    return ctl_status(ctl_finish_bath(m, bins, count, state, result, nullptr));
 }
 
 // ------------------------------------------------------------------------------------------------
 // allocation and the operator
 // ------------------------------------------------------------------------------------------------
 Collider::~Collider() {
-    if (host_small) cudaFreeHost(host_small);
+    if (host_ctl) cudaFreeHost(host_ctl);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    if (body_stream) cudaStreamDestroy(body_stream);
 }
 
+static CtlDev *ctl_of(Collider &c) { return reinterpret_cast<CtlDev *>(c.ctl.ptr); }
+
+// accumulators of a CtlResult the host has read
+static CtlResult fresh_result(int operator_index) {
+    CtlResult r{};
+    r.operator_index = operator_index;
+    r.min_duration = HUGE_VAL;
+    return r;
+}
+
+constexpr int kRecordCapacity = 65536;  // bath records kept on the device between two reads
+
 Status collider_alloc(Collider &c, const Model &m, int n) {
-    if (m.local_groups > kMaxGroups) return err(GD_ERR_INVALID_ARGUMENT, "more than 256 controller groups");
+    if (m.local_groups > kCtlGroups) return err(GD_ERR_INVALID_ARGUMENT, "more than 256 controller groups");
     c.n = n;
     for (DevBuf<double> *b : {&c.size_old, &c.numr_old, &c.time, &c.hazard, &c.jump1, &c.jump2, &c.jumpmax, &c.rate,
                               &c.change_rate, &c.second_rate})
@@ -1563,19 +1427,86 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
     GD_TRY_CUDA(c.group_sorted.alloc(n));
     GD_TRY_CUDA(c.spatial.alloc(n));
     Small L = small_layout(m);
+    c.events_offset = L.events;
     GD_TRY_CUDA(c.small.alloc(L.total));
     GD_TRY_CUDA(cudaMemset(c.small.ptr, 0, L.total));
     GD_TRY_CUDA(cudaMemset(c.error.ptr, 0, sizeof(int) * n));
-    GD_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&c.host_small), L.total));
-    c.state.assign(m.local_groups, BathState());
     GD_TRY_CUDA(c.event_count.alloc(kEventCategories));
     GD_TRY_CUDA(c.event_log_mass.alloc(kEventCategories));
+    // the device controller: default bath states, no operator yet, empty accumulators
+    GD_TRY_CUDA(c.ctl.alloc(sizeof(CtlDev)));
+    {
+        std::unique_ptr<CtlDev> init(new CtlDev());  // value-initialised: zeros, default bath states
+        init->res = fresh_result(0);
+        GD_TRY_CUDA(cudaMemcpy(c.ctl.ptr, init.get(), sizeof(CtlDev), cudaMemcpyHostToDevice));
+    }
+    std::vector<double> logs(static_cast<size_t>(m.raw_bins) + 1);
+    for (int k = 0; k <= m.raw_bins; ++k) logs[k] = ctl_confidence_log(k, m.col_bath_alpha);
+    GD_TRY_CUDA(c.conf_log.alloc(logs.size()));
+    GD_TRY_CUDA(cudaMemcpy(c.conf_log.ptr, logs.data(), sizeof(double) * logs.size(), cudaMemcpyHostToDevice));
+    c.record_capacity = kRecordCapacity;
+    GD_TRY_CUDA(c.records.alloc(c.record_capacity));
+    GD_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&c.host_ctl), sizeof(CtlResult) + sizeof(unsigned long long)));
+    GD_TRY_CUDA(cudaStreamCreateWithFlags(&c.capture_stream, cudaStreamNonBlocking));
+    GD_TRY_CUDA(cudaStreamCreateWithFlags(&c.body_stream, cudaStreamNonBlocking));
     return Status::ok();
 }
 
-void collider_reset_state(Collider &c) {
-    for (auto &s : c.state) s = BathState();
-    c.summary = ControllerSummary();  // swarm_runtime.cu:490-496 resets both at an output boundary
+// The results of the operators run since the last read: error, counters, bath records.  Every
+// operator adds to one accumulator on the device, so a graph that holds several operators is read
+// once after it ran.
+Status collider_check(Collider &c, cudaStream_t s) {
+    CtlResult *hr = reinterpret_cast<CtlResult *>(c.host_ctl);
+    unsigned long long *hev = reinterpret_cast<unsigned long long *>(c.host_ctl + sizeof(CtlResult));
+    GD_TRY_CUDA(cudaMemcpyAsync(hr, &ctl_of(c)->res, sizeof(CtlResult), cudaMemcpyDeviceToHost, s));
+    GD_TRY_CUDA(cudaMemcpyAsync(hev, c.small.ptr + c.events_offset, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    const CtlResult r = *hr;
+    const unsigned long long events = *hev;
+    if (r.rec_count > 0) {
+        std::vector<BathRecord> recs(static_cast<size_t>(r.rec_count));
+        GD_TRY_CUDA(cudaMemcpyAsync(recs.data(), c.records.ptr, sizeof(BathRecord) * recs.size(),
+                                    cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaStreamSynchronize(s));
+        for (const BathRecord &rec : recs) c.summary.record(rec);
+    }
+    *hr = fresh_result(r.operator_index);
+    GD_TRY_CUDA(cudaMemcpyAsync(&ctl_of(c)->res, hr, sizeof(CtlResult), cudaMemcpyHostToDevice, s));
+    GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + c.events_offset, 0, sizeof(unsigned long long), s));
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    // the persistent chain is one launch per wave (the reference relaunches capped chains)
+    c.summary.operator_count = r.operator_index;
+    c.summary.wave_count += r.waves;
+    c.summary.continuation_launches += r.waves;
+    c.summary.records_dropped += r.rec_dropped;
+    c.stats = gd_operator_stats{};
+    c.stats.waves = r.waves;
+    c.stats.chain_launches = r.waves;
+    c.stats.owner_updates = r.owner_updates;
+    c.stats.events = static_cast<long long>(events);
+    c.stats.min_duration = r.min_duration;
+    c.stats.max_duration = r.max_duration;
+    c.launches += c.pending_launches + static_cast<long long>(c.body_launches) * r.waves;
+    c.pending_launches = 0;
+    c.results_pending = false;
+    if (r.error) {
+        Status st = ctl_status(r.error);
+        if (r.error < 100 && r.error_detail) st.detail = r.error_detail;
+        return st;
+    }
+    return Status::ok();
+}
+
+// An output boundary: bath states and the summary start afresh (swarm_runtime.cu:490-496); the
+// results of operators not read yet are read first.
+Status collider_reset_state(Collider &c, cudaStream_t s) {
+    Status st = Status::ok();
+    if (c.results_pending) st = collider_check(c, s);
+    ctl_launch_clear(ctl_of(c), s);
+    GD_TRY_CUDA(cudaGetLastError());
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    c.summary = ControllerSummary();
+    return st;
 }
 
 // _record_col_bath (_col_bound.cuh:219-238)
@@ -1643,124 +1574,141 @@ std::string ControllerSummary::json() const {
     return f.str();
 }
 
-static int chain_grid(const Model &m, size_t smem) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
+// Kernel attributes and persistent grid sizes, once per collider.
+static Status collider_setup(Collider &c, const Model &m) {
+    if (c.setup_done) return Status::ok();
+    const int K = m.n_k, R = m.raw_bins;
+    int dev = 0;
+    GD_TRY_CUDA(cudaGetDevice(&dev));
+    GD_TRY_CUDA(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
+    if (c.sms <= 0) c.sms = 1;
+    c.rate_smem = static_cast<size_t>(4) * (4 * 8 + 4) * K;
+    if (c.rate_smem > 48 * 1024) {
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(c.rate_smem)));
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(c.rate_smem)));
     }
+    if (R <= kAuditSmemBins)
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(audit_blocked_smem(R))));
+    c.chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
+    if (c.chain_smem > 48 * 1024)
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(c.chain_smem)));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chain, kChainWarps * 32, smem);
-    if (per_sm < 1) per_sm = 1;
-    return sms * per_sm;
+    GD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chain, kChainWarps * 32, c.chain_smem));
+    c.chain_grid = c.sms * (per_sm < 1 ? 1 : per_sm);
+    c.setup_done = true;
+    return Status::ok();
 }
 
-Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
-                          const double *measure, const unsigned char *active, int32_t *spatial_out, double duration,
-                          double total_dust_mass, cudaStream_t s) {
+// The operator's kernels, in stream order on q: the bath-start pass before the loop, then a
+// conditional WHILE node whose body, captured on the collider's body stream, is one wave.  q is
+// capturing (the collider's own capture or the caller's): no launch here depends on a value the
+// host reads back.
+static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
+                               const int32_t *codes, const double *measure, const unsigned char *active,
+                               int32_t *spatial_out, double duration, const double *duration_dev,
+                               double duration_scale, double total_dust_mass, cudaStream_t q) {
     const int K = m.n_k;
     const int G = m.local_groups, S = m.col_bin_s, R = m.raw_bins, W = (G + 31) / 32;
     const Small L = small_layout(m);
     int32_t *spatial = c.spatial.ptr;
     const int TPB = 256;
-    c.stats = gd_operator_stats{};
-    c.stats.min_duration = std::numeric_limits<double>::infinity();
-    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
-        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
-    // the reference's horizon check (_col_sched.cuh:30-33), made before any work is queued
-    if (!(duration > 0) || !std::isfinite(duration)) return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
+    const int persist = c.sms * 8;  // blocks of the grid-stride kernels
+    auto grid_for = [&](long long items, int per_block) {
+        return static_cast<int>(std::max(1ll, std::min<long long>((items + per_block - 1) / per_block, persist)));
+    };
+    CtlDev *ctl = ctl_of(c);
+    const WaveInfo *w = &ctl->wave;
+    long long pre = 0;
+    int body = 0;
 
-    GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.events, 0, 8, s));
     const bool env_on = use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM;
-    if (env_on) k_env_cache<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, reinterpret_cast<Env *>(c.env.ptr));
+    if (c.diagnostics) {
+        GD_TRY_CUDA(cudaMemsetAsync(c.event_count.ptr, 0, sizeof(unsigned long long) * kEventCategories, q));
+        GD_TRY_CUDA(cudaMemsetAsync(c.event_log_mass.ptr, 0, sizeof(double) * kEventCategories, q));
+    }
+    if (env_on) {
+        ++pre;
+        k_env_cache<<<(n + TPB - 1) / TPB, TPB, 0, q>>>(m, n, part, reinterpret_cast<Env *>(c.env.ptr));
+    }
+    CtlPtrs p;
+    p.gcount = at<int>(c.small, L.gcount);
+    p.gcursor = at<int>(c.small, L.gcursor);
+    p.graph = at<unsigned>(c.small, L.graph);
+    p.binmap = at<int>(c.small, L.binmap);
+    p.merged = at<int>(c.small, L.merged);
+    p.ratebin = at<RateBin>(c.small, L.ratebin);
+    p.audit = at<AuditBin>(c.small, L.audit);
+    p.error_flag = at<int>(c.small, L.error_flag);
+    p.dt = at<double>(c.small, L.dt);
+    p.records = c.records.ptr;
+    p.record_capacity = c.record_capacity;
+    p.conf_log = c.conf_log.ptr;
 
     // owner lists and the group dependency graph, once per geometry epoch
     if (!c.local_geometry_valid) {
-        GD_TRY(space_bin(m, part, n, spatial, s));
+        GD_TRY(space_bin(m, part, n, spatial, q));
+        ++pre;
         if (spatial_out && spatial_out != spatial)
-            GD_TRY_CUDA(cudaMemcpyAsync(spatial_out, spatial, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
-        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.gcount, 0, 4 * G, s));
-        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.graph, 0, 4 * G * W, s));
-        ++c.launches;
-        k_group_count<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, G, spatial, at<int>(c.small, L.gcount));
-        ++c.launches;
-        k_dep_graph<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, K, G, W, at<unsigned int>(c.small, L.graph),
+            GD_TRY_CUDA(cudaMemcpyAsync(spatial_out, spatial, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, q));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.gcount, 0, 4 * G, q));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.graph, 0, 4 * G * W, q));
+        pre += 4;
+        k_group_count<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, q>>>(n, G, spatial, at<int>(c.small, L.gcount));
+        k_dep_graph<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, q>>>(n, K, G, W, at<unsigned int>(c.small, L.graph),
                                                                              spatial, codes, active);
-        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.graph, c.small.ptr + L.graph, L.gcursor - L.graph,
-                                    cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaStreamSynchronize(s));
-        const int *gcount = at<int>(c.host_small, L.gcount);
-        c.group_start.assign(G + 1, 0);
-        for (int g = 0; g < G; ++g) c.group_start[g + 1] = c.group_start[g] + gcount[g];
-        const unsigned int *gr = at<unsigned int>(c.host_small, L.graph);
-        c.edges.assign(gr, gr + G * W);
-        GD_TRY_CUDA(cudaMemcpyAsync(c.small.ptr + L.gcursor, c.group_start.data(), 4 * G, cudaMemcpyHostToDevice, s));
-        ++c.launches;
-        k_group_fill<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, s>>>(n, G, spatial, at<int>(c.small, L.gcursor),
+        ctl_launch_geometry(ctl, p, G, q);
+        k_group_fill<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, q>>>(n, G, spatial, at<int>(c.small, L.gcursor),
                                                                               c.group_sorted.ptr);
         GD_TRY_CUDA(cudaGetLastError());
         // new neighbour lists and measures: no stored rate stands
-        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, q));
         c.local_geometry_valid = true;
     }
 
     const double lambda0 = n / static_cast<double>(K) / total_dust_mass;
     if (lambda0 != c.rated_lambda0) {
-        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, q));
         c.rated_lambda0 = lambda0;
     }
     const Env *env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
-    const size_t rate_smem = static_cast<size_t>(4) * (4 * 8 + 4) * K;
-    if (rate_smem > 48 * 1024) {
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(rate_smem)));
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(rate_smem)));
-    }
     const bool rate_cached = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m) && env;
-    if (R <= kAuditSmemBins)
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(audit_blocked_smem(R))));
-    const size_t chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
-    if (chain_smem > 48 * 1024)
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(chain_smem)));
 
     int *ids = c.ids.ptr;
     double *lower = at<double>(c.small, L.lower), *upper = at<double>(c.small, L.upper);
-    double *dt = at<double>(c.small, L.dt);
+    double *dt = p.dt;
     int *binmap = at<int>(c.small, L.binmap);
     RateBin *ratebin = at<RateBin>(c.small, L.ratebin);
     AuditBin *audit = at<AuditBin>(c.small, L.audit);
 
-    auto initialize = [&](const int *idp, int count) {
-        ++c.launches;
-        ++c.publish;
-        k_bath_init<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, c.size_old.ptr, c.numr_old.ptr, c.time.ptr,
-                                                            c.events.ptr, c.complete.ptr, c.hazard.ptr, c.jump1.ptr,
-                                                            c.jump2.ptr, c.jumpmax.ptr, c.stamp.ptr, c.publish);
+    // publish the reservoir of the wave's owners (kernels skip a wave without new rates)
+    auto initialize = [&](cudaStream_t st, int &launches) {
+        ++launches;
+        k_bath_init<<<grid_for(n, TPB), TPB, 0, st>>>(w, ids, part, c.size_old.ptr, c.numr_old.ptr, c.time.ptr,
+                                                       c.events.ptr, c.complete.ptr, c.hazard.ptr, c.jump1.ptr,
+                                                       c.jump2.ptr, c.jumpmax.ptr, c.stamp.ptr);
     };
-    // rates, size bins and merged rate bins, then one copy of binmap + rate bins to the host
-    auto rates_and_bins = [&](const int *idp, int count, int &merged) -> Status {
-        ++c.launches;
-        k_size_zero<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
-                                                         at<unsigned long long>(c.small, L.mmax));
-        ++c.launches;
+    // rates, size bins and merged rate bins of the wave's owners
+    auto rates_and_bins = [&](cudaStream_t st, int &launches) -> Status {
+        launches += 7;
+        k_size_zero<<<(G + TPB - 1) / TPB, TPB, 0, st>>>(G, at<unsigned long long>(c.small, L.mmin),
+                                                          at<unsigned long long>(c.small, L.mmax));
         if (G <= kScanSmemEntries)
-            k_size_scan_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(unsigned long long) * 2 * G,
-                                  s>>>(idp, count, part, spatial, active, G, at<unsigned long long>(c.small, L.mmin),
-                                       at<unsigned long long>(c.small, L.mmax));
+            k_size_scan_blocked<<<(n + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(unsigned long long) * 2 * G,
+                                  st>>>(w, ids, part, spatial, active, G, at<unsigned long long>(c.small, L.mmin),
+                                        at<unsigned long long>(c.small, L.mmax));
         else
-            k_size_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(idp, count, part, spatial, active,
-                                                                 at<unsigned long long>(c.small, L.mmin),
-                                                                 at<unsigned long long>(c.small, L.mmax));
-        ++c.launches;
-        k_size_bnds<<<(G + TPB - 1) / TPB, TPB, 0, s>>>(G, at<unsigned long long>(c.small, L.mmin),
-                                                         at<unsigned long long>(c.small, L.mmax), lower, upper);
+            k_size_scan<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(w, ids, part, spatial, active,
+                                                              at<unsigned long long>(c.small, L.mmin),
+                                                              at<unsigned long long>(c.small, L.mmax));
+        k_size_bnds<<<(G + TPB - 1) / TPB, TPB, 0, st>>>(G, at<unsigned long long>(c.small, L.mmin),
+                                                          at<unsigned long long>(c.small, L.mmax), lower, upper);
         RateArgs ra;
-        ra.ids = count == n ? nullptr : idp;  // every particle once: index order (per-owner results)
-        ra.count = count;
+        ra.ids = ids;
+        ra.w = w;
         ra.part = part;
         ra.codes = codes;
         ra.measure = measure;
@@ -1775,106 +1723,73 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
         ra.stamp = c.stamp.ptr;
         ra.rated = c.rated.ptr;
-        ra.publish = c.publish;
-        ++c.launches;
         if (rate_cached)
-            k_bath_rate<true><<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
+            k_bath_rate<true><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
         else
-            k_bath_rate<false><<<(count + 3) / 4, 128, rate_smem, s>>>(m, ra);
-        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, s));
-        ++c.launches;
+            k_bath_rate<false><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, st));
         if (R <= kScanSmemEntries)
-            k_count_bin_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(int) * R, s>>>(
-                m, idp, count, at<int>(c.small, L.counts), part, spatial, active, lower, upper, R);
+            k_count_bin_blocked<<<(n + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(int) * R, st>>>(
+                m, w, ids, at<int>(c.small, L.counts), part, spatial, active, lower, upper, R);
         else
-            k_count_bin<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, at<int>(c.small, L.counts), part,
-                                                                 spatial, active, lower, upper);
-        GD_TRY_CUDA(cudaMemsetAsync(ratebin, 0, sizeof(RateBin) * R, s));
-        ++c.launches;
-        k_binmap<<<1, 1, 0, s>>>(m, at<int>(c.small, L.counts), binmap, at<int>(c.small, L.merged), ratebin);
-        ++c.launches;
+            k_count_bin<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(m, w, ids, at<int>(c.small, L.counts), part, spatial,
+                                                              active, lower, upper);
+        GD_TRY_CUDA(cudaMemsetAsync(ratebin, 0, sizeof(RateBin) * R, st));
+        k_binmap<<<1, 1, 0, st>>>(m, w, at<int>(c.small, L.counts), binmap, at<int>(c.small, L.merged));
         if (R <= kScanSmemEntries)
-            k_rate_bins_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB,
-                                  (sizeof(double) * 4 + sizeof(int) * 2) * R, s>>>(
-                m, idp, count, ratebin, part, c.rate.ptr, c.change_rate.ptr, c.second_rate.ptr, spatial, binmap,
-                active, lower, upper, R);
+            k_rate_bins_blocked<<<(n + kAuditSpan - 1) / kAuditSpan, kAuditTPB,
+                                  (sizeof(double) * 4 + sizeof(int) * 2) * R, st>>>(
+                m, w, ids, ratebin, part, c.rate.ptr, c.change_rate.ptr, c.second_rate.ptr, spatial, binmap, active,
+                lower, upper, R);
         else
-            k_rate_bins<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(m, idp, count, ratebin, part, c.rate.ptr,
-                                                                 c.change_rate.ptr, c.second_rate.ptr, spatial, binmap,
-                                                                 active, lower, upper);
+            k_rate_bins<<<(n + TPB - 1) / TPB, TPB, 0, st>>>(m, w, ids, ratebin, part, c.rate.ptr, c.change_rate.ptr,
+                                                              c.second_rate.ptr, spatial, binmap, active, lower, upper);
         GD_TRY_CUDA(cudaGetLastError());
-        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.merged, c.small.ptr + L.merged, 4, cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.binmap, c.small.ptr + L.binmap, L.audit - L.binmap,
-                                    cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaStreamSynchronize(s));
-        merged = *at<int>(c.host_small, L.merged);
         return Status::ok();
     };
-    const int *h_binmap = at<int>(c.host_small, L.binmap);
-    const RateBin *h_ratebin = at<RateBin>(c.host_small, L.ratebin);
-    auto bin_end = [&](int g, int merged) { return g + 1 < G ? h_binmap[(g + 1) * S] : merged; };
-    auto requested_step = [&](int g, int merged, double &out) -> Status {
-        int first = h_binmap[g * S];
-        int last = bin_end(g, merged);
-        return choose_bath(m, h_ratebin + first, last - first, duration, c.state[g].limit_scale, out, nullptr);
-    };
 
-    c.summary.operator_count++;
-    const int operator_index = c.summary.operator_count;
-    if (c.diagnostics) {
-        GD_TRY_CUDA(cudaMemsetAsync(c.event_count.ptr, 0, sizeof(unsigned long long) * kEventCategories, s));
-        GD_TRY_CUDA(cudaMemsetAsync(c.event_log_mass.ptr, 0, sizeof(double) * kEventCategories, s));
-    }
-    int bath_index = 0;
-    // tick zero: every group starts from the same published reservoir
-    initialize(nullptr, n);
-    int merged = 0;
-    GD_TRY(rates_and_bins(nullptr, n, merged));
-    std::vector<double> requested(G);
-    for (int g = 0; g < G; ++g) GD_TRY(requested_step(g, merged, requested[g]));
-    Schedule sched;
-    GD_TRY(sched.init(duration, requested, c.edges));
-    std::vector<double> steps(G);
-    for (int g = 0; g < G; ++g) steps[g] = sched.seconds(sched.step[g]);
-    std::vector<bool> passed(G, true);
-    std::vector<double> current = requested;
-    const int grid_chain = chain_grid(m, chain_smem);
+    // the conditional that repeats the wave body, created in the graph q is capturing into
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t graph = nullptr;
+    GD_TRY_CUDA(cudaStreamGetCaptureInfo(q, &cs, nullptr, &graph));
+    if (cs != cudaStreamCaptureStatusActive) return err(GD_ERR_CUDA, "collision operator stream is not capturing");
+    cudaGraphConditionalHandle handle;
+    GD_TRY_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
 
-    while (sched.time() < sched.end) {
-        const std::uint64_t tick = sched.time();
-        std::vector<int> groups = sched.due(tick);
-        WaveTable wt;
-        wt.groups = 0;
-        int count = 0;
-        for (int g : groups) {
-            const int len = c.group_start[g + 1] - c.group_start[g];
-            if (len == 0) continue;
-            wt.start[wt.groups] = c.group_start[g];
-            wt.len[wt.groups] = len;
-            wt.out[wt.groups] = count;
-            wt.groups++;
-            count += len;
-        }
-        if (count == 0) {
-            sched.advance(groups);
-            continue;
-        }
-        ++c.launches;
-        k_wave_ids<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(wt, count, c.group_sorted.ptr, ids);
-        if (tick != 0) {
-            initialize(ids, count);
-            GD_TRY(rates_and_bins(ids, count, merged));
-            for (int g : groups) GD_TRY(requested_step(g, merged, current[g]));
-            GD_TRY(sched.adapt(tick, groups, current, passed));
-            for (int g : groups) steps[g] = sched.seconds(sched.step[g]);
-        }
-        GD_TRY_CUDA(cudaMemcpyAsync(dt, steps.data(), sizeof(double) * G, cudaMemcpyHostToDevice, s));
-        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, s));  // error_flag, queued, head
+    // tick zero: every group starts from the same published reservoir (_col_chain.cuh:175-214)
+    int pre_int = 0;
+    ctl_launch_reset(ctl, duration, duration_dev, duration_scale, n, G, S, R, q);
+    initialize(q, pre_int);
+    GD_TRY(rates_and_bins(q, pre_int));
+    ctl_launch_begin(ctl, m, p, handle, q);
+    ctl_launch_wave_ids(ctl, c.group_sorted.ptr, ids, grid_for(n, TPB), q);
+    pre += pre_int + 3;
+    GD_TRY_CUDA(cudaGetLastError());
+
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    GD_TRY_CUDA(cudaStreamGetCaptureInfo(q, &cs, nullptr, &graph, &deps, &ndeps));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop;
+    GD_TRY_CUDA(cudaGraphAddNode(&loop, graph, deps, ndeps, &cp));
+    cudaGraph_t wave_graph = cp.conditional.phGraph_out[0];
+    GD_TRY_CUDA(cudaStreamUpdateCaptureDependencies(q, &loop, 1, cudaStreamSetCaptureDependencies));
+
+    // the wave body (_col_chain.cuh:215-537): chains, audit, bath finish and schedule advance, then
+    // the next wave's owners, reservoir, rates and bath lengths
+    cudaStream_t b = c.body_stream;
+    GD_TRY_CUDA(cudaStreamBeginCaptureToGraph(b, wave_graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    Status st = [&]() -> Status {
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, b));  // error_flag, queued, head
         ChainArgs ca;
         // A wave of every group holds every particle once: the skip scan (whose queue order the chain
         // does not depend on) then walks them in index order, with coalesced per-particle loads.
-        ca.ids = count == n ? nullptr : ids;
-        ca.count = count;
+        ca.ids = ids;
+        ca.w = w;
         ca.rng = rng;
         ca.active = active;
         ca.measure = measure;
@@ -1890,8 +1805,7 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         ca.complete = c.complete.ptr;
         ca.queue = c.queue.ptr;
         ca.queued = at<int>(c.small, L.queued);
-        ++c.launches;
-        k_skip_scan<<<(count + TPB - 1) / TPB, TPB, 0, s>>>(ca);
+        k_skip_scan<<<grid_for(n, TPB), TPB, 0, b>>>(ca);
         ChainRun cr;
         cr.part_ro = part;
         cr.part = part;
@@ -1906,14 +1820,14 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         cr.events_total = at<unsigned long long>(c.small, L.events);
         cr.event_count = c.diagnostics ? c.event_count.ptr : nullptr;
         cr.event_log_mass = c.diagnostics ? c.event_log_mass.ptr : nullptr;
-        const int blocks = std::min(grid_chain, (count + kChainWarps - 1) / kChainWarps);
-        ++c.launches;
-        k_chain<<<blocks, kChainWarps * 32, chain_smem, s>>>(m, ca, cr);
+        const int blocks = std::min(c.chain_grid, (n + kChainWarps - 1) / kChainWarps);
+        k_chain<<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
         // audit of the completed baths
-        GD_TRY_CUDA(cudaMemsetAsync(audit, 0, sizeof(AuditBin) * R, s));
+        GD_TRY_CUDA(cudaMemsetAsync(audit, 0, sizeof(AuditBin) * R, b));
         AuditArgs aa;
         aa.ids = ids;
-        aa.count = count;
+        aa.w = w;
+        aa.count = 0;
         aa.bin = audit;
         aa.part = part;
         aa.size_old = c.size_old.ptr;
@@ -1930,59 +1844,77 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         aa.dt = dt;
         aa.lower = lower;
         aa.upper = upper;
-        ++c.launches;
         if (R <= kAuditSmemBins)
-            k_audit_bin_blocked<<<(count + kAuditSpan - 1) / kAuditSpan, kAuditTPB, audit_blocked_smem(R), s>>>(m, aa, R);
+            k_audit_bin_blocked<<<(n + kAuditSpan - 1) / kAuditSpan, kAuditTPB, audit_blocked_smem(R), b>>>(m, aa, R);
         else
-            k_audit_bin<<<(count + kAuditTPB - 1) / kAuditTPB, kAuditTPB, 0, s>>>(m, aa);
+            k_audit_bin<<<(n + kAuditTPB - 1) / kAuditTPB, kAuditTPB, 0, b>>>(m, aa);
+        ctl_launch_finish(ctl, m, p, handle, b);
+        ctl_launch_wave_ids(ctl, c.group_sorted.ptr, ids, grid_for(n, TPB), b);
+        body += 5;
+        initialize(b, body);
+        GD_TRY(rates_and_bins(b, body));
+        ctl_launch_adapt(ctl, m, p, handle, b);
+        body += 1;
         GD_TRY_CUDA(cudaGetLastError());
-        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small, c.small.ptr, L.binmap, cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaMemcpyAsync(c.host_small + L.audit, c.small.ptr + L.audit, sizeof(AuditBin) * merged,
-                                    cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaStreamSynchronize(s));
-        const int error_flag = *at<int>(c.host_small, L.error_flag);
-        c.stats.waves++;
-        c.stats.chain_launches++;
-        c.stats.owner_updates += count;
-        c.stats.events = static_cast<long long>(*at<unsigned long long>(c.host_small, L.events));
-        if (error_flag == 7)
-            return err(GD_ERR_CONTINUATION_LIMIT, "local collision continuation limit exceeded", error_flag);
-        if (error_flag) return err(GD_ERR_CHAIN, "local collision chain error " + std::to_string(error_flag), error_flag);
-        const AuditBin *h_audit = at<AuditBin>(c.host_small, L.audit);
-        for (int g : groups) {
-            if (c.group_start[g + 1] == c.group_start[g]) continue;
-            int first = h_binmap[g * S];
-            int last = bin_end(g, merged);
-            double mass = 0.0;
-            for (int b = first; b < last; ++b) {
-                if (h_audit[b].invalid_count) return err(GD_ERR_CONTROLLER, "invalid local audit state");
-                mass += h_audit[b].mass;
-            }
-            if (!(mass > 0)) continue;
-            BathResult res;
-            const double before = c.state[g].limit_scale;
-            GD_TRY(finish_bath(m, h_audit + first, last - first, c.state[g], res));
-            passed[g] = !(res.activity_overshoot || res.distribution_overshoot || res.persistent_overshoot);
-            BathRecord rec;
-            rec.group_index = g;
-            rec.operator_index = operator_index;
-            rec.bath_index = ++bath_index;
-            rec.merged_bins = last - first;
-            rec.duration = steps[g];
-            rec.limit_before = before;
-            rec.limit_after = c.state[g].limit_scale;
-            rec.result = res;
-            c.summary.record(rec);
-        }
-        c.summary.continuation_launches += 1;  // the persistent chain: one launch per wave
-        c.summary.wave_count++;
-        for (int g : groups) {
-            c.stats.min_duration = std::min(c.stats.min_duration, steps[g]);
-            c.stats.max_duration = std::max(c.stats.max_duration, steps[g]);
-        }
-        sched.advance(groups);
-    }
+        return Status::ok();
+    }();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b, &captured);
+    GD_TRY(st);
+    GD_TRY_CUDA(e);
+    c.pending_launches += pre;
+    c.body_launches = body;
     return Status::ok();
+}
+
+Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
+                          const double *measure, const unsigned char *active, int32_t *spatial_out, double duration,
+                          double total_dust_mass, cudaStream_t s, const double *duration_dev, double duration_scale) {
+    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
+        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+    // the reference's horizon check (_col_sched.cuh:30-33), made before any work is queued; a
+    // horizon on the device is checked by the controller
+    if (!duration_dev && (!(duration > 0) || !std::isfinite(duration)))
+        return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
+    GD_TRY(collider_setup(c, m));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    GD_TRY_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusInvalidated) return err(GD_ERR_CUDA, "the caller's stream capture is invalidated");
+    if (cs == cudaStreamCaptureStatusActive) {
+        // inside the caller's capture: the operator becomes part of the caller's graph, whose results
+        // gd_check_operator (collider_check) reads after it ran
+        GD_TRY(enqueue_operator(c, m, n, part, rng, codes, measure, active, spatial_out, duration, duration_dev,
+                                duration_scale, total_dust_mass, s));
+        c.results_pending = true;
+        return Status::ok();
+    }
+    // eager: capture the operator on the collider's stream, run the graph on s, read the results
+    cudaStream_t q = c.capture_stream;
+    GD_TRY_CUDA(cudaStreamBeginCapture(q, cudaStreamCaptureModeThreadLocal));
+    const Status st = enqueue_operator(c, m, n, part, rng, codes, measure, active, spatial_out, duration,
+                                       duration_dev, duration_scale, total_dust_mass, q);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(q, &graph);
+    if (!st || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        c.local_geometry_valid = false;
+        if (!st) return st;
+        GD_TRY_CUDA(e);
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie == cudaSuccess) ie = cudaGraphLaunch(exec, s);
+    if (ie != cudaSuccess) {
+        if (exec) cudaGraphExecDestroy(exec);
+        c.local_geometry_valid = false;
+        c.pending_launches = 0;
+        return cuda_status(ie, "collision operator graph");
+    }
+    c.results_pending = true;
+    const Status r = collider_check(c, s);
+    cudaGraphExecDestroy(exec);
+    return r;
 }
 
 }  // namespace gd

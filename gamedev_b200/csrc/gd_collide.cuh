@@ -55,39 +55,43 @@ struct ControllerSummary {
     double minimum_duration = HUGE_VAL, maximum_duration = 0.0, minimum_limit_scale = 1.0;
     double maximum_f = 0.0, maximum_e = 0.0, maximum_touched = 0.0, maximum_events = 0.0, maximum_g = 0.0,
            maximum_g_upper = 0.0, maximum_d_bath = 0.0;
+    long long records_dropped = 0;  // baths beyond the device record buffer between two reads
     std::vector<BathRecord> baths;
     void record(const BathRecord &r);
     std::string json() const;
 };
 
-// Power-of-two group scheduler on a 2^52-tick lattice (local_schedule, _col_sched.cuh:17-183).
-struct Schedule {
-    double horizon = 0;
-    std::vector<std::pair<int, int>> links;
-    std::vector<int> level;
-    std::vector<std::uint64_t> step, next;
-    std::uint64_t end = 0;
-    Status init(double h, const std::vector<double> &requested, const std::vector<unsigned int> &edges);
-    std::uint64_t time() const;
-    double seconds(std::uint64_t tick) const { return horizon * (double(tick) / double(end)); }
-    std::vector<int> due(std::uint64_t tick) const;
-    Status adapt(std::uint64_t tick, const std::vector<int> &groups, const std::vector<double> &requested,
-                 const std::vector<bool> &passed);
-    void advance(const std::vector<int> &groups) {
-        for (int c : groups) next[c] += step[c];
-    }
-};
-
-// Host controller pieces (inc/swarm/_col_bound.cuh:209-403), usable without a GPU.
-struct ChangeBound {
-    double duration;
-    int reason;
-};
-Status change_limit(double A, double B, double epsilon, double horizon, ChangeBound &out);
+// Host controller pieces (inc/swarm/_col_bound.cuh:209-403), usable without a GPU; the arithmetic
+// is gd_ctl_core.cuh's, shared with the device controller.
 int build_binmap(const Model &m, const std::vector<int> &raw_count, std::vector<int> &raw_to_merged);
 Status choose_bath(const Model &m, const RateBin *bins, int count, double remaining, double limit_scale,
                    double &out, int *binding);
 Status finish_bath(const Model &m, const AuditBin *bins, int count, BathState &state, BathResult &out);
+Status ctl_status(int code);  // a CtlCode as a status with the reference's message
+
+// The wave the operator's kernels serve, read from device memory: the device controller writes it,
+// so a wave's launches depend on nothing the host knows and the operator runs as one CUDA graph.
+struct WaveInfo {
+    int count;       // owners of this wave
+    int full;        // 1: the wave holds every particle (kernels walk them in index order)
+    int go;          // 1 while the operator runs
+    int need_rates;  // 1: this wave publishes its reservoir and evaluates its rates (tick > 0, or tick 0)
+    int publish;     // publish wave of the reservoir stamps (persists across operators)
+    int pad[3];
+};
+
+// Results of an operator the host reads back: error, counters, the baths recorded.
+struct CtlResult {
+    int error;             // a CtlCode, or 100 + the chain's error flag
+    int error_detail;
+    int waves;
+    int rec_count, rec_dropped;
+    int operator_index;
+    long long owner_updates;
+    double min_duration, max_duration;
+};
+
+struct CtlDev;  // the device controller's state (gd_devctl.cu)
 
 struct Collider {
     int n = 0;
@@ -99,22 +103,30 @@ struct Collider {
     // changed; rated[i] = publish wave at which owner i's rates were last evaluated (-1: never on
     // this geometry).  Rates depend only on the reservoir of the owner and its neighbours, the
     // neighbour list, measure, positions and lambda0, so an owner whose inputs are unchanged keeps
-    // bit-identical stored rates.
+    // bit-identical stored rates.  The publish counter lives in the device controller's WaveInfo.
     DevBuf<int> stamp, rated;
-    int publish = 0;
     double rated_lambda0 = 0.0;
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
     DevBuf<int> ids, queue, group_sorted, spatial;
-    // per-group / per-bin device scratch, one contiguous block so one copy returns it
-    DevBuf<unsigned char> small;      // see small_layout() in gd_collide.cu
-    // pinned host mirror of `small`
-    unsigned char *host_small = nullptr;
-    // host controller state
-    std::vector<int> group_start;     // [groups + 1] offsets into group_sorted
-    std::vector<unsigned int> edges;  // dependency rows, LOCAL_WORDS per group
-    std::vector<BathState> state;
-    ControllerSummary summary;        // reset with `state` at output boundaries
+    // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)
+    DevBuf<unsigned char> small;
+    size_t events_offset = 0;         // the events counter inside `small`
+    // device controller: scheduler, bath states, wave table, accumulated results (gd_devctl.cu)
+    DevBuf<unsigned char> ctl;        // one CtlDev
+    DevBuf<double> conf_log;          // log(2 c / COL_BATH_ALPHA) for c = 0..raw bins, host-evaluated
+    DevBuf<BathRecord> records;       // the baths of the operators since the last read
+    int record_capacity = 0;
+    unsigned char *host_ctl = nullptr;  // pinned: the CtlResult and the events counter read back
+    bool results_pending = false;     // operators ran whose results were not read yet
+    cudaStream_t capture_stream = nullptr;  // an eager operator is captured here, then launched
+    cudaStream_t body_stream = nullptr;     // the wave body is captured here into the conditional node
+    bool setup_done = false;          // kernel attributes raised, grids sized
+    int sms = 0, chain_grid = 0;
+    size_t rate_smem = 0, chain_smem = 0;
+    long long pending_launches = 0;   // launches outside the wave loop of the operators not read yet
+    int body_launches = 0;            // kernels of one wave body
+    ControllerSummary summary;        // reset with the bath states at output boundaries
     // COL_DIAGNOSTICS event bookkeeping of the last operator (when `diagnostics` is on): events
     // and summed log mass change per outcome category (event_work, _col_types.cuh:32-33)
     bool diagnostics = false;
@@ -127,16 +139,25 @@ struct Collider {
 };
 
 Status collider_alloc(Collider &c, const Model &m, int n);
-void collider_reset_state(Collider &c);
+// Bath states and the summary afresh (an output boundary); reads pending results first.
+Status collider_reset_state(Collider &c, cudaStream_t s);
+// Reads the results of the operators run since the last read (error, statistics, bath records)
+// and clears the device accumulators: synchronises s.
+Status collider_check(Collider &c, cudaStream_t s);
 
 // per-pair terms of the bath-start rate for the listed owners (diagnostics and parity checks)
 Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
                   const double *measure, const unsigned char *active, double total_dust_mass, int n, double *out,
                   cudaStream_t s);
 
-// evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539)
+// evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539) as one CUDA graph: the bath-start
+// pass, then a conditional WHILE node running one wave per iteration, every controller decision on
+// the device.  Eager when s is not capturing (the graph runs, the results are read, an error is
+// returned); inside the caller's capture it becomes part of that graph and collider_check reads the
+// results later.  The horizon is `duration`, or duration_scale * *duration_dev when given.
 Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
                           const int32_t *codes, const double *measure, const unsigned char *active,
-                          int32_t *spatial, double duration, double total_dust_mass, cudaStream_t s);
+                          int32_t *spatial, double duration, double total_dust_mass, cudaStream_t s,
+                          const double *duration_dev = nullptr, double duration_scale = 1.0);
 
 }  // namespace gd

@@ -1,14 +1,16 @@
-// Exported host controller (include/gd_b200_controller.h): thin C wrappers over the scheduler and
-// bath bounds the collision operator itself uses (gd_collide.cu).
+// Exported host controller (include/gd_b200_controller.h): thin C wrappers over the controller
+// arithmetic the collision operator's device controller runs (gd_ctl_core.cuh), here on the host.
 #include <cstring>
+#include <memory>
 #include <new>
 #include <vector>
 
 #include "../../include/gd_b200_controller.h"
 #include "gd_collide.cuh"
+#include "gd_ctl_core.cuh"
 
 struct gd_schedule {
-    gd::Schedule s;
+    gd::SchedCore s;
 };
 
 extern "C" {
@@ -75,7 +77,7 @@ gd_status gd_ctl_finish_bath(const gd_config *cfg, const double *audit, int n, d
 
 gd_schedule *gd_ctl_schedule_create(double horizon, const double *requested, int n, const unsigned *edges,
                                     gd_status *status) {
-    if (!requested || !edges || n <= 0) {
+    if (!requested || !edges || n <= 0 || n > gd::kCtlGroups) {
         if (status) *status = GD_ERR_INVALID_ARGUMENT;
         return nullptr;
     }
@@ -84,9 +86,7 @@ gd_schedule *gd_ctl_schedule_create(double horizon, const double *requested, int
         if (status) *status = GD_ERR_OUT_OF_MEMORY;
         return nullptr;
     }
-    std::vector<double> req(requested, requested + n);
-    std::vector<unsigned> e(edges, edges + n * ((n + 31) / 32));
-    gd::Status st = s->s.init(horizon, req, e);
+    const gd::Status st = gd::ctl_status(gd::sched_init(s->s, horizon, requested, n, edges));
     if (status) *status = st.code;
     if (!st) {
         delete s;
@@ -96,36 +96,36 @@ gd_schedule *gd_ctl_schedule_create(double horizon, const double *requested, int
 }
 
 void gd_ctl_schedule_destroy(gd_schedule *s) { delete s; }
-unsigned long long gd_ctl_schedule_time(const gd_schedule *s) { return s ? s->s.time() : 0ull; }
+unsigned long long gd_ctl_schedule_time(const gd_schedule *s) { return s ? gd::sched_time(s->s) : 0ull; }
 unsigned long long gd_ctl_schedule_end(const gd_schedule *s) { return s ? s->s.end : 0ull; }
 
 int gd_ctl_schedule_due(const gd_schedule *s, unsigned long long tick, int *groups) {
     if (!s) return 0;
-    std::vector<int> v = s->s.due(tick);
-    if (groups)
-        for (size_t i = 0; i < v.size(); ++i) groups[i] = v[i];
-    return static_cast<int>(v.size());
+    int due[gd::kCtlGroups];
+    const int k = gd::sched_due(s->s, tick, due);
+    if (groups) std::memcpy(groups, due, sizeof(int) * k);
+    return k;
 }
 
 gd_status gd_ctl_schedule_adapt(gd_schedule *s, unsigned long long tick, const int *groups, int n_groups,
                                 const double *requested, const int *passed) {
-    if (!s || (!groups && n_groups) || !requested || !passed) return GD_ERR_INVALID_ARGUMENT;
-    const int n = static_cast<int>(s->s.level.size());
-    std::vector<int> g(groups, groups + n_groups);
-    std::vector<double> req(requested, requested + n);
-    std::vector<bool> pass(n);
+    if (!s || (!groups && n_groups) || !requested || !passed || n_groups < 0 || n_groups > s->s.n)
+        return GD_ERR_INVALID_ARGUMENT;
+    const int n = s->s.n;
+    std::vector<unsigned char> pass(n);
     for (int c = 0; c < n; ++c) pass[c] = passed[c] != 0;
-    return s->s.adapt(tick, g, req, pass).code;
+    std::vector<int> work(3 * static_cast<size_t>(n));
+    return gd::ctl_status(gd::sched_adapt(s->s, tick, groups, n_groups, requested, pass.data(), work.data())).code;
 }
 
 void gd_ctl_schedule_advance(gd_schedule *s, const int *groups, int n_groups) {
-    if (!s || !groups) return;
-    s->s.advance(std::vector<int>(groups, groups + n_groups));
+    if (!s || !groups || n_groups < 0) return;
+    gd::sched_advance(s->s, groups, n_groups);
 }
 
 void gd_ctl_schedule_levels(const gd_schedule *s, int *levels) {
     if (!s || !levels) return;
-    for (size_t c = 0; c < s->s.level.size(); ++c) levels[c] = s->s.level[c];
+    for (int c = 0; c < s->s.n; ++c) levels[c] = s->s.level[c];
 }
 
 }  // extern "C"

@@ -1569,6 +1569,7 @@ Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle
     k_bad_index_reset<<<1, 32, 0, s>>>(g.counters.ptr);
     k_state_screen<<<(g.n + 255) / 256, 256, 0, s>>>(g.n, dev_particle, g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
+    if (g.deferred_check) return Status::ok();  // read by geometry_check later
     int cnt[2];
     GD_TRY(read_counters(g, s, cnt));
     if (cnt[1] != INT_MAX) {
@@ -1578,6 +1579,19 @@ Status state_screen(Geometry &g, const Model &m, const gd_particle *dev_particle
         st.msg = "non-finite particle state before collision search at particle " + std::to_string(cnt[1]);
         return st;
     }
+    return Status::ok();
+}
+
+// keeps the first failed screen of a captured step: a later build of the same step resets the
+// geometry's counter, and the reference stops at the first screen that fails
+__global__ void k_screen_keep(const int *counters, int *first) {
+    if (threadIdx.x == 0 && *first == INT_MAX && counters[1] != INT_MAX) *first = counters[1];
+}
+
+Status screen_keep(Geometry &g, int *first, cudaStream_t s) {
+    g.launches += 1;
+    k_screen_keep<<<1, 32, 0, s>>>(g.counters.ptr, first);
+    GD_TRY_CUDA(cudaGetLastError());
     return Status::ok();
 }
 

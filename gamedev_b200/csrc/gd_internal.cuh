@@ -158,6 +158,8 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
 // The non-finite screen of the last build: GD_ERR_NONFINITE with the smallest bad index, if any.
 // Synchronises the stream.
 Status geometry_check(Geometry &g, cudaStream_t s);
+// *first = the first bad index of the latest screen, unless an earlier one was kept (INT_MAX: none)
+Status screen_keep(Geometry &g, int *first, cudaStream_t s);
 // Exact top-K over the bucket tree.  Writes codes/measure/kth (any may be null).
 // With `radius` (per particle, may be null) the walk is first bounded by min(q, radius) and falls
 // back to q for owners that find fewer than K sites inside; `stats` (may be null) accumulates

@@ -187,6 +187,12 @@ class SwarmCollision:
         self._check(self.lib.gd_collision_operator(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
                                                    float(duration), float(total_dust_mass)))
 
+    def check_operator(self):
+        """gd_check_operator: the status, statistics and bath records of the operators a captured
+        CUDA graph ran (raises GdError with the first error any of them met)."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_check_operator(self.h))
+
     def evolve_collisions(self, particles, rng, duration: float, total_dust_mass: float):
         self.lib.gd_set_stream(self.h, _stream())
         self._check(self.lib.gd_evolve_collisions(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
@@ -253,6 +259,12 @@ class SwarmCollision:
         self.lib.gd_set_stream(self.h, _stream())
         self._check(self.lib.gd_step(self.h, C.byref(run), C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
                                      float(total_dust_mass), radius_model.h if radius_model else None))
+
+    def check_step(self):
+        """gd_check_step: after a replay of captured steps, the non-finite screen of the last
+        geometry build, else the first error of their collision operators (raises GdError)."""
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_check_step(self.h))
 
     def radius_features(self, particles, prev_kth_d2, total_mass: float, out=None):
         """Learned-radius features [n_p, 8] of the current geometry (gd_radius_features)."""

@@ -294,7 +294,8 @@ gd_status gd_space_bin(gd_handle *h, const gd_particle *dev_particle, int32_t *d
 gd_status gd_invalidate_geometry(gd_handle *h);
 
 /* Reset the per-group bath controller memory (local.state), as the reference does at every
- * output boundary (swarm_runtime.cu:490-496). */
+ * output boundary (swarm_runtime.cu:490-496).  Results of captured operators not read yet are
+ * read first (gd_check_operator) and their status returned. */
 gd_status gd_reset_controller(gd_handle *h);
 
 /* COL_DIAGNOSTICS controller summary of the current output interval (since the handle was created
@@ -317,16 +318,32 @@ gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_
  * fixed-position frozen-bath collision operator of length `duration`, mutating par_size and
  * par_numr of dev_particle and the RNG states in dev_rng.  Uses the neighbour cache built by
  * gd_knn (or set by gd_set_cache).  total_dust_mass enters lambda_0 = N_P/(N_K*M_dust)
- * (_col_chain.cuh:187). */
+ * (_col_chain.cuh:187).
+ *
+ * The operator is one CUDA graph: the bath-start pass, then a conditional WHILE node whose body
+ * is one wave (chains, audit, bath finish, schedule advance, the next wave's rates and bath
+ * lengths), with the controller's decisions made on the device; the host reads nothing between
+ * waves.  On a stream that is not capturing, the call runs that graph and returns its status.  On
+ * a stream the caller is capturing (cudaStreamBeginCapture on the handle's stream), the operator
+ * joins the caller's graph and the call returns GD_OK; after the caller's graph ran,
+ * gd_check_operator returns the status of the operators it held and brings their statistics and
+ * bath records to the host. */
 gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *dev_rng,
                                 double duration, double total_dust_mass);
+
+/* Results of the collision operators run since the last read (synchronises the handle's stream):
+ * the first error any of them met, the summed statistics (gd_last_operator_stats) and their bath
+ * records (gd_controller_summary).  An operator that meets an error stops after the wave that met
+ * it, as the reference's host loop does, and later operators do nothing until this call. */
+gd_status gd_check_operator(gd_handle *h);
 
 /* evolve_collisions (swarm_runtime.cu:357-471): non-finite screen (colstate_flag) when the
  * geometry is valid, else geometry build + gd_knn + space bins; then the collision operator. */
 gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *dev_rng,
                                double duration, double total_dust_mass);
 
-/* Controller statistics of the last operator: waves, chain launches, owners updated. */
+/* Controller statistics of the last operator (of the operators of the last gd_check_operator
+ * read, summed): waves, chain launches, owners updated, events, bath lengths. */
 typedef struct gd_operator_stats {
     int    waves;
     int    chain_launches;
@@ -475,9 +492,19 @@ gd_status gd_get_clock(gd_handle *h, double *clock_sim, double *clock_out, doubl
 gd_status gd_dynamics_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng);
 /* One full step, collisions included.  With radius_model (may be NULL) each geometry rebuild after
  * the first searches with the learned proposal seeded by the previous search's K-th distances; the
- * rows are the plain query's either way.  Reads the step's dt back once. */
+ * rows are the plain query's either way.  The collision halves read dt / 2 on the device, so the
+ * step reads nothing back between its kernels except the operators' results: eagerly, the call
+ * returns the first error met.  On a stream the caller is capturing, the whole step (screen or
+ * geometry, learned top-K, two graph-captured collision operators, dynamics, clocks) joins the
+ * caller's graph; capture it after one eager gd_step with the same arguments (the buffers are
+ * allocated then), and call gd_check_step after each replay. */
 gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particle, void *dev_rng,
                   double total_dust_mass, gd_radius_model *radius_model);
+/* After a replay of captured gd_step calls: the non-finite screen of the last geometry build
+ * (GD_ERR_NONFINITE with the particle index, as the eager step reports it), else the first error
+ * of their collision operators; brings the operators' statistics and bath records to the host.
+ * Synchronises the handle's stream. */
+gd_status gd_check_step(gd_handle *h);
 
 #ifdef __cplusplus
 }

@@ -139,3 +139,59 @@ def test_full_step_conserves_mass_and_learned_search_changes_nothing(gd, cuda):
             model.close()
         sw.close()
     assert np.array_equal(outs[0].view(np.uint64), outs[1].view(np.uint64))
+
+
+def test_captured_steps_equal_eager_steps(gd, cuda):
+    """gd_step captured once into a CUDA graph (after one eager step) and replayed: the particles,
+    the RNG streams and the clocks of eager steps, bit for bit; a non-finite particle written into
+    the buffer before a replay is reported by gd_check_step with its index."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    name = "t0_transport_3d"
+    cfg = workloads.config(name)
+    run = workloads.run_info(name)
+    p = workloads.particles(name, n=N)
+    mass = _mass(p)
+
+    def fresh():
+        sw = gd.SwarmCollision(cfg, N)
+        dp = gd.particles_to_device(p)
+        rng = gd.rngstate_init(N, seed=9)
+        sw.set_clock(0.0, 0.0, run.dt_out)
+        return sw, dp, rng
+
+    sw, dp, rng = fresh()
+    for _ in range(4):
+        sw.step(run, dp, rng, mass)
+    torch.cuda.synchronize()
+    e_part = dp.cpu().numpy()
+    e_uni = gd.rng_uniforms(rng, N, 4).cpu().numpy()
+    e_clk = sw.clock()
+    sw.close()
+
+    sw, dp, rng = fresh()
+    sw.step(run, dp, rng, mass)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        sw.step(run, dp, rng, mass)
+    for _ in range(3):
+        graph.replay()
+        sw.check_step()
+    torch.cuda.synchronize()
+    c_part = dp.cpu().numpy()
+    c_uni = gd.rng_uniforms(rng, N, 4).cpu().numpy()
+    c_clk = sw.clock()
+    assert np.array_equal(e_part.view(np.uint64), c_part.view(np.uint64))
+    assert np.array_equal(e_uni, c_uni)
+    assert c_clk == e_clk and c_clk["steps"] == 4
+    assert sw.last_operator_stats()["waves"] >= 2  # the replay's two operators
+
+    dp[777, 1] = float("nan")
+    graph.replay()
+    with pytest.raises(gd.GdError) as e:
+        sw.check_step()
+    assert e.value.status == 3 and e.value.detail == 777
+    del graph
+    sw.close()
