@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-step", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the C4 full Strang step line")
+    ap.add_argument("--c4-n", type=int, default=None, help="C4 particle count (default: the workload's 1e7)")
+    ap.add_argument("--c4-steps", type=int, default=2, help="timed C4 steps (the workload runs 1000)")
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     return ap.parse_args()
 
@@ -304,9 +307,84 @@ def run_reference(args):
         line.update({"value": cb["value"], "ms_per_step": n_active / cb["value"] * 1e3,
                      "reference_build": {"kind": "port", "why": "the reference's CUDA build (oracle/_ref) or a GPU "
                                                                 "is absent: the CPU port stands in"}})
+    if not args.no_c4 and args.workload == "c3_learned_3d" and have_gpu:
+        try:
+            line["c4_step"] = c4_reference(args, args.c4_n or workloads.CONFIGS[C4]["n"], 1, max(1, args.c4_steps))
+        except Exception as e:  # reported, never hidden
+            line["c4_step"] = {"error": str(e)}
     line["cpu_baseline"] = cb
     line["e2e"] = {"value": line["value"], "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
+
+
+C4 = "c4_production_3d"
+C4_DEFINITION = ("one Strang step of the c4 model (3D, N = 1e7, K = 64; drag and gravity, radiation pressure with "
+                 "Poynting-Robertson drag, Ito diffusion, coagulation and fragmentation): dt = min(DT_MAX, 1/max rate, "
+                 "dt_out - clock_out); C(dt/2) D(dt/2) T(dt) D(dt/2) C(dt/2), each C a geometry rebuild + exact top-K "
+                 "+ frozen-bath collision operator")
+
+
+def c4_step(args, gd, model, dev, world, rank, stream):
+    """The C4 line: gd_step captured once into a CUDA graph (after two eager steps: buffers, then the
+    learned search seeded by the first step's K-th distances) and replayed; device-timed."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    n = args.c4_n or workloads.CONFIGS[C4]["n"]
+    cfg = workloads.config(C4)
+    run = workloads.run_info(C4)
+    p = workloads.particles(C4, n=n, seed=workloads.CONFIGS[C4]["seed"] + rank)
+    mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p, device=dev)
+    rng = gd.rngstate_init(n, seed=4 + rank, device=dev)
+    sw.set_clock(0.0, 0.0, run.dt_out)
+    for _ in range(2):
+        sw.step(run, dp, rng, mass, model)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        sw.step(run, dp, rng, mass, model)
+    graph.replay()
+    sw.check_step()
+    k = max(1, args.c4_steps)
+    barrier(world)
+    a, b = _timed(stream, lambda: [graph.replay() for _ in range(k)])
+    barrier(world)
+    ms = reduce_max(a.elapsed_time(b), world) / k
+    sw.check_step()
+    clk = sw.clock()
+    ops = sw.last_operator_stats()
+    del graph
+    sw.close()
+    return {"steps_per_s": world * 1e3 / ms, "ms_per_step": ms, "n": n, "k": cfg.n_k, "steps_timed": k,
+            "steps_before": 3, "dt_s": clk["dt"], "graph_captured": True, "learned_radius": True,
+            "definition": C4_DEFINITION, "operators_of_timed_steps": ops,
+            "note": "the workload runs 1000 such steps; a few are timed here"}
+
+
+def c4_reference(args, n, warmup, steps):
+    """The reference's C4 step on this GPU: its dynamics (oracle/_ref/step_c4_production_3d_<n>/ref_step:
+    dyn_rate_calc + max_element, diffusion_pos, ssa_substep_1, optdepth_*, ssa_substep_2) plus two
+    half-operators (oracle/_ref/collide_c4_production_3d_<n>/ref_collide: geometry + evolve_collisions
+    of dt/2 each, dt the reference's own first timestep)."""
+    from gamedev_b200 import workloads
+    from oracle.ref import refcollide, refstep
+
+    if not (refcollide.available(C4, n) and refstep.available(C4, n)):
+        return {"unavailable": f"oracle/_ref builds of {C4} at {n} are absent"}
+    p = workloads.particles(C4, n=n, seed=workloads.CONFIGS[C4]["seed"])
+    mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+    _, _, dyn = refstep.run(C4, p, 4, warmup + steps, mass, timeout=1800)
+    dyn_ms = statistics.mean(dyn["ms"][warmup:])
+    half = 0.5 * dyn["dt"][0]
+    _, info = refcollide.run(C4, p, 4, half, mass, operators=1, steps=2 * (warmup + steps), timeout=1800)
+    halves = info["steps"][2 * warmup:]
+    col_ms = 2.0 * statistics.mean(sum(h) for h in halves)
+    ms = dyn_ms + col_ms
+    return {"steps_per_s": 1e3 / ms, "ms_per_step": ms, "n": n, "steps_timed": steps, "dt_s": dyn["dt"][0],
+            "dynamics_ms": dyn_ms, "collision_halves_ms": col_ms, "definition": C4_DEFINITION,
+            "programs": [f"oracle/_ref/step_{C4}_{n}/ref_step", f"oracle/_ref/collide_{C4}_{n}/ref_collide"]}
 
 
 def _which(name):
@@ -738,6 +816,13 @@ def run_ours(args):
                                     "last_operator": last_operator}
         except Exception as e:  # reported, never hidden
             result["swarm_step"] = {"error": str(e)}
+
+    # ---- C4: the full Strang step C(dt/2) D(dt/2) T(dt) D(dt/2) C(dt/2), one captured graph ----
+    if not args.no_c4 and args.workload == "c3_learned_3d":
+        try:
+            result["c4_step"] = c4_step(args, gd, model, dev, world, rank, stream)
+        except Exception as e:  # reported, never hidden
+            result["c4_step"] = {"error": str(e)}
 
     # ---- CPU baseline: the oracle on the host cores, rank 0 at N = 1 -----------------------
     if not args.no_cpu and rank == 0 and world == 1:

@@ -103,6 +103,9 @@ SIGNATURES = {
     "gd_batch_set_stream": (C.c_int, [_P, _P]),
     "gd_batch_knn": (C.c_int, [_P, _P, _P, _P, _P]),
     "gd_batch_check": (C.c_int, [_P]),
+    "gd_batch_collide": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "gd_batch_operator_stats": (C.c_int, [_P, C.c_int, C.POINTER(GdOperatorStats)]),
+    "gd_batch_invalidate": (C.c_int, [_P]),
     "gd_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_batch_error_detail": (C.c_longlong, [_P]),
     "gd_batch_launch_count": (C.c_longlong, [_P]),
@@ -128,6 +131,7 @@ SIGNATURES = {
     "gd_radius_model_predict": (C.c_int, [_P, _P, C.c_int, _P, _P]),
     "gd_radius_model_check": (C.c_int, [_P]),
     "gd_controller_summary": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "gd_operator_log": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_set_diagnostics": (C.c_int, [_P, C.c_int]),
     "gd_event_totals": (C.c_int, [_P, _P, _P]),
     "gd_frame_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t]),

@@ -228,7 +228,7 @@ size_t gd_last_error(const gd_handle *h, char *buf, size_t len) {
 long long gd_error_detail(const gd_handle *h) { return h ? h->detail : 0; }
 
 gd_status gd_rng_init(void *dev_rng, int n, unsigned long long seed, void *stream) {
-    if (!dev_rng || n < 0) return GD_ERR_INVALID_ARGUMENT;
+    if (!dev_rng || n < 0 || !gd::aligned_to(dev_rng, alignof(curandState))) return GD_ERR_INVALID_ARGUMENT;
     if (n == 0) return GD_OK;
     gd::k_rng_init<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<curandState *>(dev_rng), n, seed);
@@ -237,6 +237,7 @@ gd_status gd_rng_init(void *dev_rng, int n, unsigned long long seed, void *strea
 
 gd_status gd_geometry_build(gd_handle *h, const gd_particle *dev_particle) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!gd::aligned_to(dev_particle, 8)) return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle pointer");
     h->geom_valid = false;
     h->cache_valid = false;
     h->geo.sort_bits = h->tune.sort_bits;
@@ -291,6 +292,7 @@ gd_status gd_set_tuning(gd_handle *h, const gd_tuning *t) {
 gd_status gd_autotune(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int tune_sort,
                       gd_tuning *out_best, double *out_ms) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!gd::aligned_to(dev_particle, 8)) return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle pointer");
     const bool deferred = h->geo.deferred_check;
     h->geo.deferred_check = false;  // the tuner screens its input once, eagerly
     cudaEvent_t a = nullptr, b = nullptr;
@@ -427,6 +429,7 @@ gd_status gd_check_geometry(gd_handle *h) {
 gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
                  float *dev_kth_d2) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!gd::aligned_to(dev_particle, 8)) return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle pointer");
     if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "gd_knn called before gd_geometry_build");
     const bool own = !dev_codes && !dev_measure;
     int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
@@ -443,6 +446,7 @@ gd_status gd_knn(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_cod
 gd_status gd_knn_bounded(gd_handle *h, const gd_particle *dev_particle, const float *dev_radius, int32_t *dev_codes,
                          double *dev_measure, float *dev_kth_d2, unsigned long long *dev_stats) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null handle or particle pointer");
+    if (!gd::aligned_to(dev_particle, 8)) return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle pointer");
     if (!h->geom_valid) return fail(h, GD_ERR_NOT_READY, "gd_knn_bounded called before gd_geometry_build");
     const bool own = !dev_codes && !dev_measure;
     int32_t *codes = dev_codes ? dev_codes : h->codes.ptr;
@@ -537,6 +541,7 @@ gd_status gd_set_cache(gd_handle *h, const int32_t *dev_codes, const double *dev
 
 gd_status gd_space_bin(gd_handle *h, const gd_particle *dev_particle, int32_t *dev_spatial) {
     if (!h || !dev_particle) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!gd::aligned_to(dev_particle, 8)) return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle pointer");
     return done(h, gd::space_bin(h->m, dev_particle, h->n, dev_spatial ? dev_spatial : h->spatial.ptr, h->stream));
 }
 
@@ -560,8 +565,23 @@ gd_status gd_check_operator(gd_handle *h) {
 
 gd_status gd_set_diagnostics(gd_handle *h, int on) {
     if (!h || (on != 0 && on != 1)) return GD_ERR_INVALID_ARGUMENT;
+    if (on) {
+        gd::Status s = gd::collider_enable_log(h->col);
+        if (!s) return fail(h, s);
+    }
     h->col.diagnostics = on != 0;
     return GD_OK;
+}
+
+size_t gd_operator_log(const gd_handle *h, char *buf, size_t len) {
+    if (!h) return 0;
+    const std::string &text = h->col.operator_log;
+    if (buf && len) {
+        const size_t k = text.size() < len - 1 ? text.size() : len - 1;
+        std::memcpy(buf, text.data(), k);
+        buf[k] = '\0';
+    }
+    return text.size();
 }
 
 gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_mass) {
@@ -590,6 +610,8 @@ size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len) {
 gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *dev_rng, double duration,
                                 double total_dust_mass) {
     if (!h || !dev_particle || !dev_rng) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_rng, alignof(curandState)))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle or RNG pointer");
     if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "collision operator needs a neighbour cache");
     gd::Status s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
                                           h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr,
@@ -600,6 +622,8 @@ gd_status gd_collision_operator(gd_handle *h, gd_particle *dev_particle, void *d
 gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *dev_rng, double duration,
                                double total_dust_mass) {
     if (!h || !dev_particle || !dev_rng) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_rng, alignof(curandState)))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle or RNG pointer");
     gd::Status s;
     if (h->geom_valid && h->cache_valid) {
         s = gd::state_screen(h->geo, h->m, dev_particle, h->stream);
@@ -626,7 +650,9 @@ gd_status gd_evolve_collisions(gd_handle *h, gd_particle *dev_particle, void *de
 long long gd_launch_count(const gd_handle *h) { return h ? h->geo.launches + h->col.launches : 0; }
 
 gd_status gd_rng_uniforms(const void *dev_rng, int n, int count, double *dev_out, void *stream) {
-    if (!dev_rng || !dev_out || n < 0 || count < 0) return GD_ERR_INVALID_ARGUMENT;
+    if (!dev_rng || !dev_out || n < 0 || count < 0 || !gd::aligned_to(dev_rng, alignof(curandState)) ||
+        !gd::aligned_to(dev_out, 8))
+        return GD_ERR_INVALID_ARGUMENT;
     if (n == 0 || count == 0) return GD_OK;
     gd::k_rng_uniforms<<<(n + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const curandState *>(dev_rng), n, count, dev_out);
@@ -888,6 +914,8 @@ void invalidate(gd_handle *h) {
 
 gd::Status step_prepare(gd_handle *h, const gd_run_info *run, gd_particle *part, void *rng, gd::Dyn &d) {
     if (!run || !part || !rng) return gd::Status{GD_ERR_INVALID_ARGUMENT, "null pointer", 0};
+    if (!gd::aligned_to(part, 8) || !gd::aligned_to(rng, alignof(curandState)))
+        return gd::Status{GD_ERR_INVALID_ARGUMENT, "misaligned particle or RNG pointer", 0};
     GD_TRY(gd::dyn_validate(h->m, *run));
     d = gd::make_dyn(*run);
     GD_TRY(gd::dyn_alloc(h->dyn, h->m));
@@ -978,6 +1006,7 @@ gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particl
     // dt / 2 there (the operator's controller rejects a non-positive or non-finite one)
     if (s) s = gd::dyn_timestep(h->dyn, h->m, d, h->n, dev_particle, h->stream, &launches);
     const double *dt_dev = h->dyn.clock.ptr ? &h->dyn.clock.ptr->dt : nullptr;
+    const double *clock_sim_dev = h->dyn.clock.ptr ? &h->dyn.clock.ptr->clock_sim : nullptr;
     // C(dt/2): the geometry stays while the positions have not moved
     if (s) {
         if (h->geom_valid && h->cache_valid) s = gd::state_screen(h->geo, h->m, dev_particle, h->stream);
@@ -986,14 +1015,14 @@ gd_status gd_step(gd_handle *h, const gd_run_info *run, gd_particle *dev_particl
     if (s && captured) s = gd::screen_keep(h->geo, h->step_screen.ptr, h->stream);
     if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
                                       h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, 0.0,
-                                      total_dust_mass, h->stream, dt_dev, 0.5);
+                                      total_dust_mass, h->stream, dt_dev, 0.5, clock_sim_dev);
     // D(dt/2) T(dt) D(dt/2), then C(dt/2) on the moved positions
     if (s) s = step_dynamics(h, d, dev_particle, dev_rng, &launches);
     if (s) s = step_search(h, dev_particle, total_dust_mass, radius_model);
     if (s && captured) s = gd::screen_keep(h->geo, h->step_screen.ptr, h->stream);
     if (s) s = gd::collision_operator(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rng),
                                       h->codes.ptr, h->measure.ptr, h->geo.active.ptr, h->spatial.ptr, 0.0,
-                                      total_dust_mass, h->stream, dt_dev, 0.5);
+                                      total_dust_mass, h->stream, dt_dev, 0.5, clock_sim_dev);
     if (s) s = gd::dyn_clock_advance(h->dyn, h->stream, &launches);
     h->geo.launches += launches;
     h->geo.deferred_check = deferred;

@@ -8,14 +8,22 @@
 // screen is deferred to gd_batch_check, so a call makes no host synchronisation and can be
 // captured into a CUDA graph: about fifty kernels per call, whatever the number of swarms.
 #include <cuda_runtime.h>
+#include <curand_kernel.h>
 
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
 #include <string>
 #include <vector>
 
+#include "gd_collide.cuh"
 #include "gd_internal.cuh"
+
+// operators of one batch run side by side on this many forked streams (graph branches)
+constexpr int kBatchOperatorStreams = 16;
+// bath records each swarm's controller keeps between two reads
+constexpr int kBatchRecordCapacity = 1024;
 
 struct gd_batch {
     gd_config cfg;
@@ -35,6 +43,20 @@ struct gd_batch {
     gd::Tuning tune;
     std::string err;
     long long detail = 0;
+    // the batched collision operator: one collider per swarm, allocated at its first call
+    std::vector<std::unique_ptr<gd::Collider>> col;
+    cudaStream_t capture = nullptr;
+    cudaStream_t fork[kBatchOperatorStreams] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kBatchOperatorStreams] = {};
+    bool collide_pending = false;
+    ~gd_batch() {
+        for (int i = 0; i < kBatchOperatorStreams; ++i) {
+            if (fork[i]) cudaStreamDestroy(fork[i]);
+            if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (capture) cudaStreamDestroy(capture);
+    }
 };
 
 namespace {
@@ -130,6 +152,9 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
                        float *dev_kth_d2) {
     if (!b || !dev_particle || !dev_codes || !dev_measure || !dev_kth_d2)
         return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "null batch, particle or output pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_codes, 4) || !gd::aligned_to(dev_measure, 8) ||
+        !gd::aligned_to(dev_kth_d2, 4))
+        return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "misaligned particle or output pointer");
     const long long before = b->geo.launches;
     gd::Status st = gd::batch_geometry_build(b->geo, b->models[0], dev_particle, b->stream);
     b->launches += b->geo.launches - before;
@@ -138,9 +163,24 @@ gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *de
                              b->kcap, b->next.ptr, dev_particle, dev_codes, dev_measure, dev_kth_d2, b->stream,
                              &b->launches, b->tune);
     if (!st) return batch_fail(b, st);
+    for (auto &c : b->col) c->local_geometry_valid = false;  // new rows: the operators' owner lists follow
     b->err.clear();
     b->detail = 0;
     return GD_OK;
+}
+
+// the colliders' results since the last read; detail of an error = the swarm index
+static gd::Status batch_collide_check(gd_batch *b) {
+    std::vector<gd::Collider *> cs;
+    for (auto &c : b->col) cs.push_back(c.get());
+    int failed = -1;
+    gd::Status st = gd::collider_check_many(cs.data(), static_cast<int>(cs.size()), b->stream, &failed);
+    b->collide_pending = false;
+    if (!st) {
+        st.msg = "swarm " + std::to_string(failed) + ": " + st.msg;
+        st.detail = failed;
+    }
+    return st;
 }
 
 gd_status gd_batch_check(gd_batch *b) {
@@ -148,8 +188,123 @@ gd_status gd_batch_check(gd_batch *b) {
     int swarm = -1;
     gd::Status st = gd::batch_geometry_check(b->geo, b->stream, &swarm);
     if (!st) return batch_fail(b, st);
+    if (b->collide_pending) {
+        st = batch_collide_check(b);
+        if (!st) return batch_fail(b, st);
+    }
     b->err.clear();
     b->detail = 0;
+    return GD_OK;
+}
+
+// The operators of all swarms enqueued on q (capturing): forked onto the batch's streams after q's
+// work so far, joined back into q.
+static gd::Status batch_collide_enqueue(gd_batch *b, gd_particle *part, curandState *rng, const int32_t *codes,
+                                        const double *measure, const double *durations, const double *masses,
+                                        cudaStream_t q) {
+    const int F = b->S < kBatchOperatorStreams ? b->S : kBatchOperatorStreams;
+    GD_TRY_CUDA(cudaEventRecord(b->ev_fork, q));
+    for (int i = 0; i < F; ++i) GD_TRY_CUDA(cudaStreamWaitEvent(b->fork[i], b->ev_fork, 0));
+    gd::Status st = gd::Status::ok();
+    for (int s = 0; s < b->S && st; ++s) {
+        st = gd::collision_operator_enqueue(*b->col[s], b->models[s], b->n[s], part + b->part_off[s],
+                                            rng + b->part_off[s], codes + b->codes_off[s], measure + b->part_off[s],
+                                            b->geo.active.ptr + b->part_off[s], durations[s], masses[s],
+                                            b->fork[s % F]);
+    }
+    // join every forked stream, whatever happened, so that the capture can end
+    for (int i = 0; i < F; ++i) {
+        cudaEventRecord(b->ev_join[i], b->fork[i]);
+        cudaStreamWaitEvent(q, b->ev_join[i], 0);
+    }
+    GD_TRY(st);
+    GD_TRY_CUDA(cudaGetLastError());
+    return gd::Status::ok();
+}
+
+gd_status gd_batch_collide(gd_batch *b, gd_particle *dev_particle, void *dev_rng, const int32_t *dev_codes,
+                           const double *dev_measure, const double *durations, const double *total_dust_masses) {
+    if (!b || !dev_particle || !dev_rng || !dev_codes || !dev_measure || !durations || !total_dust_masses)
+        return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "null batch, particle, RNG, cache or argument pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_rng, alignof(curandState)) ||
+        !gd::aligned_to(dev_codes, 4) || !gd::aligned_to(dev_measure, 8))
+        return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "misaligned particle, RNG or cache pointer");
+    for (int s = 0; s < b->S; ++s)
+        if (!(durations[s] > 0) || !std::isfinite(durations[s]) || !(total_dust_masses[s] > 0) ||
+            !std::isfinite(total_dust_masses[s]))
+            return batch_fail(b, GD_ERR_INVALID_ARGUMENT, "invalid operator length or dust mass", s);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(b->stream, &cs) != cudaSuccess || cs == cudaStreamCaptureStatusInvalidated)
+        return batch_fail(b, GD_ERR_CUDA, "the batch stream's capture is invalid");
+    const bool outer = cs == cudaStreamCaptureStatusActive;
+    if (b->col.empty()) {
+        if (outer) return batch_fail(b, GD_ERR_NOT_READY, "run gd_batch_collide once before capturing it");
+        for (int s = 0; s < b->S; ++s) {
+            std::unique_ptr<gd::Collider> c(new (std::nothrow) gd::Collider());
+            if (!c) return batch_fail(b, GD_ERR_OUT_OF_MEMORY, "batch colliders");
+            gd::Status st = gd::collider_alloc(*c, b->models[s], b->n[s], kBatchRecordCapacity);
+            if (!st) {
+                b->col.clear();
+                return batch_fail(b, st);
+            }
+            b->col.push_back(std::move(c));
+        }
+        bool ok = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int i = 0; i < kBatchOperatorStreams && ok; ++i)
+            ok = cudaStreamCreateWithFlags(&b->fork[i], cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) return batch_fail(b, GD_ERR_CUDA, "batch operator streams");
+    }
+    gd_particle *part = dev_particle;
+    curandState *rng = static_cast<curandState *>(dev_rng);
+    if (outer) {
+        gd::Status st = batch_collide_enqueue(b, part, rng, dev_codes, dev_measure, durations, total_dust_masses,
+                                              b->stream);
+        if (!st) return batch_fail(b, st);
+        b->collide_pending = true;
+        return GD_OK;
+    }
+    // eager: one graph of every swarm's operator, run on the batch's stream, results read
+    if (cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return batch_fail(b, GD_ERR_CUDA, "batch operator capture");
+    gd::Status st = batch_collide_enqueue(b, part, rng, dev_codes, dev_measure, durations, total_dust_masses,
+                                          b->capture);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->capture, &graph);
+    if (!st || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        for (auto &c : b->col) c->local_geometry_valid = false;
+        if (!st) return batch_fail(b, st);
+        return batch_fail(b, gd::cuda_status(e, "batch operator capture"));
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie == cudaSuccess) ie = cudaGraphLaunch(exec, b->stream);
+    if (ie != cudaSuccess) {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto &c : b->col) c->local_geometry_valid = false;
+        return batch_fail(b, gd::cuda_status(ie, "batch operator graph"));
+    }
+    st = batch_collide_check(b);
+    cudaGraphExecDestroy(exec);
+    if (!st) return batch_fail(b, st);
+    b->err.clear();
+    b->detail = 0;
+    return GD_OK;
+}
+
+gd_status gd_batch_invalidate(gd_batch *b) {
+    if (!b) return GD_ERR_INVALID_ARGUMENT;
+    for (auto &c : b->col) c->local_geometry_valid = false;
+    return GD_OK;
+}
+
+gd_status gd_batch_operator_stats(const gd_batch *b, int s, gd_operator_stats *out) {
+    if (!b || !out || s < 0 || s >= b->S) return GD_ERR_INVALID_ARGUMENT;
+    if (b->col.empty()) return GD_ERR_NOT_READY;
+    *out = b->col[s]->stats;
     return GD_OK;
 }
 

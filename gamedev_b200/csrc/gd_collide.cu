@@ -1405,9 +1405,7 @@ static CtlResult fresh_result(int operator_index) {
     return r;
 }
 
-constexpr int kRecordCapacity = 65536;  // bath records kept on the device between two reads
-
-Status collider_alloc(Collider &c, const Model &m, int n) {
+Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
     if (m.local_groups > kCtlGroups) return err(GD_ERR_INVALID_ARGUMENT, "more than 256 controller groups");
     c.n = n;
     for (DevBuf<double> *b : {&c.size_old, &c.numr_old, &c.time, &c.hazard, &c.jump1, &c.jump2, &c.jumpmax, &c.rate,
@@ -1444,7 +1442,7 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
     for (int k = 0; k <= m.raw_bins; ++k) logs[k] = ctl_confidence_log(k, m.col_bath_alpha);
     GD_TRY_CUDA(c.conf_log.alloc(logs.size()));
     GD_TRY_CUDA(cudaMemcpy(c.conf_log.ptr, logs.data(), sizeof(double) * logs.size(), cudaMemcpyHostToDevice));
-    c.record_capacity = kRecordCapacity;
+    c.record_capacity = record_capacity > 0 ? record_capacity : 1;
     GD_TRY_CUDA(c.records.alloc(c.record_capacity));
     GD_TRY_CUDA(cudaMallocHost(reinterpret_cast<void **>(&c.host_ctl), sizeof(CtlResult) + sizeof(unsigned long long)));
     GD_TRY_CUDA(cudaStreamCreateWithFlags(&c.capture_stream, cudaStreamNonBlocking));
@@ -1454,47 +1452,119 @@ Status collider_alloc(Collider &c, const Model &m, int n) {
 
 // The results of the operators run since the last read: error, counters, bath records.  Every
 // operator adds to one accumulator on the device, so a graph that holds several operators is read
-// once after it ran.
-Status collider_check(Collider &c, cudaStream_t s) {
-    CtlResult *hr = reinterpret_cast<CtlResult *>(c.host_ctl);
-    unsigned long long *hev = reinterpret_cast<unsigned long long *>(c.host_ctl + sizeof(CtlResult));
-    GD_TRY_CUDA(cudaMemcpyAsync(hr, &ctl_of(c)->res, sizeof(CtlResult), cudaMemcpyDeviceToHost, s));
-    GD_TRY_CUDA(cudaMemcpyAsync(hev, c.small.ptr + c.events_offset, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    GD_TRY_CUDA(cudaStreamSynchronize(s));
-    const CtlResult r = *hr;
-    const unsigned long long events = *hev;
-    if (r.rec_count > 0) {
-        std::vector<BathRecord> recs(static_cast<size_t>(r.rec_count));
-        GD_TRY_CUDA(cudaMemcpyAsync(recs.data(), c.records.ptr, sizeof(BathRecord) * recs.size(),
-                                    cudaMemcpyDeviceToHost, s));
-        GD_TRY_CUDA(cudaStreamSynchronize(s));
-        for (const BathRecord &rec : recs) c.summary.record(rec);
-    }
-    *hr = fresh_result(r.operator_index);
-    GD_TRY_CUDA(cudaMemcpyAsync(&ctl_of(c)->res, hr, sizeof(CtlResult), cudaMemcpyHostToDevice, s));
-    GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + c.events_offset, 0, sizeof(unsigned long long), s));
-    GD_TRY_CUDA(cudaStreamSynchronize(s));
-    // the persistent chain is one launch per wave (the reference relaunches capped chains)
-    c.summary.operator_count = r.operator_index;
-    c.summary.wave_count += r.waves;
-    c.summary.continuation_launches += r.waves;
-    c.summary.records_dropped += r.rec_dropped;
-    c.stats = gd_operator_stats{};
-    c.stats.waves = r.waves;
-    c.stats.chain_launches = r.waves;
-    c.stats.owner_updates = r.owner_updates;
-    c.stats.events = static_cast<long long>(events);
-    c.stats.min_duration = r.min_duration;
-    c.stats.max_duration = r.max_duration;
-    c.launches += c.pending_launches + static_cast<long long>(c.body_launches) * r.waves;
-    c.pending_launches = 0;
-    c.results_pending = false;
-    if (r.error) {
-        Status st = ctl_status(r.error);
-        if (r.error < 100 && r.error_detail) st.detail = r.error_detail;
-        return st;
-    }
+// once after it ran.  Many colliders are read with three synchronisations in all.
+constexpr int kOperatorLogCapacity = 64;  // per-operator log records kept on the device between reads
+
+Status collider_enable_log(Collider &c) {
+    if (c.oplog.ptr) return Status::ok();
+    GD_TRY_CUDA(c.oplog.alloc(kOperatorLogCapacity));
+    c.oplog_capacity = kOperatorLogCapacity;
     return Status::ok();
+}
+
+// One line of the per-operator JSONL log, with the keys, order and number format the reference
+// writes (_col_chain.cuh:488-535, std::setprecision(17)).
+static std::string operator_log_line(const OperatorLog &r) {
+    std::ostringstream f;
+    f << std::setprecision(17);
+    f << "{\"schema\":1,\"method\":\"local_cached_collision\",\"operator\":" << r.operator_id
+      << ",\"clock_sim\":" << r.clock_sim << ",\"duration\":" << r.duration << ",\"waves\":" << r.waves
+      << ",\"owner_updates\":" << r.owner_updates << ",\"chain_blocks\":" << r.chain_blocks
+      << ",\"chain_launches\":" << r.chain_launches << ",\"chain_seconds\":" << r.chain_seconds
+      << ",\"audit_seconds\":" << r.audit_seconds << ",\"scheduler_wall_seconds\":" << r.wall_seconds
+      << ",\"finest_ticks\":" << r.finest_ticks << ",\"groups\":[";
+    for (int g = 0; g < r.G; ++g) {
+        const OperatorLogGroup &o = r.g[g];
+        if (g) f << ',';
+        f << "{\"id\":" << g << ",\"owners\":" << o.owners << ",\"level\":" << o.level << ",\"dt\":" << o.dt
+          << ",\"initial_level\":" << o.initial_level << ",\"coarsened_updates\":" << o.coarsened
+          << ",\"refined_updates\":" << o.refined << ",\"neighbor_constrained_updates\":" << o.constrained
+          << ",\"minimum_requested_dt\":" << o.min_request << ",\"maximum_requested_dt\":" << o.max_request
+          << ",\"final_requested_dt\":" << o.final_request << ",\"initial_requested_dt\":" << o.initial_request
+          << ",\"initial_binding_constraint\":" << o.binding << ",\"updates\":" << o.updates
+          << ",\"overshoots\":" << o.overshoots << ",\"persistent_overshoots\":" << o.persistent
+          << ",\"max_snapshot_age_at_start\":" << o.max_age << ",\"max_requested_dt_ratio\":" << o.max_ratio
+          << ",\"max_growth\":" << o.max_growth << ",\"max_predicted_activity\":" << o.max_activity << '}';
+    }
+    f << "],\"event_counts\":[";
+    for (int k = 0; k < kEventCategories; ++k) f << (k ? "," : "") << r.event_count[k];
+    f << "],\"event_log_mass_sums\":[";
+    for (int k = 0; k < kEventCategories; ++k) f << (k ? "," : "") << r.event_log_mass[k];
+    f << "]}\n";
+    return f.str();
+}
+
+Status collider_check_many(Collider *const *cs, int count, cudaStream_t s, int *first_failed) {
+    if (first_failed) *first_failed = -1;
+    for (int k = 0; k < count; ++k) {
+        Collider &c = *cs[k];
+        CtlResult *hr = reinterpret_cast<CtlResult *>(c.host_ctl);
+        unsigned long long *hev = reinterpret_cast<unsigned long long *>(c.host_ctl + sizeof(CtlResult));
+        GD_TRY_CUDA(cudaMemcpyAsync(hr, &ctl_of(c)->res, sizeof(CtlResult), cudaMemcpyDeviceToHost, s));
+        GD_TRY_CUDA(cudaMemcpyAsync(hev, c.small.ptr + c.events_offset, sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, s));
+    }
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    std::vector<CtlResult> res(count);
+    std::vector<unsigned long long> events(count);
+    std::vector<std::vector<BathRecord>> recs(count);
+    std::vector<std::vector<OperatorLog>> logs(count);
+    for (int k = 0; k < count; ++k) {
+        Collider &c = *cs[k];
+        res[k] = *reinterpret_cast<CtlResult *>(c.host_ctl);
+        events[k] = *reinterpret_cast<unsigned long long *>(c.host_ctl + sizeof(CtlResult));
+        const int nrec = res[k].rec_count < c.record_capacity ? res[k].rec_count : c.record_capacity;
+        if (nrec > 0) {
+            recs[k].resize(static_cast<size_t>(nrec));
+            GD_TRY_CUDA(cudaMemcpyAsync(recs[k].data(), c.records.ptr, sizeof(BathRecord) * recs[k].size(),
+                                        cudaMemcpyDeviceToHost, s));
+        }
+        const int nlog = res[k].log_count < c.oplog_capacity ? res[k].log_count : c.oplog_capacity;
+        if (nlog > 0) {
+            logs[k].resize(static_cast<size_t>(nlog));
+            GD_TRY_CUDA(cudaMemcpyAsync(logs[k].data(), c.oplog.ptr, sizeof(OperatorLog) * logs[k].size(),
+                                        cudaMemcpyDeviceToHost, s));
+        }
+        CtlResult *hr = reinterpret_cast<CtlResult *>(c.host_ctl);
+        *hr = fresh_result(res[k].operator_index);
+        GD_TRY_CUDA(cudaMemcpyAsync(&ctl_of(c)->res, hr, sizeof(CtlResult), cudaMemcpyHostToDevice, s));
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + c.events_offset, 0, sizeof(unsigned long long), s));
+    }
+    GD_TRY_CUDA(cudaStreamSynchronize(s));
+    Status first = Status::ok();
+    for (int k = 0; k < count; ++k) {
+        Collider &c = *cs[k];
+        const CtlResult &r = res[k];
+        for (const BathRecord &rec : recs[k]) c.summary.record(rec);
+        for (const OperatorLog &rec : logs[k]) c.operator_log += operator_log_line(rec);
+        c.summary.records_dropped += r.log_dropped;
+        // the persistent chain is one launch per wave (the reference relaunches capped chains)
+        c.summary.operator_count = r.operator_index;
+        c.summary.wave_count += r.waves;
+        c.summary.continuation_launches += r.waves;
+        c.summary.records_dropped += r.rec_dropped;
+        c.stats = gd_operator_stats{};
+        c.stats.waves = r.waves;
+        c.stats.chain_launches = r.waves;
+        c.stats.owner_updates = r.owner_updates;
+        c.stats.events = static_cast<long long>(events[k]);
+        c.stats.min_duration = r.min_duration;
+        c.stats.max_duration = r.max_duration;
+        c.launches += c.pending_launches + static_cast<long long>(c.body_launches) * r.waves;
+        c.pending_launches = 0;
+        c.results_pending = false;
+        if (r.error && first) {
+            first = ctl_status(r.error);
+            if (r.error < 100 && r.error_detail) first.detail = r.error_detail;
+            if (first_failed) *first_failed = k;
+        }
+    }
+    return first;
+}
+
+Status collider_check(Collider &c, cudaStream_t s) {
+    Collider *one = &c;
+    return collider_check_many(&one, 1, s, nullptr);
 }
 
 // An output boundary: bath states and the summary start afresh (swarm_runtime.cu:490-496); the
@@ -1610,7 +1680,8 @@ static Status collider_setup(Collider &c, const Model &m) {
 static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
                                const int32_t *codes, const double *measure, const unsigned char *active,
                                int32_t *spatial_out, double duration, const double *duration_dev,
-                               double duration_scale, double total_dust_mass, cudaStream_t q) {
+                               double duration_scale, const double *clock_sim_dev, double total_dust_mass,
+                               cudaStream_t q) {
     const int K = m.n_k;
     const int G = m.local_groups, S = m.col_bin_s, R = m.raw_bins, W = (G + 31) / 32;
     const Small L = small_layout(m);
@@ -1647,6 +1718,12 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
     p.records = c.records.ptr;
     p.record_capacity = c.record_capacity;
     p.conf_log = c.conf_log.ptr;
+    const bool log_on = c.diagnostics && c.oplog.ptr;
+    p.queued = log_on ? at<int>(c.small, L.queued) : nullptr;
+    p.oplog = log_on ? c.oplog.ptr : nullptr;
+    p.oplog_capacity = log_on ? c.oplog_capacity : 0;
+    p.event_count = log_on ? c.event_count.ptr : nullptr;
+    p.event_log_mass = log_on ? c.event_log_mass.ptr : nullptr;
 
     // owner lists and the group dependency graph, once per geometry epoch
     if (!c.local_geometry_valid) {
@@ -1758,7 +1835,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
 
     // tick zero: every group starts from the same published reservoir (_col_chain.cuh:175-214)
     int pre_int = 0;
-    ctl_launch_reset(ctl, duration, duration_dev, duration_scale, n, G, S, R, q);
+    ctl_launch_reset(ctl, duration, duration_dev, duration_scale, clock_sim_dev, n, G, S, R, q);
     initialize(q, pre_int);
     GD_TRY(rates_and_bins(q, pre_int));
     ctl_launch_begin(ctl, m, p, handle, q);
@@ -1784,6 +1861,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
     cudaStream_t b = c.body_stream;
     GD_TRY_CUDA(cudaStreamBeginCaptureToGraph(b, wave_graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     Status st = [&]() -> Status {
+        if (log_on) ctl_launch_mark(ctl, 0, b);
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, b));  // error_flag, queued, head
         ChainArgs ca;
         // A wave of every group holds every particle once: the skip scan (whose queue order the chain
@@ -1822,6 +1900,10 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         cr.event_log_mass = c.diagnostics ? c.event_log_mass.ptr : nullptr;
         const int blocks = std::min(c.chain_grid, (n + kChainWarps - 1) / kChainWarps);
         k_chain<<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
+        if (log_on) {
+            ctl_launch_mark(ctl, 1, b);
+            body += 2;
+        }
         // audit of the completed baths
         GD_TRY_CUDA(cudaMemsetAsync(audit, 0, sizeof(AuditBin) * R, b));
         AuditArgs aa;
@@ -1867,9 +1949,23 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
     return Status::ok();
 }
 
+Status collision_operator_enqueue(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
+                                  const int32_t *codes, const double *measure, const unsigned char *active,
+                                  double duration, double total_dust_mass, cudaStream_t q) {
+    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
+        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+    if (!(duration > 0) || !std::isfinite(duration)) return err(GD_ERR_INVALID_ARGUMENT, "invalid local collision horizon");
+    GD_TRY(collider_setup(c, m));
+    GD_TRY(enqueue_operator(c, m, n, part, rng, codes, measure, active, nullptr, duration, nullptr, 1.0, nullptr,
+                            total_dust_mass, q));
+    c.results_pending = true;
+    return Status::ok();
+}
+
 Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
                           const double *measure, const unsigned char *active, int32_t *spatial_out, double duration,
-                          double total_dust_mass, cudaStream_t s, const double *duration_dev, double duration_scale) {
+                          double total_dust_mass, cudaStream_t s, const double *duration_dev, double duration_scale,
+                          const double *clock_sim_dev) {
     if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
         return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
     // the reference's horizon check (_col_sched.cuh:30-33), made before any work is queued; a
@@ -1884,7 +1980,7 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
         // inside the caller's capture: the operator becomes part of the caller's graph, whose results
         // gd_check_operator (collider_check) reads after it ran
         GD_TRY(enqueue_operator(c, m, n, part, rng, codes, measure, active, spatial_out, duration, duration_dev,
-                                duration_scale, total_dust_mass, s));
+                                duration_scale, clock_sim_dev, total_dust_mass, s));
         c.results_pending = true;
         return Status::ok();
     }
@@ -1892,7 +1988,7 @@ Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part,
     cudaStream_t q = c.capture_stream;
     GD_TRY_CUDA(cudaStreamBeginCapture(q, cudaStreamCaptureModeThreadLocal));
     const Status st = enqueue_operator(c, m, n, part, rng, codes, measure, active, spatial_out, duration,
-                                       duration_dev, duration_scale, total_dust_mass, q);
+                                       duration_dev, duration_scale, clock_sim_dev, total_dust_mass, q);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(q, &graph);
     if (!st || e != cudaSuccess) {

@@ -89,6 +89,30 @@ struct CtlResult {
     int operator_index;
     long long owner_updates;
     double min_duration, max_duration;
+    int log_count, log_dropped;  // operator-log records written since the last read
+};
+
+// One group's line of the COL_DIAGNOSTICS per-operator log (local_group_stats and the schedule
+// counters of _col_chain.cuh:25-31, 266-289, 488-517).
+struct OperatorLogGroup {
+    int owners, level, initial_level, binding;
+    double dt, min_request, max_request, final_request, initial_request;
+    double max_age, max_ratio, max_growth, max_activity;
+    unsigned long long coarsened, refined, constrained, updates;
+    int overshoots, persistent;
+};
+constexpr int kLogGroups = 256;  // groups one record holds (the controller's maximum)
+// One operator's record of that log (_col_chain.cuh:488-535).  chain_launches counts the persistent
+// chain's launches (one per wave) and chain_blocks the owners each launch started with; the
+// reference relaunches capped chains and counts every relaunch.  The seconds are device time
+// (%globaltimer) between the controller's marks.
+struct OperatorLog {
+    unsigned long long operator_id, finest_ticks, owner_updates, chain_blocks;
+    int waves, chain_launches, G, pad;
+    double clock_sim, duration, chain_seconds, audit_seconds, wall_seconds;
+    unsigned long long event_count[kEventCategories];
+    double event_log_mass[kEventCategories];
+    OperatorLogGroup g[kLogGroups];
 };
 
 struct CtlDev;  // the device controller's state (gd_devctl.cu)
@@ -132,18 +156,33 @@ struct Collider {
     bool diagnostics = false;
     DevBuf<unsigned long long> event_count;
     DevBuf<double> event_log_mass;
+    // the per-operator JSONL log of COL_DIAGNOSTICS: device records until read, then text
+    DevBuf<OperatorLog> oplog;
+    int oplog_capacity = 0;
+    std::string operator_log;
     bool local_geometry_valid = false;
     gd_operator_stats stats{};
     long long launches = 0;           // kernels launched by the operator (reported by the ABI)
     ~Collider();
 };
 
-Status collider_alloc(Collider &c, const Model &m, int n);
+constexpr int kRecordCapacity = 65536;  // bath records kept on the device between two reads
+Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity = kRecordCapacity);
 // Bath states and the summary afresh (an output boundary); reads pending results first.
 Status collider_reset_state(Collider &c, cudaStream_t s);
 // Reads the results of the operators run since the last read (error, statistics, bath records)
 // and clears the device accumulators: synchronises s.
 Status collider_check(Collider &c, cudaStream_t s);
+// The same for many colliders with three synchronisations in all; the first error, and in
+// *first_failed the index of its collider (-1: none).
+Status collider_check_many(Collider *const *cs, int count, cudaStream_t s, int *first_failed);
+
+// One operator enqueued on q, which must be capturing (a graph the caller builds, e.g. many
+// swarms' operators on forked streams): the results are read by collider_check(_many) after the
+// graph ran.
+Status collision_operator_enqueue(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
+                                  const int32_t *codes, const double *measure, const unsigned char *active,
+                                  double duration, double total_dust_mass, cudaStream_t q);
 
 // per-pair terms of the bath-start rate for the listed owners (diagnostics and parity checks)
 Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
@@ -158,6 +197,9 @@ Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *
 Status collision_operator(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
                           const int32_t *codes, const double *measure, const unsigned char *active,
                           int32_t *spatial, double duration, double total_dust_mass, cudaStream_t s,
-                          const double *duration_dev = nullptr, double duration_scale = 1.0);
+                          const double *duration_dev = nullptr, double duration_scale = 1.0,
+                          const double *clock_sim_dev = nullptr);
+// The per-operator log (COL_DIAGNOSTICS) needs its device records: allocated when diagnostics turn on.
+Status collider_enable_log(Collider &c);
 
 }  // namespace gd

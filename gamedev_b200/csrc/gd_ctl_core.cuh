@@ -334,6 +334,18 @@ struct CtlDev {
     BathState state[kCtlGroups];  // persists across operators until a controller reset
     int work[3 * kCtlGroups];
     SchedCore sched;
+    // COL_DIAGNOSTICS bookkeeping of the current operator (_col_chain.cuh:261-289)
+    struct GroupStat {
+        double published, initial_request, min_request, max_request, max_age, max_ratio, max_growth, max_activity;
+        unsigned long long coarsened, refined, constrained, updates;
+        int initial_level, binding, overshoots, persistent;
+    } gstat[kCtlGroups];
+    int previous_level[kCtlGroups];
+    unsigned long long log_operator;    // operators since the controller was created (never reset)
+    unsigned long long op_updates, op_blocks;
+    int op_waves;
+    unsigned long long t_begin, t_mark0, t_mark1, chain_ns, audit_ns;
+    double clock_sim;
 };
 
 // Device pointers the controller kernels read and write (the operator's small scratch).
@@ -350,16 +362,23 @@ struct CtlPtrs {
     BathRecord *records;
     int record_capacity;
     const double *conf_log;
+    // COL_DIAGNOSTICS (all null when off)
+    const int *queued;                    // owners the wave's skip scan queued
+    OperatorLog *oplog;
+    int oplog_capacity;
+    const unsigned long long *event_count;
+    const double *event_log_mass;
 };
 
 // host launchers (gd_devctl.cu)
 void ctl_launch_geometry(CtlDev *c, const CtlPtrs &p, int G, cudaStream_t s);
-void ctl_launch_reset(CtlDev *c, double duration, const double *duration_dev, double scale, int n, int G, int S,
-                      int R, cudaStream_t s);
+void ctl_launch_reset(CtlDev *c, double duration, const double *duration_dev, double scale, const double *clock_sim,
+                      int n, int G, int S, int R, cudaStream_t s);
 void ctl_launch_clear(CtlDev *c, cudaStream_t s);
 void ctl_launch_begin(CtlDev *c, const Model &m, const CtlPtrs &p, cudaGraphConditionalHandle h, cudaStream_t s);
 void ctl_launch_finish(CtlDev *c, const Model &m, const CtlPtrs &p, cudaGraphConditionalHandle h, cudaStream_t s);
 void ctl_launch_adapt(CtlDev *c, const Model &m, const CtlPtrs &p, cudaGraphConditionalHandle h, cudaStream_t s);
 void ctl_launch_wave_ids(CtlDev *c, const int *sorted, int *ids, int grid, cudaStream_t s);
+void ctl_launch_mark(CtlDev *c, int which, cudaStream_t s);  // device-time marks of COL_DIAGNOSTICS
 
 }  // namespace gd

@@ -16,6 +16,12 @@ namespace {
 
 constexpr long long kEmptyWaveLimit = 1ll << 20;  // empty waves in a row before the scheduler gives up
 
+__device__ __forceinline__ unsigned long long device_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ void ctl_fail(CtlDev &c, int code, int detail) {
     if (!c.res.error) {
         c.res.error = code;
@@ -47,6 +53,9 @@ __device__ void next_wave(CtlDev &c) {
         }
         c.tick = t;
         c.ndue = sched_due(c.sched, t, c.due);
+        // every due group publishes at the wave's time, empty ones too (_col_chain.cuh:296-301)
+        const double now = sched_seconds(c.sched, t);
+        for (int k = 0; k < c.ndue; ++k) c.gstat[c.due[k]].published = now;
         int count = 0, w = 0;
         for (int k = 0; k < c.ndue; ++k) {
             const int g = c.due[k];
@@ -72,6 +81,71 @@ __device__ void next_wave(CtlDev &c) {
     }
 }
 
+// COL_DIAGNOSTICS statistics of the wave's nonempty due groups once their bath lengths are set
+// (_col_chain.cuh:344-356): the oldest linked reservoir and the bath length over the request.
+__device__ void wave_stats(CtlDev &c, const CtlPtrs &p, const double *request) {
+    const double now = sched_seconds(c.sched, c.tick);
+    const int words = (c.G + 31) / 32;
+    for (int k = 0; k < c.ndue; ++k) {
+        const int g = c.due[k];
+        if (c.group_start[g + 1] == c.group_start[g]) continue;
+        CtlDev::GroupStat &st = c.gstat[g];
+        for (int d = 0; d < c.G; ++d)
+            if (ctl_edge(p.graph, words, g, d)) st.max_age = ctl_max(st.max_age, now - c.gstat[d].published);
+        st.max_ratio = ctl_max(st.max_ratio, c.steps_s[g] / request[g]);
+    }
+}
+
+// the operator's record of the per-operator log (_col_chain.cuh:488-535)
+__device__ void write_log(CtlDev &c, const CtlPtrs &p) {
+    if (c.res.log_count >= p.oplog_capacity) {
+        c.res.log_dropped += 1;
+        return;
+    }
+    OperatorLog &r = p.oplog[c.res.log_count];
+    c.res.log_count += 1;
+    r.operator_id = ++c.log_operator;
+    r.finest_ticks = c.sched.end;
+    r.owner_updates = c.op_updates;
+    r.chain_blocks = c.op_blocks;
+    r.waves = c.op_waves;
+    r.chain_launches = c.op_waves;
+    r.G = c.G;
+    r.pad = 0;
+    r.clock_sim = c.clock_sim;
+    r.duration = c.duration;
+    r.chain_seconds = 1.0e-9 * static_cast<double>(c.chain_ns);
+    r.audit_seconds = 1.0e-9 * static_cast<double>(c.audit_ns);
+    r.wall_seconds = 1.0e-9 * static_cast<double>(device_ns() - c.t_begin);
+    for (int k = 0; k < kEventCategories; ++k) {
+        r.event_count[k] = p.event_count ? p.event_count[k] : 0ull;
+        r.event_log_mass[k] = p.event_log_mass ? p.event_log_mass[k] : 0.0;
+    }
+    for (int g = 0; g < c.G; ++g) {
+        const CtlDev::GroupStat &st = c.gstat[g];
+        OperatorLogGroup &o = r.g[g];
+        o.owners = c.group_start[g + 1] - c.group_start[g];
+        o.level = c.sched.level[g];
+        o.initial_level = st.initial_level;
+        o.binding = st.binding;
+        o.dt = c.steps_s[g];
+        o.min_request = st.min_request;
+        o.max_request = st.max_request;
+        o.final_request = c.current[g];
+        o.initial_request = st.initial_request;
+        o.max_age = st.max_age;
+        o.max_ratio = st.max_ratio;
+        o.max_growth = st.max_growth;
+        o.max_activity = st.max_activity;
+        o.coarsened = st.coarsened;
+        o.refined = st.refined;
+        o.constrained = st.constrained;
+        o.updates = st.updates;
+        o.overshoots = st.overshoots;
+        o.persistent = st.persistent;
+    }
+}
+
 }  // namespace
 
 // owner lists per group from the counting sort's counts (the host's group_start, _col_chain.cuh:162-167)
@@ -88,10 +162,15 @@ __global__ void k_ctl_geometry(CtlDev *c, CtlPtrs p, int G) {
 
 // An operator starts: the tick-0 wave holds every particle and publishes the whole reservoir.  The
 // horizon is `duration`, or scale * *duration_dev when the caller's timestep lives on the device.
-__global__ void k_ctl_reset(CtlDev *c, double duration, const double *duration_dev, double scale, int n, int G,
-                            int S, int R) {
+__global__ void k_ctl_reset(CtlDev *c, double duration, const double *duration_dev, double scale,
+                            const double *clock_sim, int n, int G, int S, int R) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (duration_dev) duration = scale * *duration_dev;
+    c->clock_sim = clock_sim ? *clock_sim : 0.0;
+    c->t_begin = device_ns();
+    c->op_updates = c->op_blocks = 0;
+    c->op_waves = 0;
+    c->chain_ns = c->audit_ns = 0;
     c->duration = duration;
     c->n = n;
     c->G = G;
@@ -125,8 +204,9 @@ __global__ void k_ctl_begin(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditional
         for (int g = 0; g < c.G && st == kCtlOk; ++g) {
             int first, last;
             group_bins(c, p, g, first, last);
+            c.gstat[g].binding = 0;
             st = ctl_choose_bath(m, p.ratebin + first, last - first, c.duration, c.state[g].limit_scale,
-                                 c.requested[g], nullptr);
+                                 c.requested[g], &c.gstat[g].binding);
         }
         if (st == kCtlOk) st = sched_init(c.sched, c.duration, c.requested, c.G, p.graph);
         if (st != kCtlOk) {
@@ -137,8 +217,16 @@ __global__ void k_ctl_begin(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditional
                 c.current[g] = c.requested[g];
                 c.passed[g] = 1;
                 p.dt[g] = c.steps_s[g];
+                CtlDev::GroupStat &gs = c.gstat[g];
+                gs.published = 0.0;
+                gs.initial_request = gs.min_request = gs.max_request = c.requested[g];
+                gs.max_age = gs.max_ratio = gs.max_growth = gs.max_activity = 0.0;
+                gs.coarsened = gs.refined = gs.constrained = gs.updates = 0;
+                gs.initial_level = c.sched.level[g];
+                gs.overshoots = gs.persistent = 0;
             }
             next_wave(c);
+            if (c.wave.go && p.oplog) wave_stats(c, p, c.requested);
         }
     }
     cudaGraphSetConditional(h, c.wave.go ? 1u : 0u);
@@ -150,6 +238,13 @@ __global__ void k_ctl_finish(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditiona
     CtlDev &c = *cp;
     c.res.waves += 1;
     c.res.owner_updates += c.wave.count;
+    c.op_waves += 1;
+    c.op_updates += c.wave.count;
+    if (p.queued) c.op_blocks += static_cast<unsigned long long>(*p.queued);
+    if (p.oplog) {
+        c.chain_ns += c.t_mark1 - c.t_mark0;
+        c.audit_ns += device_ns() - c.t_mark1;
+    }
     const int flag = *p.error_flag;
     if (flag) {
         ctl_fail(c, 100 + flag, flag);
@@ -182,6 +277,12 @@ __global__ void k_ctl_finish(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditiona
             return;
         }
         c.passed[g] = !(res.activity_overshoot || res.distribution_overshoot || res.persistent_overshoot);
+        CtlDev::GroupStat &gs = c.gstat[g];
+        gs.updates += 1;
+        gs.overshoots += (res.activity_overshoot || res.distribution_overshoot) ? 1 : 0;
+        gs.persistent += res.persistent_overshoot ? 1 : 0;
+        gs.max_growth = ctl_max(gs.max_growth, res.max_g);
+        gs.max_activity = ctl_max(gs.max_activity, res.max_f);
         c.bath_index += 1;
         if (c.res.rec_count < p.record_capacity) {
             BathRecord &r = p.records[c.res.rec_count];
@@ -206,6 +307,8 @@ __global__ void k_ctl_finish(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditiona
     }
     sched_advance(c.sched, c.due, c.ndue);
     next_wave(c);
+    // the operator ends normally: its record of the per-operator log
+    if (!c.wave.go && !c.res.error && p.oplog) write_log(c, p);
     cudaGraphSetConditional(h, c.wave.go ? 1u : 0u);
 }
 
@@ -221,6 +324,10 @@ __global__ void k_ctl_adapt(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditional
         group_bins(c, p, g, first, last);
         st = ctl_choose_bath(m, p.ratebin + first, last - first, c.duration, c.state[g].limit_scale, c.current[g],
                              nullptr);
+        CtlDev::GroupStat &gs = c.gstat[g];
+        gs.min_request = ctl_min(gs.min_request, c.current[g]);
+        gs.max_request = ctl_max(gs.max_request, c.current[g]);
+        c.previous_level[g] = c.sched.level[g];
     }
     if (st == kCtlOk) st = sched_adapt(c.sched, c.tick, c.due, c.ndue, c.current, c.passed, c.work);
     if (st != kCtlOk) {
@@ -231,8 +338,20 @@ __global__ void k_ctl_adapt(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditional
     for (int k = 0; k < c.ndue; ++k) {
         const int g = c.due[k];
         c.steps_s[g] = sched_seconds(c.sched, c.sched.step[g]);
+        CtlDev::GroupStat &gs = c.gstat[g];
+        gs.coarsened += c.sched.level[g] < c.previous_level[g] ? 1 : 0;
+        gs.refined += c.sched.level[g] > c.previous_level[g] ? 1 : 0;
+        gs.constrained += c.steps_s[g] > c.current[g] ? 1 : 0;
     }
     for (int g = 0; g < c.G; ++g) p.dt[g] = c.steps_s[g];
+    if (p.oplog) wave_stats(c, p, c.current);
+}
+
+// device time at the start of a wave's chains (0) and of its audit (1)
+__global__ void k_ctl_mark(CtlDev *c, int which) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !c->wave.go) return;
+    if (which == 0) c->t_mark0 = device_ns();
+    else c->t_mark1 = device_ns();
 }
 
 // the wave's owners: the owner lists of its nonempty due groups, concatenated
@@ -252,11 +371,12 @@ __global__ void k_ctl_wave_ids(const CtlDev *c, const int *__restrict__ sorted, 
 }
 
 void ctl_launch_geometry(CtlDev *c, const CtlPtrs &p, int G, cudaStream_t s) { k_ctl_geometry<<<1, 32, 0, s>>>(c, p, G); }
-void ctl_launch_reset(CtlDev *c, double duration, const double *duration_dev, double scale, int n, int G, int S,
-                      int R, cudaStream_t s) {
-    k_ctl_reset<<<1, 32, 0, s>>>(c, duration, duration_dev, scale, n, G, S, R);
+void ctl_launch_reset(CtlDev *c, double duration, const double *duration_dev, double scale, const double *clock_sim,
+                      int n, int G, int S, int R, cudaStream_t s) {
+    k_ctl_reset<<<1, 32, 0, s>>>(c, duration, duration_dev, scale, clock_sim, n, G, S, R);
 }
 void ctl_launch_clear(CtlDev *c, cudaStream_t s) { k_ctl_clear<<<1, 256, 0, s>>>(c); }
+void ctl_launch_mark(CtlDev *c, int which, cudaStream_t s) { k_ctl_mark<<<1, 32, 0, s>>>(c, which); }
 void ctl_launch_begin(CtlDev *c, const Model &m, const CtlPtrs &p, cudaGraphConditionalHandle h, cudaStream_t s) {
     k_ctl_begin<<<1, 32, 0, s>>>(m, c, p, h);
 }

@@ -76,6 +76,10 @@ struct Status {
 };
 
 Status cuda_status(cudaError_t e, const char *what);
+// Caller-owned device arrays must sit on their element's alignment: particle records and RNG states
+// (doubles inside) on 8 bytes, codes on 4.  A misaligned pointer would fault the first kernel that
+// loads through it, so the entry points reject one as GD_ERR_INVALID_ARGUMENT.
+inline bool aligned_to(const void *p, size_t a) { return reinterpret_cast<uintptr_t>(p) % a == 0; }
 
 #define GD_TRY_CUDA(expr)                                              \
     do {                                                               \

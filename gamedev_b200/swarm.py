@@ -181,6 +181,16 @@ class SwarmCollision:
         self.lib.gd_controller_summary(self.h, buf, n + 1)
         return json.loads(buf.value.decode())
 
+    def operator_log(self) -> list:
+        """COL_DIAGNOSTICS per-operator log (gd_operator_log): one parsed JSON line per operator run
+        with diagnostics on, in the reference's collision_local_*.jsonl format."""
+        import json
+
+        n = self.lib.gd_operator_log(self.h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        self.lib.gd_operator_log(self.h, buf, n + 1)
+        return [json.loads(line) for line in buf.value.decode().splitlines() if line.strip()]
+
     # ---- collision operator ---------------------------------------------------------------
     def evolve_local_collisions(self, particles, rng, duration: float, total_dust_mass: float):
         self.lib.gd_set_stream(self.h, _stream())
@@ -533,10 +543,25 @@ class SwarmBatch:
                                           C.c_void_p(_ptr(measure)), C.c_void_p(_ptr(kth))))
 
     def check(self):
-        """The deferred non-finite screens of the last knn(); raises GdError (detail = index in the
-        concatenated particle array)."""
+        """The deferred non-finite screens of the last knn(), then the results of captured
+        collide() calls; raises GdError (detail = index in the concatenated particle array, or the
+        swarm of an operator error)."""
         self.lib.gd_batch_set_stream(self.h, _stream())
         self._check(self.lib.gd_batch_check(self.h))
+
+    def collide(self, particles, rng, codes, measure, durations, total_dust_masses):
+        """gd_batch_collide: every swarm's collision operator on the rows of the last knn(), side
+        by side; durations and total_dust_masses per swarm."""
+        d = (C.c_double * self.S)(*[float(v) for v in durations])
+        m = (C.c_double * self.S)(*[float(v) for v in total_dust_masses])
+        self.lib.gd_batch_set_stream(self.h, _stream())
+        self._check(self.lib.gd_batch_collide(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
+                                              C.c_void_p(_ptr(codes)), C.c_void_p(_ptr(measure)), d, m))
+
+    def operator_stats(self, s: int) -> dict:
+        st = GdOperatorStats()
+        self._check(self.lib.gd_batch_operator_stats(self.h, int(s), C.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
 
     def codes_of(self, codes, s: int):
         a, b = int(self.codes_off[s]), int(self.codes_off[s + 1])

@@ -312,6 +312,19 @@ size_t gd_controller_summary(const gd_handle *h, char *buf, size_t len);
  * q <= 1e-6, 1e-4, 1e-2 or above; 4 catastrophic fragmentation; 5 remnant erosion; 6 debris.
  * gd_event_totals copies the last operator's 7 counts and 7 sums to host arrays (synchronous). */
 gd_status gd_set_diagnostics(gd_handle *h, int on);
+/* With diagnostics on, every collision operator also writes its line of the reference's
+ * per-operator JSONL log (collision_local_*.jsonl, inc/swarm/_col_chain.cuh:488-535): operator
+ * number, clock_sim (the device clock under gd_step, else 0), duration, waves, owner updates,
+ * chain blocks and launches, the chain, audit and whole-operator seconds (device time), the finest
+ * tick count, and per controller group its owners, final level and bath length, initial level,
+ * coarsened / refined / neighbour-constrained updates, minimum, maximum, final and initial
+ * requested bath lengths, initial binding constraint, updates, overshoots, persistent overshoots,
+ * oldest linked reservoir, largest bath length over request, largest growth and predicted activity;
+ * then the event counts and log-mass sums.  The lines accumulate over the handle's life (as the
+ * reference's file does); gd_operator_log copies them (up to len - 1 bytes and a NUL) and returns
+ * the full length.  The persistent chain is one launch per wave, so chain_launches = waves and
+ * chain_blocks = the owners the waves queued; the reference counts each capped relaunch. */
+size_t gd_operator_log(const gd_handle *h, char *buf, size_t len);
 gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_mass);
 
 /* evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539): advance every owner through one
@@ -396,6 +409,23 @@ gd_status gd_batch_set_stream(gd_batch *b, void *stream);
 gd_status gd_batch_knn(gd_batch *b, const gd_particle *dev_particle, int32_t *dev_codes, double *dev_measure,
                        float *dev_kth_d2);
 gd_status gd_batch_check(gd_batch *b);
+/* The collision operator of every swarm of the batch (evolve_local_collisions,
+ * inc/swarm/_col_chain.cuh:108-539), on the rows of the last gd_batch_knn: swarm s advances its
+ * particles (dev_particle from part offset s) and RNG states by durations[s] with
+ * lambda_0 = n_p[s] / (n_k[s] total_dust_masses[s]), with its own bath controller.  Each swarm's
+ * operator is one conditional-node graph (as gd_collision_operator's), and the swarms' graphs run
+ * side by side on forked streams; each swarm's result is bit-identical to gd_collision_operator on
+ * that swarm alone.  On a stream that is not capturing the call runs them and returns the first
+ * error (detail = the swarm); inside the caller's capture of the batch's stream (after one eager
+ * call, which allocates the swarms' operator state) the operators join the caller's graph, whose
+ * results gd_batch_check returns after it ran.  dev_codes and dev_measure are gd_batch_knn's
+ * outputs. */
+gd_status gd_batch_collide(gd_batch *b, gd_particle *dev_particle, void *dev_rng, const int32_t *dev_codes,
+                           const double *dev_measure, const double *durations, const double *total_dust_masses);
+/* Controller statistics of swarm s's last operators (as gd_last_operator_stats). */
+gd_status gd_batch_operator_stats(const gd_batch *b, int s, gd_operator_stats *out);
+/* Positions changed without a new gd_batch_knn: the operators rebuild their owner lists. */
+gd_status gd_batch_invalidate(gd_batch *b);
 gd_status gd_batch_set_tuning(gd_batch *b, const gd_tuning *t);  /* walk, prescan, block width, sort */
 size_t    gd_batch_last_error(const gd_batch *b, char *buf, size_t len);
 long long gd_batch_error_detail(const gd_batch *b);

@@ -10,7 +10,9 @@
 //   ref_step <in.bin> <out.bin> <seed> <steps> <total_dust_mass> <clock_sim> <clock_out>
 //   in.bin : int32 n (= N_P), then n particle records (the 64 B struct swarm)
 //   out.bin: int32 n, the n records after `steps` steps, then the n curand states
-//   stdout : one JSON line {"n", "steps", "dt": [...], "clock_sim", "clock_out"}
+//   stdout : one JSON line {"n", "steps", "dt": [...], "ms": [...] (each step, host clock around the
+//            synchronised step, as the reference loop synchronises), "clock_sim", "clock_out"}
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -66,8 +68,10 @@ int main(int argc, char **argv) {
         real *dev_optdepth = dev_alloc<real>(N_G, "optdepth");
 #endif
         (void)total_dust_mass;
-        std::string dts;
+        std::string dts, mss;
+        check(gpuDeviceSynchronize(), "setup");
         for (int step = 0; step < steps; ++step) {
+            const auto t0 = std::chrono::steady_clock::now();
             // swarm_runtime.cu:504-514
             dyn_rate_calc<<<NB_P, TPB>>>(dev_dyn_rate, dev_particle);
             check(gpuGetLastError(), "dyn_rate_calc");
@@ -101,11 +105,14 @@ int main(int argc, char **argv) {
             check(gpuGetLastError(), "diffusion_pos");
 #endif
             check(gpuDeviceSynchronize(), "step");
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             clock_sim += dt_dyn;
             clock_out += dt_dyn;
             char buf[64];
             std::snprintf(buf, sizeof(buf), "%s%.17g", step ? ", " : "", dt_dyn);
             dts += buf;
+            std::snprintf(buf, sizeof(buf), "%s%.6g", step ? ", " : "", ms);
+            mss += buf;
         }
         check(gpuMemcpy(particle.data(), dev_particle, sizeof(swarm) * N_P, gpuMemcpyDeviceToHost), "copy back");
         std::vector<curs> rng(N_P);
@@ -115,8 +122,8 @@ int main(int argc, char **argv) {
         out.write(reinterpret_cast<const char *>(particle.data()), sizeof(swarm) * N_P);
         out.write(reinterpret_cast<const char *>(rng.data()), sizeof(curs) * N_P);
         if (!out) throw std::runtime_error("cannot write output");
-        std::printf("{\"n\": %d, \"steps\": %d, \"dt\": [%s], \"clock_sim\": %.17g, \"clock_out\": %.17g}\n", N_P, steps,
-                    dts.c_str(), clock_sim, clock_out);
+        std::printf("{\"n\": %d, \"steps\": %d, \"dt\": [%s], \"ms\": [%s], \"clock_sim\": %.17g, "
+                    "\"clock_out\": %.17g}\n", N_P, steps, dts.c_str(), mss.c_str(), clock_sim, clock_out);
         return 0;
     } catch (const std::exception &e) {
         std::fprintf(stderr, "ref_step: %s\n", e.what());

@@ -132,3 +132,14 @@ def test_particle_record_is_reference_layout(gd):
     from gamedev_b200 import PARTICLE_DTYPE
 
     assert PARTICLE_DTYPE.itemsize == 64  # const_defs.cuh:194-203 with MULTISIZE
+
+
+def test_misaligned_device_pointers_are_rejected_before_any_launch(gd):
+    """RNG states and particle records hold doubles: a pointer off their 8-byte alignment (e.g. a
+    byte-offset slice of a state buffer) would fault the first kernel that loads through it, so
+    the entry points return GD_ERR_INVALID_ARGUMENT before touching the device."""
+    lib = gd.load()
+    odd = C.c_void_p(0x10000 + 4)  # never dereferenced: the check comes first
+    assert lib.gd_rng_init(odd, 1, 1, None) == 1
+    assert lib.gd_rng_uniforms(odd, 1, 1, C.c_void_p(0x20000), None) == 1
+    assert lib.gd_rng_uniforms(C.c_void_p(0x20000), 1, 1, odd, None) == 1

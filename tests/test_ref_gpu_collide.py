@@ -229,3 +229,62 @@ def test_morton_event_categories_match_reference(gd, cuda):
         assert int(counts.sum()) > 1000
         for a, b in zip(lm, line["event_log_mass_sums"]):
             assert math.isclose(float(a), float(b), rel_tol=1e-9, abs_tol=1e-12), (lm, line["event_log_mass_sums"])
+
+
+def test_operator_log_equals_reference_log(gd, cuda):
+    """The per-operator COL_DIAGNOSTICS log (gd_operator_log) against the reference's
+    collision_local_*.jsonl on the Morton shapes, where the event chains are the same: per operator
+    its number, duration, waves, owner updates, finest ticks and event counts exactly; per group its
+    owners, final and initial levels, bath length, requested lengths (minimum, maximum, final,
+    initial), binding constraint, coarsened / refined / constrained updates, updates, overshoots and
+    persistent overshoots exactly, the oldest linked reservoir and the bath length over request to
+    1e-12, the growth and predicted-activity maxima to 1e-9 (FP64 atomic audit sums).  Chain blocks
+    and launches count this build's persistent chain, and the seconds are device time: present and
+    non-negative."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    refcollide = _refc()
+    model = "c1_multisize_2d"
+    if not refcollide.available(model, N, diagnostics=True):
+        pytest.fail("oracle/_ref reference COL_DIAGNOSTICS build absent: build the checker first")
+    cfg = workloads.config(model)
+    p = workloads.particles(model, n=N, seed=11)
+    d = _duration(gd, cfg, p, 2000.0)
+    sw = gd.SwarmCollision(cfg, N)
+    sw.set_diagnostics(True)
+    dp = gd.particles_to_device(p)
+    rng = gd.rngstate_init(N, seed=1)
+    for _ in range(2):
+        sw.evolve_collisions(dp, rng, d, _mass(p))
+    torch.cuda.synchronize()
+    ours = sw.operator_log()
+    sw.close()
+    _, info = refcollide.run(model, p, 1, d, _mass(p), 2, timeout=600, diagnostics=True)
+    ref = info["operator_log"]
+    assert len(ours) == len(ref) == 2
+    exact_top = ("schema", "method", "operator", "duration", "waves", "owner_updates", "finest_ticks", "event_counts")
+    exact_group = ("id", "owners", "level", "dt", "initial_level", "coarsened_updates", "refined_updates",
+                   "neighbor_constrained_updates", "minimum_requested_dt", "maximum_requested_dt",
+                   "final_requested_dt", "initial_requested_dt", "initial_binding_constraint", "updates",
+                   "overshoots", "persistent_overshoots")
+    close_group = {"max_snapshot_age_at_start": 1e-12, "max_requested_dt_ratio": 1e-12, "max_growth": 1e-9,
+                   "max_predicted_activity": 1e-9}
+    assert set(ours[0]) == set(ref[0])
+    for a, b in zip(ours, ref):
+        for key in exact_top:
+            assert a[key] == b[key], (key, a[key], b[key])
+        for key in ("chain_blocks", "chain_launches", "chain_seconds", "audit_seconds", "scheduler_wall_seconds"):
+            assert a[key] >= 0
+        assert a["waves"] > 1
+        assert len(a["groups"]) == len(b["groups"])
+        for ga, gb in zip(a["groups"], b["groups"]):
+            assert set(ga) == set(gb)
+            for key in exact_group:
+                assert ga[key] == gb[key], (ga["id"], key, ga[key], gb[key])
+            for key, tol in close_group.items():
+                assert math.isclose(ga[key], gb[key], rel_tol=tol, abs_tol=1e-15), (ga["id"], key, ga[key], gb[key])
+        for x, y in zip(a["event_log_mass_sums"], b["event_log_mass_sums"]):
+            assert math.isclose(x, y, rel_tol=1e-9, abs_tol=1e-12)
+    assert sum(g["updates"] for g in ours[0]["groups"]) > 3
