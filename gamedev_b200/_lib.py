@@ -106,6 +106,7 @@ SIGNATURES = {
     "gd_batch_collide": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "gd_batch_operator_stats": (C.c_int, [_P, C.c_int, C.POINTER(GdOperatorStats)]),
     "gd_batch_invalidate": (C.c_int, [_P]),
+    "gd_batch_reset_controller": (C.c_int, [_P]),
     "gd_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_batch_error_detail": (C.c_longlong, [_P]),
     "gd_batch_launch_count": (C.c_longlong, [_P]),

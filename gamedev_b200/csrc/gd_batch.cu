@@ -295,6 +295,20 @@ gd_status gd_batch_collide(gd_batch *b, gd_particle *dev_particle, void *dev_rng
     return GD_OK;
 }
 
+gd_status gd_batch_reset_controller(gd_batch *b) {
+    if (!b) return GD_ERR_INVALID_ARGUMENT;
+    for (size_t s = 0; s < b->col.size(); ++s) {
+        gd::Status st = gd::collider_reset_state(*b->col[s], b->stream);
+        if (!st) {
+            st.msg = "swarm " + std::to_string(s) + ": " + st.msg;
+            st.detail = static_cast<long long>(s);
+            return batch_fail(b, st);
+        }
+    }
+    b->collide_pending = false;
+    return GD_OK;
+}
+
 gd_status gd_batch_invalidate(gd_batch *b) {
     if (!b) return GD_ERR_INVALID_ARGUMENT;
     for (auto &c : b->col) c->local_geometry_valid = false;

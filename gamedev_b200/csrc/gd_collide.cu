@@ -45,7 +45,9 @@ namespace gd {
 constexpr int kMaxSlots = kMaxK / 32;  // neighbour slots per lane
 constexpr int kMaxGroups = 256;
 constexpr int kChainWarps = 4;
+constexpr int kChainDoubles = 5;  // doubles per slot of a chain warp's staging: rates and folds
 constexpr long long kEventBudget = 1ll << 22;  // events per owner per bath before giving up
+constexpr double kHeavyEvents = 16.0;          // expected events that put an owner at the queue's front
 
 // ------------------------------------------------------------------------------------------------
 // device scratch layout: one block copied to pinned host memory with one cudaMemcpyAsync
@@ -53,7 +55,8 @@ constexpr long long kEventBudget = 1ll << 22;  // events per owner per bath befo
 struct Small {
     size_t merged;       // int
     size_t error_flag;   // int
-    size_t queued;       // int
+    size_t queued;       // int: owners the skip scan queued from the front (expected work above the cut)
+    size_t light;        // int: owners queued from the back (the rest)
     size_t head;         // int
     size_t events;       // unsigned long long
     size_t binmap;       // int[raw]
@@ -78,7 +81,9 @@ static Small small_layout(const Model &m) {
     L.merged = o; o += 4;
     L.error_flag = o; o += 4;
     L.queued = o; o += 4;
+    L.light = o; o += 4;
     L.head = o; o += 4;
+    o += 4;
     L.events = o; o += 8;
     o = align256(o);
     L.binmap = o; o = align256(o + 4 * R);
@@ -114,6 +119,16 @@ __device__ __forceinline__ int owner_at(const int *ids, int slot) { return ids ?
 __global__ void k_env_cache(Model m, int n, const gd_particle *__restrict__ part, Env *__restrict__ env) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && part[i].position[1] > 0.0) env[i] = make_env(m, part[i].position[1], part[i].position[2]);
+}
+
+// R h_g(R) of every particle (the partner term of the N_Z = 1 physical kernel, _col_rates.cuh:205-210),
+// once per geometry epoch: positions do not change inside an operator.
+__global__ void k_disk_height(Model m, int n, const gd_particle *__restrict__ part, double *__restrict__ height) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double R = cyl_R(m, part[i].position[1], part[i].position[2]);
+        height[i] = R * get_hg(m, R);
+    }
 }
 
 // col_bath_init (col_bath_init.cu:11-23) + col_comp_zero (col_comp_zero.cu:11-19)
@@ -345,8 +360,35 @@ __device__ __forceinline__ void warp_fold(int K, int lane, F &&combine) {
     }
 }
 
+// pair_rate with the partner's disk height (N_Z = 1 physical kernel) read from the per-particle
+// array k_disk_height fills, and the owner's Stokes terms of the cached physical kernel passed in
+// (evaluated once per owner, or once per event in the chain).  The same operations as pair_rate,
+// so the same bits.
+__device__ __forceinline__ double chain_pair_rate(const Model &m, const OwnerCtx &o, const PairOwner &po,
+                                                  double size_i, double size_j, double numr_j, double H_gj,
+                                                  double &vrel, const PairPartner *pre = nullptr) {
+    vrel = 0.0;
+    double r;
+    if (m.coag_kernel == GD_KERNEL_CONSTANT) {
+        r = o.lambda0 * numr_j;
+    } else if (m.coag_kernel == GD_KERNEL_LINEAR) {
+        r = o.lambda0 * numr_j * (grain_mass(m, size_i) + grain_mass(m, size_j));
+    } else if (m.coag_kernel == GD_KERNEL_PRODUCT) {
+        r = o.lambda0 * numr_j * grain_mass(m, size_i) * grain_mass(m, size_j);
+    } else {
+        if (use_env_cache(m))
+            vrel = pre ? cached_pair_speed_pp(m, o.env, po, *pre) : cached_pair_speed_o(m, o.env, po, size_j);
+        else
+            vrel = direct_pair_speed(m, o.y, o.z, size_i, size_j);
+        r = numr_j * vrel * M_PI * (size_i + size_j) * (size_i + size_j) / 4.0;
+        if (m.n_z == 1) r /= sqrt(2.0 * M_PI * (o.H_i * o.H_i + H_gj * H_gj));
+    }
+    return r / o.measure;
+}
+
 struct RateArgs {
     const int *ids;
+    const double *height;  // R h_g(R) per particle (N_Z = 1 physical kernel), else null
     const WaveInfo *w;  // the wave's owner count and order, and its publish wave
     const gd_particle *part;
     const int32_t *codes;
@@ -417,8 +459,8 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
             double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
             if (use) {
                 double vrel;
-                double pr = kCached ? pair_rate_cached(m, o, po, size_i, size_j, numr_j, a.part, j, vrel)
-                                    : pair_rate(m, o, size_i, size_j, numr_j, a.part, j, vrel);
+                const double h_j = a.height ? a.height[j] : 0.0;
+                double pr = chain_pair_rate(m, o, po, size_i, size_j, numr_j, h_j, vrel);
                 double mean = 0.0, sec = 0.0, maxi = 0.0;
                 pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
                 mx = pr > 0.0 ? maxi : 0.0;
@@ -527,8 +569,9 @@ struct ChainArgs {
     double *time, *hazard, *jump1, *jump2, *jumpmax;
     int *events;
     unsigned char *complete;
-    int *queue;
-    int *queued;
+    int *queue;     // [n]: heavy owners from the front, the rest from the back
+    int *queued;    // [2]: owners queued from the front, from the back
+    int n;
 };
 
 // col_skip_scan (col_skip_scan.cu:13-59)
@@ -539,7 +582,7 @@ __global__ void k_skip_scan(ChainArgs a) {
     // a persistent grid; every warp of a block runs the same number of passes (ballots below)
     for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     const int slot = base + threadIdx.x;
-    bool enqueue = false;
+    bool enqueue = false, heavy = false;
     int i = 0;
     if (slot < count) {
         i = owner_at(ids, slot);
@@ -560,6 +603,7 @@ __global__ void k_skip_scan(ChainArgs a) {
                         curandState st = a.rng[i];
                         const double wait = -log(col_uniform(&st)) / c.rate;
                         const double remaining = end - a.time[i];
+                        heavy = c.rate * remaining >= kHeavyEvents;
                         if (isfinite(wait) && wait > 0.0 && wait >= remaining) {
                             a.hazard[i] += c.rate * remaining;
                             a.jump1[i] += c.first * remaining;
@@ -576,19 +620,28 @@ __global__ void k_skip_scan(ChainArgs a) {
             }
         }
     }
-    // warp-aggregated queue append
-    const unsigned int mask = __ballot_sync(0xffffffffu, enqueue);
-    if (mask) {
-        const int lane = threadIdx.x & 31;
+    // warp-aggregated queue append: owners expecting many events at the front, so that the chain
+    // starts its longest owners first (the order of the owners does not change any owner's result)
+    const int lane = threadIdx.x & 31;
+    const unsigned int hmask = __ballot_sync(0xffffffffu, enqueue && heavy);
+    const unsigned int lmask = __ballot_sync(0xffffffffu, enqueue && !heavy);
+    if (hmask) {
         int qbase = 0;
-        if (lane == __ffs(mask) - 1) qbase = atomicAdd(a.queued, __popc(mask));
-        qbase = __shfl_sync(0xffffffffu, qbase, __ffs(mask) - 1);
-        if (enqueue) a.queue[qbase + __popc(mask & ((1u << lane) - 1u))] = i;
+        if (lane == __ffs(hmask) - 1) qbase = atomicAdd(&a.queued[0], __popc(hmask));
+        qbase = __shfl_sync(0xffffffffu, qbase, __ffs(hmask) - 1);
+        if (enqueue && heavy) a.queue[qbase + __popc(hmask & ((1u << lane) - 1u))] = i;
+    }
+    if (lmask) {
+        int qbase = 0;
+        if (lane == __ffs(lmask) - 1) qbase = atomicAdd(&a.queued[1], __popc(lmask));
+        qbase = __shfl_sync(0xffffffffu, qbase, __ffs(lmask) - 1);
+        if (enqueue && !heavy) a.queue[a.n - 1 - (qbase + __popc(lmask & ((1u << lane) - 1u)))] = i;
     }
     }
 }
 
 struct ChainRun {
+    const double *height;  // R h_g(R) per particle (N_Z = 1 physical kernel), else null
     const gd_particle *part_ro;
     gd_particle *part;
     const int32_t *codes;
@@ -608,19 +661,21 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 5 * K;
+    double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * kChainDoubles * K;
     double *prate = w, *tot = w + K, *pj1 = w + 2 * K, *pj2 = w + 3 * K, *pjm = w + 4 * K;
-    int *last_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(kChainWarps) * 5 * K) +
+    int *last_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) +
+                                          static_cast<size_t>(kChainWarps) * kChainDoubles * K) +
                   static_cast<size_t>(wib) * K;
     const int nslot = (K + 31) / 32;
-    const int queued = *a.queued;
+    const int heavy = a.queued[0];
+    const int queued = heavy + a.queued[1];
 
     while (true) {
         int qs = 0;
         if (lane == 0) qs = atomicAdd(r.head, 1);
         qs = __shfl_sync(0xffffffffu, qs, 0);
         if (qs >= queued) break;
-        const int i = a.queue[qs];
+        const int i = qs < heavy ? a.queue[qs] : a.queue[a.n - 1 - (qs - heavy)];
         const double bath_end = a.dt[a.spatial[i]];
         const double meas = a.measure[i];
 
@@ -640,18 +695,23 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
         // frozen partners of this owner, kept in registers for every event
         const OwnerCtx o = owner_ctx(m, r.part_ro, r.env, i, meas, r.lambda0);
         int nb[kMaxSlots];
-        double sj[kMaxSlots], nj[kMaxSlots];
+        double sj[kMaxSlots], nj[kMaxSlots], hj[kMaxSlots];
+        const bool physical = m.coag_kernel == GD_KERNEL_CUSTOM;
+        const bool cached = physical && use_env_cache(m);
 #pragma unroll
         for (int t = 0; t < kMaxSlots; ++t) {
             nb[t] = -1;
             sj[t] = 0.0;
             nj[t] = 0.0;
+            hj[t] = 0.0;
             const int s = lane + 32 * t;
             if (t < nslot && s < K) {
                 nb[t] = r.codes[static_cast<size_t>(i) * K + s];
                 if (nb[t] >= 0) {
-                    sj[t] = r.size_old[nb[t] / 3];
-                    nj[t] = r.numr_old[nb[t] / 3];
+                    const int j = nb[t] / 3;
+                    sj[t] = r.size_old[j];
+                    nj[t] = r.numr_old[j];
+                    if (r.height) hj[t] = r.height[j];  // the partner's disk height (_col_rates.cuh:205-210)
                 }
             }
         }
@@ -663,6 +723,8 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
                 running = false;
                 break;
             }
+            PairOwner po{0.0, 0.0, 0.0};
+            if (cached) po = cached_owner_terms(m, o.env, size_i);
 #pragma unroll
             for (int t = 0; t < kMaxSlots; ++t) {
                 const int s = lane + 32 * t;
@@ -670,7 +732,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
                     double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
                     if (nb[t] >= 0) {
                         double vrel;
-                        pv = pair_rate(m, o, size_i, sj[t], nj[t], r.part_ro, nb[t] / 3, vrel);
+                        pv = chain_pair_rate(m, o, po, size_i, sj[t], nj[t], hj[t], vrel);
                         double mean = 0.0, sec = 0.0, maxi = 0.0;
                         pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
                         j1 = pv * mean;
@@ -734,17 +796,21 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
             jump1_i += total_j1 * wait;
             jump2_i += total_j2 * wait;
             jumpmax_i = fmax(jumpmax_i, total_jm);
-            // partner: first slot whose cumulative rate exceeds U*total, in slot order
+            // partner: first slot whose cumulative rate exceeds U*total, in slot order.  The sum skips
+            // slots without a positive rate, as the reference's does (adding +0 would not change it
+            // either); eight slots per step, their loads issued together, the first crossing kept.
             const double target = col_uniform(&rng) * total_rate;
             double cumulative = 0.0;
             int pick = -1;
-            for (int s = 0; s < K; ++s) {
-                const double pr = prate[s];
-                if (pr <= 0.0) continue;
-                cumulative += pr;
-                if (cumulative > target) {
-                    pick = s;
-                    break;
+            for (int s0 = 0; s0 < K && pick < 0; s0 += 8) {
+                double pr8[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) pr8[u] = (s0 + u < K) ? prate[s0 + u] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const bool pos = pr8[u] > 0.0;
+                    if (pos) cumulative += pr8[u];
+                    if (pick < 0 && pos && cumulative > target) pick = s0 + u;
                 }
             }
             if (pick < 0) pick = last_positive;
@@ -1431,6 +1497,7 @@ Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
     GD_TRY_CUDA(cudaMemset(c.error.ptr, 0, sizeof(int) * n));
     GD_TRY_CUDA(c.event_count.alloc(kEventCategories));
     GD_TRY_CUDA(c.event_log_mass.alloc(kEventCategories));
+    if (m.coag_kernel == GD_KERNEL_CUSTOM && m.n_z == 1) GD_TRY_CUDA(c.height.alloc(n));
     // the device controller: default bath states, no operator yet, empty accumulators
     GD_TRY_CUDA(c.ctl.alloc(sizeof(CtlDev)));
     {
@@ -1662,7 +1729,7 @@ static Status collider_setup(Collider &c, const Model &m) {
     if (R <= kAuditSmemBins)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(audit_blocked_smem(R))));
-    c.chain_smem = static_cast<size_t>(kChainWarps) * (5 * 8 + 4) * K;
+    c.chain_smem = static_cast<size_t>(kChainWarps) * (kChainDoubles * 8 + 4) * K;
     if (c.chain_smem > 48 * 1024)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(c.chain_smem)));
@@ -1740,6 +1807,10 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ctl_launch_geometry(ctl, p, G, q);
         k_group_fill<<<(n + kGroupSpan - 1) / kGroupSpan, kGroupTPB, 0, q>>>(n, G, spatial, at<int>(c.small, L.gcursor),
                                                                               c.group_sorted.ptr);
+        if (c.height.ptr) {
+            ++pre;
+            k_disk_height<<<(n + TPB - 1) / TPB, TPB, 0, q>>>(m, n, part, c.height.ptr);
+        }
         GD_TRY_CUDA(cudaGetLastError());
         // new neighbour lists and measures: no stored rate stands
         GD_TRY_CUDA(cudaMemsetAsync(c.rated.ptr, 0xff, sizeof(int) * n, q));
@@ -1785,6 +1856,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
                                                           at<unsigned long long>(c.small, L.mmax), lower, upper);
         RateArgs ra;
         ra.ids = ids;
+        ra.height = c.height.ptr;
         ra.w = w;
         ra.part = part;
         ra.codes = codes;
@@ -1862,7 +1934,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
     GD_TRY_CUDA(cudaStreamBeginCaptureToGraph(b, wave_graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     Status st = [&]() -> Status {
         if (log_on) ctl_launch_mark(ctl, 0, b);
-        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 12, b));  // error_flag, queued, head
+        GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.merged + 4, 0, 16, b));  // error_flag, queued, light, head
         ChainArgs ca;
         // A wave of every group holds every particle once: the skip scan (whose queue order the chain
         // does not depend on) then walks them in index order, with coalesced per-particle loads.
@@ -1883,8 +1955,10 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ca.complete = c.complete.ptr;
         ca.queue = c.queue.ptr;
         ca.queued = at<int>(c.small, L.queued);
+        ca.n = n;
         k_skip_scan<<<grid_for(n, TPB), TPB, 0, b>>>(ca);
         ChainRun cr;
+        cr.height = c.height.ptr;
         cr.part_ro = part;
         cr.part = part;
         cr.codes = codes;

@@ -131,6 +131,7 @@ struct Collider {
     DevBuf<int> stamp, rated;
     double rated_lambda0 = 0.0;
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
+    DevBuf<double> height;            // R h_g(R) per particle (N_Z = 1 physical kernel), per geometry epoch
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
     DevBuf<int> ids, queue, group_sorted, spatial;
     // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)

@@ -363,7 +363,7 @@ struct CtlPtrs {
     int record_capacity;
     const double *conf_log;
     // COL_DIAGNOSTICS (all null when off)
-    const int *queued;                    // owners the wave's skip scan queued
+    const int *queued;                    // [2] owners the wave's skip scan queued (front, back)
     OperatorLog *oplog;
     int oplog_capacity;
     const unsigned long long *event_count;

@@ -240,7 +240,7 @@ __global__ void k_ctl_finish(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditiona
     c.res.owner_updates += c.wave.count;
     c.op_waves += 1;
     c.op_updates += c.wave.count;
-    if (p.queued) c.op_blocks += static_cast<unsigned long long>(*p.queued);
+    if (p.queued) c.op_blocks += static_cast<unsigned long long>(p.queued[0] + p.queued[1]);
     if (p.oplog) {
         c.chain_ns += c.t_mark1 - c.t_mark0;
         c.audit_ns += device_ns() - c.t_mark1;

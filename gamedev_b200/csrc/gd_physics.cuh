@@ -155,21 +155,41 @@ __device__ __forceinline__ PairOwner cached_owner_terms(const Model &m, const En
     return o;
 }
 
-// _cached_pair_velocity with the owner terms evaluated once (the same operations as below)
-__device__ __forceinline__ double cached_pair_speed_o(const Model &m, const Env &e, const PairOwner &o,
-                                                      double size_j) {
-    const double si = o.si, fi = o.fi, mi = o.mi;
+// The partner's terms of _cached_pair_velocity at the owner's environment: its Stokes number, drag
+// factor and grain mass.  They depend on the partner's frozen reservoir and the owner's position
+// only, so a chain evaluates them once per owner instead of once per event.
+struct PairPartner {
+    double sj, fj, mj;
+};
+
+__device__ __forceinline__ PairPartner cached_partner_terms(const Model &m, const Env &e, double size_j) {
+    PairPartner p;
     double sj = m.stokes_0 * (size_j / m.S_0);
     sj /= e.radial;
     sj /= e.strat;
-    double fj = 1.0 / (1.0 + sj * sj);
+    p.sj = sj;
+    p.fj = 1.0 / (1.0 + sj * sj);
+    p.mj = grain_mass(m, size_j);
+    return p;
+}
+
+// _cached_pair_velocity from the owner's and the partner's terms (the same operations as below)
+__device__ __forceinline__ double cached_pair_speed_pp(const Model &m, const Env &e, const PairOwner &o,
+                                                       const PairPartner &p) {
+    const double si = o.si, fi = o.fi, mi = o.mi;
+    const double sj = p.sj, fj = p.fj, mj = p.mj;
     double dvr = 2.0 * e.vn * drift_difference(si, fi, sj, fj);
     double dvphi = e.vn * (fi - fj);
     double dvz = e.Z * e.omega * (fmin(si, 0.5) - fmin(sj, 0.5));
     double vt = oc07_speed(si, sj, e.re_inv_sqrt, e.vg_sq);
-    double mj = grain_mass(m, size_j);
     double vb = fmin(sqrt(8.0 * e.cs * e.cs * m.m_mol * (mi + mj) / (M_PI * mi * mj)), e.cs);
     return sqrt(dvr * dvr + dvphi * dvphi + dvz * dvz + vt * vt + vb * vb);
+}
+
+// _cached_pair_velocity with the owner terms evaluated once
+__device__ __forceinline__ double cached_pair_speed_o(const Model &m, const Env &e, const PairOwner &o,
+                                                      double size_j) {
+    return cached_pair_speed_pp(m, e, o, cached_partner_terms(m, e, size_j));
 }
 
 // _cached_pair_velocity (inc/swarm/_col_rates.cuh:127-141): physical units, analytic gas

@@ -558,6 +558,11 @@ class SwarmBatch:
         self._check(self.lib.gd_batch_collide(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
                                               C.c_void_p(_ptr(codes)), C.c_void_p(_ptr(measure)), d, m))
 
+    def reset_controller(self):
+        """gd_batch_reset_controller: every swarm's bath controller memory afresh."""
+        self.lib.gd_batch_set_stream(self.h, _stream())
+        self._check(self.lib.gd_batch_reset_controller(self.h))
+
     def operator_stats(self, s: int) -> dict:
         st = GdOperatorStats()
         self._check(self.lib.gd_batch_operator_stats(self.h, int(s), C.byref(st)))

@@ -424,6 +424,9 @@ gd_status gd_batch_collide(gd_batch *b, gd_particle *dev_particle, void *dev_rng
                            const double *dev_measure, const double *durations, const double *total_dust_masses);
 /* Controller statistics of swarm s's last operators (as gd_last_operator_stats). */
 gd_status gd_batch_operator_stats(const gd_batch *b, int s, gd_operator_stats *out);
+/* Every swarm's bath controller memory afresh (gd_reset_controller for each swarm, an output
+ * boundary); results of captured operators not read yet are read first. */
+gd_status gd_batch_reset_controller(gd_batch *b);
 /* Positions changed without a new gd_batch_knn: the operators rebuild their owner lists. */
 gd_status gd_batch_invalidate(gd_batch *b);
 gd_status gd_batch_set_tuning(gd_batch *b, const gd_tuning *t);  /* walk, prescan, block width, sort */

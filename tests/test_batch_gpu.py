@@ -138,6 +138,7 @@ def test_batched_operators_equal_solo_operators(gd, cuda):
     # particles of two solo operators per swarm
     dp.copy_(gd.particles_to_device(p))
     rng.copy_(batch_rng())
+    batch.reset_controller()  # the solo runs start with fresh bath controllers too
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         batch.knn(dp, codes, measure, kth)

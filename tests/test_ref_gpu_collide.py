@@ -235,12 +235,12 @@ def test_operator_log_equals_reference_log(gd, cuda):
     """The per-operator COL_DIAGNOSTICS log (gd_operator_log) against the reference's
     collision_local_*.jsonl on the Morton shapes, where the event chains are the same: per operator
     its number, duration, waves, owner updates, finest ticks and event counts exactly; per group its
-    owners, final and initial levels, bath length, requested lengths (minimum, maximum, final,
-    initial), binding constraint, coarsened / refined / constrained updates, updates, overshoots and
-    persistent overshoots exactly, the oldest linked reservoir and the bath length over request to
-    1e-12, the growth and predicted-activity maxima to 1e-9 (FP64 atomic audit sums).  Chain blocks
-    and launches count this build's persistent chain, and the seconds are device time: present and
-    non-negative."""
+    owners, final and initial levels, bath length, binding constraint, coarsened / refined /
+    constrained updates, updates, overshoots and persistent overshoots exactly; the requested
+    lengths, the oldest linked reservoir and the bath length over request to 1e-12 (FP64 atomic
+    rate-bin sums), the growth and predicted-activity maxima to 1e-9 (FP64 atomic audit sums).
+    Chain blocks and launches count this build's persistent chain, and the seconds are device time:
+    present and non-negative."""
     import torch
 
     from gamedev_b200 import workloads
@@ -266,11 +266,13 @@ def test_operator_log_equals_reference_log(gd, cuda):
     assert len(ours) == len(ref) == 2
     exact_top = ("schema", "method", "operator", "duration", "waves", "owner_updates", "finest_ticks", "event_counts")
     exact_group = ("id", "owners", "level", "dt", "initial_level", "coarsened_updates", "refined_updates",
-                   "neighbor_constrained_updates", "minimum_requested_dt", "maximum_requested_dt",
-                   "final_requested_dt", "initial_requested_dt", "initial_binding_constraint", "updates",
-                   "overshoots", "persistent_overshoots")
-    close_group = {"max_snapshot_age_at_start": 1e-12, "max_requested_dt_ratio": 1e-12, "max_growth": 1e-9,
-                   "max_predicted_activity": 1e-9}
+                   "neighbor_constrained_updates", "initial_binding_constraint", "updates", "overshoots",
+                   "persistent_overshoots")
+    # the requested lengths come from FP64 atomic rate-bin sums: their last bits follow the sum order
+    # on both sides, while the power-of-two levels and bath lengths built from them agree exactly
+    close_group = {"minimum_requested_dt": 1e-12, "maximum_requested_dt": 1e-12, "final_requested_dt": 1e-12,
+                   "initial_requested_dt": 1e-12, "max_snapshot_age_at_start": 1e-12,
+                   "max_requested_dt_ratio": 1e-12, "max_growth": 1e-9, "max_predicted_activity": 1e-9}
     assert set(ours[0]) == set(ref[0])
     for a, b in zip(ours, ref):
         for key in exact_top:

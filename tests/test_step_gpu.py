@@ -7,8 +7,8 @@ loop without the collision halves.  Both sides get the same particles and the sa
 (curand_init(seed, i, 0)).  Errors are measured against each particle's own scales: angles
 absolutely, the spherical radius relative to itself, angular momenta relative to the Keplerian
 sqrt(G M R) and the radial speed relative to the Keplerian speed at R.  Bars:
-  * t0 (3D, transport + diffusion, no radiation field): every step's dt and the clocks equal, the
-    cuRAND states byte-identical (the same normal draws, in the same order), positions and
+  * t0 (3D, transport + diffusion, no radiation field): every step's dt and the clocks equal, every
+    member of the cuRAND states identical (the same normal draws, in the same order), positions and
     velocities within 1e-12 of those scales;
   * c4 (3D, radiation pressure with Poynting-Robertson drag): the optical depth is a sum of FP64
     atomic deposits, whose order varies from run to run on both sides, so positions and velocities
@@ -78,7 +78,10 @@ def _compare(name, bar, steps=4):
     ref, rst, info = refstep.run(name, p, 3, steps, _mass(p))
     assert np.array_equal(np.array(dts).view(np.uint64), np.array(info["dt"]).view(np.uint64)), (dts, info["dt"])
     assert clk["clock_sim"] == info["clock_sim"] and clk["clock_out"] == info["clock_out"]
-    assert np.array_equal(st, rst), int((st != rst).any(axis=1).sum())
+    # every member of each curandStateXORWOW (d, v[5], the two Box-Muller flags, the float and the
+    # double spare); bytes 36-39 are alignment padding before the double, which copies need not keep
+    members = np.r_[0:36, 40:48]
+    assert np.array_equal(st[:, members], rst[:, members]), int((st[:, members] != rst[:, members]).any(axis=1).sum())
     for col, err in enumerate(_scaled_errors(cfg, ours, ref)):
         assert err.max() <= bar, (name, col, float(err.max()), int(np.argmax(err)))
     # grain sizes and counts are not the dynamics' to change
