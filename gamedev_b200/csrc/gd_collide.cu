@@ -657,6 +657,10 @@ struct ChainRun {
 };
 
 // col_chain_run (col_chain_run.cu:21-404): persistent warps, one owner at a time
+// kSlots = neighbour slots per lane (2 for K <= 64, 4 for K <= 128, else 8): the owner's partners
+// and, for the cached physical kernel, their Stokes terms at the owner's environment stay in
+// registers for the whole chain.
+template <int kSlots>
 __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a, ChainRun r) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
@@ -694,16 +698,18 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
 
         // frozen partners of this owner, kept in registers for every event
         const OwnerCtx o = owner_ctx(m, r.part_ro, r.env, i, meas, r.lambda0);
-        int nb[kMaxSlots];
-        double sj[kMaxSlots], nj[kMaxSlots], hj[kMaxSlots];
+        int nb[kSlots];
+        double sj[kSlots], nj[kSlots], hj[kSlots];
+        PairPartner pp[kSlots];
         const bool physical = m.coag_kernel == GD_KERNEL_CUSTOM;
         const bool cached = physical && use_env_cache(m);
 #pragma unroll
-        for (int t = 0; t < kMaxSlots; ++t) {
+        for (int t = 0; t < kSlots; ++t) {
             nb[t] = -1;
             sj[t] = 0.0;
             nj[t] = 0.0;
             hj[t] = 0.0;
+            pp[t] = PairPartner{0.0, 0.0, 0.0};
             const int s = lane + 32 * t;
             if (t < nslot && s < K) {
                 nb[t] = r.codes[static_cast<size_t>(i) * K + s];
@@ -712,6 +718,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
                     sj[t] = r.size_old[j];
                     nj[t] = r.numr_old[j];
                     if (r.height) hj[t] = r.height[j];  // the partner's disk height (_col_rates.cuh:205-210)
+                    if (cached) pp[t] = cached_partner_terms(m, o.env, sj[t]);
                 }
             }
         }
@@ -726,13 +733,13 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
             PairOwner po{0.0, 0.0, 0.0};
             if (cached) po = cached_owner_terms(m, o.env, size_i);
 #pragma unroll
-            for (int t = 0; t < kMaxSlots; ++t) {
+            for (int t = 0; t < kSlots; ++t) {
                 const int s = lane + 32 * t;
                 if (t < nslot && s < K) {
                     double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
                     if (nb[t] >= 0) {
                         double vrel;
-                        pv = chain_pair_rate(m, o, po, size_i, sj[t], nj[t], hj[t], vrel);
+                        pv = chain_pair_rate(m, o, po, size_i, sj[t], nj[t], hj[t], vrel, cached ? &pp[t] : nullptr);
                         double mean = 0.0, sec = 0.0, maxi = 0.0;
                         pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
                         j1 = pv * mean;
@@ -1730,11 +1737,14 @@ static Status collider_setup(Collider &c, const Model &m) {
         GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(audit_blocked_smem(R))));
     c.chain_smem = static_cast<size_t>(kChainWarps) * (kChainDoubles * 8 + 4) * K;
+    c.chain_kernel = K <= 64 ? reinterpret_cast<const void *>(&k_chain<2>)
+                             : (K <= 128 ? reinterpret_cast<const void *>(&k_chain<4>)
+                                         : reinterpret_cast<const void *>(&k_chain<8>));
     if (c.chain_smem > 48 * 1024)
-        GD_TRY_CUDA(cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GD_TRY_CUDA(cudaFuncSetAttribute(c.chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(c.chain_smem)));
     int per_sm = 0;
-    GD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chain, kChainWarps * 32, c.chain_smem));
+    GD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, c.chain_kernel, kChainWarps * 32, c.chain_smem));
     c.chain_grid = c.sms * (per_sm < 1 ? 1 : per_sm);
     c.setup_done = true;
     return Status::ok();
@@ -1973,7 +1983,12 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         cr.event_count = c.diagnostics ? c.event_count.ptr : nullptr;
         cr.event_log_mass = c.diagnostics ? c.event_log_mass.ptr : nullptr;
         const int blocks = std::min(c.chain_grid, (n + kChainWarps - 1) / kChainWarps);
-        k_chain<<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
+        if (K <= 64)
+            k_chain<2><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
+        else if (K <= 128)
+            k_chain<4><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
+        else
+            k_chain<8><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
         if (log_on) {
             ctl_launch_mark(ctl, 1, b);
             body += 2;

@@ -148,6 +148,7 @@ struct Collider {
     cudaStream_t body_stream = nullptr;     // the wave body is captured here into the conditional node
     bool setup_done = false;          // kernel attributes raised, grids sized
     int sms = 0, chain_grid = 0;
+    const void *chain_kernel = nullptr;  // the k_chain instantiation for the model's K
     size_t rate_smem = 0, chain_smem = 0;
     long long pending_launches = 0;   // launches outside the wave loop of the operators not read yet
     int body_launches = 0;            // kernels of one wave body
