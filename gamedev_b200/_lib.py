@@ -133,6 +133,7 @@ SIGNATURES = {
     "gd_radius_model_check": (C.c_int, [_P]),
     "gd_controller_summary": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_operator_log": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "gd_operator_phase_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "gd_set_diagnostics": (C.c_int, [_P, C.c_int]),
     "gd_event_totals": (C.c_int, [_P, _P, _P]),
     "gd_frame_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t]),

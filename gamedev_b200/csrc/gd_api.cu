@@ -573,6 +573,12 @@ gd_status gd_set_diagnostics(gd_handle *h, int on) {
     return GD_OK;
 }
 
+gd_status gd_operator_phase_seconds(const gd_handle *h, double *out4) {
+    if (!h || !out4) return GD_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 4; ++k) out4[k] = h->col.phase_seconds[k];
+    return GD_OK;
+}
+
 size_t gd_operator_log(const gd_handle *h, char *buf, size_t len) {
     if (!h) return 0;
     const std::string &text = h->col.operator_log;

@@ -402,6 +402,7 @@ struct RateArgs {
     RateMoments *cached;
     const int *stamp;  // publish wave of each particle's last reservoir change
     int *rated;        // publish wave of each owner's stored rates (-1: none)
+    double *leaf;      // [n][K][4] each pair's stored (rate, rate*mean, rate*second, maximum), or null
 };
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner.  kCached selects, at compile time,
@@ -442,31 +443,53 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
     PairOwner po{0.0, 0.0, 0.0};
     if (kCached) po = cached_owner_terms(m, o.env, size_i);
     const int32_t *row = a.codes + static_cast<size_t>(i) * K;
+    // A pair's terms depend on the owner's and the partner's reservoir entries (and on the fixed
+    // geometry and lambda0): when the owner's entry is unchanged, the pairs whose partner is
+    // unchanged keep their stored terms, the same bits a recomputation would give, and only the
+    // others are evaluated.  The fold below always runs over all K in the same order.
+    const bool full = rated < 0 || a.stamp[i] > rated || !a.leaf;
+    double *leaf_row = a.leaf ? a.leaf + static_cast<size_t>(i) * K * 4 : nullptr;
     for (int s0 = lane; s0 < K; s0 += 64) {
         const int s1 = s0 + 32;
         const int nb0 = row[s0];
         const int nb1 = s1 < K ? row[s1] : -1;
         const bool use0 = act && nb0 >= 0 && meas > 0.0, use1 = act && nb1 >= 0 && meas > 0.0;
-        const double sj0 = use0 ? a.size_old[nb0 / 3] : 0.0, nj0 = use0 ? a.numr_old[nb0 / 3] : 0.0;
-        const double sj1 = use1 ? a.size_old[nb1 / 3] : 0.0, nj1 = use1 ? a.numr_old[nb1 / 3] : 0.0;
+        const bool fresh0 = full || (use0 && a.stamp[nb0 / 3] > rated);
+        const bool fresh1 = s1 < K && (full || (use1 && a.stamp[nb1 / 3] > rated));
+        const double sj0 = use0 && fresh0 ? a.size_old[nb0 / 3] : 0.0, nj0 = use0 && fresh0 ? a.numr_old[nb0 / 3] : 0.0;
+        const double sj1 = use1 && fresh1 ? a.size_old[nb1 / 3] : 0.0, nj1 = use1 && fresh1 ? a.numr_old[nb1 / 3] : 0.0;
 #pragma unroll 1
         for (int t = 0; t < 2; ++t) {
             const int s = t ? s1 : s0;
             if (s >= K) break;
             const bool use = t ? use1 : use0;
+            const bool fresh = t ? fresh1 : fresh0;
             const int j = (t ? nb1 : nb0) / 3;
             const double size_j = t ? sj1 : sj0, numr_j = t ? nj1 : nj0;
             double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
-            if (use) {
-                double vrel;
-                const double h_j = a.height ? a.height[j] : 0.0;
-                double pr = chain_pair_rate(m, o, po, size_i, size_j, numr_j, h_j, vrel);
-                double mean = 0.0, sec = 0.0, maxi = 0.0;
-                pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
-                mx = pr > 0.0 ? maxi : 0.0;
-                c = pr * mean;
-                sc = pr * sec;
-                r = pr;
+            if (!fresh) {
+                const double2 a01 = reinterpret_cast<const double2 *>(leaf_row + 4 * s)[0];
+                const double2 a23 = reinterpret_cast<const double2 *>(leaf_row + 4 * s)[1];
+                r = a01.x;
+                c = a01.y;
+                sc = a23.x;
+                mx = a23.y;
+            } else {
+                if (use) {
+                    double vrel;
+                    const double h_j = a.height ? a.height[j] : 0.0;
+                    double pr = chain_pair_rate(m, o, po, size_i, size_j, numr_j, h_j, vrel);
+                    double mean = 0.0, sec = 0.0, maxi = 0.0;
+                    pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+                    mx = pr > 0.0 ? maxi : 0.0;
+                    c = pr * mean;
+                    sc = pr * sec;
+                    r = pr;
+                }
+                if (leaf_row) {
+                    reinterpret_cast<double2 *>(leaf_row + 4 * s)[0] = make_double2(r, c);
+                    reinterpret_cast<double2 *>(leaf_row + 4 * s)[1] = make_double2(sc, mx);
+                }
             }
             rate_w[s] = r;
             change_w[s] = c;
@@ -1505,6 +1528,12 @@ Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
     GD_TRY_CUDA(c.event_count.alloc(kEventCategories));
     GD_TRY_CUDA(c.event_log_mass.alloc(kEventCategories));
     if (m.coag_kernel == GD_KERNEL_CUSTOM && m.n_z == 1) GD_TRY_CUDA(c.height.alloc(n));
+    // the pairs' stored terms (32 B per pair): without the memory the rates are recomputed in full,
+    // with the same results
+    if (c.leaf.alloc(static_cast<size_t>(n) * m.n_k * 4) != cudaSuccess) {
+        cudaGetLastError();
+        c.leaf.ptr = nullptr;
+    }
     // the device controller: default bath states, no operator yet, empty accumulators
     GD_TRY_CUDA(c.ctl.alloc(sizeof(CtlDev)));
     {
@@ -1610,7 +1639,13 @@ Status collider_check_many(Collider *const *cs, int count, cudaStream_t s, int *
         Collider &c = *cs[k];
         const CtlResult &r = res[k];
         for (const BathRecord &rec : recs[k]) c.summary.record(rec);
-        for (const OperatorLog &rec : logs[k]) c.operator_log += operator_log_line(rec);
+        for (const OperatorLog &rec : logs[k]) {
+            c.operator_log += operator_log_line(rec);
+            c.phase_seconds[0] += rec.rate_seconds;
+            c.phase_seconds[1] += rec.chain_seconds;
+            c.phase_seconds[2] += rec.audit_seconds;
+            c.phase_seconds[3] += rec.wall_seconds;
+        }
         c.summary.records_dropped += r.log_dropped;
         // the persistent chain is one launch per wave (the reference relaunches capped chains)
         c.summary.operator_count = r.operator_index;
@@ -1882,6 +1917,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
         ra.stamp = c.stamp.ptr;
         ra.rated = c.rated.ptr;
+        ra.leaf = c.leaf.ptr;
         if (rate_cached)
             k_bath_rate<true><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
         else
@@ -2022,8 +2058,16 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ctl_launch_finish(ctl, m, p, handle, b);
         ctl_launch_wave_ids(ctl, c.group_sorted.ptr, ids, grid_for(n, TPB), b);
         body += 5;
+        if (log_on) {
+            ctl_launch_mark(ctl, 2, b);
+            body += 1;
+        }
         initialize(b, body);
         GD_TRY(rates_and_bins(b, body));
+        if (log_on) {
+            ctl_launch_mark(ctl, 3, b);
+            body += 1;
+        }
         ctl_launch_adapt(ctl, m, p, handle, b);
         body += 1;
         GD_TRY_CUDA(cudaGetLastError());

@@ -110,6 +110,7 @@ struct OperatorLog {
     unsigned long long operator_id, finest_ticks, owner_updates, chain_blocks;
     int waves, chain_launches, G, pad;
     double clock_sim, duration, chain_seconds, audit_seconds, wall_seconds;
+    double rate_seconds;  // the waves' reservoir publish, bath rates and bins (COL_PERF_VAL's rate phase)
     unsigned long long event_count[kEventCategories];
     double event_log_mass[kEventCategories];
     OperatorLogGroup g[kLogGroups];
@@ -132,6 +133,7 @@ struct Collider {
     double rated_lambda0 = 0.0;
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
     DevBuf<double> height;            // R h_g(R) per particle (N_Z = 1 physical kernel), per geometry epoch
+    DevBuf<double> leaf;              // [n][K][4] each pair's stored bath-rate terms (null: recompute)
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
     DevBuf<int> ids, queue, group_sorted, spatial;
     // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)
@@ -162,6 +164,9 @@ struct Collider {
     DevBuf<OperatorLog> oplog;
     int oplog_capacity = 0;
     std::string operator_log;
+    // device seconds per phase over the logged operators (the reference's COL_PERF_VAL split,
+    // _col_chain.cuh:215-241): bath rates, events (skip scan + chains), audit, whole operators
+    double phase_seconds[4] = {0.0, 0.0, 0.0, 0.0};
     bool local_geometry_valid = false;
     gd_operator_stats stats{};
     long long launches = 0;           // kernels launched by the operator (reported by the ABI)

@@ -344,7 +344,7 @@ struct CtlDev {
     unsigned long long log_operator;    // operators since the controller was created (never reset)
     unsigned long long op_updates, op_blocks;
     int op_waves;
-    unsigned long long t_begin, t_mark0, t_mark1, chain_ns, audit_ns;
+    unsigned long long t_begin, t_mark0, t_mark1, t_mark2, t_mark3, chain_ns, audit_ns, rate_ns;
     double clock_sim;
 };
 

@@ -117,6 +117,7 @@ __device__ void write_log(CtlDev &c, const CtlPtrs &p) {
     r.chain_seconds = 1.0e-9 * static_cast<double>(c.chain_ns);
     r.audit_seconds = 1.0e-9 * static_cast<double>(c.audit_ns);
     r.wall_seconds = 1.0e-9 * static_cast<double>(device_ns() - c.t_begin);
+    r.rate_seconds = 1.0e-9 * static_cast<double>(c.rate_ns);
     for (int k = 0; k < kEventCategories; ++k) {
         r.event_count[k] = p.event_count ? p.event_count[k] : 0ull;
         r.event_log_mass[k] = p.event_log_mass ? p.event_log_mass[k] : 0.0;
@@ -170,7 +171,7 @@ __global__ void k_ctl_reset(CtlDev *c, double duration, const double *duration_d
     c->t_begin = device_ns();
     c->op_updates = c->op_blocks = 0;
     c->op_waves = 0;
-    c->chain_ns = c->audit_ns = 0;
+    c->chain_ns = c->audit_ns = c->rate_ns = 0;
     c->duration = duration;
     c->n = n;
     c->G = G;
@@ -344,14 +345,21 @@ __global__ void k_ctl_adapt(Model m, CtlDev *cp, CtlPtrs p, cudaGraphConditional
         gs.constrained += c.steps_s[g] > c.current[g] ? 1 : 0;
     }
     for (int g = 0; g < c.G; ++g) p.dt[g] = c.steps_s[g];
-    if (p.oplog) wave_stats(c, p, c.current);
+    if (p.oplog) {
+        wave_stats(c, p, c.current);
+        c.rate_ns += c.t_mark3 - c.t_mark2;
+    }
 }
 
-// device time at the start of a wave's chains (0) and of its audit (1)
+// device time at the start of a wave's chains (0), of its audit (1), of the next wave's reservoir
+// publish and rates (2) and at their end (3)
 __global__ void k_ctl_mark(CtlDev *c, int which) {
     if (threadIdx.x != 0 || blockIdx.x != 0 || !c->wave.go) return;
-    if (which == 0) c->t_mark0 = device_ns();
-    else c->t_mark1 = device_ns();
+    const unsigned long long t = device_ns();
+    if (which == 0) c->t_mark0 = t;
+    else if (which == 1) c->t_mark1 = t;
+    else if (which == 2) c->t_mark2 = t;
+    else c->t_mark3 = t;
 }
 
 // the wave's owners: the owner lists of its nonempty due groups, concatenated

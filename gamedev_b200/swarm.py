@@ -191,6 +191,12 @@ class SwarmCollision:
         self.lib.gd_operator_log(self.h, buf, n + 1)
         return [json.loads(line) for line in buf.value.decode().splitlines() if line.strip()]
 
+    def operator_phase_seconds(self) -> dict:
+        """gd_operator_phase_seconds: device seconds of the logged operators by phase."""
+        out = (C.c_double * 4)()
+        self._check(self.lib.gd_operator_phase_seconds(self.h, out))
+        return {"rates": out[0], "events": out[1], "audit": out[2], "operators": out[3]}
+
     # ---- collision operator ---------------------------------------------------------------
     def evolve_local_collisions(self, particles, rng, duration: float, total_dust_mass: float):
         self.lib.gd_set_stream(self.h, _stream())

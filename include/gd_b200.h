@@ -325,6 +325,11 @@ gd_status gd_set_diagnostics(gd_handle *h, int on);
  * the full length.  The persistent chain is one launch per wave, so chain_launches = waves and
  * chain_blocks = the owners the waves queued; the reference counts each capped relaunch. */
 size_t gd_operator_log(const gd_handle *h, char *buf, size_t len);
+/* The device time of the operators logged so far, split as the reference's COL_PERF_VAL build
+ * splits it (_col_chain.cuh:215-241): out4 = seconds of the waves' reservoir publish, bath rates
+ * and bins; of the skip scans and chains; of the audits and bath finishes; of the whole operators
+ * (the rest is the bath-start pass and the controller's scheduling). */
+gd_status gd_operator_phase_seconds(const gd_handle *h, double *out4);
 gd_status gd_event_totals(gd_handle *h, unsigned long long *counts, double *log_mass);
 
 /* evolve_local_collisions (inc/swarm/_col_chain.cuh:108-539): advance every owner through one

@@ -13,6 +13,7 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libgd_b200.so")
 
 
+
 @pytest.fixture(scope="session")
 def oracle_lib():
     from oracle import oracle

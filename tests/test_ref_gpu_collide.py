@@ -290,3 +290,14 @@ def test_operator_log_equals_reference_log(gd, cuda):
         for x, y in zip(a["event_log_mass_sums"], b["event_log_mass_sums"]):
             assert math.isclose(x, y, rel_tol=1e-9, abs_tol=1e-12)
     assert sum(g["updates"] for g in ours[0]["groups"]) > 3
+
+
+def _bootstrap_ratio(a, b, reps=4000, seed=0):
+    """Ratio of the means of two per-seed samples and its 95% bootstrap interval (seeds resampled
+    independently on each side)."""
+    rng = np.random.default_rng(seed)
+    a, b = np.asarray(a), np.asarray(b)
+    ra = rng.integers(0, len(a), (reps, len(a)))
+    rb = rng.integers(0, len(b), (reps, len(b)))
+    ratios = a[ra].mean(axis=1) / b[rb].mean(axis=1)
+    return float(a.mean() / b.mean()), float(np.quantile(ratios, 0.025)), float(np.quantile(ratios, 0.975))
