@@ -364,9 +364,18 @@ __device__ __forceinline__ void warp_fold(int K, int lane, F &&combine) {
 // array k_disk_height fills, and the owner's Stokes terms of the cached physical kernel passed in
 // (evaluated once per owner, or once per event in the chain).  The same operations as pair_rate,
 // so the same bits.
+// kPhys: the caller knows at compile time that the model is the physical kernel on the cached
+// environment, and the synthetic kernels and the direct pair speed are left out of the code.
+template <bool kPhys = false>
 __device__ __forceinline__ double chain_pair_rate(const Model &m, const OwnerCtx &o, const PairOwner &po,
                                                   double size_i, double size_j, double numr_j, double H_gj,
                                                   double &vrel, const PairPartner *pre = nullptr) {
+    if constexpr (kPhys) {
+        vrel = pre ? cached_pair_speed_pp(m, o.env, po, *pre) : cached_pair_speed_o(m, o.env, po, size_j);
+        double r = numr_j * vrel * M_PI * (size_i + size_j) * (size_i + size_j) / 4.0;
+        if (m.n_z == 1) r /= sqrt(2.0 * M_PI * (o.H_i * o.H_i + H_gj * H_gj));
+        return r / o.measure;
+    }
     vrel = 0.0;
     double r;
     if (m.coag_kernel == GD_KERNEL_CONSTANT) {
@@ -402,7 +411,6 @@ struct RateArgs {
     RateMoments *cached;
     const int *stamp;  // publish wave of each particle's last reservoir change
     int *rated;        // publish wave of each owner's stored rates (-1: none)
-    double *leaf;      // [n][K][4] each pair's stored (rate, rate*mean, rate*second, maximum), or null
 };
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner.  kCached selects, at compile time,
@@ -443,53 +451,31 @@ __global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
     PairOwner po{0.0, 0.0, 0.0};
     if (kCached) po = cached_owner_terms(m, o.env, size_i);
     const int32_t *row = a.codes + static_cast<size_t>(i) * K;
-    // A pair's terms depend on the owner's and the partner's reservoir entries (and on the fixed
-    // geometry and lambda0): when the owner's entry is unchanged, the pairs whose partner is
-    // unchanged keep their stored terms, the same bits a recomputation would give, and only the
-    // others are evaluated.  The fold below always runs over all K in the same order.
-    const bool full = rated < 0 || a.stamp[i] > rated || !a.leaf;
-    double *leaf_row = a.leaf ? a.leaf + static_cast<size_t>(i) * K * 4 : nullptr;
     for (int s0 = lane; s0 < K; s0 += 64) {
         const int s1 = s0 + 32;
         const int nb0 = row[s0];
         const int nb1 = s1 < K ? row[s1] : -1;
         const bool use0 = act && nb0 >= 0 && meas > 0.0, use1 = act && nb1 >= 0 && meas > 0.0;
-        const bool fresh0 = full || (use0 && a.stamp[nb0 / 3] > rated);
-        const bool fresh1 = s1 < K && (full || (use1 && a.stamp[nb1 / 3] > rated));
-        const double sj0 = use0 && fresh0 ? a.size_old[nb0 / 3] : 0.0, nj0 = use0 && fresh0 ? a.numr_old[nb0 / 3] : 0.0;
-        const double sj1 = use1 && fresh1 ? a.size_old[nb1 / 3] : 0.0, nj1 = use1 && fresh1 ? a.numr_old[nb1 / 3] : 0.0;
+        const double sj0 = use0 ? a.size_old[nb0 / 3] : 0.0, nj0 = use0 ? a.numr_old[nb0 / 3] : 0.0;
+        const double sj1 = use1 ? a.size_old[nb1 / 3] : 0.0, nj1 = use1 ? a.numr_old[nb1 / 3] : 0.0;
 #pragma unroll 1
         for (int t = 0; t < 2; ++t) {
             const int s = t ? s1 : s0;
             if (s >= K) break;
             const bool use = t ? use1 : use0;
-            const bool fresh = t ? fresh1 : fresh0;
             const int j = (t ? nb1 : nb0) / 3;
             const double size_j = t ? sj1 : sj0, numr_j = t ? nj1 : nj0;
             double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
-            if (!fresh) {
-                const double2 a01 = reinterpret_cast<const double2 *>(leaf_row + 4 * s)[0];
-                const double2 a23 = reinterpret_cast<const double2 *>(leaf_row + 4 * s)[1];
-                r = a01.x;
-                c = a01.y;
-                sc = a23.x;
-                mx = a23.y;
-            } else {
-                if (use) {
-                    double vrel;
-                    const double h_j = a.height ? a.height[j] : 0.0;
-                    double pr = chain_pair_rate(m, o, po, size_i, size_j, numr_j, h_j, vrel);
-                    double mean = 0.0, sec = 0.0, maxi = 0.0;
-                    pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
-                    mx = pr > 0.0 ? maxi : 0.0;
-                    c = pr * mean;
-                    sc = pr * sec;
-                    r = pr;
-                }
-                if (leaf_row) {
-                    reinterpret_cast<double2 *>(leaf_row + 4 * s)[0] = make_double2(r, c);
-                    reinterpret_cast<double2 *>(leaf_row + 4 * s)[1] = make_double2(sc, mx);
-                }
+            if (use) {
+                double vrel;
+                const double h_j = a.height ? a.height[j] : 0.0;
+                double pr = chain_pair_rate<kCached>(m, o, po, size_i, size_j, numr_j, h_j, vrel);
+                double mean = 0.0, sec = 0.0, maxi = 0.0;
+                pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+                mx = pr > 0.0 ? maxi : 0.0;
+                c = pr * mean;
+                sc = pr * sec;
+                r = pr;
             }
             rate_w[s] = r;
             change_w[s] = c;
@@ -683,7 +669,7 @@ struct ChainRun {
 // kSlots = neighbour slots per lane (2 for K <= 64, 4 for K <= 128, else 8): the owner's partners
 // and, for the cached physical kernel, their Stokes terms at the owner's environment stay in
 // registers for the whole chain.
-template <int kSlots>
+template <int kSlots, bool kPhys>
 __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a, ChainRun r) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
@@ -724,8 +710,8 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
         int nb[kSlots];
         double sj[kSlots], nj[kSlots], hj[kSlots];
         PairPartner pp[kSlots];
-        const bool physical = m.coag_kernel == GD_KERNEL_CUSTOM;
-        const bool cached = physical && use_env_cache(m);
+        // kPhys: the physical kernel on the cached environment, known at compile time
+        const bool cached = kPhys;
 #pragma unroll
         for (int t = 0; t < kSlots; ++t) {
             nb[t] = -1;
@@ -762,7 +748,7 @@ __global__ void __launch_bounds__(kChainWarps * 32) k_chain(Model m, ChainArgs a
                     double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
                     if (nb[t] >= 0) {
                         double vrel;
-                        pv = chain_pair_rate(m, o, po, size_i, sj[t], nj[t], hj[t], vrel, cached ? &pp[t] : nullptr);
+                        pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel, cached ? &pp[t] : nullptr);
                         double mean = 0.0, sec = 0.0, maxi = 0.0;
                         pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
                         j1 = pv * mean;
@@ -1528,12 +1514,6 @@ Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
     GD_TRY_CUDA(c.event_count.alloc(kEventCategories));
     GD_TRY_CUDA(c.event_log_mass.alloc(kEventCategories));
     if (m.coag_kernel == GD_KERNEL_CUSTOM && m.n_z == 1) GD_TRY_CUDA(c.height.alloc(n));
-    // the pairs' stored terms (32 B per pair): without the memory the rates are recomputed in full,
-    // with the same results
-    if (c.leaf.alloc(static_cast<size_t>(n) * m.n_k * 4) != cudaSuccess) {
-        cudaGetLastError();
-        c.leaf.ptr = nullptr;
-    }
     // the device controller: default bath states, no operator yet, empty accumulators
     GD_TRY_CUDA(c.ctl.alloc(sizeof(CtlDev)));
     {
@@ -1772,9 +1752,15 @@ static Status collider_setup(Collider &c, const Model &m) {
         GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(audit_blocked_smem(R))));
     c.chain_smem = static_cast<size_t>(kChainWarps) * (kChainDoubles * 8 + 4) * K;
-    c.chain_kernel = K <= 64 ? reinterpret_cast<const void *>(&k_chain<2>)
-                             : (K <= 128 ? reinterpret_cast<const void *>(&k_chain<4>)
-                                         : reinterpret_cast<const void *>(&k_chain<8>));
+    const bool phys = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m);
+    if (phys)
+        c.chain_kernel = K <= 64 ? reinterpret_cast<const void *>(&k_chain<2, true>)
+                                 : (K <= 128 ? reinterpret_cast<const void *>(&k_chain<4, true>)
+                                             : reinterpret_cast<const void *>(&k_chain<8, true>));
+    else
+        c.chain_kernel = K <= 64 ? reinterpret_cast<const void *>(&k_chain<2, false>)
+                                 : (K <= 128 ? reinterpret_cast<const void *>(&k_chain<4, false>)
+                                             : reinterpret_cast<const void *>(&k_chain<8, false>));
     if (c.chain_smem > 48 * 1024)
         GD_TRY_CUDA(cudaFuncSetAttribute(c.chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(c.chain_smem)));
@@ -1917,7 +1903,6 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
         ra.stamp = c.stamp.ptr;
         ra.rated = c.rated.ptr;
-        ra.leaf = c.leaf.ptr;
         if (rate_cached)
             k_bath_rate<true><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
         else
@@ -2019,12 +2004,10 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         cr.event_count = c.diagnostics ? c.event_count.ptr : nullptr;
         cr.event_log_mass = c.diagnostics ? c.event_log_mass.ptr : nullptr;
         const int blocks = std::min(c.chain_grid, (n + kChainWarps - 1) / kChainWarps);
-        if (K <= 64)
-            k_chain<2><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
-        else if (K <= 128)
-            k_chain<4><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
-        else
-            k_chain<8><<<blocks, kChainWarps * 32, c.chain_smem, b>>>(m, ca, cr);
+        {
+            void *args[] = {const_cast<Model *>(&m), &ca, &cr};
+            GD_TRY_CUDA(cudaLaunchKernel(c.chain_kernel, dim3(blocks), dim3(kChainWarps * 32), args, c.chain_smem, b));
+        }
         if (log_on) {
             ctl_launch_mark(ctl, 1, b);
             body += 2;

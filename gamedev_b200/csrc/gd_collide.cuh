@@ -133,7 +133,6 @@ struct Collider {
     double rated_lambda0 = 0.0;
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
     DevBuf<double> height;            // R h_g(R) per particle (N_Z = 1 physical kernel), per geometry epoch
-    DevBuf<double> leaf;              // [n][K][4] each pair's stored bath-rate terms (null: recompute)
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
     DevBuf<int> ids, queue, group_sorted, spatial;
     // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)
