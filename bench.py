@@ -1025,10 +1025,54 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+def run_rates(args):
+    """The FP64 bath-rate kernel alone (gd_bath_rates: col_bath_rate for every owner) on the c4
+    shapes: every owner's K pair rates, outcome moments and fold, timed with CUDA events.  A line
+    for the kernel that holds half of the C4 operator; also the command its ncu capture profiles
+    (the operator's own launches sit inside a conditional graph, which ncu does not list)."""
+    import torch
+
+    import gamedev_b200 as gd
+    from gamedev_b200 import workloads
+
+    world, rank, local = dist_init(args.gpus)
+    n = args.n or workloads.CONFIGS[C4]["n"]
+    cfg = workloads.config(C4)
+    p = workloads.particles(C4, n=n, seed=workloads.CONFIGS[C4]["seed"] + rank)
+    mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+    sw = gd.SwarmCollision(cfg, n)
+    dp = gd.particles_to_device(p)
+    sw.build_cache(dp)
+    out = torch.empty((n, 4), dtype=torch.float64, device=dp.device)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        sw.bath_rates(dp, mass, out)
+    barrier(world)
+    evs = [_timed(stream, lambda: sw.bath_rates(dp, mass, out)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ms = reduce_max(statistics.mean(a.elapsed_time(b) for a, b in evs), world)
+    pairs = reduce_sum(float(n) * cfg.n_k, world)
+    if rank == 0:
+        print(json.dumps({"metric": "bath-start pair rates/s (col_bath_rate alone)", "value": pairs / (ms / 1e3),
+                          "unit": "pair rates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": "c4_rates", "n": n, "k": cfg.n_k,
+                                     "step": "env cache + disk heights + every owner's K pair rates and moments"}}),
+              flush=True)
+    sw.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "c4_rates":
+        import gamedev_b200
+
+        gamedev_b200.load()
+        run_rates(args)
         return
     if args.workload == "c2_batched":
         import gamedev_b200

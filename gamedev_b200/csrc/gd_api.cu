@@ -470,6 +470,18 @@ gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int
                                   h->geo.active.ptr, total_dust_mass, h->n, dev_out, h->stream));
 }
 
+gd_status gd_bath_rates(gd_handle *h, const gd_particle *dev_particle, double total_dust_mass, double *dev_cached4) {
+    if (!h || !dev_particle || !dev_cached4) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_cached4, 8))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle or output pointer");
+    if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "gd_bath_rates needs a neighbour cache");
+    int launches = 0;
+    gd::Status s = gd::bath_rates(h->col, h->m, h->n, dev_particle, h->codes.ptr, h->measure.ptr, h->geo.active.ptr,
+                                  total_dust_mass, dev_cached4, &launches, h->stream);
+    h->col.launches += launches;
+    return done(h, s);
+}
+
 gd_status gd_drift_keplerian(gd_handle *h, gd_particle *dev_particle, double dt) {
     if (!h || !dev_particle || !std::isfinite(dt)) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer or bad dt");
     h->geo.launches += 1;

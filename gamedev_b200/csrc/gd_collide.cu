@@ -419,8 +419,13 @@ struct RateArgs {
 // and issues the gathers of both before the pair arithmetic, so their latencies overlap.  The
 // FP64 pair arithmetic is latency-bound: 8 blocks per SM (64 registers, a few spilled) beat 4
 // blocks at 128 registers without spills by a fifth on the c3 shapes.
+// blocks of 128 per SM the bath-rate kernel is compiled for (its register budget): 8 (64 registers,
+// a few spilled) measured best against 6 and 7 on the c3 and c4 shapes
+#ifndef GD_RATE_BLOCKS
+#define GD_RATE_BLOCKS 8
+#endif
 template <bool kCached>
-__global__ void __launch_bounds__(128, 8) k_bath_rate(Model m, RateArgs a) {
+__global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_bath_rate(Model m, RateArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int K = m.n_k;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -2062,6 +2067,68 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
     GD_TRY_CUDA(e);
     c.pending_launches += pre;
     c.body_launches = body;
+    return Status::ok();
+}
+
+// col_bath_rate (col_bath_rate.cu:13-130) for every owner, alone and eagerly launched: the
+// bath-start rate moments with the current particles as the published reservoir.  Scratch arrays
+// hold the reservoir and the stored-rate stamps, so no operator state changes.
+Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, double *out4,
+                  int *launches, cudaStream_t s) {
+    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
+        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+    GD_TRY(collider_setup(c, m));
+    const int K = m.n_k;
+    DevBuf<double> size_old, numr_old, rate, change, second;
+    DevBuf<int> stamp, rated;
+    DevBuf<WaveInfo> wave;
+    GD_TRY_CUDA(size_old.alloc(n));
+    GD_TRY_CUDA(numr_old.alloc(n));
+    GD_TRY_CUDA(rate.alloc(n));
+    GD_TRY_CUDA(change.alloc(n));
+    GD_TRY_CUDA(second.alloc(n));
+    GD_TRY_CUDA(stamp.alloc(n));
+    GD_TRY_CUDA(rated.alloc(n));
+    GD_TRY_CUDA(wave.alloc(1));
+    const WaveInfo w{n, 1, 1, 1, 1, {0, 0, 0}};
+    GD_TRY_CUDA(cudaMemcpyAsync(wave.ptr, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    GD_TRY_CUDA(cudaMemsetAsync(stamp.ptr, 0, sizeof(int) * n, s));
+    GD_TRY_CUDA(cudaMemsetAsync(rated.ptr, 0xff, sizeof(int) * n, s));
+    GD_TRY_CUDA(cudaMemcpy2DAsync(size_old.ptr, sizeof(double), &part[0].par_size, sizeof(gd_particle), sizeof(double),
+                                  n, cudaMemcpyDeviceToDevice, s));
+    GD_TRY_CUDA(cudaMemcpy2DAsync(numr_old.ptr, sizeof(double), &part[0].par_numr, sizeof(gd_particle), sizeof(double),
+                                  n, cudaMemcpyDeviceToDevice, s));
+    const bool env_on = use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM;
+    const int TPB = 256;
+    if (env_on) k_env_cache<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, reinterpret_cast<Env *>(c.env.ptr));
+    if (c.height.ptr) k_disk_height<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, c.height.ptr);
+    RateArgs ra;
+    ra.ids = nullptr;
+    ra.height = c.height.ptr;
+    ra.w = wave.ptr;
+    ra.part = part;
+    ra.codes = codes;
+    ra.measure = measure;
+    ra.active = active;
+    ra.size_old = size_old.ptr;
+    ra.numr_old = numr_old.ptr;
+    ra.env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
+    ra.lambda0 = n / static_cast<double>(K) / total_dust_mass;
+    ra.rate = rate.ptr;
+    ra.change = change.ptr;
+    ra.second = second.ptr;
+    ra.cached = reinterpret_cast<RateMoments *>(out4);
+    ra.stamp = stamp.ptr;
+    ra.rated = rated.ptr;
+    const int grid = std::max(1, std::min((n + 3) / 4, c.sms * 8));
+    if (env_on)
+        k_bath_rate<true><<<grid, 128, c.rate_smem, s>>>(m, ra);
+    else
+        k_bath_rate<false><<<grid, 128, c.rate_smem, s>>>(m, ra);
+    if (launches) *launches += (env_on ? 2 : 1) + (c.height.ptr ? 1 : 0);
+    GD_TRY_CUDA(cudaGetLastError());
+    GD_TRY_CUDA(cudaStreamSynchronize(s));  // the scratch is freed on return
     return Status::ok();
 }
 

@@ -190,6 +190,11 @@ Status collision_operator_enqueue(Collider &c, const Model &m, int n, gd_particl
                                   const int32_t *codes, const double *measure, const unsigned char *active,
                                   double duration, double total_dust_mass, cudaStream_t q);
 
+// col_bath_rate for every owner, alone (gd_bath_rates): out4 [n][4] the cached rate moments
+Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, double *out4,
+                  int *launches, cudaStream_t s);
+
 // per-pair terms of the bath-start rate for the listed owners (diagnostics and parity checks)
 Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
                   const double *measure, const unsigned char *active, double total_dust_mass, int n, double *out,

@@ -227,6 +227,16 @@ class SwarmCollision:
                                                           (cached, time, events, size_old, numr_old))))
         return cached, time, events, size_old, numr_old
 
+    def bath_rates(self, particles, total_mass: float, out=None):
+        """gd_bath_rates: every owner's bath-start rate moments [n, 4] on the current cache."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.n_p, 4), dtype=torch.float64, device=particles.device)
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_bath_rates(self.h, C.c_void_p(_ptr(particles)), float(total_mass),
+                                           C.c_void_p(_ptr(out))))
+        return out
+
     def pair_rates(self, particles, owner_ids, total_mass: float):
         """Per-pair bath-start terms [count, n_k, 5] = rate, rate*mean, rate*second, maximum, speed."""
         torch = _torch()

@@ -390,6 +390,12 @@ gd_status gd_get_owner_state(gd_handle *h, double *dev_cached4, double *dev_time
 gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int32_t *dev_owner_ids, int count,
                         double total_dust_mass, double *dev_out);
 
+/* col_bath_rate (src/swarm/col_bath_rate.cu:13-130) for every owner, alone: the bath-start rate
+ * moments [n_p][4] = (rate or -1 when invalid, first, second, maximum) on the handle's neighbour
+ * cache, with the current particle state as the published reservoir; the operator's own state is
+ * left unchanged (the call uses scratch and synchronises). */
+gd_status gd_bath_rates(gd_handle *h, const gd_particle *dev_particle, double total_dust_mass, double *dev_cached4);
+
 /* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
 long long gd_launch_count(const gd_handle *h);
 

@@ -133,6 +133,26 @@ def test_operator_one_wave_matches_oracle_chain(gd, cuda, oracle_lib, idx):
     sw.close()
 
 
+@pytest.mark.parametrize("idx", range(6))
+def test_bath_rates_match_oracle(gd, cuda, oracle_lib, idx):
+    """gd_bath_rates (col_bath_rate alone, eager) against the oracle's bath rate on the current
+    particles as reservoir, and against the operator's own bath-start moments bit for bit."""
+    name, cfg, p, _ = _chain_cases(gd)[idx]
+    sw, dp, rng, codes, measure, active = _setup(gd, cfg, p)
+    mass = _total_mass(p)
+    lam = len(p) / cfg.n_k / mass
+    cached_o, _, _, _ = oracle_lib.bath_rate(cfg, p, codes, measure, active, p[:, 6], p[:, 7], lam)
+    got = sw.bath_rates(dp, mass).cpu().numpy()
+    act = active.astype(bool)
+    np.testing.assert_allclose(got[act][:, [0, 3]], cached_o[act][:, [0, 3]], rtol=RATE_RTOL, atol=0, err_msg=name)
+    np.testing.assert_allclose(got[act][:, 1:3], cached_o[act][:, 1:3], rtol=MOMENT_RTOL, atol=0, err_msg=name)
+    # the operator's tick-0 rates are the same kernel on the same reservoir: the same bits
+    sw.evolve_local_collisions(dp, rng, 1.0e-30, mass)
+    op = sw.owner_state()[0].cpu().numpy()
+    assert np.array_equal(got[act].view(np.uint64), op[act].view(np.uint64)), name
+    sw.close()
+
+
 def test_operator_repeat_is_bit_identical_and_multiwave(gd, cuda):
     """Full controller (moving bins, merged bins, many waves): two runs from the same state give
     byte-identical particles and RNG states, and represented mass is conserved."""
