@@ -114,6 +114,49 @@ __global__ void k_site_init(Model m, int n, int n_sites, const gd_particle *__re
         atomicAdd(&counters[0], __popc(ballot) * (m.wedge ? 3 : 1));
 }
 
+// Distance from a site to the radial plane a rotation of `offset` radians carries it across: the
+// perpendicular distance R|sin(offset)| while that plane lies ahead of the site (cos >= 0), else the
+// site's cylindrical radius (_get_morton_seam_dist, morton_ghost.cuh:28-35, the same float steps).
+__device__ __forceinline__ float seam_distance(float x, float y, float offset) {
+    const float R = hypotf(x, y);
+    return (cosf(offset) >= 0.0f) ? R * fabsf(sinf(offset)) : R;
+}
+
+// The Morton search's ghost rule (morton_gcount / morton_gwrite, morton_ghost.cuh:38-88, called
+// with the largest search radius, swarm_runtime.cu:413-421): a rotated image is indexed only when
+// the seam it stands for lies within q_max of the physical site.  Image 2 (+width) stands for the
+// x_min seam, image 1 (-width) for the x_max seam.  k_site_init wrote both images and q_max; this
+// pass, run once the radius maximum is complete, drops the images the rule rejects: their keys
+// become all ones (sorted past the indexed sites, like inactive ones) and their codes -1, and the
+// indexed-site count loses them.  Images of inactive particles are marked too (the reference
+// writes ghost records for every finite particle), but were never indexed.
+__global__ void k_morton_ghosts(Model m, int n, const gd_particle *__restrict__ part,
+                                const unsigned char *__restrict__ active, float4 *__restrict__ site,
+                                unsigned long long *__restrict__ key, int *__restrict__ counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int dropped = 0;
+    if (i < n) {
+        const float q_max = __int_as_float(counters[2]);
+        const float x_min = static_cast<float>(m.x_min), x_max = static_cast<float>(m.x_max);
+        const float posx = static_cast<float>(part[i].position[0]);
+        const float4 s = site[i];
+        const bool keep[2] = {seam_distance(s.x, s.y, x_max - posx) <= q_max,   // image 1
+                              seam_distance(s.x, s.y, posx - x_min) <= q_max};  // image 2
+#pragma unroll
+        for (int image = 0; image < 2; ++image) {
+            if (keep[image]) continue;
+            const int t = (image + 1) * n + i;
+            site[t].w = __int_as_float(-1);
+            key[t] = ~0ull;
+            dropped += active[i] ? 1 : 0;
+        }
+    }
+    // one atomic per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
+    if ((threadIdx.x & 31) == 0 && dropped) atomicSub(&counters[0], dropped);
+}
+
 // colstate_flag (colstate_flag.cu:13-29): non-finite screen when the geometry is reused.
 __global__ void k_state_screen(int n, const gd_particle *__restrict__ part, int *__restrict__ counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1082,6 +1125,12 @@ Status geometry_build(Geometry &g, const Model &m, const gd_particle *dev_partic
                                                         g.active.ptr, g.key_a.ptr, g.val_a.ptr, g.n_sort,
                                                         g.counters.ptr);
     GD_TRY_CUDA(cudaGetLastError());
+    if (m.wedge && m.morton_images) {
+        g.launches += 1;
+        k_morton_ghosts<<<(n + 255) / 256, 256, 0, s>>>(m, n, dev_particle, g.active.ptr, g.site.ptr,
+                                                         g.key_a.ptr, g.counters.ptr);
+        GD_TRY_CUDA(cudaGetLastError());
+    }
     // the reference stops on the first non-finite particle before building (swarm_runtime.cu:382-393);
     // a deferred screen is read by geometry_check instead (non-finite particles are inactive and
     // carry the all-ones key, so the rest of the build and the query run safely past them)

@@ -24,6 +24,8 @@ Config names:
                    images
   w1_narrow_2d     radial-azimuthal 0.05 rad wedge, N = 65,536, K = 32, Morton search, with periodic
                    images
+  w2_wide_3d       3D 3.8 rad wedge (wider than pi), N = 65,536, K = 32, Morton search: the images
+                   the Morton ghost rule keeps
 """
 
 from __future__ import annotations
@@ -100,6 +102,10 @@ CONFIGS = {
                         sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=7, x_range=(-0.6, 0.6)),
     "w1_narrow_2d": dict(n=65536, k=32, three_d=False, search=GD_SEARCH_MORTON, v_frag=100.0,
                          sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=8, x_range=(0.0, 0.05)),
+    # a 3.8 rad wedge (wider than pi) searched by the Morton index: a rotated image of a particle far
+    # from both seams lands among the physical particles, and only the ghost rule keeps it out
+    "w2_wide_3d": dict(n=65536, k=32, three_d=True, search=GD_SEARCH_MORTON, v_frag=100.0,
+                       sizes=("loguniform", 2.0e-4, 20.0), radial="loguniform", seed=12, x_range=(0.0, 3.8)),
     # a radial-only model in code units with a constant viscosity, radiation pressure, viscous flow and
     # logarithmic output: the settings the other models leave off, so that every branch of the run's
     # parameter file (variables.txt) has a model that writes it

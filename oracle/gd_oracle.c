@@ -201,6 +201,26 @@ static void heap_replace_at(uint64_t *h, int K, int slot, uint64_t cand) {
     h[slot] = cand;
 }
 
+/* The Morton ghost rule (morton_gcount, inc/swarm/morton/morton_ghost.cuh:28-50): particle i's
+ * image 2 (+width) is kept when its seam distance to the x_min plane is at most q_max, image 1
+ * (-width) when its distance to the x_max plane is.  `point` holds the physical float sites (x, y, z,
+ * code) and `posx` the float azimuths; keep[2i] is image 1, keep[2i+1] image 2.  The seam distance
+ * is computed in double from the float inputs and `margin` is returned for each decision as
+ * (distance - q_max) / q_max, so a checker can set aside decisions closer than float rounding. */
+void gdo_morton_ghosts(int n, const float *site4, const float *posx, float q_max, float x_min, float x_max,
+                       unsigned char *keep, double *margin) {
+    for (int i = 0; i < n; ++i) {
+        const double R = hypot((double)site4[4 * (size_t)i], (double)site4[4 * (size_t)i + 1]);
+        const float off[2] = {x_max - posx[i], posx[i] - x_min};
+        for (int image = 0; image < 2; ++image) {
+            const double c = cos((double)off[image]);
+            const double d = (c >= 0.0) ? R * fabs(sin((double)off[image])) : R;
+            keep[2 * (size_t)i + image] = d <= (double)q_max;
+            margin[2 * (size_t)i + image] = q_max > 0.f ? (d - q_max) / q_max : d;
+        }
+    }
+}
+
 void gdo_knn_brute_images(int n, int n_sites, const float *site4, const float *q, const unsigned char *active,
                           int K, float image_dist_min, float q_dedup, int32_t *codes, float *d2, int threads) {
 #pragma omp parallel num_threads(threads > 0 ? threads : 1)
@@ -221,6 +241,7 @@ void gdo_knn_brute_images(int n, int n_sites, const float *site4, const float *q
             const float *qp = site4 + 4 * (size_t)i;
             for (int j = 0; j < n_sites; ++j) {
                 const uint32_t code = site_code(site4 + 4 * (size_t)j);
+                if (code == 0xffffffffu) continue; /* an image the Morton ghost rule dropped */
                 const uint32_t idx_old = code / 3u;
                 if (!active[idx_old]) continue;
                 const uint64_t cand = make_key(gdo_dist2(qp, site4 + 4 * (size_t)j), code);

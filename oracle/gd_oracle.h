@@ -42,9 +42,16 @@ void gdo_knn_kdtree(int n, const float *site4, const float *q, const unsigned ch
  * candidate, active when its particle is.  An owner with image_dist_min <= 2 q keeps one image per
  * particle, the one with the smaller key (the dedup of kdtree/index_heap.cuh:118-141); q is the
  * owner's own q_i (KD search, _col_cache.cuh:38-39) or q_dedup >= 0 (Morton search: the largest
- * q, swarm_runtime.cu:413-415).  image_dist_min < 0: no dedup. */
+ * q, swarm_runtime.cu:413-415).  image_dist_min < 0: no dedup.  A site whose code is -1 is an
+ * image the Morton ghost rule dropped and is no candidate. */
 void gdo_knn_brute_images(int n, int n_sites, const float *site4, const float *q, const unsigned char *active,
                           int K, float image_dist_min, float q_dedup, int32_t *codes, float *d2, int threads);
+
+/* The Morton ghost rule (morton_ghost.cuh:28-50) over n physical sites: keep[2i] for image 1
+ * (-width, the x_max seam), keep[2i+1] for image 2 (+width, the x_min seam); margin[] the relative
+ * distance of each decision from q_max. */
+void gdo_morton_ghosts(int n, const float *site4, const float *posx, float q_max, float x_min, float x_max,
+                       unsigned char *keep, double *margin);
 
 /* The pinned single-precision squared distance. */
 float gdo_dist2(const float *a, const float *b);

@@ -41,6 +41,8 @@ def load():
         lib.gdo_knn_brute_images.restype = None
         lib.gdo_knn_brute_images.argtypes = [C.c_int, C.c_int, P, P, P, C.c_int, C.c_float, C.c_float, P, P,
                                              C.c_int]
+        lib.gdo_morton_ghosts.restype = None
+        lib.gdo_morton_ghosts.argtypes = [C.c_int, P, P, C.c_float, C.c_float, C.c_float, P, P]
         lib.gdo_knn_kdtree.restype = None
         lib.gdo_knn_kdtree.argtypes = [C.c_int, P, P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_int]
         lib.gdo_kdtree_build.restype = P
@@ -125,6 +127,19 @@ def knn_brute_images(site4, n: int, q, active, k: int, image_dist_min: float, q_
     load().gdo_knn_brute_images(n, site4.shape[0], _p(site4), _p(q), _p(active), k, float(image_dist_min),
                                 float(q_dedup), _p(codes), _p(d2), threads or os.cpu_count())
     return codes, d2
+
+
+def morton_ghosts(site4, posx, q_max: float, x_min: float, x_max: float):
+    """The Morton ghost rule over the n physical sites `site4[:n]` (gdo_morton_ghosts): returns
+    keep (n, 2), columns image 1 and image 2, and each decision's relative margin from q_max."""
+    site4 = np.ascontiguousarray(site4, np.float32)
+    posx = np.ascontiguousarray(posx, np.float32)
+    n = posx.shape[0]
+    keep = np.empty((n, 2), np.uint8)
+    margin = np.empty((n, 2), np.float64)
+    load().gdo_morton_ghosts(n, _p(site4), _p(posx), float(q_max), float(np.float32(x_min)),
+                             float(np.float32(x_max)), _p(keep), _p(margin))
+    return keep.astype(bool), margin
 
 
 def knn_kdtree(site4, q, active, k: int, threads: int | None = None, first: int = 0, count: int = -1):

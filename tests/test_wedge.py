@@ -83,7 +83,8 @@ def _libm_sinf():
     return lambda x: np.float32(libm.sinf(np.float32(x)))
 
 
-@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d", "c0_plain_small", "c1_multisize_2d"])
+@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d", "w2_wide_3d", "c0_plain_small",
+                                      "c1_multisize_2d"])
 def test_wedge_info_restates_x_wedge_and_image_dist_min(gd, workload):
     from gamedev_b200 import GD_SEARCH_MORTON, workloads
 
@@ -107,7 +108,7 @@ def test_wedge_info_restates_x_wedge_and_image_dist_min(gd, workload):
     assert f(idm).view(np.uint32) == f(expect).view(np.uint32)
 
 
-@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d"])
+@pytest.mark.parametrize("workload", ["w0_wedge_3d", "w1_narrow_2d", "w2_wide_3d"])
 def test_wedge_swarms_lie_inside_the_wedge(workload):
     from gamedev_b200 import workloads
 
@@ -115,6 +116,32 @@ def test_wedge_swarms_lie_inside_the_wedge(workload):
     p = workloads.particles(workload, n=4096)
     assert (p[:, 0] >= cfg.x_min).all() and (p[:, 0] < cfg.x_max).all()
     assert cfg.n_x > 1 and cfg.x_max - cfg.x_min < 2.0 * math.pi
+
+
+def test_morton_ghost_rule_cases():
+    """The oracle's ghost rule (morton_gcount, morton_ghost.cuh:28-50) on hand-placed sites of a
+    3.8 rad wedge [0, 3.8): image 2 (+width) stands for the x_min seam and is kept within q_max of
+    it, image 1 (-width) for the x_max seam; past a quarter turn from a seam the distance is the
+    cylindrical radius, not the plane distance."""
+    from oracle import oracle
+
+    x_min, x_max, q_max = 0.0, 3.8, 0.5
+    R = np.array([1.0, 1.0, 1.0, 10.0, 0.4, 1.0], np.float64)
+    th = np.array([0.1, 3.75, 1.9, 0.01, 1.9, 3.8 - 2.0], np.float64)
+    site4 = np.zeros((R.size, 4), np.float32)
+    site4[:, 0] = R * np.cos(th)
+    site4[:, 1] = R * np.sin(th)
+    keep, margin = oracle.morton_ghosts(site4, th.astype(np.float32), q_max, x_min, x_max)
+    want = np.array([
+        [False, True],   # 0.1 rad past x_min: sin(0.1) = 0.0998 <= 0.5; 3.7 rad before x_max (cos < 0): R
+        [True, False],   # 0.05 rad before x_max
+        [False, False],  # the middle: 1.9 rad from both seams, beyond a quarter turn, R = 1 > 0.5
+        [False, True],   # R = 10: 10 sin(0.01) = 0.1 <= 0.5
+        [True, True],    # R = 0.4 <= q_max: both seams within reach whatever the angle
+        [False, False],  # 2.0 rad from x_max (cos < 0, so R = 1) and 1.8 rad from x_min (R)
+    ])
+    assert np.array_equal(keep, want), keep
+    assert np.all(np.abs(margin) > 1e-3)
 
 
 def _morton_ghost_rows(all_codes, all_d2, k, unique_ids):

@@ -4,14 +4,17 @@ reference's own CUDA build of the same wedge models.
 Bars:
   * the device's sites: particle i at site i (code 3i); its images at sites n + i and 2n + i
     (codes 3i + 1 and 3i + 2), the physical site rotated by -width and +width (col_site_init.cu:58-76)
-    to 1e-6 of the radius;
+    to 1e-6 of the radius; on the Morton search only the images its ghost rule keeps (code -1 for
+    the rest, morton_ghost.cuh:28-50), as the oracle decides them;
+  * past pi (w2_wide_3d) the rule matters: indexing every image would change many rows;
   * every neighbour row bit-identical to the oracle's restatement of the reference heap with its
     dedup (gdo_knn_brute_images, index_heap.cuh:112-176) over the device's own sites, and the kept
     K-th d^2 bit-identical; the radius-bounded search gives the same rows;
   * against the reference's CUDA build of the same model (oracle/_ref/collide_w*_65536: its
     col_site_init with images, its KD tree or Morton ghost index, and col_cache_get):
-      - every image coordinate bit-identical to the reference's KD node or Morton ghost record of
-        the same code, and every physical site too;
+      - the same set of indexed images (every image for KD, the ghost records for Morton), every
+        image coordinate bit-identical to the reference's KD node or Morton ghost record of the same
+        code, and every physical site too;
       - the KD rows as sets (the reference writes heap order), the Morton rows in order, every
         measure to 1e-12 relative;
       - on the Morton wedge, the collision operator leaves every particle as the reference's does
@@ -25,7 +28,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-WEDGES = ["w0_wedge_3d", "w1_narrow_2d"]
+WEDGES = ["w0_wedge_3d", "w1_narrow_2d", "w2_wide_3d"]
 
 
 def _run(gd, cfg, p, radius_scale=None):
@@ -61,8 +64,20 @@ def test_wedge_sites_and_rows_match_the_oracle(gd, cuda, workload):
     assert wedge and site4.shape == (3 * n, 4)
     code = site4[:, 3].view(np.int32)
     i = np.arange(n)
-    for img in range(3):
-        assert np.array_equal(code[img * n:(img + 1) * n], 3 * i + img)
+    assert np.array_equal(code[:n], 3 * i)
+    present = np.ones((n, 2), bool)
+    if cfg.search == GD_SEARCH_MORTON:
+        # the Morton ghost rule keeps an image only near the seam it stands for; the decisions the
+        # oracle makes farther than float rounding from q_max must agree
+        present = np.stack([code[n:2 * n] != -1, code[2 * n:] != -1], axis=1)
+        keep, margin = oracle.morton_ghosts(site4[:n], p[:, 0].astype(np.float32), float(q.max()),
+                                            cfg.x_min, cfg.x_max)
+        sure = np.abs(margin) > 1e-5
+        assert sure.mean() > 0.999
+        assert np.array_equal(present[sure], keep[sure]), int((present[sure] != keep[sure]).sum())
+    for img in (1, 2):
+        pr = present[:, img - 1]
+        assert np.array_equal(code[img * n:(img + 1) * n][pr], (3 * i + img)[pr])
     for img, ang in ((1, -width), (2, width)):
         c, s = math.cos(ang), math.sin(ang)
         x, y = site4[:n, 0].astype(np.float64), site4[:n, 1].astype(np.float64)
@@ -76,6 +91,15 @@ def test_wedge_sites_and_rows_match_the_oracle(gd, cuda, workload):
     bad = np.nonzero((want != codes).any(axis=1))[0]
     assert bad.size == 0, (workload, int(bad.size), int(bad[0]), want[bad[0]][:8], codes[bad[0]][:8])
     act = active.astype(bool)
+    if width > math.pi:
+        # wider than pi, images far from both seams land among the physical sites: the rule drops
+        # most images, and with every image indexed many rows would change
+        assert (~present).mean() > 0.5
+        every = site4.copy()
+        every[n:2 * n, 3] = (3 * i + 1).astype(np.int32).view(np.float32)
+        every[2 * n:, 3] = (3 * i + 2).astype(np.int32).view(np.float32)
+        naive, _ = oracle.knn_brute_images(every, n, q, active, cfg.n_k, idm, q_dedup)
+        assert (naive != want).any(axis=1)[act].mean() > 0.05
     kth_want = np.where(want >= 0, wd2, 0.0).max(axis=1).astype(np.float32)
     assert np.array_equal(kth_want[act].view(np.uint32), kth[act].view(np.uint32))
     # the rows reach images, and some owners have the dedup on (their K nearest here never hold two
@@ -144,12 +168,19 @@ def test_wedge_images_and_rows_match_the_reference_build(gd, cuda, workload):
     # every reference record (KD nodes; Morton points and ghosts) against our site of the same code
     rec = info["records"]
     rcode = rec[:, 3].view(np.int32)
-    pos = np.empty(3 * n, np.int64)
-    pos[site4[:, 3].view(np.int32)] = np.arange(3 * n)
+    scode = site4[:, 3].view(np.int32)
+    kept = scode != -1
+    # the KD tree holds every image; the Morton ghost index exactly the images its ghost rule keeps
+    # (morton_ghost.cuh:28-88), which are the ones this build indexes
+    assert np.array_equal(np.sort(rcode), np.sort(scode[kept])), (workload, rcode.size, int(kept.sum()))
+    pos = np.full(3 * n, -1, np.int64)
+    pos[scode[kept]] = np.nonzero(kept)[0]
     ours = site4[pos[rcode], :3]
     same_site = (ours.view(np.uint32) == rec[:, :3].view(np.uint32)).all(axis=1)
     assert same_site.all(), (workload, int((~same_site).sum()), rcode[~same_site][:4])
-    assert (rcode % 3 != 0).sum() > n // 10  # images are present in the reference's records
+    _, width, _ = gd.wedge_info(cfg)
+    # images are present in the reference's records (far fewer past pi: only those near a seam)
+    assert (rcode % 3 != 0).sum() > (n // 100 if width > math.pi else n // 10)
     # the neighbour cache
     rc, rm = info["codes"], info["measure"]
     if cfg.search == GD_SEARCH_MORTON:
@@ -163,13 +194,13 @@ def test_wedge_images_and_rows_match_the_reference_build(gd, cuda, workload):
     assert np.allclose(measure, rm, rtol=1e-12, atol=0)
 
 
-def test_morton_wedge_operator_matches_the_reference_per_particle(gd, cuda):
+@pytest.mark.parametrize("workload", ["w1_narrow_2d", "w2_wide_3d"])
+def test_morton_wedge_operator_matches_the_reference_per_particle(gd, cuda, workload):
     import torch
 
     from gamedev_b200 import workloads
 
     n = 65536
-    workload = "w1_narrow_2d"
     refcollide = _refc(workload, n)
     cfg = workloads.config(workload)
     p = workloads.particles(workload, n=n, seed=21)
