@@ -59,6 +59,8 @@ struct Small {
     size_t light;        // int: owners queued from the back (the rest)
     size_t head;         // int
     size_t events;       // unsigned long long
+    size_t pair_count;   // int: changed pairs listed for k_pair_eval this wave
+    size_t fold_count;   // int: owners listed for k_rate_fold this wave
     size_t binmap;       // int[raw]
     size_t ratebin;      // RateBin[raw]
     size_t audit;        // AuditBin[raw]
@@ -85,6 +87,8 @@ static Small small_layout(const Model &m) {
     L.head = o; o += 4;
     o += 4;
     L.events = o; o += 8;
+    L.pair_count = o; o += 4;
+    L.fold_count = o; o += 4;
     o = align256(o);
     L.binmap = o; o = align256(o + 4 * R);
     L.ratebin = o; o = align256(o + sizeof(RateBin) * R);
@@ -413,9 +417,53 @@ struct RateArgs {
     double lambda0;
     double *rate, *change, *second;
     RateMoments *cached;
-    const int *stamp;  // publish wave of each particle's last reservoir change
-    int *rated;        // publish wave of each owner's stored rates (-1: none)
+    const int *stamp;   // publish wave of each particle's last reservoir change
+    int *rated;         // publish wave of each owner's stored rates (-1: none)
+    // Stored pairs: plane p of `leaf` (planes `plane` = n*K doubles apart) holds each pair's rate,
+    // rate*mean, rate*second and maximum (p = 0..3) at owner*K + slot, or null.  With `pairs`, an
+    // owner whose own entry is unchanged appends its changed pairs (owner*K + slot) there and
+    // itself to `folds`; k_pair_eval and k_rate_fold finish it.
+    double *leaf;
+    size_t plane;
+    unsigned int *pairs;
+    int *pair_count;
+    int *folds;
+    int *fold_count;
 };
+
+__device__ __forceinline__ void store_pair(const RateArgs &a, size_t e, double r, double c, double sc, double mx) {
+    a.leaf[e] = r;
+    a.leaf[a.plane + e] = c;
+    a.leaf[2 * a.plane + e] = sc;
+    a.leaf[3 * a.plane + e] = mx;
+}
+
+// The warp's staged pairs of owner i folded in slot order's (count+1)/2 tree and written as its
+// stored bath-start rates (col_bath_rate.cu:105-129).
+__device__ __forceinline__ void fold_owner(const RateArgs &a, int K, int lane, int i, int publish, double *rate_w,
+                                           double *change_w, double *second_w, double *max_w, int *valid_w) {
+    __syncwarp();
+    warp_fold(K, lane, [&](int j, int h) {
+        rate_w[j] += rate_w[h];
+        change_w[j] += change_w[h];
+        second_w[j] += second_w[h];
+        max_w[j] = fmax(max_w[j], max_w[h]);
+        valid_w[j] = valid_w[j] && valid_w[h];
+    });
+    if (lane == 0) {
+        RateMoments cm;
+        cm.rate = valid_w[0] ? rate_w[0] : -1.0;
+        cm.first = change_w[0];
+        cm.second = second_w[0];
+        cm.maximum = max_w[0];
+        a.cached[i] = cm;
+        a.rate[i] = rate_w[0];
+        a.change[i] = change_w[0];
+        a.second[i] = second_w[0];
+        a.rated[i] = publish;
+    }
+    __syncwarp();  // the warp's staging is rewritten by its next owner
+}
 
 // col_bath_rate (col_bath_rate.cu:13-130): one warp per owner.  kCached selects, at compile time,
 // the physical kernel on the cached environment (owner terms hoisted); the other instantiation
@@ -443,15 +491,41 @@ __global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_bath_rate(Model m, Rate
     int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
                    static_cast<size_t>(wib) * K;
     const int i = owner_at(ids, slot);
-    // stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
-    // since they were evaluated (same geometry and lambda0)
+    // Stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
+    // since they were evaluated (same geometry and lambda0).  A pair's terms depend only on the
+    // owner's and the partner's entries, so when the owner's entry is unchanged only the pairs of
+    // changed partners need evaluating: with stored pairs they go to the pair list, where
+    // k_pair_eval evaluates them one per thread (no lane idles on an unchanged pair), and
+    // k_rate_fold folds the owner's K stored pairs in the same order.  The same bits either way.
     const int rated = a.rated[i];
-    bool need = rated < 0 || a.stamp[i] > rated;
-    for (int s = lane; s < K && !need; s += 32) {
-        const int nb = a.codes[static_cast<size_t>(i) * K + s];
-        need = nb >= 0 && a.stamp[nb / 3] > rated;
+    const bool own = rated < 0 || a.stamp[i] > rated;
+    int fresh = 0;  // this lane's pairs whose partner changed
+    if (!own)
+        for (int s = lane; s < K; s += 32) {
+            const int nb = a.codes[static_cast<size_t>(i) * K + s];
+            fresh += (nb >= 0 && a.stamp[nb / 3] > rated) ? 1 : 0;
+        }
+    if (!__any_sync(0xffffffffu, own || fresh > 0)) continue;
+    if (!own && a.pairs) {
+        int incl = fresh;  // inclusive prefix over the lanes
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int base = 0;
+        if (lane == 0) {
+            base = atomicAdd(a.pair_count, total);
+            a.folds[atomicAdd(a.fold_count, 1)] = i;
+        }
+        base = __shfl_sync(0xffffffffu, base, 0) + incl - fresh;
+        for (int s = lane; s < K; s += 32) {
+            const int nb = a.codes[static_cast<size_t>(i) * K + s];
+            if (nb >= 0 && a.stamp[nb / 3] > rated) a.pairs[base++] = static_cast<unsigned int>(i) * K + s;
+        }
+        continue;
     }
-    if (!__any_sync(0xffffffffu, need)) continue;
     const bool act = a.active[i] != 0;
     const double meas = a.measure[i];
     const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
@@ -491,29 +565,73 @@ __global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_bath_rate(Model m, Rate
             second_w[s] = sc;
             max_w[s] = mx;
             valid_w[s] = isfinite(r) && r >= 0.0;
+            if (a.leaf) store_pair(a, static_cast<size_t>(i) * K + s, r, c, sc, mx);
         }
     }
-    __syncwarp();
-    warp_fold(K, lane, [&](int j, int h) {
-        rate_w[j] += rate_w[h];
-        change_w[j] += change_w[h];
-        second_w[j] += second_w[h];
-        max_w[j] = fmax(max_w[j], max_w[h]);
-        valid_w[j] = valid_w[j] && valid_w[h];
-    });
-    if (lane == 0) {
-        RateMoments cm;
-        cm.rate = valid_w[0] ? rate_w[0] : -1.0;
-        cm.first = change_w[0];
-        cm.second = second_w[0];
-        cm.maximum = max_w[0];
-        a.cached[i] = cm;
-        a.rate[i] = rate_w[0];
-        a.change[i] = change_w[0];
-        a.second[i] = second_w[0];
-        a.rated[i] = publish;
+    fold_owner(a, K, lane, i, publish, rate_w, change_w, second_w, max_w, valid_w);
     }
-    __syncwarp();  // the warp's staging is rewritten by its next owner
+}
+
+// The changed pairs of owners whose own reservoir entry is unchanged (the list k_bath_rate
+// appended): one pair per thread, the same operations as k_bath_rate's per-pair evaluation, the
+// terms stored in the owner's row.
+template <bool kCached>
+__global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_pair_eval(Model m, RateArgs a) {
+    if (!a.w->go || !a.w->need_rates) return;
+    const int K = m.n_k;
+    const int count = *a.pair_count;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const unsigned int code = a.pairs[e];
+        const int i = static_cast<int>(code / static_cast<unsigned int>(K));
+        const size_t at = static_cast<size_t>(code);
+        const int nb = a.codes[at];
+        const double meas = a.measure[i];
+        double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
+        if (a.active[i] && nb >= 0 && meas > 0.0) {
+            const OwnerCtx o = owner_ctx(m, a.part, a.env, i, meas, a.lambda0);
+            const double size_i = a.size_old[i];
+            PairOwner po{0.0, 0.0, 0.0};
+            if (kCached) po = cached_owner_terms(m, o.env, size_i);
+            const int j = nb / 3;
+            const double size_j = a.size_old[j], numr_j = a.numr_old[j];
+            const double h_j = a.height ? a.height[j] : 0.0;
+            double vrel;
+            double pr = chain_pair_rate<kCached>(m, o, po, size_i, size_j, numr_j, h_j, vrel);
+            double mean = 0.0, sec = 0.0, maxi = 0.0;
+            pr *= outcome_moments(m, size_i, size_j, vrel >= m.v_frag, mean, sec, maxi);
+            mx = pr > 0.0 ? maxi : 0.0;
+            c = pr * mean;
+            sc = pr * sec;
+            r = pr;
+        }
+        store_pair(a, at, r, c, sc, mx);
+    }
+}
+
+// The owners k_bath_rate listed, folded from their K stored pairs once k_pair_eval has renewed the
+// changed ones: one warp per owner, the staging and fold of k_bath_rate.
+__global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_rate_fold(Model m, RateArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (!a.w->go || !a.w->need_rates) return;
+    const int K = m.n_k;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int count = *a.fold_count, publish = a.w->publish;
+    double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 4 * K;
+    double *rate_w = w, *change_w = w + K, *second_w = w + 2 * K, *max_w = w + 3 * K;
+    int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
+                   static_cast<size_t>(wib) * K;
+    for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < count; slot += gridDim.x * (blockDim.x >> 5)) {
+        const int i = a.folds[slot];
+        for (int s = lane; s < K; s += 32) {
+            const size_t e = static_cast<size_t>(i) * K + s;
+            const double r = a.leaf[e];
+            rate_w[s] = r;
+            change_w[s] = a.leaf[a.plane + e];
+            second_w[s] = a.leaf[2 * a.plane + e];
+            max_w[s] = a.leaf[3 * a.plane + e];
+            valid_w[s] = isfinite(r) && r >= 0.0;
+        }
+        fold_owner(a, K, lane, i, publish, rate_w, change_w, second_w, max_w, valid_w);
     }
 }
 
@@ -584,6 +702,7 @@ struct ChainArgs {
     const int32_t *spatial;
     const double *dt;
     const RateMoments *cached;
+    const double *slot_rate;  // [n*K] the bath-start pair rates k_bath_rate stored, or null
     double *time, *hazard, *jump1, *jump2, *jumpmax;
     int *events;
     unsigned char *complete;
@@ -746,6 +865,17 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
             }
         }
 
+        // At bath start (clock at zero, no event yet, the owner's size still its reservoir value)
+        // the loop's first pass would evaluate exactly the pair rates and folded totals k_bath_rate
+        // stored for this owner: the same owner size, frozen partners, environment, formulas and
+        // fold.  That pass reads them instead of evaluating K pairs again.
+        bool stored = false;
+        RateMoments c0{0.0, 0.0, 0.0, 0.0};
+        if (a.slot_rate && running && time_i == 0.0 && event_count == 0 && size_i == r.size_old[i]) {
+            c0 = a.cached[i];
+            stored = isfinite(c0.rate) && c0.rate > 0.0;
+        }
+
         long long accepted = 0;
         while (running) {
             if (accepted >= kEventBudget) {
@@ -753,42 +883,72 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
                 running = false;
                 break;
             }
-            PairOwner po{0.0, 0.0, 0.0};
-            if (cached) po = cached_owner_terms(m, o.env, size_i);
+            double total_rate, total_j1, total_j2, total_jm;
+            int last_positive;
+            if (stored) {
+                // every stored rate is finite and >= 0 (the totals are valid), so the last positive
+                // slot is the highest set bit of the ballots
+                stored = false;
+                int last = -1;
 #pragma unroll
-            for (int t = 0; t < kSlots; ++t) {
-                const int s = lane + 32 * t;
-                if (t < nslot && s < K) {
-                    double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
-                    if (nb[t] >= 0) {
-                        double vrel;
-                        pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel, cached ? &pp[t] : nullptr);
-                        double mean = 0.0, sec = 0.0, maxi = 0.0;
-                        pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
-                        j1 = pv * mean;
-                        j2 = pv * sec;
-                        jm = (pv > 0.0) ? maxi : 0.0;
+                for (int t = 0; t < kSlots; ++t) {
+                    const int s = lane + 32 * t;
+                    double pv = 0.0;
+                    if (t < nslot && s < K) {
+                        pv = a.slot_rate[static_cast<size_t>(i) * K + s];
+                        prate[s] = pv;
                     }
-                    prate[s] = pv;
-                    tot[s] = pv;
-                    pj1[s] = j1;
-                    pj2[s] = j2;
-                    pjm[s] = jm;
-                    last_w[s] = (!isfinite(pv) || pv < 0.0) ? -2 : (pv > 0.0 ? s : -1);
+                    const unsigned int pos = __ballot_sync(0xffffffffu, pv > 0.0);
+                    if (pos) last = 32 * t + 31 - __clz(pos);
                 }
+                __syncwarp();
+                total_rate = c0.rate;
+                total_j1 = c0.first;
+                total_j2 = c0.second;
+                total_jm = c0.maximum;
+                last_positive = last;
+            } else {
+                PairOwner po{0.0, 0.0, 0.0};
+                if (cached) po = cached_owner_terms(m, o.env, size_i);
+#pragma unroll
+                for (int t = 0; t < kSlots; ++t) {
+                    const int s = lane + 32 * t;
+                    if (t < nslot && s < K) {
+                        double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
+                        if (nb[t] >= 0) {
+                            double vrel;
+                            pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel,
+                                                        cached ? &pp[t] : nullptr);
+                            double mean = 0.0, sec = 0.0, maxi = 0.0;
+                            pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
+                            j1 = pv * mean;
+                            j2 = pv * sec;
+                            jm = (pv > 0.0) ? maxi : 0.0;
+                        }
+                        prate[s] = pv;
+                        tot[s] = pv;
+                        pj1[s] = j1;
+                        pj2[s] = j2;
+                        pjm[s] = jm;
+                        last_w[s] = (!isfinite(pv) || pv < 0.0) ? -2 : (pv > 0.0 ? s : -1);
+                    }
+                }
+                __syncwarp();
+                warp_fold(K, lane, [&](int j, int h) {
+                    tot[j] += tot[h];
+                    pj1[j] += pj1[h];
+                    pj2[j] += pj2[h];
+                    pjm[j] = fmax(pjm[j], pjm[h]);
+                    const int left = last_w[j], right = last_w[h];
+                    last_w[j] = (left == -2 || right == -2) ? -2 : (left > right ? left : right);
+                });
+                total_rate = tot[0];
+                total_j1 = pj1[0];
+                total_j2 = pj2[0];
+                total_jm = pjm[0];
+                last_positive = last_w[0];
+                __syncwarp();
             }
-            __syncwarp();
-            warp_fold(K, lane, [&](int j, int h) {
-                tot[j] += tot[h];
-                pj1[j] += pj1[h];
-                pj2[j] += pj2[h];
-                pjm[j] = fmax(pjm[j], pjm[h]);
-                const int left = last_w[j], right = last_w[h];
-                last_w[j] = (left == -2 || right == -2) ? -2 : (left > right ? left : right);
-            });
-            const double total_rate = tot[0], total_j1 = pj1[0], total_j2 = pj2[0], total_jm = pjm[0];
-            const int last_positive = last_w[0];
-            __syncwarp();
             // the reference's thread-0 section, replayed identically by every lane
             if (last_positive == -2) {
                 err = 1;
@@ -1512,6 +1672,11 @@ Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
     GD_TRY_CUDA(c.complete.alloc(n));
     GD_TRY_CUDA(c.env.alloc(static_cast<size_t>(n) * 8));
     GD_TRY_CUDA(c.cached.alloc(static_cast<size_t>(n) * 4));
+    if (static_cast<long long>(n) * m.n_k < (1ll << 31)) {
+        GD_TRY_CUDA(c.leaf.alloc(static_cast<size_t>(n) * m.n_k * 4));
+        GD_TRY_CUDA(c.pairs.alloc(static_cast<size_t>(n) * m.n_k));
+        GD_TRY_CUDA(c.folds.alloc(n));
+    }
     GD_TRY_CUDA(c.stamp.alloc(n));
     GD_TRY_CUDA(c.rated.alloc(n));
     GD_TRY_CUDA(cudaMemset(c.stamp.ptr, 0, sizeof(int) * n));
@@ -1761,6 +1926,8 @@ static Status collider_setup(Collider &c, const Model &m) {
                                          static_cast<int>(c.rate_smem)));
         GD_TRY_CUDA(cudaFuncSetAttribute(k_bath_rate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(c.rate_smem)));
+        GD_TRY_CUDA(cudaFuncSetAttribute(k_rate_fold, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(c.rate_smem)));
     }
     if (R <= kAuditSmemBins)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1917,10 +2084,27 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ra.cached = reinterpret_cast<RateMoments *>(c.cached.ptr);
         ra.stamp = c.stamp.ptr;
         ra.rated = c.rated.ptr;
+        const bool stored = c.leaf.ptr != nullptr;
+        ra.leaf = c.leaf.ptr;
+        ra.plane = static_cast<size_t>(n) * m.n_k;
+        ra.pairs = c.pairs.ptr;
+        ra.pair_count = at<int>(c.small, L.pair_count);
+        ra.folds = c.folds.ptr;
+        ra.fold_count = at<int>(c.small, L.fold_count);
+        if (stored) GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.pair_count, 0, 8, st));
         if (rate_cached)
             k_bath_rate<true><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
         else
             k_bath_rate<false><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
+        if (stored) {
+            // the changed pairs of the owners whose own entry is unchanged, then their folds
+            launches += 2;
+            if (rate_cached)
+                k_pair_eval<true><<<grid_for(static_cast<long long>(n) * m.n_k, 128), 128, 0, st>>>(m, ra);
+            else
+                k_pair_eval<false><<<grid_for(static_cast<long long>(n) * m.n_k, 128), 128, 0, st>>>(m, ra);
+            k_rate_fold<<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
+        }
         GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.counts, 0, 4 * R, st));
         if (R <= kScanSmemEntries)
             k_count_bin_blocked<<<(n + kAuditSpan - 1) / kAuditSpan, kAuditTPB, sizeof(int) * R, st>>>(
@@ -1991,6 +2175,7 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ca.spatial = spatial;
         ca.dt = dt;
         ca.cached = reinterpret_cast<const RateMoments *>(c.cached.ptr);
+        ca.slot_rate = c.leaf.ptr;  // plane 0: each stored pair's rate
         ca.time = c.time.ptr;
         ca.hazard = c.hazard.ptr;
         ca.jump1 = c.jump1.ptr;
@@ -2128,6 +2313,12 @@ Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, c
     ra.change = change.ptr;
     ra.second = second.ptr;
     ra.cached = reinterpret_cast<RateMoments *>(out4);
+    ra.leaf = nullptr;  // every owner evaluated whole, nothing stored
+    ra.plane = 0;
+    ra.pairs = nullptr;
+    ra.pair_count = nullptr;
+    ra.folds = nullptr;
+    ra.fold_count = nullptr;
     ra.stamp = stamp.ptr;
     ra.rated = rated.ptr;
     const int grid = std::max(1, std::min((n + 3) / 4, c.sms * 8));

@@ -134,6 +134,12 @@ struct Collider {
     DevBuf<double> env;               // 8 doubles per owner (query_environment)
     DevBuf<double> height;            // R h_g(R) per particle (N_Z = 1 physical kernel), per geometry epoch
     DevBuf<double> cached;            // 4 doubles per owner (cached_rate_moments)
+    // Stored pairs (n*K < 2^31 only, else left empty): four planes of n*K doubles, each pair's rate,
+    // rate*mean, rate*second and maximum at owner*K + slot; the list of changed pairs of owners
+    // whose own entry is unchanged (owner*K + slot), and those owners.
+    DevBuf<double> leaf;
+    DevBuf<unsigned int> pairs;
+    DevBuf<int> folds;
     DevBuf<int> ids, queue, group_sorted, spatial;
     // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)
     DevBuf<unsigned char> small;

@@ -160,3 +160,30 @@ def test_batched_operators_equal_solo_operators(gd, cuda):
     assert e.value.status in (4, 8) and e.value.detail == 4
     del graph
     batch.close()
+
+
+def test_batch_at_the_full_batched_shape(gd, cuda):
+    """The batched configuration itself: 256 swarms of 2^10 to 2^18 particles (about 1.2e7 in all),
+    K from {16, 32, 64}, one persistent search.  Every swarm's rows, measures and K-th d^2 equal a
+    solo search of that swarm."""
+    import torch
+
+    from gamedev_b200 import workloads
+
+    cfg, sizes, ks, p = workloads.c2_batch()
+    assert len(sizes) == 256 and min(sizes) >= 1 << 10 and max(sizes) <= 1 << 18
+    batch = gd.SwarmBatch(cfg, sizes, ks)
+    dp = gd.particles_to_device(p)
+    codes, measure, kth = batch.outputs()
+    batch.knn(dp, codes, measure, kth)
+    batch.check()
+    torch.cuda.synchronize()
+    c, m, t = codes.cpu(), measure.cpu(), kth.cpu()
+    del codes, measure, kth, dp
+    off = batch.part_off
+    for s in range(len(sizes)):
+        sc, sm, st = _solo(gd, workloads.c2_batch()[0], p[off[s]:off[s + 1]], ks[s])
+        assert np.array_equal(batch.codes_of(c, s).numpy(), sc), s
+        assert np.array_equal(batch.rows_of(m, s).numpy().view(np.uint64), sm.view(np.uint64)), s
+        assert np.array_equal(batch.rows_of(t, s).numpy().view(np.uint32), st.view(np.uint32)), s
+    batch.close()
