@@ -93,8 +93,9 @@ def test_wedge_sites_and_rows_match_the_oracle(gd, cuda, workload):
     act = active.astype(bool)
     if width > math.pi:
         # wider than pi, images far from both seams land among the physical sites: the rule drops
-        # most images, and with every image indexed many rows would change
-        assert (~present).mean() > 0.5
+        # them (about a third of all images here, where q_max is large against the inner radii),
+        # and with every image indexed many rows would change (about 30% of the active owners)
+        assert (~present).mean() > 0.25
         every = site4.copy()
         every[n:2 * n, 3] = (3 * i + 1).astype(np.int32).view(np.float32)
         every[2 * n:, 3] = (3 * i + 2).astype(np.int32).view(np.float32)
