@@ -702,7 +702,6 @@ struct ChainArgs {
     const int32_t *spatial;
     const double *dt;
     const RateMoments *cached;
-    const double *slot_rate;  // [n*K] the bath-start pair rates k_bath_rate stored, or null
     double *time, *hazard, *jump1, *jump2, *jumpmax;
     int *events;
     unsigned char *complete;
@@ -865,17 +864,6 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
             }
         }
 
-        // At bath start (clock at zero, no event yet, the owner's size still its reservoir value)
-        // the loop's first pass would evaluate exactly the pair rates and folded totals k_bath_rate
-        // stored for this owner: the same owner size, frozen partners, environment, formulas and
-        // fold.  That pass reads them instead of evaluating K pairs again.
-        bool stored = false;
-        RateMoments c0{0.0, 0.0, 0.0, 0.0};
-        if (a.slot_rate && running && time_i == 0.0 && event_count == 0 && size_i == r.size_old[i]) {
-            c0 = a.cached[i];
-            stored = isfinite(c0.rate) && c0.rate > 0.0;
-        }
-
         long long accepted = 0;
         while (running) {
             if (accepted >= kEventBudget) {
@@ -883,72 +871,45 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
                 running = false;
                 break;
             }
-            double total_rate, total_j1, total_j2, total_jm;
-            int last_positive;
-            if (stored) {
-                // every stored rate is finite and >= 0 (the totals are valid), so the last positive
-                // slot is the highest set bit of the ballots
-                stored = false;
-                int last = -1;
-#pragma unroll
-                for (int t = 0; t < kSlots; ++t) {
-                    const int s = lane + 32 * t;
-                    double pv = 0.0;
-                    if (t < nslot && s < K) {
-                        pv = a.slot_rate[static_cast<size_t>(i) * K + s];
-                        prate[s] = pv;
+            PairOwner po{0.0, 0.0, 0.0};
+            if (cached) po = cached_owner_terms(m, o.env, size_i);
+            // one copy of the pair code, not kSlots: the loop body is the kernel's largest, and
+            // unrolled it made instruction fetch the leading stall (10% slower chains at N = 1e7)
+#pragma unroll 1
+            for (int t = 0; t < kSlots; ++t) {
+                const int s = lane + 32 * t;
+                if (t < nslot && s < K) {
+                    double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
+                    if (nb[t] >= 0) {
+                        double vrel;
+                        pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel,
+                                                    cached ? &pp[t] : nullptr);
+                        double mean = 0.0, sec = 0.0, maxi = 0.0;
+                        pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
+                        j1 = pv * mean;
+                        j2 = pv * sec;
+                        jm = (pv > 0.0) ? maxi : 0.0;
                     }
-                    const unsigned int pos = __ballot_sync(0xffffffffu, pv > 0.0);
-                    if (pos) last = 32 * t + 31 - __clz(pos);
+                    prate[s] = pv;
+                    tot[s] = pv;
+                    pj1[s] = j1;
+                    pj2[s] = j2;
+                    pjm[s] = jm;
+                    last_w[s] = (!isfinite(pv) || pv < 0.0) ? -2 : (pv > 0.0 ? s : -1);
                 }
-                __syncwarp();
-                total_rate = c0.rate;
-                total_j1 = c0.first;
-                total_j2 = c0.second;
-                total_jm = c0.maximum;
-                last_positive = last;
-            } else {
-                PairOwner po{0.0, 0.0, 0.0};
-                if (cached) po = cached_owner_terms(m, o.env, size_i);
-#pragma unroll
-                for (int t = 0; t < kSlots; ++t) {
-                    const int s = lane + 32 * t;
-                    if (t < nslot && s < K) {
-                        double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
-                        if (nb[t] >= 0) {
-                            double vrel;
-                            pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel,
-                                                        cached ? &pp[t] : nullptr);
-                            double mean = 0.0, sec = 0.0, maxi = 0.0;
-                            pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
-                            j1 = pv * mean;
-                            j2 = pv * sec;
-                            jm = (pv > 0.0) ? maxi : 0.0;
-                        }
-                        prate[s] = pv;
-                        tot[s] = pv;
-                        pj1[s] = j1;
-                        pj2[s] = j2;
-                        pjm[s] = jm;
-                        last_w[s] = (!isfinite(pv) || pv < 0.0) ? -2 : (pv > 0.0 ? s : -1);
-                    }
-                }
-                __syncwarp();
-                warp_fold(K, lane, [&](int j, int h) {
-                    tot[j] += tot[h];
-                    pj1[j] += pj1[h];
-                    pj2[j] += pj2[h];
-                    pjm[j] = fmax(pjm[j], pjm[h]);
-                    const int left = last_w[j], right = last_w[h];
-                    last_w[j] = (left == -2 || right == -2) ? -2 : (left > right ? left : right);
-                });
-                total_rate = tot[0];
-                total_j1 = pj1[0];
-                total_j2 = pj2[0];
-                total_jm = pjm[0];
-                last_positive = last_w[0];
-                __syncwarp();
             }
+            __syncwarp();
+            warp_fold(K, lane, [&](int j, int h) {
+                tot[j] += tot[h];
+                pj1[j] += pj1[h];
+                pj2[j] += pj2[h];
+                pjm[j] = fmax(pjm[j], pjm[h]);
+                const int left = last_w[j], right = last_w[h];
+                last_w[j] = (left == -2 || right == -2) ? -2 : (left > right ? left : right);
+            });
+            const double total_rate = tot[0], total_j1 = pj1[0], total_j2 = pj2[0], total_jm = pjm[0];
+            const int last_positive = last_w[0];
+            __syncwarp();
             // the reference's thread-0 section, replayed identically by every lane
             if (last_positive == -2) {
                 err = 1;
@@ -2175,7 +2136,6 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ca.spatial = spatial;
         ca.dt = dt;
         ca.cached = reinterpret_cast<const RateMoments *>(c.cached.ptr);
-        ca.slot_rate = c.leaf.ptr;  // plane 0: each stored pair's rate
         ca.time = c.time.ptr;
         ca.hazard = c.hazard.ptr;
         ca.jump1 = c.jump1.ptr;
