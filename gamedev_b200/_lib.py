@@ -135,6 +135,7 @@ SIGNATURES = {
     "gd_operator_log": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "gd_operator_phase_seconds": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "gd_bath_rates": (C.c_int, [_P, _P, C.c_double, _P]),
+    "gd_bath_chain": (C.c_int, [_P, _P, _P, C.c_double, C.c_double, C.POINTER(C.c_ulonglong)]),
     "gd_set_diagnostics": (C.c_int, [_P, C.c_int]),
     "gd_event_totals": (C.c_int, [_P, _P, _P]),
     "gd_frame_name": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_size_t]),

@@ -482,6 +482,20 @@ gd_status gd_bath_rates(gd_handle *h, const gd_particle *dev_particle, double to
     return done(h, s);
 }
 
+gd_status gd_bath_chain(gd_handle *h, gd_particle *dev_particle, void *dev_rngstate, double total_dust_mass,
+                        double bath, unsigned long long *events) {
+    if (!h || !dev_particle || !dev_rngstate) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!gd::aligned_to(dev_particle, 8) || !gd::aligned_to(dev_rngstate, 8))
+        return fail(h, GD_ERR_INVALID_ARGUMENT, "misaligned particle or RNG pointer");
+    if (!h->cache_valid) return fail(h, GD_ERR_NOT_READY, "gd_bath_chain needs a neighbour cache");
+    int launches = 0;
+    gd::Status s = gd::bath_chain(h->col, h->m, h->n, dev_particle, static_cast<curandState *>(dev_rngstate),
+                                  h->codes.ptr, h->measure.ptr, h->geo.active.ptr, total_dust_mass, bath, events,
+                                  &launches, h->stream);
+    h->col.launches += launches;
+    return done(h, s);
+}
+
 gd_status gd_drift_keplerian(gd_handle *h, gd_particle *dev_particle, double dt) {
     if (!h || !dev_particle || !std::isfinite(dt)) return fail(h, GD_ERR_INVALID_ARGUMENT, "null pointer or bad dt");
     h->geo.launches += 1;

@@ -2292,6 +2292,124 @@ Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, c
     return Status::ok();
 }
 
+// One frozen bath of `bath` seconds for every owner, launched eagerly: the bath-start rates, the skip
+// scan and the chain (col_bath_rate, col_skip_scan, col_chain_run) with the current particles as the
+// published reservoir; the particles and RNG streams advance in place.  This is the operator's wave
+// when a single bath covers the whole operator (every group due once, dt = bath), outside any graph,
+// so the chain can be timed and profiled alone.  Scratch arrays hold the per-owner chain state; the
+// collider's operator state is left unchanged.
+Status bath_chain(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, double bath,
+                  unsigned long long *events, int *launches, cudaStream_t s) {
+    if (!(total_dust_mass > 0) || !std::isfinite(total_dust_mass))
+        return err(GD_ERR_INVALID_ARGUMENT, "total dust mass must be positive and finite");
+    if (!(bath > 0) || !std::isfinite(bath)) return err(GD_ERR_INVALID_ARGUMENT, "bath duration must be positive and finite");
+    GD_TRY(collider_setup(c, m));
+    const int K = m.n_k;
+    DevBuf<double> size_old, numr_old, rate, change, second, cached, time, hazard, jump1, jump2, jumpmax, dt;
+    DevBuf<int> stamp, rated, ev, error, queue, spatial;
+    DevBuf<unsigned char> complete, small;
+    DevBuf<WaveInfo> wave;
+    for (DevBuf<double> *b : {&size_old, &numr_old, &rate, &change, &second, &time, &hazard, &jump1, &jump2, &jumpmax})
+        GD_TRY_CUDA(b->alloc(n));
+    GD_TRY_CUDA(cached.alloc(static_cast<size_t>(n) * 4));
+    GD_TRY_CUDA(dt.alloc(1));
+    for (DevBuf<int> *b : {&stamp, &rated, &ev, &error, &queue, &spatial}) GD_TRY_CUDA(b->alloc(n));
+    GD_TRY_CUDA(complete.alloc(n));
+    GD_TRY_CUDA(small.alloc(32));  // queued [2] at 0, head at 8, error flag at 12, events total at 16
+    GD_TRY_CUDA(wave.alloc(1));
+    const WaveInfo w{n, 1, 1, 1, 1, {0, 0, 0}};
+    GD_TRY_CUDA(cudaMemcpyAsync(wave.ptr, &w, sizeof(w), cudaMemcpyHostToDevice, s));
+    GD_TRY_CUDA(cudaMemcpyAsync(dt.ptr, &bath, sizeof(double), cudaMemcpyHostToDevice, s));
+    GD_TRY_CUDA(cudaMemsetAsync(stamp.ptr, 0, sizeof(int) * n, s));
+    GD_TRY_CUDA(cudaMemsetAsync(rated.ptr, 0xff, sizeof(int) * n, s));
+    for (DevBuf<double> *b : {&time, &hazard, &jump1, &jump2, &jumpmax})
+        GD_TRY_CUDA(cudaMemsetAsync(b->ptr, 0, sizeof(double) * n, s));
+    for (DevBuf<int> *b : {&ev, &error, &spatial}) GD_TRY_CUDA(cudaMemsetAsync(b->ptr, 0, sizeof(int) * n, s));
+    GD_TRY_CUDA(cudaMemsetAsync(complete.ptr, 0, n, s));
+    GD_TRY_CUDA(cudaMemsetAsync(small.ptr, 0, 32, s));
+    GD_TRY_CUDA(cudaMemcpy2DAsync(size_old.ptr, sizeof(double), &part[0].par_size, sizeof(gd_particle), sizeof(double),
+                                  n, cudaMemcpyDeviceToDevice, s));
+    GD_TRY_CUDA(cudaMemcpy2DAsync(numr_old.ptr, sizeof(double), &part[0].par_numr, sizeof(gd_particle), sizeof(double),
+                                  n, cudaMemcpyDeviceToDevice, s));
+    const bool env_on = use_env_cache(m) && m.coag_kernel == GD_KERNEL_CUSTOM;
+    const Env *env = env_on ? reinterpret_cast<const Env *>(c.env.ptr) : nullptr;
+    const int TPB = 256;
+    if (env_on) k_env_cache<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, reinterpret_cast<Env *>(c.env.ptr));
+    if (c.height.ptr) k_disk_height<<<(n + TPB - 1) / TPB, TPB, 0, s>>>(m, n, part, c.height.ptr);
+    RateArgs ra{};
+    ra.height = c.height.ptr;
+    ra.w = wave.ptr;
+    ra.part = part;
+    ra.codes = codes;
+    ra.measure = measure;
+    ra.active = active;
+    ra.size_old = size_old.ptr;
+    ra.numr_old = numr_old.ptr;
+    ra.env = env;
+    ra.lambda0 = n / static_cast<double>(K) / total_dust_mass;
+    ra.rate = rate.ptr;
+    ra.change = change.ptr;
+    ra.second = second.ptr;
+    ra.cached = reinterpret_cast<RateMoments *>(cached.ptr);
+    ra.stamp = stamp.ptr;
+    ra.rated = rated.ptr;
+    const int grid = std::max(1, std::min((n + 3) / 4, c.sms * 8));
+    if (env_on)
+        k_bath_rate<true><<<grid, 128, c.rate_smem, s>>>(m, ra);
+    else
+        k_bath_rate<false><<<grid, 128, c.rate_smem, s>>>(m, ra);
+    ChainArgs ca{};
+    ca.w = wave.ptr;
+    ca.rng = rng;
+    ca.active = active;
+    ca.measure = measure;
+    ca.spatial = spatial.ptr;  // every owner in group 0, whose bath ends at dt[0]
+    ca.dt = dt.ptr;
+    ca.cached = reinterpret_cast<const RateMoments *>(cached.ptr);
+    ca.time = time.ptr;
+    ca.hazard = hazard.ptr;
+    ca.jump1 = jump1.ptr;
+    ca.jump2 = jump2.ptr;
+    ca.jumpmax = jumpmax.ptr;
+    ca.events = ev.ptr;
+    ca.complete = complete.ptr;
+    ca.queue = queue.ptr;
+    ca.queued = reinterpret_cast<int *>(small.ptr);
+    ca.n = n;
+    k_skip_scan<<<std::max(1, std::min((n + TPB - 1) / TPB, c.sms * 8)), TPB, 0, s>>>(ca);
+    ChainRun cr{};
+    cr.height = c.height.ptr;
+    cr.part_ro = part;
+    cr.part = part;
+    cr.codes = codes;
+    cr.size_old = size_old.ptr;
+    cr.numr_old = numr_old.ptr;
+    cr.env = env;
+    cr.lambda0 = ra.lambda0;
+    cr.error = error.ptr;
+    cr.error_flag = reinterpret_cast<int *>(small.ptr + 12);
+    cr.head = reinterpret_cast<int *>(small.ptr + 8);
+    cr.events_total = reinterpret_cast<unsigned long long *>(small.ptr + 16);
+    const int blocks = std::min(c.chain_grid, (n + kChainWarps - 1) / kChainWarps);
+    {
+        void *args[] = {const_cast<Model *>(&m), &ca, &cr};
+        GD_TRY_CUDA(cudaLaunchKernel(c.chain_kernel, dim3(blocks), dim3(kChainWarps * 32), args, c.chain_smem, s));
+    }
+    if (launches) *launches += 3 + (env_on ? 1 : 0) + (c.height.ptr ? 1 : 0);
+    unsigned char host[32];
+    GD_TRY_CUDA(cudaMemcpyAsync(host, small.ptr, sizeof(host), cudaMemcpyDeviceToHost, s));
+    GD_TRY_CUDA(cudaStreamSynchronize(s));  // the scratch is freed on return
+    int flag = 0;
+    std::memcpy(&flag, host + 12, sizeof(int));
+    unsigned long long total = 0;
+    std::memcpy(&total, host + 16, sizeof(total));
+    if (events) *events = total;
+    if (flag == 7) return err(GD_ERR_CONTINUATION_LIMIT, "an owner's chain exceeded its event budget", flag);
+    if (flag) return err(GD_ERR_CHAIN, "event-chain error", flag);
+    return Status::ok();
+}
+
 Status collision_operator_enqueue(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng,
                                   const int32_t *codes, const double *measure, const unsigned char *active,
                                   double duration, double total_dust_mass, cudaStream_t q) {

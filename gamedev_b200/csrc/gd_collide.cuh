@@ -201,6 +201,12 @@ Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, c
                   const double *measure, const unsigned char *active, double total_dust_mass, double *out4,
                   int *launches, cudaStream_t s);
 
+// one frozen bath of `bath` seconds for every owner, eagerly (gd_bath_chain): bath-start rates,
+// skip scan and chain; the particles and RNG streams advance in place, `events` counts the events
+Status bath_chain(Collider &c, const Model &m, int n, gd_particle *part, curandState *rng, const int32_t *codes,
+                  const double *measure, const unsigned char *active, double total_dust_mass, double bath,
+                  unsigned long long *events, int *launches, cudaStream_t s);
+
 // per-pair terms of the bath-start rate for the listed owners (diagnostics and parity checks)
 Status pair_rates(const Model &m, const int *ids, int count, const gd_particle *part, const int32_t *codes,
                   const double *measure, const unsigned char *active, double total_dust_mass, int n, double *out,

@@ -237,6 +237,15 @@ class SwarmCollision:
                                            C.c_void_p(_ptr(out))))
         return out
 
+    def bath_chain(self, particles, rng, total_mass: float, bath: float) -> int:
+        """gd_bath_chain: one frozen bath of `bath` seconds for every owner, eagerly; returns the
+        number of events.  The particles and RNG streams advance in place."""
+        events = C.c_ulonglong(0)
+        self.lib.gd_set_stream(self.h, _stream())
+        self._check(self.lib.gd_bath_chain(self.h, C.c_void_p(_ptr(particles)), C.c_void_p(_ptr(rng)),
+                                           float(total_mass), float(bath), C.byref(events)))
+        return int(events.value)
+
     def pair_rates(self, particles, owner_ids, total_mass: float):
         """Per-pair bath-start terms [count, n_k, 5] = rate, rate*mean, rate*second, maximum, speed."""
         torch = _torch()

@@ -396,6 +396,18 @@ gd_status gd_pair_rates(gd_handle *h, const gd_particle *dev_particle, const int
  * left unchanged (the call uses scratch and synchronises). */
 gd_status gd_bath_rates(gd_handle *h, const gd_particle *dev_particle, double total_dust_mass, double *dev_cached4);
 
+/* One frozen bath of `bath` seconds for every owner, launched eagerly, not in a graph: col_bath_rate
+ * (src/swarm/col_bath_rate.cu:13-130), col_skip_scan (src/swarm/col_skip_scan.cu:13-59) and
+ * col_chain_run (src/swarm/col_chain_run.cu:21-404) on the handle's neighbour cache, with the current
+ * particles as the published reservoir.  This is one wave of evolve_local_collisions
+ * (inc/swarm/_col_chain.cuh:36-539) when a single bath covers the operator: the particles and the
+ * RNG streams advance exactly as gd_collision_operator with that one wave advances them.  *events
+ * (optional) receives the number of events.  The per-owner chain state is scratch (the call
+ * synchronises); the handle's operator state is left unchanged.  Chain errors are reported as
+ * GD_ERR_CHAIN / GD_ERR_CONTINUATION_LIMIT with the reference's code as detail. */
+gd_status gd_bath_chain(gd_handle *h, gd_particle *dev_particle, void *dev_rngstate, double total_dust_mass,
+                        double bath, unsigned long long *events);
+
 /* Number of CUDA kernels this handle has launched since gd_create (for launch accounting). */
 long long gd_launch_count(const gd_handle *h);
 
