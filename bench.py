@@ -1063,16 +1063,69 @@ def run_rates(args):
     sw.close()
 
 
+def run_chain(args):
+    """One frozen bath of the event chain for every owner (gd_bath_chain: bath-start rates, skip scan
+    and chain, launched eagerly) on the c4 shapes, with the bath of the C4 operator's finest level
+    (dt/2 over 32 waves, 3383 s).  Every timed call starts from the same particles and RNG streams.
+    The command the chain kernel's ncu capture profiles: inside the operator it runs in a
+    conditional graph, which ncu does not list."""
+    import torch
+
+    import gamedev_b200 as gd
+    from gamedev_b200 import workloads
+
+    world, rank, local = dist_init(args.gpus)
+    n = args.n or workloads.CONFIGS[C4]["n"]
+    cfg = workloads.config(C4)
+    p = workloads.particles(C4, n=n, seed=workloads.CONFIGS[C4]["seed"] + rank)
+    mass = float((p[:, 7] * math.pi * p[:, 6] ** 3 / 6.0).sum())
+    bath = 3383.0
+    sw = gd.SwarmCollision(cfg, n)
+    dp0 = gd.particles_to_device(p)
+    sw.build_cache(dp0)
+    rng0 = gd.rngstate_init(n, seed=4 + rank)
+    dp, rng = dp0.clone(), rng0.clone()
+    stream = torch.cuda.current_stream()
+    counts = []
+
+    def one():
+        counts.append(sw.bath_chain(dp, rng, mass, bath))
+
+    for _ in range(args.warmup):
+        dp.copy_(dp0)
+        rng.copy_(rng0)
+        one()
+    barrier(world)
+    evs = []
+    for _ in range(args.steps):
+        dp.copy_(dp0)
+        rng.copy_(rng0)
+        evs.append(_timed(stream, one))
+    torch.cuda.synchronize()
+    ms = reduce_max(statistics.mean(a.elapsed_time(b) for a, b in evs), world)
+    events = reduce_sum(float(counts[-1]), world)
+    if rank == 0:
+        print(json.dumps({"metric": "events/s of one frozen bath (col_bath_rate + col_skip_scan + col_chain_run)",
+                          "value": events / (ms / 1e3), "unit": "events/s", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": "c4_chain", "n": n, "k": cfg.n_k, "bath_s": bath,
+                                     "events_per_step": counts[-1], "same_events_every_step": len(set(counts)) == 1,
+                                     "step": "env cache + every owner's bath-start rates + skip scan + chain"}}),
+              flush=True)
+    sw.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
         return
-    if args.workload == "c4_rates":
+    if args.workload in ("c4_rates", "c4_chain"):
         import gamedev_b200
 
         gamedev_b200.load()
-        run_rates(args)
+        (run_rates if args.workload == "c4_rates" else run_chain)(args)
         return
     if args.workload == "c2_batched":
         import gamedev_b200

@@ -153,6 +153,31 @@ def test_bath_rates_match_oracle(gd, cuda, oracle_lib, idx):
     sw.close()
 
 
+@pytest.mark.parametrize("idx", range(6))
+def test_bath_chain_equals_the_one_wave_operator(gd, cuda, oracle_lib, idx):
+    """gd_bath_chain (one frozen bath for every owner, launched eagerly) leaves the particles and the
+    RNG streams bit for bit as the one-wave operator of the same duration does, with the same event
+    count: the same rates, skip scan and chain outside the operator's graph."""
+    import torch
+
+    name, cfg, p, evpo = _chain_cases(gd)[idx]
+    sw, dp, rng, codes, measure, active = _setup(gd, cfg, p)
+    duration, _, _ = _calibrated_duration(oracle_lib, cfg, p, codes, measure, active, evpo)
+    mass = _total_mass(p)
+    dp2, rng2 = dp.clone(), rng.clone()
+    sw.evolve_local_collisions(dp, rng, duration, mass)
+    stats = sw.last_operator_stats()
+    assert stats["waves"] == 1, stats
+    events = sw.bath_chain(dp2, rng2, mass, duration)
+    torch.cuda.synchronize()
+    assert events == stats["events"] and events > 0, (name, events, stats["events"])
+    assert np.array_equal(dp2.cpu().numpy().view(np.uint64), dp.cpu().numpy().view(np.uint64)), name
+    assert torch.equal(rng2.cpu(), rng.cpu()), name
+    # a second bath from the advanced state runs too (the call keeps no state of its own)
+    assert sw.bath_chain(dp2, rng2, mass, duration) >= 0
+    sw.close()
+
+
 def test_operator_repeat_is_bit_identical_and_multiwave(gd, cuda):
     """Full controller (moving bins, merged bins, many waves): two runs from the same state give
     byte-identical particles and RNG states, and represented mass is conserved."""
