@@ -811,6 +811,12 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
     int *last_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) +
                                           static_cast<size_t>(kChainWarps) * kChainDoubles * K) +
                   static_cast<size_t>(wib) * K;
+    // per slot: the pair's speed reaches the fragmentation threshold (the event's outcome branch)
+    unsigned char *high_w = reinterpret_cast<unsigned char *>(
+                                reinterpret_cast<int *>(reinterpret_cast<double *>(smem) +
+                                                        static_cast<size_t>(kChainWarps) * kChainDoubles * K) +
+                                static_cast<size_t>(kChainWarps) * K) +
+                            static_cast<size_t>(wib) * K;
     const int nslot = (K + 31) / 32;
     const int heavy = a.queued[0];
     const int queued = heavy + a.queued[1];
@@ -880,17 +886,20 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
                 const int s = lane + 32 * t;
                 if (t < nslot && s < K) {
                     double pv = 0.0, j1 = 0.0, j2 = 0.0, jm = 0.0;
+                    bool high = false;
                     if (nb[t] >= 0) {
                         double vrel;
                         pv = chain_pair_rate<kPhys>(m, o, po, size_i, sj[t], nj[t], hj[t], vrel,
                                                     cached ? &pp[t] : nullptr);
+                        high = vrel >= m.v_frag;
                         double mean = 0.0, sec = 0.0, maxi = 0.0;
-                        pv *= outcome_moments(m, size_i, sj[t], vrel >= m.v_frag, mean, sec, maxi);
+                        pv *= outcome_moments(m, size_i, sj[t], high, mean, sec, maxi);
                         j1 = pv * mean;
                         j2 = pv * sec;
                         jm = (pv > 0.0) ? maxi : 0.0;
                     }
                     prate[s] = pv;
+                    high_w[s] = high ? 1 : 0;
                     tot[s] = pv;
                     pj1[s] = j1;
                     pj2[s] = j2;
@@ -971,13 +980,8 @@ __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Mod
             }
             const int code_j = r.codes[static_cast<size_t>(i) * K + pick];
             const double size_j = r.size_old[code_j / 3];
-            double vrel = 0.0;
-            if (m.coag_kernel == GD_KERNEL_CUSTOM) {
-                vrel = use_env_cache(m) ? cached_pair_speed(m, o.env, size_i, size_j)
-                                        : direct_pair_speed(m, o.y, o.z, size_i, size_j);
-            }
             const double mass_before = numr_i * size_i * size_i * size_i;
-            const bool high_speed = vrel >= m.v_frag;
+            const bool high_speed = high_w[pick] != 0;
             const double sample = high_speed ? col_uniform(&rng) : 0.0;
             const double size_new = sample_outcome(m, size_i, size_j, high_speed, sample);
             if (r.event_count && lane == 0) {
@@ -1893,7 +1897,7 @@ static Status collider_setup(Collider &c, const Model &m) {
     if (R <= kAuditSmemBins)
         GD_TRY_CUDA(cudaFuncSetAttribute(k_audit_bin_blocked, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(audit_blocked_smem(R))));
-    c.chain_smem = static_cast<size_t>(kChainWarps) * (kChainDoubles * 8 + 4) * K;
+    c.chain_smem = static_cast<size_t>(kChainWarps) * (kChainDoubles * 8 + 4 + 1) * K;  // doubles, last_w, high_w
     const bool phys = m.coag_kernel == GD_KERNEL_CUSTOM && use_env_cache(m);
     if (phys)
         c.chain_kernel = K <= 64 ? reinterpret_cast<const void *>(&k_chain<2, true>)
