@@ -61,6 +61,7 @@ struct Small {
     size_t events;       // unsigned long long
     size_t pair_count;   // int: changed pairs listed for k_pair_eval this wave
     size_t fold_count;   // int: owners listed for k_rate_fold this wave
+    size_t whole_count;  // int: owners listed for k_bath_rate (evaluated whole) this wave
     size_t binmap;       // int[raw]
     size_t ratebin;      // RateBin[raw]
     size_t audit;        // AuditBin[raw]
@@ -89,6 +90,7 @@ static Small small_layout(const Model &m) {
     L.events = o; o += 8;
     L.pair_count = o; o += 4;
     L.fold_count = o; o += 4;
+    L.whole_count = o; o += 4;
     o = align256(o);
     L.binmap = o; o = align256(o + 4 * R);
     L.ratebin = o; o = align256(o + sizeof(RateBin) * R);
@@ -429,6 +431,10 @@ struct RateArgs {
     int *pair_count;
     int *folds;
     int *fold_count;
+    // With the lists, k_rate_plan sorts the wave's owners first: `whole` lists the owners evaluated
+    // whole (their own entry changed, or never rated on this geometry), which k_bath_rate then runs.
+    int *whole;
+    int *whole_count;
 };
 
 __device__ __forceinline__ void store_pair(const RateArgs &a, size_t e, double r, double c, double sc, double mx) {
@@ -476,6 +482,88 @@ __device__ __forceinline__ void fold_owner(const RateArgs &a, int K, int lane, i
 #ifndef GD_RATE_BLOCKS
 #define GD_RATE_BLOCKS 8
 #endif
+
+// Sorts a wave's owners for the rate pass.  Stored rates stand when neither the owner's reservoir
+// entry nor any neighbour's changed since they were evaluated (same geometry and lambda0).  A
+// pair's terms depend only on the owner's and the partner's entries, so when the owner's own entry
+// is unchanged only the pairs of changed partners need evaluating: they go to the pair list, where
+// k_pair_eval evaluates them one per thread (no lane idles on an unchanged pair), and the owner to
+// the fold list, where k_rate_fold folds its K stored pairs in the same order.  Owners whose own
+// entry changed go to the list k_bath_rate evaluates whole.  The same bits either way.  One warp
+// per batch of 32 consecutive owner slots, one reservation per batch in each list (one per owner
+// on the same counters serialised the pass).
+__global__ void __launch_bounds__(256) k_rate_plan(Model m, RateArgs a) {
+    if (!a.w->go || !a.w->need_rates) return;
+    const int K = m.n_k;
+    const int lane = threadIdx.x & 31;
+    const int count = a.w->count;
+    const int *ids = a.w->full ? nullptr : a.ids;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < count; base += warps * 32) {
+        int my_fresh = 0;  // lane b: the changed pairs of batch owner b when only they are evaluated
+        bool my_listed = false, my_whole = false;
+        for (int bo = 0; bo < 32 && base + bo < count; ++bo) {
+            const int i = owner_at(ids, base + bo);
+            const int rated = a.rated[i];
+            if (rated < 0 || a.stamp[i] > rated) {
+                if (lane == bo) my_whole = true;
+                continue;
+            }
+            int fresh = 0;
+            for (int s = lane; s < K; s += 32) {
+                const int nb = a.codes[static_cast<size_t>(i) * K + s];
+                fresh += (nb >= 0 && a.stamp[nb / 3] > rated) ? 1 : 0;
+            }
+            const int sum = __reduce_add_sync(0xffffffffu, fresh);
+            if (sum > 0 && lane == bo) {
+                my_fresh = sum;
+                my_listed = true;
+            }
+        }
+        int incl_p = my_fresh, incl_f = my_listed ? 1 : 0, incl_w = my_whole ? 1 : 0;  // lane prefixes
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int vp = __shfl_up_sync(0xffffffffu, incl_p, d);
+            const int vf = __shfl_up_sync(0xffffffffu, incl_f, d);
+            const int vw = __shfl_up_sync(0xffffffffu, incl_w, d);
+            if (lane >= d) {
+                incl_p += vp;
+                incl_f += vf;
+                incl_w += vw;
+            }
+        }
+        int pbase = 0, fbase = 0, wbase = 0;
+        if (lane == 31) {
+            if (incl_p) pbase = atomicAdd(a.pair_count, incl_p);
+            if (incl_f) fbase = atomicAdd(a.fold_count, incl_f);
+            if (incl_w) wbase = atomicAdd(a.whole_count, incl_w);
+        }
+        pbase = __shfl_sync(0xffffffffu, pbase, 31);
+        fbase = __shfl_sync(0xffffffffu, fbase, 31);
+        wbase = __shfl_sync(0xffffffffu, wbase, 31);
+        if (my_whole) a.whole[wbase + incl_w - 1] = owner_at(ids, base + lane);
+        if (my_listed) a.folds[fbase + incl_f - 1] = owner_at(ids, base + lane);
+        const int my_start = pbase + incl_p - my_fresh;
+        for (unsigned int left = __ballot_sync(0xffffffffu, my_listed); left; left &= left - 1) {
+            const int bo = __ffs(left) - 1;
+            const int i = owner_at(ids, base + bo);
+            const int rated = a.rated[i];
+            int at = __shfl_sync(0xffffffffu, my_start, bo);
+            for (int s0 = 0; s0 < K; s0 += 32) {
+                const int s = s0 + lane;
+                bool f = false;
+                if (s < K) {
+                    const int nb = a.codes[static_cast<size_t>(i) * K + s];
+                    f = nb >= 0 && a.stamp[nb / 3] > rated;
+                }
+                const unsigned int fm = __ballot_sync(0xffffffffu, f);
+                if (f) a.pairs[at + __popc(fm & ((1u << lane) - 1u))] = static_cast<unsigned int>(i) * K + s;
+                at += __popc(fm);
+            }
+        }
+    }
+}
+
 template <bool kCached>
 __global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_bath_rate(Model m, RateArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -484,47 +572,27 @@ __global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_bath_rate(Model m, Rate
     if (!a.w->go || !a.w->need_rates) return;
     const int count = a.w->count, publish = a.w->publish;
     const int *ids = a.w->full ? nullptr : a.ids;
+    // with the planner's lists, the owners to evaluate whole; without them, the wave's owners, each
+    // checked here
+    const bool listed = a.whole != nullptr;
+    const int total = listed ? *a.whole_count : count;
     // a persistent grid: each warp takes owners strided by the number of warps
-    for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < count; slot += gridDim.x * (blockDim.x >> 5)) {
+    for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < total; slot += gridDim.x * (blockDim.x >> 5)) {
     double *w = reinterpret_cast<double *>(smem) + static_cast<size_t>(wib) * 4 * K;
     double *rate_w = w, *change_w = w + K, *second_w = w + 2 * K, *max_w = w + 3 * K;
     int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
                    static_cast<size_t>(wib) * K;
-    const int i = owner_at(ids, slot);
-    // Stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
-    // since they were evaluated (same geometry and lambda0).  A pair's terms depend only on the
-    // owner's and the partner's entries, so when the owner's entry is unchanged only the pairs of
-    // changed partners need evaluating: with stored pairs they go to the pair list, where
-    // k_pair_eval evaluates them one per thread (no lane idles on an unchanged pair), and
-    // k_rate_fold folds the owner's K stored pairs in the same order.  The same bits either way.
-    const int rated = a.rated[i];
-    const bool own = rated < 0 || a.stamp[i] > rated;
-    int fresh = 0;  // this lane's pairs whose partner changed
-    if (!own)
-        for (int s = lane; s < K; s += 32) {
+    const int i = listed ? a.whole[slot] : owner_at(ids, slot);
+    if (!listed) {
+        // stored rates stand when neither the owner's reservoir entry nor any neighbour's changed
+        // since they were evaluated (same geometry and lambda0)
+        const int rated = a.rated[i];
+        bool need = rated < 0 || a.stamp[i] > rated;
+        for (int s = lane; s < K && !need; s += 32) {
             const int nb = a.codes[static_cast<size_t>(i) * K + s];
-            fresh += (nb >= 0 && a.stamp[nb / 3] > rated) ? 1 : 0;
+            need = nb >= 0 && a.stamp[nb / 3] > rated;
         }
-    if (!__any_sync(0xffffffffu, own || fresh > 0)) continue;
-    if (!own && a.pairs) {
-        int incl = fresh;  // inclusive prefix over the lanes
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += v;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        int base = 0;
-        if (lane == 0) {
-            base = atomicAdd(a.pair_count, total);
-            a.folds[atomicAdd(a.fold_count, 1)] = i;
-        }
-        base = __shfl_sync(0xffffffffu, base, 0) + incl - fresh;
-        for (int s = lane; s < K; s += 32) {
-            const int nb = a.codes[static_cast<size_t>(i) * K + s];
-            if (nb >= 0 && a.stamp[nb / 3] > rated) a.pairs[base++] = static_cast<unsigned int>(i) * K + s;
-        }
-        continue;
+        if (!__any_sync(0xffffffffu, need)) continue;
     }
     const bool act = a.active[i] != 0;
     const double meas = a.measure[i];
@@ -1641,6 +1709,7 @@ Status collider_alloc(Collider &c, const Model &m, int n, int record_capacity) {
         GD_TRY_CUDA(c.leaf.alloc(static_cast<size_t>(n) * m.n_k * 4));
         GD_TRY_CUDA(c.pairs.alloc(static_cast<size_t>(n) * m.n_k));
         GD_TRY_CUDA(c.folds.alloc(n));
+        GD_TRY_CUDA(c.whole.alloc(n));
     }
     GD_TRY_CUDA(c.stamp.alloc(n));
     GD_TRY_CUDA(c.rated.alloc(n));
@@ -2056,7 +2125,14 @@ static Status enqueue_operator(Collider &c, const Model &m, int n, gd_particle *
         ra.pair_count = at<int>(c.small, L.pair_count);
         ra.folds = c.folds.ptr;
         ra.fold_count = at<int>(c.small, L.fold_count);
-        if (stored) GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.pair_count, 0, 8, st));
+        ra.whole = stored ? c.whole.ptr : nullptr;
+        ra.whole_count = at<int>(c.small, L.whole_count);
+        if (stored) {
+            // the wave's owners sorted: evaluated whole, changed pairs only, or standing
+            GD_TRY_CUDA(cudaMemsetAsync(c.small.ptr + L.pair_count, 0, 12, st));
+            launches += 1;
+            k_rate_plan<<<grid_for(n, 256), 256, 0, st>>>(m, ra);
+        }
         if (rate_cached)
             k_bath_rate<true><<<grid_for(n, 4), 128, c.rate_smem, st>>>(m, ra);
         else
@@ -2283,6 +2359,8 @@ Status bath_rates(Collider &c, const Model &m, int n, const gd_particle *part, c
     ra.pair_count = nullptr;
     ra.folds = nullptr;
     ra.fold_count = nullptr;
+    ra.whole = nullptr;
+    ra.whole_count = nullptr;
     ra.stamp = stamp.ptr;
     ra.rated = rated.ptr;
     const int grid = std::max(1, std::min((n + 3) / 4, c.sms * 8));

@@ -140,6 +140,7 @@ struct Collider {
     DevBuf<double> leaf;
     DevBuf<unsigned int> pairs;
     DevBuf<int> folds;
+    DevBuf<int> whole;                // the owners a wave evaluates whole (their own entry changed)
     DevBuf<int> ids, queue, group_sorted, spatial;
     // per-group / per-bin device scratch, one contiguous block (small_layout() in gd_collide.cu)
     DevBuf<unsigned char> small;
