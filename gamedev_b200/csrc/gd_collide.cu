@@ -688,6 +688,53 @@ __global__ void __launch_bounds__(128, GD_RATE_BLOCKS) k_rate_fold(Model m, Rate
     double *rate_w = w, *change_w = w + K, *second_w = w + 2 * K, *max_w = w + 3 * K;
     int *valid_w = reinterpret_cast<int *>(reinterpret_cast<double *>(smem) + static_cast<size_t>(blockDim.x >> 5) * 4 * K) +
                    static_cast<size_t>(wib) * K;
+    // K = 64, or a power of two up to 32: the fold of warp_fold in registers, the lane's two slots
+    // first (a[j] += a[j + 32]), then shuffles (a[j] += a[j + half]), the same additions in the
+    // same tree; the validity is an AND, whose order does not matter
+    if (K == 64 || (K <= 32 && (K & (K - 1)) == 0)) {
+        const int n_slots = K == 64 ? 2 : 1;
+        for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < count; slot += gridDim.x * (blockDim.x >> 5)) {
+            const int i = a.folds[slot];
+            double r = 0.0, c = 0.0, sc = 0.0, mx = 0.0;
+            bool valid = true;
+            if (lane < K) {
+                const size_t e = static_cast<size_t>(i) * K + lane;
+                r = a.leaf[e];
+                c = a.leaf[a.plane + e];
+                sc = a.leaf[2 * a.plane + e];
+                mx = a.leaf[3 * a.plane + e];
+                valid = isfinite(r) && r >= 0.0;
+                if (n_slots == 2) {
+                    const double r1 = a.leaf[e + 32];
+                    r += r1;
+                    c += a.leaf[a.plane + e + 32];
+                    sc += a.leaf[2 * a.plane + e + 32];
+                    mx = fmax(mx, a.leaf[3 * a.plane + e + 32]);
+                    valid = valid && isfinite(r1) && r1 >= 0.0;
+                }
+            }
+            for (int d = K >= 32 ? 16 : K / 2; d >= 1; d >>= 1) {
+                r += __shfl_down_sync(0xffffffffu, r, d);
+                c += __shfl_down_sync(0xffffffffu, c, d);
+                sc += __shfl_down_sync(0xffffffffu, sc, d);
+                mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, d));
+            }
+            valid = __all_sync(0xffffffffu, valid);
+            if (lane == 0) {
+                RateMoments cm;
+                cm.rate = valid ? r : -1.0;
+                cm.first = c;
+                cm.second = sc;
+                cm.maximum = mx;
+                a.cached[i] = cm;
+                a.rate[i] = r;
+                a.change[i] = c;
+                a.second[i] = sc;
+                a.rated[i] = publish;
+            }
+        }
+        return;
+    }
     for (int slot = blockIdx.x * (blockDim.x >> 5) + wib; slot < count; slot += gridDim.x * (blockDim.x >> 5)) {
         const int i = a.folds[slot];
         for (int s = lane; s < K; s += 32) {
