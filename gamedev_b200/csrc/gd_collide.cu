@@ -496,30 +496,44 @@ __global__ void __launch_bounds__(256) k_rate_plan(Model m, RateArgs a) {
     if (!a.w->go || !a.w->need_rates) return;
     const int K = m.n_k;
     const int lane = threadIdx.x & 31;
+    const unsigned int below = (1u << lane) - 1u;
     const int count = a.w->count;
     const int *ids = a.w->full ? nullptr : a.ids;
     const int warps = gridDim.x * (blockDim.x >> 5);
+    // K <= 64: each owner's changed slots are kept as two ballots from the one scan of its row
+    const bool masks = K <= 64;
     for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < count; base += warps * 32) {
-        int my_fresh = 0;  // lane b: the changed pairs of batch owner b when only they are evaluated
-        bool my_listed = false, my_whole = false;
-        for (int bo = 0; bo < 32 && base + bo < count; ++bo) {
-            const int i = owner_at(ids, base + bo);
-            const int rated = a.rated[i];
-            if (rated < 0 || a.stamp[i] > rated) {
-                if (lane == bo) my_whole = true;
-                continue;
-            }
+        // the batch's owners, one per lane: lane b holds owner b's index, rating and decision
+        const bool here = base + lane < count;
+        const int my_i = here ? owner_at(ids, base + lane) : 0;
+        const int my_rated = here ? a.rated[my_i] : 0;
+        const bool my_whole = here && (my_rated < 0 || a.stamp[my_i] > my_rated);
+        unsigned int my_m0 = 0u, my_m1 = 0u;  // lane b: owner b's changed slots 0-31 and 32-63
+        int my_fresh = 0;
+        for (unsigned int left = __ballot_sync(0xffffffffu, here && !my_whole); left; left &= left - 1) {
+            const int bo = __ffs(left) - 1;
+            const int i = __shfl_sync(0xffffffffu, my_i, bo);
+            const int rated = __shfl_sync(0xffffffffu, my_rated, bo);
             int fresh = 0;
-            for (int s = lane; s < K; s += 32) {
-                const int nb = a.codes[static_cast<size_t>(i) * K + s];
-                fresh += (nb >= 0 && a.stamp[nb / 3] > rated) ? 1 : 0;
+            unsigned int m0 = 0u, m1 = 0u;
+            for (int s0 = 0; s0 < K; s0 += 32) {
+                const int s = s0 + lane;
+                bool f = false;
+                if (s < K) {
+                    const int nb = a.codes[static_cast<size_t>(i) * K + s];
+                    f = nb >= 0 && a.stamp[nb / 3] > rated;
+                }
+                const unsigned int fm = __ballot_sync(0xffffffffu, f);
+                fresh += __popc(fm);
+                if (s0 == 0) m0 = fm; else m1 = fm;
             }
-            const int sum = __reduce_add_sync(0xffffffffu, fresh);
-            if (sum > 0 && lane == bo) {
-                my_fresh = sum;
-                my_listed = true;
+            if (lane == bo) {
+                my_fresh = fresh;
+                my_m0 = m0;
+                my_m1 = m1;
             }
         }
+        const bool my_listed = my_fresh > 0;
         int incl_p = my_fresh, incl_f = my_listed ? 1 : 0, incl_w = my_whole ? 1 : 0;  // lane prefixes
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -541,14 +555,22 @@ __global__ void __launch_bounds__(256) k_rate_plan(Model m, RateArgs a) {
         pbase = __shfl_sync(0xffffffffu, pbase, 31);
         fbase = __shfl_sync(0xffffffffu, fbase, 31);
         wbase = __shfl_sync(0xffffffffu, wbase, 31);
-        if (my_whole) a.whole[wbase + incl_w - 1] = owner_at(ids, base + lane);
-        if (my_listed) a.folds[fbase + incl_f - 1] = owner_at(ids, base + lane);
+        if (my_whole) a.whole[wbase + incl_w - 1] = my_i;
+        if (my_listed) a.folds[fbase + incl_f - 1] = my_i;
         const int my_start = pbase + incl_p - my_fresh;
         for (unsigned int left = __ballot_sync(0xffffffffu, my_listed); left; left &= left - 1) {
             const int bo = __ffs(left) - 1;
-            const int i = owner_at(ids, base + bo);
-            const int rated = a.rated[i];
+            const int i = __shfl_sync(0xffffffffu, my_i, bo);
             int at = __shfl_sync(0xffffffffu, my_start, bo);
+            if (masks) {
+                const unsigned int m0 = __shfl_sync(0xffffffffu, my_m0, bo);
+                const unsigned int m1 = __shfl_sync(0xffffffffu, my_m1, bo);
+                if ((m0 >> lane) & 1u) a.pairs[at + __popc(m0 & below)] = static_cast<unsigned int>(i) * K + lane;
+                at += __popc(m0);
+                if ((m1 >> lane) & 1u) a.pairs[at + __popc(m1 & below)] = static_cast<unsigned int>(i) * K + 32 + lane;
+                continue;
+            }
+            const int rated = __shfl_sync(0xffffffffu, my_rated, bo);
             for (int s0 = 0; s0 < K; s0 += 32) {
                 const int s = s0 + lane;
                 bool f = false;
@@ -557,7 +579,7 @@ __global__ void __launch_bounds__(256) k_rate_plan(Model m, RateArgs a) {
                     f = nb >= 0 && a.stamp[nb / 3] > rated;
                 }
                 const unsigned int fm = __ballot_sync(0xffffffffu, f);
-                if (f) a.pairs[at + __popc(fm & ((1u << lane) - 1u))] = static_cast<unsigned int>(i) * K + s;
+                if (f) a.pairs[at + __popc(fm & below)] = static_cast<unsigned int>(i) * K + s;
                 at += __popc(fm);
             }
         }
