@@ -933,10 +933,11 @@ struct ChainRun {
 // kSlots = neighbour slots per lane (2 for K <= 64, 4 for K <= 128, else 8): the owner's partners
 // and, for the cached physical kernel, their Stokes terms at the owner's environment stay in
 // registers for the whole chain.
-// 6 blocks of 4 warps per SM (85 registers): the chains of a C4 wave at N = 1e7 ran 5% faster than
-// at 3 blocks (148 registers) and 8% faster than at 4
+// 7 blocks of 4 warps per SM (72 registers, a few spilled): the chains of the C4 operators at
+// N = 1e7 ran 1.3% faster than at 6 (80 registers); 1 or 2 blocks with every value in registers
+// ran 40% slower, 5 blocks slightly slower
 #ifndef GD_CHAIN_BLOCKS
-#define GD_CHAIN_BLOCKS 6
+#define GD_CHAIN_BLOCKS 7
 #endif
 template <int kSlots, bool kPhys>
 __global__ void __launch_bounds__(kChainWarps * 32, GD_CHAIN_BLOCKS) k_chain(Model m, ChainArgs a, ChainRun r) {
