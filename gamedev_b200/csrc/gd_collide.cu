@@ -4,7 +4,11 @@
 //   k_env_cache      [col_env_cache, col_env_cache.cu:15-20]     thread per owner
 //   k_bath_init      [col_bath_init + col_comp_zero]             thread per owner
 //   k_size_*         [col_size_zero/scan/bnds]                   moving log-size bin bounds
+//   k_rate_plan      [none: this build keeps unchanged rates]    WARP per 32 owners: whole, changed
+//                                                                pairs only, or standing
 //   k_bath_rate      [col_bath_rate, col_bath_rate.cu:13-130]    WARP per owner, exact fold order
+//   k_pair_eval, k_rate_fold [col_bath_rate's pair terms, fold]  thread per changed pair; WARP per
+//                                                                owner folding its stored pairs
 //   k_count_bin, k_binmap, k_rate_bins [col_count_bin, _build_col_binmap, col_rate_bins]
 //   k_skip_scan      [col_skip_scan, col_skip_scan.cu:13-59]     thread per owner
 //   k_chain          [col_chain_run, col_chain_run.cu:21-404]    persistent WARPS over a device queue,
@@ -422,17 +426,18 @@ struct RateArgs {
     const int *stamp;   // publish wave of each particle's last reservoir change
     int *rated;         // publish wave of each owner's stored rates (-1: none)
     // Stored pairs: plane p of `leaf` (planes `plane` = n*K doubles apart) holds each pair's rate,
-    // rate*mean, rate*second and maximum (p = 0..3) at owner*K + slot, or null.  With `pairs`, an
-    // owner whose own entry is unchanged appends its changed pairs (owner*K + slot) there and
-    // itself to `folds`; k_pair_eval and k_rate_fold finish it.
+    // rate*mean, rate*second and maximum (p = 0..3) at owner*K + slot, or null.  With the lists,
+    // k_rate_plan sorts the wave's owners first: an owner whose own entry is unchanged has its
+    // changed pairs (owner*K + slot) listed in `pairs` and itself in `folds`, for k_pair_eval and
+    // k_rate_fold; `whole` lists the owners evaluated whole (their own entry changed, or never
+    // rated on this geometry), which k_bath_rate then runs.  Null lists: k_bath_rate checks and
+    // evaluates the wave's owners itself.
     double *leaf;
     size_t plane;
     unsigned int *pairs;
     int *pair_count;
     int *folds;
     int *fold_count;
-    // With the lists, k_rate_plan sorts the wave's owners first: `whole` lists the owners evaluated
-    // whole (their own entry changed, or never rated on this geometry), which k_bath_rate then runs.
     int *whole;
     int *whole_count;
 };
