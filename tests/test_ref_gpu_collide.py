@@ -106,6 +106,9 @@ def test_morton_operator_matches_reference_cuda_per_particle(gd, cuda):
                 & np.isclose(ours[:, 7], ref[:, 7], rtol=1e-12, atol=0))
         assert same.all(), (seed, int((~same).sum()), stats)
         assert stats["events"] > 1000, stats
+        # several waves: every wave after the first re-rates only the owners and pairs whose
+        # reservoir entries changed (the stored-pair path), against the reference's full rating
+        assert stats["waves"] > 1, stats
         assert abs(_moment(ours, 1) - _mass(p) * 1.0) <= 1e-12 * _mass(p)
 
 
