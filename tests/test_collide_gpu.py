@@ -8,6 +8,8 @@ Bars (written in the checks):
     relative, and the device RNG advanced by exactly the number of deviates the oracle's replay of
     the same cuRAND stream consumed (checked bit for bit on the next deviate);
   * represented mass N_i m_i conserved per owner to 2e-12 and in total to 1e-12 relative;
+  * a second operator on the stored rates: its bath-start moments equal a full re-rating bit for
+    bit, and its chains the oracle's replay (K up to 96);
   * repeat runs bit-identical (the reference's run_chain.py hash check);
   * invalid input reported as a status, never a trap.
 """
@@ -363,3 +365,52 @@ def test_controller_summary_passes_reference_validator(gd, cuda):
     assert a["operator_count"] == 3 and a["wave_count"] > 3 and a["bath_count"] > 3
     assert _controller_valid(a)
     assert _controller_equivalent(a, b)
+
+
+@pytest.mark.parametrize("n_k,coag_kernel,three_d", [(24, 2, True), (64, 3, True), (96, 3, True), (96, 1, False)])
+def test_second_operator_on_stored_rates(gd, cuda, oracle_lib, n_k, coag_kernel, three_d):
+    """Two one-wave operators on one neighbour cache.  The second rates its owners through the
+    stored pairs: an owner whose reservoir entry changed in the first is evaluated whole, one whose
+    partners changed re-evaluates only those pairs and is folded again, the rest keep their rates.
+    Its bath-start moments equal a full re-rating of the same state (gd_bath_rates) bit for bit, and
+    its chains leave every owner as the oracle's replay from the first operator's result.  K = 96
+    takes the planner's row rescan and the shared-memory fold (K above 64, not a power of two)."""
+    cfg = _one_wave(cases.code_unit_config(gd, n_k=n_k, coag_kernel=coag_kernel, three_d=three_d))
+    p = cases.random_swarm(cfg, 3000, 50 + n_k)
+    sw, dp, rng, codes, measure, active = _setup(gd, cfg, p)
+    duration, lam, _ = _calibrated_duration(oracle_lib, cfg, p, codes, measure, active, 3.0)
+    mass = _total_mass(p)
+    sw.evolve_local_collisions(dp, rng, duration, mass)
+    first = sw.last_operator_stats()
+    assert first["waves"] == 1 and first["events"] > 0, first
+    p1 = dp.cpu().numpy()
+    full = sw.bath_rates(dp, mass).cpu().numpy()
+    # the second operator sized as the first on the grown grains: 3 expected events for the
+    # fastest owner at its bath start
+    duration = 3.0 / float(full[active.astype(bool), 0].max())
+    U = gd.rng_uniforms(rng, len(p), 512).cpu().numpy()
+    sw.evolve_local_collisions(dp, rng, duration, mass)
+    stats = sw.last_operator_stats()
+    assert stats["waves"] == 1, stats
+    cached, time_g, events_g, _, _ = (t.cpu().numpy() for t in sw.owner_state())
+    out = dp.cpu().numpy()
+    nxt = gd.rng_uniforms(rng, len(p), 1).cpu().numpy()[:, 0]
+    act = active.astype(bool)
+    # the second operator's bath-start moments, from stored and re-evaluated pairs, against a full
+    # re-rating of the same reservoir
+    assert np.array_equal(cached[act].view(np.uint64), full[act].view(np.uint64))
+    changed = (p1[:, 6] != p[:, 6]) | (p1[:, 7] != p[:, 7])
+    assert changed.any() and not changed.all()
+    cached_o, _, _, _ = oracle_lib.bath_rate(cfg, p1, codes, measure, active, p1[:, 6], p1[:, 7], lam)
+    n_events = 0
+    for i in np.nonzero(act)[0]:
+        err, st, used = oracle_lib.chain_owner(cfg, int(i), p1, codes, measure, active, p1[:, 6].copy(),
+                                               p1[:, 7].copy(), lam, duration, cached_o[i], U[i])
+        assert err == 0, (n_k, i, err)
+        assert int(st[7]) == events_g[i], (n_k, i, st[7], events_g[i])
+        n_events += int(st[7])
+        assert math.isclose(st[0], out[i, 6], rel_tol=STATE_RTOL), (n_k, i, st[0], out[i, 6])
+        assert math.isclose(st[1], out[i, 7], rel_tol=STATE_RTOL), (n_k, i)
+        assert nxt[i] == U[i, used], (n_k, i, used)
+    assert stats["events"] == n_events
+    sw.close()
